@@ -1,0 +1,321 @@
+"""Benchmark of bulbit-b200 on one node.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bulbit_b200|reference]
+
+Workload (one "step"): the ray-throughput microbenchmark — a 1,048,576-triangle
+soup (centroids U[-1,1]^3, vertices centroid + N(0, 0.01^2)), 16,777,216
+closest-hit rays and 16,777,216 any-hit rays (t_max = 0.5 x distance to the
+target) from the sphere of radius 3 toward U[-1,1]^3; seeded synthetic data.
+value = (closest + any-hit rays traced by all ranks) / max-over-ranks device
+time, in Mrays/s. The path-tracing workload (Cornell box with a displaced
+gold icosphere) is reported beside it as paths/s when the integrator is
+available.
+
+Each rank is an independent replica (the path does not shard across GPUs);
+ranks only meet at barriers and the max-reduction of their timings.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_TRIS = 1 << 20
+N_RAYS = 1 << 24
+WORKLOAD = ("ray-throughput microbenchmark: 1,048,576-triangle soup (SAH BVH), "
+            "16,777,216 closest-hit + 16,777,216 any-hit rays per step")
+METRIC = "Mrays/s"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+# ------------------------------------------------------------------ clocks
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    mx.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ profiles
+
+def profile_traffic(name):
+    """DRAM bytes per launch from a committed ncu summary (profiles/<name>),
+    the line 'dram_bytes_per_launch: <int>'."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        for line in f:
+            if line.strip().startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    return None
+
+
+# ------------------------------------------------------------------ reference arm
+
+def run_reference(args, rank):
+    """The reference's own CPU BVH (oracle/_ref, compiled from its sources)
+    on the same workload: each step traces a bounded sample of the rays on all
+    host threads."""
+    if rank != 0:
+        return
+    from bulbit_b200 import scenes
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libbulbit_ref.so not built"}))
+        return
+    cores = ref.init(0)
+    scene = scenes.triangle_soup(N_TRIS, seed=1)
+    closest, anyq = scenes.soup_rays(N_RAYS, seed=2)
+    rs = ref.RefScene(scene)
+    sample = 1 << 19
+    for w in range(args.warmup):
+        off = (w * sample) % N_RAYS
+        rs.intersect(closest[off:off + sample])
+        rs.intersect_any(anyq[off:off + sample])
+    secs = 0.0
+    for k in range(args.steps):
+        off = ((args.warmup + k) * sample) % N_RAYS
+        secs += rs.intersect(closest[off:off + sample])[2]
+        secs += rs.intersect_any(anyq[off:off + sample])[1]
+    rays = 2 * sample * args.steps
+    value = rays / secs / 1e6
+    desc = (f"{sample} closest-hit + {sample} any-hit rays of the 16,777,216-ray set per step, "
+            f"{cores} threads, BVH build {rs.build_seconds:.2f} s excluded")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "sample_rays_per_step": 2 * sample},
+        "cpu_baseline": {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def cpu_baseline(scene, closest, anyq):
+    from oracle import ref
+    if not ref.available():
+        return None
+    cores = ref.init(0)
+    rs = ref.RefScene(scene)
+    sample = 1 << 21
+    t1 = rs.intersect(closest[:sample])[2]
+    t2 = rs.intersect_any(anyq[:sample])[1]
+    value = 2 * sample / (t1 + t2) / 1e6
+    return {"value": value, "unit": "Mrays/s", "cores": cores, "kind": "reference",
+            "sample": f"first {sample} closest-hit + {sample} any-hit rays of the workload on {cores} threads "
+                      f"(reference BVH::Intersect/IntersectAny via ParallelFor; BVH build "
+                      f"{rs.build_seconds:.2f} s excluded)"}
+
+
+# ------------------------------------------------------------------ GPU arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="bulbit_b200", choices=["bulbit_b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    from bulbit_b200 import lib, scenes
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    scene = scenes.triangle_soup(N_TRIS, seed=1)
+    closest, anyq = scenes.soup_rays(N_RAYS, seed=2)
+    t0 = time.perf_counter()
+    acc = lib.GpuAccel(scene)
+    build_s = time.perf_counter() - t0
+
+    dev_c = torch.from_numpy(closest).cuda()
+    dev_a = torch.from_numpy(anyq).cuda()
+    hits = torch.empty((N_RAYS, 4), dtype=torch.float32, device="cuda")
+    occ = torch.empty(N_RAYS, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.Stream()
+    sptr = stream.cuda_stream
+
+    # Traversal statistics for the algorithmic-bytes roofline (untimed).
+    acc.set_counting(True)
+    acc.intersect_device(dev_c, hits, sptr)
+    nodes_c, prims_c = acc.last_counts()
+    acc.intersect_any_device(dev_a, occ, sptr)
+    nodes_a, prims_a = acc.last_counts()
+    acc.set_counting(False)
+
+    def step(events=None):
+        with torch.cuda.stream(stream):
+            if events is not None:
+                events[0].record(stream)
+            acc.intersect_device(dev_c, hits, sptr)
+            if events is not None:
+                events[1].record(stream)
+            acc.intersect_any_device(dev_a, occ, sptr)
+            if events is not None:
+                events[2].record(stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(args.steps)]
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for k in range(args.steps):
+        step(ev[k])
+    end.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    ms = start.elapsed_time(end)
+    closest_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    any_ms = [e[1].elapsed_time(e[2]) for e in ev]
+
+    # End to end through the C ABI with host (pinned) buffers: copies inside.
+    pin_c = torch.from_numpy(closest).pin_memory()
+    pin_a = torch.from_numpy(anyq).pin_memory()
+    pin_h = torch.empty((N_RAYS, 4), dtype=torch.float32).pin_memory()
+    pin_o = torch.empty(N_RAYS, dtype=torch.uint8).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+    acc.intersect_host_ptr(pin_c.data_ptr(), N_RAYS, pin_h.data_ptr())
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        acc.intersect_host_ptr(pin_c.data_ptr(), N_RAYS, pin_h.data_ptr())
+        acc.intersect_any_host_ptr(pin_a.data_ptr(), N_RAYS, pin_o.data_ptr())
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    barrier()
+
+    if world > 1:
+        tt = torch.tensor([ms, e2e_s], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms, e2e_s = float(tt[0]), float(tt[1])
+
+    rays_per_step = 2 * N_RAYS
+    value = world * rays_per_step * args.steps / (ms / 1e3) / 1e6
+    e2e_value = world * rays_per_step * e2e_steps / e2e_s / 1e6
+
+    peaks, peak_kind = load_peaks()
+    avg_closest_ms = statistics.mean(closest_ms)
+    bytes_closest = N_RAYS * (32 + 16) + 32 * nodes_c + 48 * prims_c
+    achieved = bytes_closest / (avg_closest_ms / 1e3) / 1e9
+    traffic = profile_traffic("trace_closest_soup1m.md")
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays_per_step": rays_per_step,
+                   "l2": "inputs larger than L2 (512 MiB of rays per query set)",
+                   "parallelism": f"replicas x{world}", "bvh_build_s": round(build_s, 3)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "kernel": "TraceKernel<closest> (bulbit_b200/csrc/accel.cu)",
+                     "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": bytes_closest,
+                     "per_ray": {"nodes": nodes_c / N_RAYS, "prims": prims_c / N_RAYS,
+                                 "any_nodes": nodes_a / N_RAYS, "any_prims": prims_a / N_RAYS},
+                     "avg_launch_ms": {"closest": avg_closest_ms, "any": statistics.mean(any_ms)}},
+        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 2 * N_RAYS * 32,
+                "d2h_bytes_per_step": N_RAYS * 16 + N_RAYS * 1},
+        "gpu_launches": 2 * args.steps,
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(scene, closest, anyq)
+    if rank == 0:
+        print(json.dumps(line))
+    acc.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,472 @@
+// GPU accel beside the reference BVH: upload of geometry and a flattened SAH
+// tree, and the batched closest-hit / any-hit traversal kernels.
+
+#include "accel.cuh"
+
+#include <algorithm>
+#include <cstring>
+
+namespace bbg
+{
+
+constexpr int kTraceBlock = 128;
+
+bbg_status CheckDevice()
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+    {
+        return Fail(BBG_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
+    }
+    cudaDeviceProp prop;
+    BBG_CUDA(cudaGetDeviceProperties(&prop, 0));
+    if (prop.major != 10)
+    {
+        return Fail(BBG_ERR_NO_DEVICE, "device 0 is sm_%d%d; this library is built for sm_100a", prop.major,
+                    prop.minor);
+    }
+    return BBG_OK;
+}
+
+int PersistentGrid(const void* kernel, int block, size_t smem)
+{
+    int sms = 148, per_sm = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
+    return sms * std::max(per_sm, 1);
+}
+
+// One thread per ray, grid-stride over the batch. Rays are two float4
+// (o.xyz d.x)(d.yz t_min t_max); hits one float4 (prim bits, t, u, v).
+template <bool ANY, bool COUNT>
+__global__ void __launch_bounds__(kTraceBlock) TraceKernel(AccelView a, const float4* __restrict__ rays, int64_t n,
+                                                           float4* __restrict__ hits, uint8_t* __restrict__ occluded,
+                                                           unsigned long long* counters)
+{
+    uint32_t nodes = 0, prims = 0;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        float4 r0 = __ldg(rays + 2 * i);
+        float4 r1 = __ldg(rays + 2 * i + 1);
+        RayQ q = MakeRayQ(V3{ r0.x, r0.y, r0.z }, V3{ r0.w, r1.x, r1.y });
+        TraceResult res = Trace<ANY, COUNT>(a, q, r1.z, r1.w, &nodes, &prims);
+        if (ANY)
+        {
+            occluded[i] = res.prim >= 0 ? 1 : 0;
+        }
+        else
+        {
+            hits[i] = make_float4(__int_as_float(res.prim), res.t, res.u, res.v);
+        }
+    }
+    if (COUNT)
+    {
+        unsigned long long nv = nodes, np = prims;
+        for (int off = 16; off > 0; off >>= 1)
+        {
+            nv += __shfl_down_sync(0xffffffffu, nv, off);
+            np += __shfl_down_sync(0xffffffffu, np, off);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+            atomicAdd(counters, nv);
+            atomicAdd(counters + 1, np);
+        }
+    }
+}
+
+template <bool ANY>
+static bbg_status LaunchTrace(bbg_accel* a, const float4* rays, int64_t n, float4* hits, uint8_t* occ,
+                              cudaStream_t stream)
+{
+    if (n == 0)
+    {
+        return BBG_OK;
+    }
+    if (a->n_prims == 0)
+    {
+        // No geometry: every query misses (the reference cannot build a tree
+        // over zero primitives).
+        if (ANY)
+        {
+            BBG_CUDA(cudaMemsetAsync(occ, 0, size_t(n), stream));
+            return BBG_OK;
+        }
+        return Fail(BBG_ERR_UNSUPPORTED, "closest-hit query on an accel with no primitives");
+    }
+    if (a->counting)
+    {
+        auto k = TraceKernel<ANY, true>;
+        int grid = PersistentGrid(reinterpret_cast<const void*>(k), kTraceBlock);
+        grid = int(std::min<int64_t>(grid, (n + kTraceBlock - 1) / kTraceBlock));
+        k<<<grid, kTraceBlock, 0, stream>>>(a->view(), rays, n, hits, occ, a->counters.p);
+    }
+    else
+    {
+        auto k = TraceKernel<ANY, false>;
+        int grid = PersistentGrid(reinterpret_cast<const void*>(k), kTraceBlock);
+        grid = int(std::min<int64_t>(grid, (n + kTraceBlock - 1) / kTraceBlock));
+        k<<<grid, kTraceBlock, 0, stream>>>(a->view(), rays, n, hits, occ, nullptr);
+    }
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bbg_status LaunchIntersect(bbg_accel* a, const float4* rays, int64_t n, float4* hits, cudaStream_t stream)
+{
+    return LaunchTrace<false>(a, rays, n, hits, nullptr, stream);
+}
+
+bbg_status LaunchIntersectAny(bbg_accel* a, const float4* rays, int64_t n, uint8_t* occluded, cudaStream_t stream)
+{
+    return LaunchTrace<true>(a, rays, n, nullptr, occluded, stream);
+}
+
+} // namespace bbg
+
+using namespace bbg;
+
+namespace
+{
+
+float BitsToFloat(uint32_t bits)
+{
+    float f;
+    std::memcpy(&f, &bits, sizeof(f));
+    return f;
+}
+
+bbg_status CheckGeometry(const bbg_geometry* g)
+{
+    if (!g || g->n_prims < 0 || g->n_vertices < 0 || g->n_triangles < 0 || g->n_spheres < 0)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "geometry: null or negative count");
+    }
+    if (g->n_prims > 0 && (!g->prim_kind || !g->prim_index))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "geometry: prim_kind / prim_index missing");
+    }
+    if (g->n_triangles > 0 && (!g->tri_indices || !g->positions))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "geometry: triangles without indices or positions");
+    }
+    for (int32_t t = 0; t < 3 * g->n_triangles; ++t)
+    {
+        if (g->tri_indices[t] < 0 || g->tri_indices[t] >= g->n_vertices)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "geometry: triangle vertex %d out of range", g->tri_indices[t]);
+        }
+    }
+    for (int32_t i = 0; i < g->n_prims; ++i)
+    {
+        int32_t k = g->prim_kind[i], idx = g->prim_index[i];
+        bool ok = (k == BBG_PRIM_TRIANGLE && idx >= 0 && idx < g->n_triangles) ||
+                  (k == BBG_PRIM_SPHERE && idx >= 0 && idx < g->n_spheres && g->spheres);
+        if (!ok)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "geometry: primitive %d has kind %d index %d", i, k, idx);
+        }
+    }
+    return BBG_OK;
+}
+
+bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
+{
+    // Host-side checks and the tree come first: a malformed scene or tree is
+    // rejected before any device work.
+    BBG_TRY(CheckGeometry(g));
+    a->n_prims = g->n_prims;
+
+    // Host copies needed later (light set-up on area-light primitives).
+    a->host_prim_shape.resize(size_t(g->n_prims));
+    for (int32_t i = 0; i < g->n_prims; ++i)
+    {
+        a->host_prim_shape[i] = make_int2(g->prim_kind[i], g->prim_index[i]);
+    }
+    a->host_tri_indices.assign(g->tri_indices, g->tri_indices + 3 * size_t(g->n_triangles));
+    a->host_positions.assign(g->positions, g->positions + 3 * size_t(g->n_vertices));
+    a->host_spheres.assign(g->spheres, g->spheres + size_t(g->n_spheres));
+
+    if (g->n_prims == 0)
+    {
+        BBG_TRY(CheckDevice());
+        BBG_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+        return BBG_OK;
+    }
+
+    // Tree: given (the reference-built one, flattened) or built here.
+    if (bvh)
+    {
+        if (!bvh->nodes || !bvh->slot_prims || bvh->n_nodes <= 0 || bvh->n_slots != g->n_prims)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "bvh: %d slots for %d primitives", bvh->n_slots, g->n_prims);
+        }
+        a->host_nodes.assign(bvh->nodes, bvh->nodes + bvh->n_nodes);
+        a->host_slots.assign(bvh->slot_prims, bvh->slot_prims + bvh->n_slots);
+    }
+    else
+    {
+        std::vector<float> aabbs(6 * size_t(g->n_prims));
+        PrimAabbs(*g, aabbs.data());
+        a->host_nodes.resize(2 * size_t(g->n_prims) - 1);
+        a->host_slots.resize(size_t(g->n_prims));
+        int32_t n_nodes = 0;
+        BBG_TRY(BuildBvh(aabbs.data(), g->n_prims, a->host_nodes.data(), a->host_slots.data(), &n_nodes));
+        a->host_nodes.resize(size_t(n_nodes));
+    }
+    a->n_nodes = int32_t(a->host_nodes.size());
+    a->n_slots = int32_t(a->host_slots.size());
+    BBG_TRY(ValidateBvh(a->host_nodes.data(), a->n_nodes, a->n_slots, g->n_prims, a->host_slots.data(),
+                        &a->max_depth));
+    if (a->max_depth > kStackCapacity)
+    {
+        return Fail(BBG_ERR_STACK_OVERFLOW, "tree depth %d exceeds the traversal stack (%d)", a->max_depth,
+                    kStackCapacity);
+    }
+    const bbg_bvh_node& root = a->host_nodes[0];
+    std::memcpy(a->bounds, root.bmin, 3 * sizeof(float));
+    std::memcpy(a->bounds + 3, root.bmax, 3 * sizeof(float));
+
+    BBG_TRY(CheckDevice());
+    BBG_CUDA(cudaSetDevice(0));
+    BBG_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
+    for (int s = 0; s < 2; ++s)
+    {
+        BBG_CUDA(cudaStreamCreateWithFlags(&a->copy_stream[s], cudaStreamNonBlocking));
+        BBG_CUDA(cudaEventCreateWithFlags(&a->stage_done[s], cudaEventDisableTiming));
+    }
+
+    // Slot records in leaf order.
+    std::vector<float4> slot_rec(3 * size_t(a->n_slots));
+    for (int32_t s = 0; s < a->n_slots; ++s)
+    {
+        int32_t prim = a->host_slots[s];
+        float4* r = &slot_rec[3 * size_t(s)];
+        if (g->prim_kind[prim] == BBG_PRIM_TRIANGLE)
+        {
+            const int32_t* v = g->tri_indices + 3 * size_t(g->prim_index[prim]);
+            const float* p0 = g->positions + 3 * size_t(v[0]);
+            const float* p1 = g->positions + 3 * size_t(v[1]);
+            const float* p2 = g->positions + 3 * size_t(v[2]);
+            r[0] = make_float4(p0[0], p0[1], p0[2], BitsToFloat(uint32_t(prim)));
+            r[1] = make_float4(p1[0], p1[1], p1[2], 0.0f);
+            r[2] = make_float4(p2[0], p2[1], p2[2], 0.0f);
+        }
+        else
+        {
+            const bbg_sphere& sp = g->spheres[g->prim_index[prim]];
+            r[0] = make_float4(sp.p[0], sp.p[1], sp.p[2], BitsToFloat(uint32_t(prim) | kSphereBit));
+            r[1] = make_float4(sp.q[0], sp.q[1], sp.q[2], sp.q[3]);
+            r[2] = make_float4(sp.s[0], sp.s[1], sp.s[2], sp.radius);
+        }
+    }
+    static_assert(sizeof(bbg_bvh_node) == 2 * sizeof(float4), "node layout");
+    BBG_TRY(a->nodes.upload(reinterpret_cast<const float4*>(a->host_nodes.data()), 2 * size_t(a->n_nodes), a->stream));
+    BBG_TRY(a->slots.upload(slot_rec.data(), slot_rec.size(), a->stream));
+
+    // Shading data.
+    BBG_TRY(a->prim_shape.upload(a->host_prim_shape.data(), a->host_prim_shape.size(), a->stream));
+    BBG_TRY(a->tri_indices.upload(g->tri_indices, 3 * size_t(g->n_triangles), a->stream));
+    BBG_TRY(a->positions.upload(g->positions, 3 * size_t(g->n_vertices), a->stream));
+    if (g->n_spheres)
+    {
+        BBG_TRY(a->spheres.upload(g->spheres, size_t(g->n_spheres), a->stream));
+    }
+    a->has_shading = g->n_triangles == 0 || (g->normals && g->tangents);
+    if (g->normals && g->tangents)
+    {
+        BBG_TRY(a->normals.upload(g->normals, 3 * size_t(g->n_vertices), a->stream));
+        BBG_TRY(a->tangents.upload(g->tangents, 3 * size_t(g->n_vertices), a->stream));
+        if (g->uvs)
+        {
+            BBG_TRY(a->uvs.upload(g->uvs, 2 * size_t(g->n_vertices), a->stream));
+        }
+    }
+    BBG_TRY(a->counters.alloc(2));
+    BBG_CUDA(cudaStreamSynchronize(a->stream));
+    return BBG_OK;
+}
+
+constexpr int64_t kChunkRays = int64_t(1) << 20;
+
+// Host-memory query: chunks of rays staged through two streams so the copies
+// of one chunk overlap the traversal of the other.
+template <bool ANY>
+bbg_status TraceHost(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out)
+{
+    const size_t out_bytes = ANY ? 1 : sizeof(bbg_hit);
+    for (int s = 0; s < 2; ++s)
+    {
+        BBG_TRY(a->stage_in[s].alloc(2 * size_t(std::min(n, kChunkRays))));
+        BBG_TRY(a->stage_out[s].alloc((size_t(std::min(n, kChunkRays)) * out_bytes + 15) / 16));
+    }
+    for (int64_t c = 0, k = 0; c < n; c += kChunkRays, ++k)
+    {
+        int s = int(k & 1);
+        int64_t m = std::min(kChunkRays, n - c);
+        cudaStream_t st = a->copy_stream[s];
+        BBG_CUDA(cudaMemcpyAsync(a->stage_in[s].p, rays + c, size_t(m) * sizeof(bbg_ray), cudaMemcpyHostToDevice, st));
+        if (ANY)
+        {
+            BBG_TRY(LaunchIntersectAny(a, a->stage_in[s].p, m, reinterpret_cast<uint8_t*>(a->stage_out[s].p), st));
+        }
+        else
+        {
+            BBG_TRY(LaunchIntersect(a, a->stage_in[s].p, m, a->stage_out[s].p, st));
+        }
+        BBG_CUDA(cudaMemcpyAsync(static_cast<char*>(out) + size_t(c) * out_bytes, a->stage_out[s].p,
+                                 size_t(m) * out_bytes, cudaMemcpyDeviceToHost, st));
+    }
+    for (int s = 0; s < 2; ++s)
+    {
+        BBG_CUDA(cudaStreamSynchronize(a->copy_stream[s]));
+    }
+    return BBG_OK;
+}
+
+template <bool ANY>
+bbg_status Query(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out, bbg_memory mem, void* stream)
+{
+    if (!a || (n > 0 && (!rays || !out)) || n < 0 || (mem != BBG_MEM_HOST && mem != BBG_MEM_DEVICE))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "intersect: bad argument");
+    }
+    if (a->counting)
+    {
+        BBG_CUDA(cudaMemset(a->counters.p, 0, 2 * sizeof(unsigned long long)));
+    }
+    if (mem == BBG_MEM_HOST)
+    {
+        BBG_TRY(TraceHost<ANY>(a, rays, n, out));
+    }
+    else
+    {
+        cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : a->stream;
+        const float4* r = reinterpret_cast<const float4*>(rays);
+        if (ANY)
+        {
+            BBG_TRY(LaunchIntersectAny(a, r, n, static_cast<uint8_t*>(out), st));
+        }
+        else
+        {
+            BBG_TRY(LaunchIntersect(a, r, n, static_cast<float4*>(out), st));
+        }
+        BBG_CUDA(cudaStreamSynchronize(st));
+    }
+    if (a->counting)
+    {
+        unsigned long long c[2];
+        BBG_CUDA(cudaMemcpy(c, a->counters.p, sizeof(c), cudaMemcpyDeviceToHost));
+        a->last_nodes = int64_t(c[0]);
+        a->last_prims = int64_t(c[1]);
+    }
+    return BBG_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+bbg_status bbg_accel_create(const bbg_geometry* geometry, const bbg_bvh* bvh, bbg_accel** out)
+{
+    if (!out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_create: out is NULL");
+    }
+    *out = nullptr;
+    auto* a = new bbg_accel;
+    bbg_status s = CreateAccel(geometry, bvh, a);
+    if (s != BBG_OK)
+    {
+        bbg_accel_destroy(a);
+        return s;
+    }
+    *out = a;
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_destroy(bbg_accel* a)
+{
+    if (!a)
+    {
+        return BBG_OK;
+    }
+    if (a->stream)
+    {
+        cudaStreamSynchronize(a->stream);
+        cudaStreamDestroy(a->stream);
+    }
+    for (int s = 0; s < 2; ++s)
+    {
+        if (a->copy_stream[s])
+        {
+            cudaStreamSynchronize(a->copy_stream[s]);
+            cudaStreamDestroy(a->copy_stream[s]);
+        }
+        if (a->stage_done[s])
+        {
+            cudaEventDestroy(a->stage_done[s]);
+        }
+    }
+    delete a;
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_bounds(const bbg_accel* a, float* aabb_out)
+{
+    if (!a || !aabb_out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_bounds: null argument");
+    }
+    std::memcpy(aabb_out, a->bounds, sizeof(a->bounds));
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_export(const bbg_accel* a, bbg_bvh_node* nodes_out, int32_t* slot_prims_out, int32_t* n_nodes_out,
+                            int32_t* n_slots_out)
+{
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_export: null accel");
+    }
+    if (n_nodes_out) *n_nodes_out = a->n_nodes;
+    if (n_slots_out) *n_slots_out = a->n_slots;
+    if (nodes_out) std::memcpy(nodes_out, a->host_nodes.data(), a->host_nodes.size() * sizeof(bbg_bvh_node));
+    if (slot_prims_out) std::memcpy(slot_prims_out, a->host_slots.data(), a->host_slots.size() * sizeof(int32_t));
+    return BBG_OK;
+}
+
+bbg_status bbg_intersect(bbg_accel* a, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem, void* stream)
+{
+    return Query<false>(a, rays, n, hits, mem, stream);
+}
+
+bbg_status bbg_intersect_any(bbg_accel* a, const bbg_ray* rays, int64_t n, uint8_t* occluded, bbg_memory mem,
+                             void* stream)
+{
+    return Query<true>(a, rays, n, occluded, mem, stream);
+}
+
+bbg_status bbg_accel_set_counting(bbg_accel* a, int32_t enable)
+{
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_set_counting: null accel");
+    }
+    a->counting = enable != 0;
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_last_counts(const bbg_accel* a, int64_t* nodes_visited, int64_t* prims_tested)
+{
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_last_counts: null accel");
+    }
+    if (nodes_visited) *nodes_visited = a->last_nodes;
+    if (prims_tested) *prims_tested = a->last_prims;
+    return BBG_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,59 @@
+// The accel handle: geometry and flattened BVH resident on the device.
+#pragma once
+
+#include "cuda_util.cuh"
+#include "dev_geometry.cuh"
+
+#include <vector>
+
+struct bbg_accel
+{
+    cudaStream_t stream = nullptr;
+    int32_t n_prims = 0;
+    int32_t n_nodes = 0;
+    int32_t n_slots = 0;
+    int32_t max_depth = 0;
+    float bounds[6] = {};
+
+    // Traversal data.
+    bbg::DevBuf<float4> nodes; // 2 float4 per node
+    bbg::DevBuf<float4> slots; // 3 float4 per slot
+
+    // Shading data (the reference Mesh arrays and shapes).
+    bbg::DevBuf<int2> prim_shape;     // (kind, index) per primitive
+    bbg::DevBuf<int32_t> tri_indices; // 3 per triangle
+    bbg::DevBuf<float> positions;     // 3 per vertex
+    bbg::DevBuf<float> normals;       // 3 per vertex
+    bbg::DevBuf<float> tangents;      // 3 per vertex
+    bbg::DevBuf<float> uvs;           // 2 per vertex
+    bbg::DevBuf<bbg_sphere> spheres;
+    bool has_shading = false;
+
+    // Host copies of the tree (export, light set-up).
+    std::vector<bbg_bvh_node> host_nodes;
+    std::vector<int32_t> host_slots;
+    std::vector<int2> host_prim_shape;
+    std::vector<int32_t> host_tri_indices;
+    std::vector<float> host_positions;
+    std::vector<bbg_sphere> host_spheres;
+
+    // Staging for host-memory calls (two pipeline stages).
+    bbg::DevBuf<float4> stage_in[2];
+    bbg::DevBuf<float4> stage_out[2];
+    cudaStream_t copy_stream[2] = { nullptr, nullptr };
+    cudaEvent_t stage_done[2] = { nullptr, nullptr };
+
+    // Traversal counters (nodes, prims) of the last call when enabled.
+    bool counting = false;
+    bbg::DevBuf<unsigned long long> counters;
+    int64_t last_nodes = 0, last_prims = 0;
+
+    bbg::AccelView view() const { return bbg::AccelView{ nodes.p, slots.p, n_nodes }; }
+};
+
+namespace bbg
+{
+// Launches the batched traversal kernel on device-resident rays.
+bbg_status LaunchIntersect(bbg_accel* a, const float4* rays, int64_t n, float4* hits, cudaStream_t stream);
+bbg_status LaunchIntersectAny(bbg_accel* a, const float4* rays, int64_t n, uint8_t* occluded, cudaStream_t stream);
+} // namespace bbg

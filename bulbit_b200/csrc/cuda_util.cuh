@@ -1,0 +1,92 @@
+// Small CUDA helpers: status-returning error checks and owning device buffers.
+#pragma once
+
+#include "bbg_internal.h"
+
+#include <cuda_runtime.h>
+#include <utility>
+
+namespace bbg
+{
+
+#define BBG_CUDA(call)                                                                                                 \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess)                                                                                         \
+        {                                                                                                              \
+            return ::bbg::Fail(e_ == cudaErrorMemoryAllocation ? BBG_ERR_OOM : BBG_ERR_CUDA, "%s failed: %s", #call,  \
+                               cudaGetErrorString(e_));                                                                \
+        }                                                                                                              \
+    } while (0)
+
+#define BBG_TRY(expr)                                                                                                  \
+    do                                                                                                                 \
+    {                                                                                                                  \
+        bbg_status s_ = (expr);                                                                                        \
+        if (s_ != BBG_OK)                                                                                              \
+        {                                                                                                              \
+            return s_;                                                                                                 \
+        }                                                                                                              \
+    } while (0)
+
+template <typename T>
+struct DevBuf
+{
+    T* p = nullptr;
+    size_t n = 0;
+
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    ~DevBuf() { reset(); }
+
+    void reset()
+    {
+        if (p)
+        {
+            cudaFree(p);
+        }
+        p = nullptr;
+        n = 0;
+    }
+
+    bbg_status alloc(size_t count)
+    {
+        if (count <= n && p)
+        {
+            return BBG_OK;
+        }
+        reset();
+        if (count == 0)
+        {
+            return BBG_OK;
+        }
+        cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&p), count * sizeof(T));
+        if (e != cudaSuccess)
+        {
+            p = nullptr;
+            return Fail(BBG_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", count * sizeof(T), cudaGetErrorString(e));
+        }
+        n = count;
+        return BBG_OK;
+    }
+
+    bbg_status upload(const T* host, size_t count, cudaStream_t stream = 0)
+    {
+        BBG_TRY(alloc(count));
+        if (count)
+        {
+            BBG_CUDA(cudaMemcpyAsync(p, host, count * sizeof(T), cudaMemcpyHostToDevice, stream));
+        }
+        return BBG_OK;
+    }
+};
+
+// Device 0 must be a compute-capability 10.x part (the kernels are sm_100a).
+bbg_status CheckDevice();
+
+// Grid size for a grid-stride kernel: resident blocks per SM x SM count.
+int PersistentGrid(const void* kernel, int block, size_t smem = 0);
+
+} // namespace bbg

@@ -1,0 +1,269 @@
+// BVH traversal and ray-primitive tests on the device.
+//
+// Restates, operation for operation, BVH::RayCast (include/bulbit/bvh.h:102-155),
+// BoundingBox3::TestRay (include/bulbit/bounding_box.h:443-483), the
+// Möller-Trumbore test of Triangle::Intersect (src/geometry/triangle.cpp:55-110)
+// and Sphere::Intersect (src/geometry/sphere.cpp:35-85), so closest-hit
+// primitive ids and t agree bit for bit with the reference, including its
+// last-visited-wins rule for equal t.
+//
+// Layout in HBM (see bbg_internal.h):
+//   nodes: 32 B each = two float4 (min.xyz, max.x) (max.yz, offset, count|axis<<16)
+//   slots: 48 B each = three float4 per leaf slot, primitives in leaf order
+#pragma once
+
+#include "bbg_internal.h"
+#include "dev_math.cuh"
+
+namespace bbg
+{
+
+struct AccelView
+{
+    const float4* nodes; // 2 per node
+    const float4* slots; // 3 per slot
+    int32_t n_nodes;
+};
+
+struct RayQ
+{
+    V3 o, d;          // ray as given
+    V3 inv_dir;       // 1 / d per component
+    V3 dn;            // d after Vector3::Normalize (triangle test)
+    float l;          // length returned by that Normalize
+    int neg[3];       // inv_dir < 0
+};
+
+__device__ __forceinline__ RayQ MakeRayQ(V3 o, V3 d)
+{
+    RayQ q;
+    q.o = o;
+    q.d = d;
+    q.inv_dir = V3{ 1 / d.x, 1 / d.y, 1 / d.z };
+    q.neg[0] = q.inv_dir.x < 0;
+    q.neg[1] = q.inv_dir.y < 0;
+    q.neg[2] = q.inv_dir.z < 0;
+    q.dn = d;
+    q.l = NormalizeInPlace(q.dn);
+    return q;
+}
+
+// BoundingBox3::TestRay: x and y slabs narrow [t_min, t_max], z only tests.
+__device__ __forceinline__ bool TestRay(const float4& a, const float4& b, const RayQ& q, float t_min, float t_max)
+{
+    // a = (min.x, min.y, min.z, max.x), b = (max.y, max.z, ., .)
+    float lo_x = q.neg[0] ? a.w : a.x, hi_x = q.neg[0] ? a.x : a.w;
+    float lo_y = q.neg[1] ? b.x : a.y, hi_y = q.neg[1] ? a.y : b.x;
+    float lo_z = q.neg[2] ? b.y : a.z, hi_z = q.neg[2] ? a.z : b.y;
+
+    float t_min_x = (lo_x - q.o.x) * q.inv_dir.x;
+    float t_max_x = (hi_x - q.o.x) * q.inv_dir.x;
+    if (t_min > t_max_x || t_max < t_min_x)
+    {
+        return false;
+    }
+    if (t_min_x > t_min) t_min = t_min_x;
+    if (t_max_x < t_max) t_max = t_max_x;
+
+    float t_min_y = (lo_y - q.o.y) * q.inv_dir.y;
+    float t_max_y = (hi_y - q.o.y) * q.inv_dir.y;
+    if (t_min > t_max_y || t_max < t_min_y)
+    {
+        return false;
+    }
+    if (t_min_y > t_min) t_min = t_min_y;
+    if (t_max_y < t_max) t_max = t_max_y;
+
+    float t_min_z = (lo_z - q.o.z) * q.inv_dir.z;
+    float t_max_z = (hi_z - q.o.z) * q.inv_dir.z;
+    if (t_min > t_max_z || t_max < t_min_z)
+    {
+        return false;
+    }
+    return true;
+}
+
+// Möller-Trumbore on the normalised direction (src/geometry/triangle.cpp:55-94).
+// Returns true and (t, u, v) on a hit in [t_min, t_max].
+__device__ __forceinline__ bool IntersectTriangle(V3 p0, V3 p1, V3 p2, const RayQ& q, float t_min, float t_max,
+                                                  float* t_out, float* u_out, float* v_out)
+{
+    V3 e1 = p1 - p0;
+    V3 e2 = p2 - p0;
+    V3 pvec = Cross(q.dn, e2);
+    float det = Dot(e1, pvec);
+    if (fabsf(det) < kEpsilon)
+    {
+        return false;
+    }
+    float invDet = 1 / det;
+    V3 tvec = q.o - p0;
+    float u = Dot(tvec, pvec) * invDet;
+    if (u < 0 || u > 1)
+    {
+        return false;
+    }
+    V3 qvec = Cross(tvec, e1);
+    float v = Dot(q.dn, qvec) * invDet;
+    if (v < 0 || u + v > 1)
+    {
+        return false;
+    }
+    float t = Dot(e2, qvec) * invDet / q.l;
+    if (t < t_min || t > t_max)
+    {
+        return false;
+    }
+    *t_out = t;
+    *u_out = u;
+    *v_out = v;
+    return true;
+}
+
+// Quat::RotateInv / Rotate (include/bulbit/quaternion.h:140-170).
+__device__ __forceinline__ V3 QuatRotateInv(float4 q, V3 v)
+{
+    float vx = 2 * v.x, vy = 2 * v.y, vz = 2 * v.z;
+    float w2 = q.w * q.w - 0.5f;
+    float dot2 = (q.x * vx + q.y * vy + q.z * vz);
+    return V3{ (vx * w2 - (q.y * vz - q.z * vy) * q.w + q.x * dot2),
+               (vy * w2 - (q.z * vx - q.x * vz) * q.w + q.y * dot2),
+               (vz * w2 - (q.x * vy - q.y * vx) * q.w + q.z * dot2) };
+}
+
+__device__ __forceinline__ V3 QuatRotate(float4 q, V3 v)
+{
+    float vx = 2 * v.x, vy = 2 * v.y, vz = 2 * v.z;
+    float w2 = q.w * q.w - 0.5f;
+    float dot2 = (q.x * vx + q.y * vy + q.z * vz);
+    return V3{ (vx * w2 + (q.y * vz - q.z * vy) * q.w + q.x * dot2),
+               (vy * w2 + (q.z * vx - q.x * vz) * q.w + q.y * dot2),
+               (vz * w2 + (q.x * vy - q.y * vx) * q.w + q.z * dot2) };
+}
+
+// Sphere::Intersect (src/geometry/sphere.cpp:35-61) in object space:
+// MulT(transform, ray) then the half-b quadratic; near root first.
+__device__ __forceinline__ bool IntersectSphere(V3 p, float4 rot, V3 s, float radius, V3 o, V3 d, float t_min,
+                                                float t_max, float* t_out)
+{
+    V3 ro = QuatRotateInv(rot, o - p) / s;
+    V3 rd = QuatRotateInv(rot, d / s);
+    V3 oc = ro;
+    float a = Length2(rd);
+    float half_b = Dot(oc, rd);
+    float c = Length2(oc) - radius * radius;
+    float discriminant = half_b * half_b - a * c;
+    if (discriminant < 0)
+    {
+        return false;
+    }
+    float sqrt_d = sqrtf(discriminant);
+    float root = (-half_b - sqrt_d) / a;
+    if (root < t_min || t_max < root)
+    {
+        root = (-half_b + sqrt_d) / a;
+        if (root < t_min || t_max < root)
+        {
+            return false;
+        }
+    }
+    *t_out = root;
+    return true;
+}
+
+struct TraceResult
+{
+    int32_t prim; // primitive index, -1 on a miss
+    float t, u, v;
+};
+
+// Stack traversal of BVH::RayCast. ANY = IntersectAny semantics (stop at the
+// first hit); otherwise Intersect semantics (shrink t_max; a hit at exactly
+// the current t_max replaces the previous one). COUNT accumulates nodes popped
+// and primitive tests.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, float t_min, float t_max,
+                                             uint32_t* nodes_visited = nullptr, uint32_t* prims_tested = nullptr)
+{
+    TraceResult res{ -1, t_max, 0, 0 };
+    int32_t stack[kStackCapacity];
+    int sp = 0;
+    stack[sp++] = 0;
+
+    while (sp > 0)
+    {
+        int32_t index = stack[--sp];
+        float4 na = __ldg(a.nodes + 2 * index);
+        float4 nb = __ldg(a.nodes + 2 * index + 1);
+        if (COUNT) ++*nodes_visited;
+        if (!TestRay(na, nb, q, t_min, t_max))
+        {
+            continue;
+        }
+        int32_t offset = __float_as_int(nb.z);
+        uint32_t packed = __float_as_uint(nb.w);
+        int32_t count = int32_t(packed & 0xffffu);
+        if (count > 0)
+        {
+            for (int32_t i = 0; i < count; ++i)
+            {
+                const float4* s = a.slots + 3 * size_t(offset + i);
+                float4 s0 = __ldg(s);
+                float4 s1 = __ldg(s + 1);
+                float4 s2 = __ldg(s + 2);
+                uint32_t tag = __float_as_uint(s0.w);
+                if (COUNT) ++*prims_tested;
+                bool hit;
+                float t, u = 0, v = 0;
+                if (tag & kSphereBit)
+                {
+                    hit = IntersectSphere(V3{ s0.x, s0.y, s0.z }, s1, V3{ s2.x, s2.y, s2.z }, s2.w, q.o, q.d, t_min,
+                                          t_max, &t);
+                }
+                else
+                {
+                    hit = IntersectTriangle(V3{ s0.x, s0.y, s0.z }, V3{ s1.x, s1.y, s1.z }, V3{ s2.x, s2.y, s2.z },
+                                            q, t_min, t_max, &t, &u, &v);
+                }
+                // The callback's return value: t_min after an any-hit, the
+                // hit's t after a closest hit, the running t_max on a miss;
+                // RayCast stops when it is <= t_min, else takes it as t_max.
+                if (hit)
+                {
+                    res.prim = int32_t(tag & ~kSphereBit);
+                    res.t = t;
+                    res.u = u;
+                    res.v = v;
+                    if (ANY)
+                    {
+                        return res;
+                    }
+                    t_max = t;
+                }
+                if (t_max <= t_min)
+                {
+                    return res;
+                }
+            }
+        }
+        else
+        {
+            int32_t child1 = index + 1;
+            int32_t child2 = offset;
+            int axis = int((packed >> 16) & 0xffu);
+            if (q.neg[axis])
+            {
+                stack[sp++] = child1;
+                stack[sp++] = child2;
+            }
+            else
+            {
+                stack[sp++] = child2;
+                stack[sp++] = child1;
+            }
+        }
+    }
+    return res;
+}
+
+} // namespace bbg

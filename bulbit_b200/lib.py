@@ -1,0 +1,171 @@
+"""Python binding of libbulbit_b200.so (include/bbg.h) for tests and benchmarks.
+
+The GPU library is required: if the shared library is missing or a call fails,
+an exception is raised — there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbulbit_b200.so")
+
+_lib = None
+
+
+class BbgError(RuntimeError):
+    def __init__(self, status, where):
+        msg = get_lib().bbg_last_error().decode(errors="replace")
+        super().__init__(f"{where}: {abi.STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def get_lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"bulbit_b200 native library not built: {LIB_PATH} "
+                               "(python -c 'import __graft_entry__ as g; g.build()')")
+        L = C.CDLL(LIB_PATH)
+        for name, res, args in abi.EXPORTS:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(status, where):
+    if status != abi.BBG_OK:
+        raise BbgError(status, where)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data
+
+
+def _dev_ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def bvh_build(aabbs):
+    """bbg_bvh_build over (n, 6) float32 AABBs -> (nodes, slot_prims)."""
+    aabbs = np.ascontiguousarray(aabbs, np.float32)
+    n = aabbs.shape[0]
+    nodes = np.zeros(max(1, 2 * n - 1), dtype=NODE_DTYPE)
+    slots = np.zeros(n, np.int32)
+    nn = C.c_int32()
+    check(get_lib().bbg_bvh_build(_p(aabbs), n, _p(nodes), _p(slots), C.byref(nn)), "bbg_bvh_build")
+    return nodes[:nn.value].copy(), slots
+
+
+def prim_aabbs(scene):
+    g = scene.geometry()
+    out = np.zeros((scene.n_prims, 6), np.float32)
+    check(get_lib().bbg_prim_aabbs(C.byref(g), _p(out)), "bbg_prim_aabbs")
+    return out
+
+
+def camera(spec):
+    out = abi.Camera()
+    check(get_lib().bbg_camera_perspective(C.byref(spec), C.byref(out)), "bbg_camera_perspective")
+    return out
+
+
+NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("offset", "<i4"),
+                       ("count", "<u2"), ("axis", "u1"), ("pad", "u1")])
+
+
+class GpuAccel:
+    """The GPU accel beside the reference BVH (bbg_accel_*)."""
+
+    def __init__(self, scene, bvh=None):
+        self.scene = scene
+        self._g = scene.geometry()
+        self.h = C.c_void_p()
+        bvh_arg = None
+        if bvh is not None:
+            nodes, slots = bvh
+            self._bvh_nodes = np.ascontiguousarray(nodes)
+            self._bvh_slots = np.ascontiguousarray(slots, np.int32)
+            b = abi.Bvh()
+            b.n_nodes = self._bvh_nodes.shape[0]
+            b.nodes = _p(self._bvh_nodes)
+            b.n_slots = self._bvh_slots.shape[0]
+            b.slot_prims = _p(self._bvh_slots)
+            bvh_arg = C.byref(b)
+            self._bvh_struct = b
+        check(get_lib().bbg_accel_create(C.byref(self._g), bvh_arg, C.byref(self.h)), "bbg_accel_create")
+
+    def close(self):
+        if self.h:
+            get_lib().bbg_accel_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def bounds(self):
+        out = np.zeros(6, np.float32)
+        check(get_lib().bbg_accel_bounds(self.h, _p(out)), "bbg_accel_bounds")
+        return out
+
+    def export(self):
+        nn, ns = C.c_int32(), C.c_int32()
+        check(get_lib().bbg_accel_export(self.h, None, None, C.byref(nn), C.byref(ns)), "bbg_accel_export")
+        nodes = np.zeros(nn.value, NODE_DTYPE)
+        slots = np.zeros(ns.value, np.int32)
+        check(get_lib().bbg_accel_export(self.h, _p(nodes), _p(slots), None, None), "bbg_accel_export")
+        return nodes, slots
+
+    def set_counting(self, on):
+        check(get_lib().bbg_accel_set_counting(self.h, 1 if on else 0), "bbg_accel_set_counting")
+
+    def last_counts(self):
+        a, b = C.c_int64(), C.c_int64()
+        check(get_lib().bbg_accel_last_counts(self.h, C.byref(a), C.byref(b)), "bbg_accel_last_counts")
+        return a.value, b.value
+
+    def intersect(self, rays):
+        """Closest hits of (n, 8) float32 rays (host numpy) -> (prim, t, u, v)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.zeros((rays.shape[0], 4), np.float32)
+        check(get_lib().bbg_intersect(self.h, _p(rays), rays.shape[0], _p(hits), abi.BBG_MEM_HOST, None),
+              "bbg_intersect")
+        return hits[:, 0].view(np.int32).copy(), hits[:, 1].copy(), hits[:, 2].copy(), hits[:, 3].copy()
+
+    def intersect_any(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32)
+        occ = np.zeros(rays.shape[0], np.uint8)
+        check(get_lib().bbg_intersect_any(self.h, _p(rays), rays.shape[0], _p(occ), abi.BBG_MEM_HOST, None),
+              "bbg_intersect_any")
+        return occ
+
+    def intersect_device(self, rays_t, hits_t, stream=None):
+        """Device-resident query: rays_t (n, 8) float32 and hits_t (n, 4) torch CUDA tensors."""
+        check(get_lib().bbg_intersect(self.h, _dev_ptr(rays_t), rays_t.shape[0], _dev_ptr(hits_t),
+                                      abi.BBG_MEM_DEVICE, stream), "bbg_intersect")
+
+    def intersect_any_device(self, rays_t, occ_t, stream=None):
+        check(get_lib().bbg_intersect_any(self.h, _dev_ptr(rays_t), rays_t.shape[0], _dev_ptr(occ_t),
+                                          abi.BBG_MEM_DEVICE, stream), "bbg_intersect_any")
+
+    def intersect_host_ptr(self, rays_ptr, n, hits_ptr):
+        check(get_lib().bbg_intersect(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr), abi.BBG_MEM_HOST,
+                                      None), "bbg_intersect")
+
+    def intersect_any_host_ptr(self, rays_ptr, n, occ_ptr):
+        check(get_lib().bbg_intersect_any(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(occ_ptr), abi.BBG_MEM_HOST,
+                                          None), "bbg_intersect_any")
+
+
+def sampler_draws(px, py, seed, sample, n):
+    out = np.zeros(n, np.float32)
+    check(get_lib().bbg_sampler_draws(px, py, seed, sample, n, _p(out)), "bbg_sampler_draws")
+    return out

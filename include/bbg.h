@@ -1,0 +1,350 @@
+/*
+ * bbg.h — C ABI of bulbit-b200, a B200 (sm_100a) wavefront implementation of
+ * Bulbit's unidirectional path tracer: SAH-BVH closest-hit / any-hit traversal
+ * over triangles and spheres, and PathIntegrator's next-event estimation with
+ * continuation-ray MIS.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, never
+ * throws, and reports failure through a bbg_status code plus a thread-local
+ * message (bbg_last_error). Handles own their device memory; callers own every
+ * buffer they pass. Calls on one handle must not run concurrently.
+ *
+ * Reference interfaces each entry point replaces (paths inside Sopiro/Bulbit):
+ *   bbg_bvh_build          BVH::BVH / BuildRecursive / FlattenBVH
+ *                          (src/accel/bvh.cpp:8,56,273)
+ *   bbg_accel_create       the GPU accel beside BVH: takes the reference-built
+ *                          flattened tree (include/bulbit/bvh.h:46 layout) or
+ *                          builds the same tree itself
+ *   bbg_intersect          BVH::Intersect (src/accel/bvh.cpp:299), batched
+ *   bbg_intersect_any      BVH::IntersectAny (src/accel/bvh.cpp:334), batched
+ *   bbg_accel_bounds       Intersectable::GetAABB (include/bulbit/intersectable.h:41)
+ *   bbg_camera_perspective PerspectiveCamera::PerspectiveCamera
+ *                          (src/camera/perspective_camera.cpp:8)
+ *   bbg_integrator_create  PathIntegrator::PathIntegrator
+ *                          (src/integrator/path_integrator.cpp:11) together with
+ *                          Integrator::Integrator (src/integrator/integrator.cpp:107)
+ *   bbg_render             UniDirectionalRayIntegrator::Render
+ *                          (src/integrator/integrator.cpp:162) driving
+ *                          PathIntegrator::Li (src/integrator/path_integrator.cpp:26),
+ *                          filling the same per-pixel state as Film::AddSample
+ *                          (src/reconstruction/film.cpp:26)
+ *   bbg_sampler_draws      IndependentSampler::StartPixelSample / Next1D
+ *                          (src/sampler/independent_sampler.cpp:13-22)
+ */
+#ifndef BBG_H
+#define BBG_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum bbg_status
+{
+    BBG_OK = 0,
+    BBG_ERR_INVALID_ARG = 1,    /* bad pointer, size or enum value */
+    BBG_ERR_OOM = 2,            /* device allocation failed */
+    BBG_ERR_TIMEOUT = 3,        /* a bounded device loop hit its iteration cap */
+    BBG_ERR_QUEUE_OVERFLOW = 4, /* a wavefront queue exceeded its capacity */
+    BBG_ERR_STACK_OVERFLOW = 5, /* traversal stack exceeded its capacity */
+    BBG_ERR_CUDA = 6,           /* any other CUDA runtime error */
+    BBG_ERR_BAD_BVH = 7,        /* node array failed validation before upload */
+    BBG_ERR_UNSUPPORTED = 8,    /* a feature outside this library's scope */
+    BBG_ERR_NO_DEVICE = 9       /* no CUDA device of compute capability 10.0 */
+} bbg_status;
+
+/* Where the buffers of a call live. HOST buffers are copied to and from the
+ * device inside the call; DEVICE buffers are used in place. */
+typedef enum bbg_memory
+{
+    BBG_MEM_HOST = 0,
+    BBG_MEM_DEVICE = 1
+} bbg_memory;
+
+/* ---------------------------------------------------------------- geometry */
+
+/* One flattened BVH node: byte-for-byte the reference's LinearBVHNode
+ * (include/bulbit/bvh.h:46-57): AABB (min xyz, max xyz), then the union of
+ * primitives_offset / child2_offset, uint16 primitive_count, uint8 axis. */
+typedef struct bbg_bvh_node
+{
+    float bmin[3];
+    float bmax[3];
+    int32_t offset;  /* leaf: first slot; interior: index of the second child */
+    uint16_t count;  /* leaf: number of primitives; 0 marks an interior node */
+    uint8_t axis;    /* interior: split axis */
+    uint8_t pad;
+} bbg_bvh_node;
+
+/* A flattened tree: nodes in depth-first order (first child at index+1), and
+ * for each leaf slot the index of the primitive it holds in the primitive list
+ * the tree was built over. */
+typedef struct bbg_bvh
+{
+    int32_t n_nodes;
+    const bbg_bvh_node* nodes;
+    int32_t n_slots;
+    const int32_t* slot_prims;
+} bbg_bvh;
+
+/* Sphere with the reference's Transform (position p, unit quaternion q as
+ * x,y,z,w, scale s) and radius (include/bulbit/shapes.h:12-31). */
+typedef struct bbg_sphere
+{
+    float p[3];
+    float q[4];
+    float s[3];
+    float radius;
+} bbg_sphere;
+
+enum
+{
+    BBG_PRIM_TRIANGLE = 0,
+    BBG_PRIM_SPHERE = 1
+};
+
+/* Scene geometry. Vertex attributes are the reference Mesh's world-space
+ * arrays (include/bulbit/mesh.h:37-41) concatenated over all meshes. Primitive
+ * i of the list (the vector handed to BVH) is a triangle (prim_index[i] =
+ * triangle number, its vertices tri_indices[3t..3t+2]) or a sphere
+ * (prim_index[i] = sphere number). normals/tangents/uvs may be NULL for a
+ * scene that is only ever intersected, never shaded. */
+typedef struct bbg_geometry
+{
+    int32_t n_vertices;
+    const float* positions; /* 3 per vertex */
+    const float* normals;   /* 3 per vertex or NULL */
+    const float* tangents;  /* 3 per vertex or NULL */
+    const float* uvs;       /* 2 per vertex or NULL */
+    int32_t n_triangles;
+    const int32_t* tri_indices; /* 3 per triangle */
+    int32_t n_spheres;
+    const bbg_sphere* spheres;
+    int32_t n_prims;
+    const int32_t* prim_kind;  /* BBG_PRIM_* per primitive */
+    const int32_t* prim_index; /* per primitive */
+} bbg_geometry;
+
+/* A ray query: Ray{o, d} with the [t_min, t_max] interval of
+ * Intersectable::Intersect (include/bulbit/intersectable.h:42). 32 bytes. */
+typedef struct bbg_ray
+{
+    float o[3];
+    float d[3];
+    float t_min;
+    float t_max;
+} bbg_ray;
+
+/* Closest hit: primitive index in the primitive list (-1 on a miss), the
+ * reference's Intersection::t, and the barycentrics (u, v) of a triangle hit. */
+typedef struct bbg_hit
+{
+    int32_t prim;
+    float t;
+    float u;
+    float v;
+} bbg_hit;
+
+typedef struct bbg_accel bbg_accel;
+
+/* Builds the reference's 12-bucket binned SAH tree (src/accel/bvh.cpp:56-271)
+ * over per-primitive AABBs (6 floats each: min xyz, max xyz), flattened
+ * depth-first (src/accel/bvh.cpp:273-297). nodes_out must hold 2*n_prims-1
+ * nodes and slot_prims_out n_prims entries. Single-threaded and
+ * deterministic: leaves take their slots in depth-first order. */
+bbg_status bbg_bvh_build(const float* prim_aabbs, int32_t n_prims, bbg_bvh_node* nodes_out,
+                         int32_t* slot_prims_out, int32_t* n_nodes_out);
+
+/* Primitive AABBs exactly as Triangle::GetAABB (src/geometry/triangle.cpp:40)
+ * and Sphere::GetAABB (src/geometry/sphere.cpp:30) compute them. */
+bbg_status bbg_prim_aabbs(const bbg_geometry* geometry, float* aabbs_out);
+
+/* Uploads geometry and a tree to device 0. bvh == NULL builds the tree with
+ * bbg_bvh_build. The tree is validated (child and slot ranges, no cycles)
+ * before upload. */
+bbg_status bbg_accel_create(const bbg_geometry* geometry, const bbg_bvh* bvh, bbg_accel** out);
+bbg_status bbg_accel_destroy(bbg_accel* accel);
+
+/* Root AABB (6 floats), as BVH::GetAABB (src/accel/bvh.cpp:363). */
+bbg_status bbg_accel_bounds(const bbg_accel* accel, float* aabb_out);
+
+/* Copies the uploaded tree back: n_nodes nodes and n_slots slot entries. */
+bbg_status bbg_accel_export(const bbg_accel* accel, bbg_bvh_node* nodes_out, int32_t* slot_prims_out,
+                            int32_t* n_nodes_out, int32_t* n_slots_out);
+
+/* Batched BVH::Intersect: one bbg_hit per ray. stream is a cudaStream_t
+ * (NULL = the handle's own stream); the call returns after the results are in
+ * hits. */
+bbg_status bbg_intersect(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem,
+                         void* stream);
+
+/* Batched BVH::IntersectAny: occluded[i] = 1 if ray i hits anything in
+ * [t_min, t_max]. */
+bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
+                             bbg_memory mem, void* stream);
+
+/* Traversal statistics of the last bbg_intersect / bbg_intersect_any call on
+ * this handle when counting is enabled: nodes popped and slab-tested, and
+ * primitive tests, summed over all rays. */
+bbg_status bbg_accel_set_counting(bbg_accel* accel, int32_t enable);
+bbg_status bbg_accel_last_counts(const bbg_accel* accel, int64_t* nodes_visited, int64_t* prims_tested);
+
+/* ---------------------------------------------------------------- shading */
+
+enum
+{
+    BBG_MAT_NONE = -1,
+    BBG_MAT_DIFFUSE = 0,            /* DiffuseMaterial, roughness 0: LambertianBxDF */
+    BBG_MAT_CONDUCTOR = 1,          /* ConductorMaterial, energy_compensation = false */
+    BBG_MAT_DIELECTRIC = 2,         /* DielectricMaterial, energy_compensation = false */
+    BBG_MAT_METALLIC_ROUGHNESS = 3  /* MetallicRoughnessMaterial */
+};
+
+/* Constant-texture material parameters.
+ *   DIFFUSE:   reflectance = albedo
+ *   CONDUCTOR: eta, k (RGB); reflectance = lobe reflectance (1,1,1 default);
+ *              conductor_from_r != 0 selects the (R, roughness) constructor,
+ *              with R in k (include/bulbit/bxdfs.h:261-272)
+ *   DIELECTRIC: eta[0] = index of refraction; reflectance = reflectance
+ *   METALLIC_ROUGHNESS: reflectance = basecolor, metallic
+ *   roughness[0], roughness[1] = u and v roughness (alpha = roughness^2, or
+ *   max(roughness^2, 1e-3) for METALLIC_ROUGHNESS). */
+typedef struct bbg_material
+{
+    int32_t type;
+    int32_t conductor_from_r;
+    float reflectance[3];
+    float eta[3];
+    float k[3];
+    float roughness[2];
+    float metallic;
+} bbg_material;
+
+enum
+{
+    BBG_LIGHT_POINT = 0,
+    BBG_LIGHT_SPOT = 1,
+    BBG_LIGHT_UNIFORM_INFINITE = 2,
+    BBG_LIGHT_DIFFUSE_AREA = 3
+};
+
+/* Light parameters, as the reference constructors take them
+ * (include/bulbit/lights.h):
+ *   POINT:  position, intensity
+ *   SPOT:   position, direction (the ctor's "direction" argument), intensity,
+ *           angle_max / angle_falloff_start in degrees
+ *   UNIFORM_INFINITE: intensity = L, scale
+ *   DIFFUSE_AREA: prim (primitive index), intensity = constant emission,
+ *           two_sided */
+typedef struct bbg_light
+{
+    int32_t type;
+    int32_t prim;
+    int32_t two_sided;
+    float position[3];
+    float direction[3];
+    float intensity[3];
+    float scale;
+    float angle_max;
+    float angle_falloff_start;
+} bbg_light;
+
+/* PerspectiveCamera inputs (src/camera/perspective_camera.cpp:8) with a
+ * Transform::LookAt(position, target, up) pose and a BoxFilter(extent). */
+typedef struct bbg_camera_spec
+{
+    float position[3];
+    float target[3];
+    float up[3];
+    float vfov_deg;
+    float aperture_radius;
+    float focus_distance;
+    int32_t width;
+    int32_t height;
+    float filter_extent;
+} bbg_camera_spec;
+
+/* The derived state PerspectiveCamera::SampleRay reads
+ * (include/bulbit/cameras.h:50-61). */
+typedef struct bbg_camera
+{
+    int32_t width;
+    int32_t height;
+    float origin[3];
+    float lower_left[3];
+    float horizontal[3];
+    float vertical[3];
+    float u[3];
+    float v[3];
+    float lens_radius;
+    float filter_extent;
+} bbg_camera;
+
+bbg_status bbg_camera_perspective(const bbg_camera_spec* spec, bbg_camera* out);
+
+typedef struct bbg_integrator bbg_integrator;
+
+/* PathIntegrator(accel, lights, sampler, max_bounces, rr_min_bounces,
+ * regularize_bsdf) with a PowerLightSampler. prim_material[i] is the material
+ * index of primitive i or BBG_MAT_NONE (a medium boundary: rays pass
+ * through). Lights are preprocessed against the accel's bounds as the
+ * reference Integrator constructor does. */
+bbg_status bbg_integrator_create(bbg_accel* accel, const int32_t* prim_material, const bbg_material* materials,
+                                 int32_t n_materials, const bbg_light* lights, int32_t n_lights,
+                                 int32_t max_bounces, int32_t rr_min_bounces, int32_t regularize_bsdf,
+                                 bbg_integrator** out);
+bbg_status bbg_integrator_destroy(bbg_integrator* integrator);
+
+/* Light selection pmf of each light (PowerLightSampler::EvaluatePMF,
+ * src/light_sampler/power_light_sampler.cpp:44). */
+bbg_status bbg_integrator_light_pmf(const bbg_integrator* integrator, float* pmf_out);
+
+typedef struct bbg_render_params
+{
+    int32_t spp;          /* IndependentSampler samples_per_pixel */
+    int32_t seed;         /* IndependentSampler seed */
+    int64_t wave_paths;   /* paths in flight per wave; 0 = library default */
+    int32_t use_graph;    /* capture the bounce loop of a wave in a CUDA graph */
+    int32_t light_alias;  /* 1: sample lights with a Walker alias table (same
+                             pmf, different stream) instead of CDF inversion */
+} bbg_render_params;
+
+/* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields
+ * are those Film::AddSample maintains (src/reconstruction/film.cpp:26-37):
+ * radiance sum, sample count (NaN/Inf samples are skipped), and luminance
+ * moments. path_L, if not NULL, receives each path's radiance (3 floats per
+ * path, path index (y*W + x)*spp + sample). */
+typedef struct bbg_film
+{
+    float* rgb_sum;
+    int32_t* count;
+    float* moments;
+    float* path_L;
+} bbg_film;
+
+typedef struct bbg_render_stats
+{
+    int64_t paths;
+    int64_t closest_rays;   /* closest-hit rays traced */
+    int64_t shadow_rays;    /* shadow rays traced */
+    double device_ms;       /* device time of the render, CUDA events */
+} bbg_render_stats;
+
+bbg_status bbg_render(bbg_integrator* integrator, const bbg_camera* camera, const bbg_render_params* params,
+                      bbg_film* film, bbg_memory mem, bbg_render_stats* stats);
+
+/* The first n uniform draws of IndependentSampler after
+ * StartPixelSample(pixel, sample) with the given seed, computed on the device. */
+bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out);
+
+/* --------------------------------------------------------------- library */
+
+const char* bbg_last_error(void);
+const char* bbg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BBG_H */
