@@ -175,6 +175,30 @@ def cpu_baseline(scene, closest, anyq):
 
 # ------------------------------------------------------------------ GPU arm
 
+def run_e2e(args, acc, closest, anyq, barrier):
+    """Closest + any-hit through the C ABI with pinned host buffers: the
+    host->device copy of the rays and the device->host copy of the results
+    happen inside each call (bbg_intersect with BBG_MEM_HOST)."""
+    import torch
+    n = closest.shape[0]
+    pin_c = torch.from_numpy(closest).pin_memory()
+    pin_a = torch.from_numpy(anyq).pin_memory()
+    pin_h = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    pin_o = torch.empty(n, dtype=torch.uint8).pin_memory()
+    steps = max(1, min(args.steps, 5))
+    acc.intersect_host_ptr(pin_c.data_ptr(), n, pin_h.data_ptr())
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        acc.intersect_host_ptr(pin_c.data_ptr(), n, pin_h.data_ptr())
+        acc.intersect_any_host_ptr(pin_a.data_ptr(), n, pin_o.data_ptr())
+    torch.cuda.synchronize()
+    secs = time.perf_counter() - t0
+    barrier()
+    return steps, secs
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -182,6 +206,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="bulbit_b200", choices=["bulbit_b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per query set (smaller cases for profiling)")
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -202,16 +228,17 @@ def main():
         if world > 1:
             dist.barrier()
 
+    n_rays = args.rays
     scene = scenes.triangle_soup(N_TRIS, seed=1)
-    closest, anyq = scenes.soup_rays(N_RAYS, seed=2)
+    closest, anyq = scenes.soup_rays(n_rays, seed=2)
     t0 = time.perf_counter()
     acc = lib.GpuAccel(scene)
     build_s = time.perf_counter() - t0
 
     dev_c = torch.from_numpy(closest).cuda()
     dev_a = torch.from_numpy(anyq).cuda()
-    hits = torch.empty((N_RAYS, 4), dtype=torch.float32, device="cuda")
-    occ = torch.empty(N_RAYS, dtype=torch.uint8, device="cuda")
+    hits = torch.empty((n_rays, 4), dtype=torch.float32, device="cuda")
+    occ = torch.empty(n_rays, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
 
@@ -257,34 +284,21 @@ def main():
     any_ms = [e[1].elapsed_time(e[2]) for e in ev]
 
     # End to end through the C ABI with host (pinned) buffers: copies inside.
-    pin_c = torch.from_numpy(closest).pin_memory()
-    pin_a = torch.from_numpy(anyq).pin_memory()
-    pin_h = torch.empty((N_RAYS, 4), dtype=torch.float32).pin_memory()
-    pin_o = torch.empty(N_RAYS, dtype=torch.uint8).pin_memory()
-    e2e_steps = max(1, min(args.steps, 5))
-    acc.intersect_host_ptr(pin_c.data_ptr(), N_RAYS, pin_h.data_ptr())
-    barrier()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
-        acc.intersect_host_ptr(pin_c.data_ptr(), N_RAYS, pin_h.data_ptr())
-        acc.intersect_any_host_ptr(pin_a.data_ptr(), N_RAYS, pin_o.data_ptr())
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    barrier()
-
+    e2e_steps, e2e_s = 0, float("nan")
+    if not args.no_e2e:
+        e2e_steps, e2e_s = run_e2e(args, acc, closest, anyq, barrier)
     if world > 1:
         tt = torch.tensor([ms, e2e_s], device="cuda")
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms, e2e_s = float(tt[0]), float(tt[1])
 
-    rays_per_step = 2 * N_RAYS
+    rays_per_step = 2 * n_rays
     value = world * rays_per_step * args.steps / (ms / 1e3) / 1e6
-    e2e_value = world * rays_per_step * e2e_steps / e2e_s / 1e6
+    e2e_value = world * rays_per_step * e2e_steps / e2e_s / 1e6 if e2e_steps else None
 
     peaks, peak_kind = load_peaks()
     avg_closest_ms = statistics.mean(closest_ms)
-    bytes_closest = N_RAYS * (32 + 16) + 32 * nodes_c + 48 * prims_c
+    bytes_closest = n_rays * (32 + 16) + 32 * nodes_c + 48 * prims_c
     achieved = bytes_closest / (avg_closest_ms / 1e3) / 1e9
     traffic = profile_traffic("trace_closest_soup1m.md")
 
@@ -292,7 +306,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "Mrays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays_per_step": rays_per_step,
+        "config": {"workload": WORKLOAD if n_rays == N_RAYS else f"{WORKLOAD} (reduced to {n_rays} rays)",
+                   "triangles": N_TRIS, "rays_per_step": rays_per_step,
                    "l2": "inputs larger than L2 (512 MiB of rays per query set)",
                    "parallelism": f"replicas x{world}", "bvh_build_s": round(build_s, 3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
@@ -300,11 +315,11 @@ def main():
                      "kernel": "TraceKernel<closest> (bulbit_b200/csrc/accel.cu)",
                      "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_closest,
-                     "per_ray": {"nodes": nodes_c / N_RAYS, "prims": prims_c / N_RAYS,
-                                 "any_nodes": nodes_a / N_RAYS, "any_prims": prims_a / N_RAYS},
+                     "per_ray": {"nodes": nodes_c / n_rays, "prims": prims_c / n_rays,
+                                 "any_nodes": nodes_a / n_rays, "any_prims": prims_a / n_rays},
                      "avg_launch_ms": {"closest": avg_closest_ms, "any": statistics.mean(any_ms)}},
-        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 2 * N_RAYS * 32,
-                "d2h_bytes_per_step": N_RAYS * 16 + N_RAYS * 1},
+        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 2 * n_rays * 32,
+                "d2h_bytes_per_step": n_rays * 16 + n_rays * 1},
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }
