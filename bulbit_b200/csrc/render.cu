@@ -1,21 +1,1122 @@
-// Placeholder while the wavefront path tracer is written.
+// Wavefront path tracer: PathIntegrator::Li (src/integrator/path_integrator.cpp:26-196)
+// recast as queues on the device.
+//
+// A render is a sequence of waves; a wave holds whole pixels (all their
+// samples), one path per slot, slot = path index - wave base, path index =
+// (y*W + x)*spp + sample. Per wave:
+//   Raygen     seed each path's sampler and sample its camera ray
+//   repeat max_bounces + 1 times (one bounce level per iteration):
+//     Closest  closest hit of every path in the ray queue
+//     Shade    miss / emission MIS, bounce limit, BSDF, next-event estimation
+//              (enqueues a shadow ray with its full contribution), BSDF
+//              sample, Russian roulette; survivors go to the next ray queue
+//     Shadow   any-hit for each shadow ray; if unoccluded L += contribution
+//   Film       per pixel, its samples in order, as Film::AddSample does
+// The order of additions to each path's L is the reference's (emission of
+// vertex k, then its direct light, then vertex k+1), so L agrees up to the
+// transcendental functions. Kernels read their queue lengths from device
+// memory, so a wave's launches are captured once as a CUDA graph and replayed.
+
 #include "accel.cuh"
+#include "dev_bsdf.cuh"
+#include "dev_lights.cuh"
+
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+namespace bbg
+{
+
+constexpr int kBlock = 128;
+
+struct SceneDev
+{
+    AccelView accel;
+    const int4* prim_info; // kind, index, material, area light
+    const int32_t* tri_indices;
+    const float* positions;
+    const float* normals;
+    const float* tangents;
+    const bbg_sphere* spheres;
+    const MaterialDev* materials;
+    const LightDev* lights;
+    const float* light_func;
+    const float* light_cdf;
+    const float* light_pmf;  // EvaluatePMF per light
+    const float* alias_prob;
+    const int32_t* alias_idx;
+    const int32_t* infinite;  // infinite light indices, in light order
+    int32_t n_lights;
+    int32_t n_infinite;
+    float light_func_integral;
+    int32_t light_alias;
+    int32_t max_bounces;
+    int32_t rr_min_bounces;
+    int32_t regularize;
+    int32_t spp;
+    int32_t seed;
+    CameraDev camera;
+};
+
+// Per-wave device state (structure of arrays, one entry per slot).
+struct WaveDev
+{
+    float4* o_pdf;   // ray origin, prev_bsdf_pdf
+    float4* d_eta;   // ray direction, eta_scale
+    float4* beta;    // throughput
+    float4* L;       // radiance
+    uint64_t* rng;   // PCG32 state
+    int32_t* flags;  // bounce | specular << 16 | any_non_specular << 17
+    float4* hit;     // prim bits, t, u, v
+    int32_t* queue[2];
+    float4* sh_o;    // shadow ray origin, t_max
+    float4* sh_d;    // shadow ray direction, slot bits
+    float4* sh_c;    // contribution
+    int32_t* counts; // [0],[1] ray queues, [2] shadow queue
+    unsigned long long* stats; // closest rays, shadow rays
+    const int64_t* wave;       // [0] first path, [1] paths in wave
+};
+
+constexpr int32_t kSpecularBit = 1 << 16;
+constexpr int32_t kAnyNonSpecularBit = 1 << 17;
+
+// Warp-aggregated append of `pred` lanes to a queue counter.
+__device__ __forceinline__ int32_t Append(int32_t* counter, bool pred)
+{
+    unsigned active = __activemask();
+    unsigned m = __ballot_sync(active, pred);
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(active) - 1;
+    int32_t base = 0;
+    if (lane == leader && m)
+    {
+        base = atomicAdd(counter, __popc(m));
+    }
+    base = __shfl_sync(active, base, leader);
+    return base + __popc(m & ((1u << lane) - 1u));
+}
+
+// ---------------------------------------------------------------- raygen
+
+// Render loop body (src/integrator/integrator.cpp:185-190) and
+// PerspectiveCamera::SampleRay (src/camera/perspective_camera.cpp:40-52).
+__global__ void __launch_bounds__(kBlock) RaygenKernel(SceneDev s, WaveDev w)
+{
+    const int64_t base = w.wave[0];
+    const int64_t n = w.wave[1];
+    const CameraDev& c = s.camera;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        int64_t path = base + i;
+        int32_t sample = int32_t(path % s.spp);
+        int64_t pixel = path / s.spp;
+        int32_t px = int32_t(pixel % c.width);
+        int32_t py = int32_t(pixel / c.width);
+        uint64_t rng = SamplerStart(px, py, s.seed, sample);
+        P2 u1 = Next2D(rng); // lens sample: the right-hand argument, drawn first
+        P2 u0 = Next2D(rng); // filter sample
+
+        // BoxFilter::Sample: (2u - 1) * extent / 2, then + 0.5.
+        P2 f{ (u0.x * 2 - 1) * c.filter_extent / 2, (u0.y * 2 - 1) * c.filter_extent / 2 };
+        P2 off{ f.x + 0.5f, f.y + 0.5f };
+        V3 pixel_center = load3(c.lower_left) + load3(c.horizontal) * (px + off.x) / float(c.width) +
+                          load3(c.vertical) * (py + off.y) / float(c.height);
+        P2 disk = SampleUniformUnitDiskConcentric(u1);
+        P2 aperture{ disk.x * c.lens_radius, disk.y * c.lens_radius };
+        V3 offset = load3(c.u) * aperture.x + load3(c.v) * aperture.y;
+        V3 origin = load3(c.origin) + offset;
+        V3 d = Normalize(pixel_center - origin);
+
+        w.o_pdf[i] = make_float4(origin.x, origin.y, origin.z, 0.0f);
+        w.d_eta[i] = make_float4(d.x, d.y, d.z, 1.0f);
+        w.beta[i] = make_float4(1, 1, 1, 0);
+        w.L[i] = make_float4(0, 0, 0, 0);
+        w.rng[i] = rng;
+        w.flags[i] = 0;
+        w.queue[0][i] = int32_t(i);
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        w.counts[0] = int32_t(n);
+        w.counts[1] = 0;
+        w.counts[2] = 0;
+    }
+}
+
+// ---------------------------------------------------------------- intersect
+
+__global__ void __launch_bounds__(kBlock) ClosestKernel(SceneDev s, WaveDev w, int parity)
+{
+    const int32_t* q = w.queue[parity];
+    const int32_t n = w.counts[parity];
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        atomicAdd(w.stats, (unsigned long long)n);
+    }
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        int32_t slot = q[j];
+        float4 o = w.o_pdf[slot];
+        float4 d = w.d_eta[slot];
+        RayQ rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
+        TraceResult r = Trace<false, false>(s.accel, rq, kRayEpsilon, INFINITY);
+        w.hit[slot] = make_float4(__int_as_float(r.prim), r.t, r.u, r.v);
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) ShadowKernel(SceneDev s, WaveDev w)
+{
+    const int32_t n = w.counts[2];
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        atomicAdd(w.stats + 1, (unsigned long long)n);
+    }
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        float4 o = w.sh_o[j];
+        float4 d = w.sh_d[j];
+        RayQ rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
+        TraceResult r = Trace<true, false>(s.accel, rq, kRayEpsilon, o.w);
+        if (r.prim < 0)
+        {
+            int32_t slot = __float_as_int(d.w);
+            float4 c = w.sh_c[j];
+            float4 L = w.L[slot];
+            w.L[slot] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, 0.0f);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- shading
+
+struct Isect
+{
+    V3 point;
+    V3 normal;  // geometric, facing the incoming ray
+    V3 sn, st;  // shading normal / tangent
+    bool front_face;
+    float t;
+};
+
+// SetFaceNormal (include/bulbit/shape.h:32-43).
+__device__ __forceinline__ void SetFaceNormal(Isect* is, V3 ray_d, V3 outward, V3 sn, V3 st)
+{
+    bool front_face = Dot(ray_d, outward) < 0;
+    float sign = front_face ? 1.0f : -1.0f;
+    is->front_face = front_face;
+    is->normal = sign * outward;
+    is->sn = sign * sn;
+    is->st = sign * st;
+}
+
+__device__ __forceinline__ void TriVerts(const SceneDev& s, int32_t tri, int32_t v[3], V3 p[3])
+{
+    v[0] = s.tri_indices[3 * tri];
+    v[1] = s.tri_indices[3 * tri + 1];
+    v[2] = s.tri_indices[3 * tri + 2];
+    for (int k = 0; k < 3; ++k)
+    {
+        p[k] = load3(s.positions + 3 * size_t(v[k]));
+    }
+}
+
+// Triangle::Intersect hit record (src/geometry/triangle.cpp:96-109) and
+// Sphere::Intersect hit record (src/geometry/sphere.cpp:63-84).
+__device__ __forceinline__ Isect MakeIsect(const SceneDev& s, int4 info, float4 hit, V3 ro, V3 rd)
+{
+    Isect is;
+    is.t = hit.y;
+    if (info.x == BBG_PRIM_TRIANGLE)
+    {
+        int32_t v[3];
+        V3 p[3];
+        TriVerts(s, info.y, v, p);
+        float u = hit.z, vv = hit.w;
+        float ww = 1 - u - vv;
+        is.point = ro + rd * is.t;
+        V3 e1 = p[1] - p[0];
+        V3 e2 = p[2] - p[0];
+        V3 normal = Normalize(Cross(e1, e2));
+        V3 n0 = load3(s.normals + 3 * size_t(v[0])), n1 = load3(s.normals + 3 * size_t(v[1])),
+           n2 = load3(s.normals + 3 * size_t(v[2]));
+        V3 t0 = load3(s.tangents + 3 * size_t(v[0])), t1 = load3(s.tangents + 3 * size_t(v[1])),
+           t2 = load3(s.tangents + 3 * size_t(v[2]));
+        V3 sn = Normalize(ww * n0 + u * n1 + vv * n2);
+        V3 st = Normalize(ww * t0 + u * t1 + vv * t2);
+        SetFaceNormal(&is, rd, normal, sn, st);
+    }
+    else
+    {
+        const bbg_sphere& sp = s.spheres[info.y];
+        V3 c = load3(sp.p), sc = load3(sp.s);
+        float4 q = make_float4(sp.q[0], sp.q[1], sp.q[2], sp.q[3]);
+        V3 lo = QuatRotateInv(q, ro - c) / sc;
+        V3 ld = QuatRotateInv(q, rd / sc);
+        V3 point = lo + ld * is.t;
+        V3 normal = Normalize(point / sp.radius);
+        is.point = QuatRotate(q, sc * point) + c;
+        V3 n = QuatRotate(q, normal);
+        V3 t;
+        if (n.y < 1 - 1e-4f)
+        {
+            t = Normalize(Cross(V3{ 0, 1, 0 }, n));
+        }
+        else
+        {
+            t = Normalize(Cross(n, V3{ 1, 0, 0 }));
+        }
+        SetFaceNormal(&is, rd, n, n, t);
+    }
+    return is;
+}
+
+// Shape::PDF(isect, ray) for MIS on emitted light
+// (src/geometry/triangle.cpp:247-253, src/geometry/sphere.cpp:181-189).
+__device__ __forceinline__ float ShapePdf(const SceneDev& s, int4 info, const Isect& is, V3 ro, V3 rd)
+{
+    if (info.x == BBG_PRIM_TRIANGLE)
+    {
+        int32_t v[3];
+        V3 p[3];
+        TriVerts(s, info.y, v, p);
+        float distance_squared = is.t * is.t * Length2(rd);
+        float cosine = fabsf(Dot(rd, is.normal) / Length(rd));
+        float area = 0.5f * Length(Cross(p[1] - p[0], p[2] - p[0]));
+        return distance_squared / (cosine * area);
+    }
+    const bbg_sphere& sp = s.spheres[info.y];
+    float distance_squared = Length2(load3(sp.p) - ro);
+    float cos_theta_max = sqrtf(1 - sp.radius * sp.radius / distance_squared);
+    float solid_angle = kTwoPi * (1 - cos_theta_max);
+    return 1 / solid_angle;
+}
+
+// PowerLightSampler::Sample: Distribution1D::SampleDiscrete by FindInterval
+// (include/bulbit/sampling.h:395-410, include/bulbit/math.h:117-134), or the
+// alias table when enabled.
+__device__ __forceinline__ int32_t SampleLight(const SceneDev& s, float u, float* pmf)
+{
+    int32_t n = s.n_lights;
+    if (s.light_alias)
+    {
+        float x = u * n;
+        int32_t i = min(int32_t(x), n - 1);
+        float frac = x - i;
+        int32_t k = frac < s.alias_prob[i] ? i : s.alias_idx[i];
+        *pmf = s.light_pmf[k];
+        return k;
+    }
+    int32_t size = n + 1;
+    int32_t first = 0, len = size;
+    while (len > 0)
+    {
+        int32_t half = len >> 1, middle = first + half;
+        if (s.light_cdf[middle] <= u)
+        {
+            first = middle + 1;
+            len -= half + 1;
+        }
+        else
+        {
+            len = half;
+        }
+    }
+    int32_t offset = first - 1;
+    offset = offset < 0 ? 0 : (offset > size - 2 ? size - 2 : offset);
+    *pmf = s.light_func[offset] / (s.light_func_integral * n);
+    return offset;
+}
+
+__global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int parity)
+{
+    const int32_t* q = w.queue[parity];
+    int32_t* q_next = w.queue[parity ^ 1];
+    const int32_t n = w.counts[parity];
+
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        int32_t slot = q[j];
+        float4 o4 = w.o_pdf[slot], d4 = w.d_eta[slot], b4 = w.beta[slot], L4 = w.L[slot];
+        float4 hit = w.hit[slot];
+        V3 ro{ o4.x, o4.y, o4.z }, rd{ d4.x, d4.y, d4.z };
+        float prev_bsdf_pdf = o4.w, eta_scale = d4.w;
+        Spec beta{ b4.x, b4.y, b4.z }, L{ L4.x, L4.y, L4.z };
+        uint64_t rng = w.rng[slot];
+        int32_t fl = w.flags[slot];
+        int32_t bounce = fl & 0xffff;
+        bool specular_bounce = (fl & kSpecularBit) != 0;
+        bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
+
+        bool cont = false;       // path continues to the next bounce
+        bool shadow = false;     // a shadow ray was generated
+        V3 sh_o{}, sh_d{};
+        float sh_t = 0;
+        Spec sh_c{};
+
+        int32_t prim = __float_as_int(hit.x);
+        if (prim < 0)
+        {
+            // Escaped: infinite lights (path_integrator.cpp:41-63).
+            for (int32_t k = 0; k < s.n_infinite; ++k)
+            {
+                const LightDev& l = s.lights[s.infinite[k]];
+                Spec Le = l.scale * Spec{ l.L[0], l.L[1], l.L[2] };
+                if (bounce == 0 || specular_bounce)
+                {
+                    L = L + beta * Le;
+                }
+                else
+                {
+                    float light_pdf = kInvFourPi * s.light_pmf[s.infinite[k]];
+                    float mis_weight = PowerHeuristic(prev_bsdf_pdf, light_pdf);
+                    L = L + beta * mis_weight * Le;
+                }
+            }
+        }
+        else
+        {
+            int4 info = s.prim_info[prim];
+            Isect is = MakeIsect(s, info, hit, ro, rd);
+            V3 wo = Normalize(-rd);
+
+            // Emission from an area light (path_integrator.cpp:67-84).
+            if (info.w >= 0)
+            {
+                const LightDev& l = s.lights[info.w];
+                Spec Le = (is.front_face || l.two_sided) ? Spec{ l.L[0], l.L[1], l.L[2] } : spec(0);
+                if (!IsBlack(Le))
+                {
+                    if (bounce == 0 || specular_bounce)
+                    {
+                        L = L + beta * Le;
+                    }
+                    else
+                    {
+                        float light_pdf = ShapePdf(s, info, is, ro, rd) * s.light_pmf[info.w];
+                        float mis_weight = PowerHeuristic(prev_bsdf_pdf, light_pdf);
+                        L = L + beta * mis_weight * Le;
+                    }
+                }
+            }
+
+            if (bounce++ >= s.max_bounces)
+            {
+                // terminated
+            }
+            else if (info.z < 0)
+            {
+                // No material: a medium boundary; continue straight through
+                // without counting a bounce (path_integrator.cpp:95-100).
+                ro = is.point;
+                rd = -wo;
+                --bounce;
+                cont = true;
+            }
+            else
+            {
+                BSDF bsdf = MakeBSDF(s.materials[info.z], is.sn, is.st, is.front_face);
+                if (s.regularize && any_non_specular)
+                {
+                    bsdf.mf.Regularize();
+                    if (bsdf.type == BBG_MAT_CONDUCTOR)
+                    {
+                        bsdf.flags = bsdf.mf.EffectivelySmooth() ? (kFlagSpecular | kFlagReflection)
+                                                                 : (kFlagGlossy | kFlagReflection);
+                    }
+                    else if (bsdf.type == BBG_MAT_DIELECTRIC)
+                    {
+                        int32_t f = (bsdf.eta == 1) ? kFlagTransmission : (kFlagReflection | kFlagTransmission);
+                        bsdf.flags = f | (bsdf.mf.EffectivelySmooth() ? kFlagSpecular : kFlagGlossy);
+                    }
+                }
+
+                // Next-event estimation (PathIntegrator::SampleDirectLight).
+                if (IsNonSpecular(bsdf.flags))
+                {
+                    float u0 = Next1D(rng);
+                    P2 u12 = Next2D(rng);
+                    if (s.n_lights > 0)
+                    {
+                        float pmf;
+                        int32_t li = SampleLight(s, u0, &pmf);
+                        const LightDev& l = s.lights[li];
+                        V3 tri[3];
+                        const bbg_sphere* sph = nullptr;
+                        bool on_tri = false;
+                        if (l.type == BBG_LIGHT_DIFFUSE_AREA)
+                        {
+                            int4 linfo = s.prim_info[l.prim];
+                            if (linfo.x == BBG_PRIM_TRIANGLE)
+                            {
+                                int32_t v[3];
+                                TriVerts(s, linfo.y, v, tri);
+                                on_tri = true;
+                            }
+                            else
+                            {
+                                sph = &s.spheres[linfo.y];
+                            }
+                        }
+                        LightSampleLi ls;
+                        if (SampleLi(l, is.point, u12, on_tri ? tri : nullptr, sph, &ls))
+                        {
+                            float bsdf_pdf = bsdf.PDF(wo, ls.wi);
+                            if (!(IsBlack(ls.Li) || bsdf_pdf == 0))
+                            {
+                                float light_pdf = pmf * ls.pdf;
+                                Spec f_cos = bsdf.F(wo, ls.wi) * AbsDot(is.sn, ls.wi);
+                                if (IsDeltaLight(l.type))
+                                {
+                                    sh_c = beta * ls.Li * f_cos / light_pdf;
+                                }
+                                else
+                                {
+                                    float mis_weight = PowerHeuristic(light_pdf, bsdf_pdf);
+                                    sh_c = beta * mis_weight * ls.Li * f_cos / light_pdf;
+                                }
+                                shadow = true;
+                                sh_o = is.point;
+                                sh_d = ls.wi;
+                                sh_t = ls.visibility;
+                            }
+                        }
+                    }
+                }
+
+                // BSDF sample: Next2D (right argument) before Next1D.
+                P2 u12 = Next2D(rng);
+                float u0 = Next1D(rng);
+                BSDFSample bs;
+                if (bsdf.Sample(&bs, wo, u0, u12))
+                {
+                    bool spec_sample = (bs.flags & kFlagSpecular) != 0;
+                    specular_bounce = spec_sample;
+                    any_non_specular = any_non_specular || !spec_sample;
+                    if (bs.flags & kFlagTransmission)
+                    {
+                        eta_scale *= Sqr(bs.eta);
+                    }
+                    prev_bsdf_pdf = bs.pdf;
+                    beta = beta * (bs.f * AbsDot(is.sn, bs.wi) / bs.pdf);
+                    ro = is.point;
+                    rd = bs.wi;
+                    cont = true;
+
+                    // Russian roulette (path_integrator.cpp:133-146).
+                    if (bounce > s.rr_min_bounces)
+                    {
+                        float p = MaxComponent(beta) * eta_scale;
+                        if (p < 1)
+                        {
+                            if (Next1D(rng) > p)
+                            {
+                                cont = false;
+                            }
+                            else
+                            {
+                                beta = beta / p;
+                            }
+                        }
+                    }
+                }
+            }
+        }
+
+        w.L[slot] = make_float4(L.r, L.g, L.b, 0.0f);
+        if (cont)
+        {
+            w.o_pdf[slot] = make_float4(ro.x, ro.y, ro.z, prev_bsdf_pdf);
+            w.d_eta[slot] = make_float4(rd.x, rd.y, rd.z, eta_scale);
+            w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
+            w.rng[slot] = rng;
+            w.flags[slot] = bounce | (specular_bounce ? kSpecularBit : 0) | (any_non_specular ? kAnyNonSpecularBit : 0);
+        }
+        int32_t qi = Append(&w.counts[parity ^ 1], cont);
+        if (cont)
+        {
+            q_next[qi] = slot;
+        }
+        int32_t si = Append(&w.counts[2], shadow);
+        if (shadow)
+        {
+            w.sh_o[si] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_t);
+            w.sh_d[si] = make_float4(sh_d.x, sh_d.y, sh_d.z, __int_as_float(slot));
+            w.sh_c[si] = make_float4(sh_c.r, sh_c.g, sh_c.b, 0.0f);
+        }
+    }
+}
+
+__global__ void ResetKernel(WaveDev w, int parity)
+{
+    w.counts[parity ^ 1] = 0;
+    w.counts[2] = 0;
+}
+
+// ---------------------------------------------------------------- film
+
+struct FilmDev
+{
+    float* rgb_sum;
+    int32_t* count;
+    float* moments;
+    float* path_L; // optional
+};
+
+// Film::AddSample over each pixel's samples in order (src/reconstruction/film.cpp:26-37).
+__global__ void __launch_bounds__(kBlock) FilmKernel(SceneDev s, WaveDev w, FilmDev f)
+{
+    const int64_t base = w.wave[0];
+    const int64_t n_pixels = w.wave[1] / s.spp;
+    const int64_t pixel0 = base / s.spp;
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_pixels; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        Spec sum = spec(0);
+        int32_t count = 0;
+        float m0 = 0, m1 = 0;
+        for (int32_t k = 0; k < s.spp; ++k)
+        {
+            int64_t slot = i * s.spp + k;
+            float4 L4 = w.L[slot];
+            Spec L{ L4.x, L4.y, L4.z };
+            if (f.path_L)
+            {
+                float* dst = f.path_L + 3 * (base + slot);
+                dst[0] = L.r;
+                dst[1] = L.g;
+                dst[2] = L.b;
+            }
+            if (IsNullish(L))
+            {
+                continue;
+            }
+            sum = sum + L * 1.0f;
+            count += 1;
+            float l = Luminance(L);
+            float alpha = 1.0f / count;
+            m0 = m0 * (1 - alpha) + l * alpha;
+            m1 = m1 * (1 - alpha) + (l * l) * alpha;
+        }
+        int64_t p = pixel0 + i;
+        f.rgb_sum[3 * p] = sum.r;
+        f.rgb_sum[3 * p + 1] = sum.g;
+        f.rgb_sum[3 * p + 2] = sum.b;
+        f.count[p] = count;
+        f.moments[2 * p] = m0;
+        f.moments[2 * p + 1] = m1;
+    }
+}
+
+// ---------------------------------------------------------------- sampler probe
+
+__global__ void SamplerDrawsKernel(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out)
+{
+    uint64_t st = SamplerStart(px, py, seed, sample);
+    for (int32_t i = 0; i < n; ++i)
+    {
+        out[i] = Next1D(st);
+    }
+}
+
+} // namespace bbg
 
 using namespace bbg;
 
+// ---------------------------------------------------------------- handle
+
+struct bbg_integrator
+{
+    bbg_accel* accel = nullptr;
+    int32_t n_lights = 0;
+    std::vector<float> pmf;
+    int32_t max_bounces = 0, rr_min_bounces = 1, regularize = 0;
+
+    DevBuf<int4> prim_info;
+    DevBuf<MaterialDev> materials;
+    DevBuf<LightDev> lights;
+    DevBuf<float> light_func, light_cdf, light_pmf, alias_prob;
+    DevBuf<int32_t> alias_idx, infinite;
+    float func_integral = 0;
+    int32_t n_infinite = 0;
+
+    // Wave state.
+    int64_t capacity = 0;
+    DevBuf<float4> o_pdf, d_eta, beta, L, hit, sh_o, sh_d, sh_c;
+    DevBuf<uint64_t> rng;
+    DevBuf<int32_t> flags, queue0, queue1, counts;
+    DevBuf<unsigned long long> stats;
+    DevBuf<int64_t> wave;
+    int64_t* wave_host = nullptr; // pinned
+
+    // Film (device copies for host-memory renders).
+    DevBuf<float> film_rgb, film_moments, film_path_L;
+    DevBuf<int32_t> film_count;
+
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int64_t graph_capacity = -1;
+    int graph_iterations = -1;
+    FilmDev graph_film{};
+    SceneDev graph_scene{};
+
+    ~bbg_integrator()
+    {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (stream) cudaStreamDestroy(stream);
+        if (wave_host) cudaFreeHost(wave_host);
+    }
+
+    WaveDev Wave()
+    {
+        WaveDev w;
+        w.o_pdf = o_pdf.p;
+        w.d_eta = d_eta.p;
+        w.beta = beta.p;
+        w.L = L.p;
+        w.rng = rng.p;
+        w.flags = flags.p;
+        w.hit = hit.p;
+        w.queue[0] = queue0.p;
+        w.queue[1] = queue1.p;
+        w.sh_o = sh_o.p;
+        w.sh_d = sh_d.p;
+        w.sh_c = sh_c.p;
+        w.counts = counts.p;
+        w.stats = stats.p;
+        w.wave = wave.p;
+        return w;
+    }
+
+    bbg_status Reserve(int64_t n)
+    {
+        if (n <= capacity) return BBG_OK;
+        size_t m = size_t(n);
+        for (auto* b : { &o_pdf, &d_eta, &beta, &L, &hit, &sh_o, &sh_d, &sh_c })
+        {
+            b->reset();
+            BBG_TRY(b->alloc(m));
+        }
+        rng.reset();
+        BBG_TRY(rng.alloc(m));
+        for (auto* b : { &flags, &queue0, &queue1 })
+        {
+            b->reset();
+            BBG_TRY(b->alloc(m));
+        }
+        capacity = n;
+        return BBG_OK;
+    }
+};
+
+namespace
+{
+
+struct Grids
+{
+    int raygen, closest, shade, shadow, film;
+    Grids()
+    {
+        raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel), kBlock);
+        closest = PersistentGrid(reinterpret_cast<const void*>(ClosestKernel), kBlock);
+        shade = PersistentGrid(reinterpret_cast<const void*>(ShadeKernel), kBlock);
+        shadow = PersistentGrid(reinterpret_cast<const void*>(ShadowKernel), kBlock);
+        film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel), kBlock);
+    }
+};
+
+void EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, int parity, cudaStream_t st)
+{
+    ResetKernel<<<1, 1, 0, st>>>(w, parity);
+    ClosestKernel<<<gr.closest, kBlock, 0, st>>>(s, w, parity);
+    ShadeKernel<<<gr.shade, kBlock, 0, st>>>(s, w, parity);
+    ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(s, w);
+}
+
+bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const FilmDev& film, int iterations,
+                   cudaStream_t st)
+{
+    WaveDev w = I->Wave();
+    RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(s, w);
+    for (int k = 0; k < iterations; ++k)
+    {
+        EnqueueLevel(gr, s, w, k & 1, st);
+    }
+    FilmKernel<<<gr.film, kBlock, 0, st>>>(s, w, film);
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bool SameScene(const SceneDev& a, const SceneDev& b)
+{
+    return std::memcmp(&a, &b, sizeof(SceneDev)) == 0;
+}
+
+bool SameFilm(const FilmDev& a, const FilmDev& b)
+{
+    return std::memcmp(&a, &b, sizeof(FilmDev)) == 0;
+}
+
+bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p, bbg_film* film, bbg_memory mem,
+                  bbg_render_stats* stats)
+{
+    if (!cam || !p || !film || !film->rgb_sum || !film->count || !film->moments || p->spp <= 0 || cam->width <= 0 ||
+        cam->height <= 0 || (mem != BBG_MEM_HOST && mem != BBG_MEM_DEVICE))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_render: bad argument");
+    }
+    bbg_accel* a = I->accel;
+    const int64_t n_pixels = int64_t(cam->width) * cam->height;
+    const int64_t n_paths = n_pixels * p->spp;
+
+    // Wave size: whole pixels, at most the requested (or default) paths.
+    int64_t want = p->wave_paths > 0 ? p->wave_paths : (int64_t(1) << 22);
+    int64_t px_per_wave = std::max<int64_t>(1, want / p->spp);
+    px_per_wave = std::min(px_per_wave, n_pixels);
+    const int64_t wave_paths = px_per_wave * p->spp;
+    if (wave_paths > (int64_t(1) << 30))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "wave of %lld paths exceeds 2^30", (long long)wave_paths);
+    }
+    BBG_TRY(I->Reserve(wave_paths));
+
+    SceneDev s{};
+    s.accel = a->view();
+    s.prim_info = I->prim_info.p;
+    s.tri_indices = a->tri_indices.p;
+    s.positions = a->positions.p;
+    s.normals = a->normals.p;
+    s.tangents = a->tangents.p;
+    s.spheres = a->spheres.p;
+    s.materials = I->materials.p;
+    s.lights = I->lights.p;
+    s.light_func = I->light_func.p;
+    s.light_cdf = I->light_cdf.p;
+    s.light_pmf = I->light_pmf.p;
+    s.alias_prob = I->alias_prob.p;
+    s.alias_idx = I->alias_idx.p;
+    s.infinite = I->infinite.p;
+    s.n_lights = I->n_lights;
+    s.n_infinite = I->n_infinite;
+    s.light_func_integral = I->func_integral;
+    s.light_alias = p->light_alias && I->n_lights > 0 ? 1 : 0;
+    s.max_bounces = I->max_bounces;
+    s.rr_min_bounces = I->rr_min_bounces;
+    s.regularize = I->regularize;
+    s.spp = p->spp;
+    s.seed = p->seed;
+    s.camera.width = cam->width;
+    s.camera.height = cam->height;
+    std::memcpy(s.camera.origin, cam->origin, sizeof(float) * 3);
+    std::memcpy(s.camera.lower_left, cam->lower_left, sizeof(float) * 3);
+    std::memcpy(s.camera.horizontal, cam->horizontal, sizeof(float) * 3);
+    std::memcpy(s.camera.vertical, cam->vertical, sizeof(float) * 3);
+    std::memcpy(s.camera.u, cam->u, sizeof(float) * 3);
+    std::memcpy(s.camera.v, cam->v, sizeof(float) * 3);
+    s.camera.lens_radius = cam->lens_radius;
+    s.camera.filter_extent = cam->filter_extent;
+
+    FilmDev f{};
+    if (mem == BBG_MEM_DEVICE)
+    {
+        f.rgb_sum = film->rgb_sum;
+        f.count = film->count;
+        f.moments = film->moments;
+        f.path_L = film->path_L;
+    }
+    else
+    {
+        BBG_TRY(I->film_rgb.alloc(3 * size_t(n_pixels)));
+        BBG_TRY(I->film_count.alloc(size_t(n_pixels)));
+        BBG_TRY(I->film_moments.alloc(2 * size_t(n_pixels)));
+        f.rgb_sum = I->film_rgb.p;
+        f.count = I->film_count.p;
+        f.moments = I->film_moments.p;
+        if (film->path_L)
+        {
+            BBG_TRY(I->film_path_L.alloc(3 * size_t(n_paths)));
+            f.path_L = I->film_path_L.p;
+        }
+    }
+
+    cudaStream_t st = I->stream;
+    BBG_CUDA(cudaMemsetAsync(I->stats.p, 0, 2 * sizeof(unsigned long long), st));
+    cudaEvent_t e0, e1;
+    BBG_CUDA(cudaEventCreate(&e0));
+    BBG_CUDA(cudaEventCreate(&e1));
+    BBG_CUDA(cudaEventRecord(e0, st));
+
+    const int iterations = I->max_bounces + 1;
+    const Grids gr;
+    bool use_graph = p->use_graph != 0;
+    if (use_graph && (!I->graph || I->graph_capacity != wave_paths || I->graph_iterations != iterations ||
+                      !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f)))
+    {
+        if (I->graph)
+        {
+            cudaGraphExecDestroy(I->graph);
+            I->graph = nullptr;
+        }
+        cudaGraph_t g;
+        BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        bbg_status es = Enqueue(I, gr, s, f, iterations, st);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        BBG_TRY(es);
+        if (ce != cudaSuccess)
+        {
+            return Fail(BBG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        }
+        BBG_CUDA(cudaGraphInstantiate(&I->graph, g, 0));
+        cudaGraphDestroy(g);
+        I->graph_capacity = wave_paths;
+        I->graph_iterations = iterations;
+        I->graph_scene = s;
+        I->graph_film = f;
+    }
+
+    for (int64_t base = 0; base < n_paths; base += wave_paths)
+    {
+        int64_t count = std::min(wave_paths, n_paths - base);
+        BBG_CUDA(cudaStreamSynchronize(st)); // the pinned wave record is reused
+        I->wave_host[0] = base;
+        I->wave_host[1] = count;
+        BBG_CUDA(cudaMemcpyAsync(I->wave.p, I->wave_host, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        if (use_graph)
+        {
+            BBG_CUDA(cudaGraphLaunch(I->graph, st));
+        }
+        else
+        {
+            BBG_TRY(Enqueue(I, gr, s, f, iterations, st));
+        }
+        // Paths still queued after max_bounces + 1 levels only come from
+        // material-less surfaces, which do not count a bounce
+        // (path_integrator.cpp:95-100): drain them level by level.
+        int32_t left = 0;
+        int parity = iterations & 1;
+        BBG_CUDA(cudaMemcpyAsync(&left, I->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        BBG_CUDA(cudaStreamSynchronize(st));
+        int extra = 0;
+        while (left > 0)
+        {
+            if (++extra > 4096)
+            {
+                return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
+            }
+            EnqueueLevel(gr, s, I->Wave(), parity, st);
+            parity ^= 1;
+            BBG_CUDA(cudaMemcpyAsync(&left, I->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            BBG_CUDA(cudaStreamSynchronize(st));
+        }
+        if (extra > 0)
+        {
+            // Re-run the film pass for this wave after the extra levels.
+            FilmKernel<<<gr.film, kBlock, 0, st>>>(s, I->Wave(), f);
+        }
+    }
+    BBG_CUDA(cudaEventRecord(e1, st));
+    BBG_CUDA(cudaStreamSynchronize(st));
+    BBG_CUDA(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+
+    if (mem == BBG_MEM_HOST)
+    {
+        BBG_CUDA(cudaMemcpy(film->rgb_sum, f.rgb_sum, 3 * sizeof(float) * size_t(n_pixels), cudaMemcpyDeviceToHost));
+        BBG_CUDA(cudaMemcpy(film->count, f.count, sizeof(int32_t) * size_t(n_pixels), cudaMemcpyDeviceToHost));
+        BBG_CUDA(cudaMemcpy(film->moments, f.moments, 2 * sizeof(float) * size_t(n_pixels), cudaMemcpyDeviceToHost));
+        if (film->path_L)
+        {
+            BBG_CUDA(cudaMemcpy(film->path_L, f.path_L, 3 * sizeof(float) * size_t(n_paths), cudaMemcpyDeviceToHost));
+        }
+    }
+    if (stats)
+    {
+        unsigned long long c[2];
+        BBG_CUDA(cudaMemcpy(c, I->stats.p, sizeof(c), cudaMemcpyDeviceToHost));
+        stats->paths = n_paths;
+        stats->closest_rays = int64_t(c[0]);
+        stats->shadow_rays = int64_t(c[1]);
+        stats->device_ms = ms;
+    }
+    return BBG_OK;
+}
+
+bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim_material, const bbg_material* mats,
+                            int32_t n_mats, const bbg_light* lights, int32_t n_lights)
+{
+    if (!a->has_shading)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "the accel was created without normals/tangents");
+    }
+    std::vector<MaterialDev> md(size_t(std::max(n_mats, 1)));
+    for (int32_t i = 0; i < n_mats; ++i)
+    {
+        BBG_TRY(MakeMaterial(mats[i], &md[i]));
+    }
+    std::vector<int4> info(size_t(a->n_prims));
+    for (int32_t i = 0; i < a->n_prims; ++i)
+    {
+        int32_t m = prim_material ? prim_material[i] : -1;
+        if (m >= n_mats || m < -1)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "primitive %d names material %d of %d", i, m, n_mats);
+        }
+        info[i] = make_int4(a->host_prim_shape[i].x, a->host_prim_shape[i].y, m, -1);
+    }
+
+    // Geometry view for the host-side light set-up.
+    bbg_geometry g{};
+    g.n_vertices = int32_t(a->host_positions.size() / 3);
+    g.positions = a->host_positions.data();
+    g.n_triangles = int32_t(a->host_tri_indices.size() / 3);
+    g.tri_indices = a->host_tri_indices.data();
+    g.n_spheres = int32_t(a->host_spheres.size());
+    g.spheres = a->host_spheres.data();
+    g.n_prims = a->n_prims;
+    std::vector<int32_t> kind(size_t(a->n_prims)), index(size_t(a->n_prims));
+    for (int32_t i = 0; i < a->n_prims; ++i)
+    {
+        kind[i] = a->host_prim_shape[i].x;
+        index[i] = a->host_prim_shape[i].y;
+    }
+    g.prim_kind = kind.data();
+    g.prim_index = index.data();
+
+    std::vector<LightDev> ld(size_t(std::max(n_lights, 1)));
+    std::vector<float> power(size_t(std::max(n_lights, 1)));
+    std::vector<int32_t> infinite;
+    for (int32_t i = 0; i < n_lights; ++i)
+    {
+        BBG_TRY(MakeLight(lights[i], g, a->bounds, &ld[i], &power[i]));
+        if (lights[i].type == BBG_LIGHT_UNIFORM_INFINITE)
+        {
+            infinite.push_back(i);
+        }
+        if (lights[i].type == BBG_LIGHT_DIFFUSE_AREA)
+        {
+            // Integrator::Integrator keeps one light per primitive (a HashMap insert).
+            if (info[lights[i].prim].w < 0)
+            {
+                info[lights[i].prim].w = i;
+            }
+        }
+    }
+    I->n_lights = n_lights;
+    std::vector<float> func(size_t(std::max(n_lights, 1))), cdf(size_t(n_lights + 1)), pmf(size_t(std::max(n_lights, 1)));
+    std::vector<float> prob(size_t(std::max(n_lights, 1)));
+    std::vector<int32_t> alias(size_t(std::max(n_lights, 1)));
+    if (n_lights > 0)
+    {
+        BuildDistribution(power.data(), n_lights, func.data(), cdf.data(), &I->func_integral);
+        for (int32_t i = 0; i < n_lights; ++i)
+        {
+            pmf[i] = func[i] / (I->func_integral * n_lights);
+        }
+        BuildAlias(pmf.data(), n_lights, prob.data(), alias.data());
+    }
+    I->pmf.assign(pmf.begin(), pmf.begin() + n_lights);
+    I->n_infinite = int32_t(infinite.size());
+    if (infinite.empty())
+    {
+        infinite.push_back(0);
+    }
+
+    BBG_CUDA(cudaStreamCreateWithFlags(&I->stream, cudaStreamNonBlocking));
+    BBG_TRY(I->prim_info.upload(info.data(), info.size(), I->stream));
+    BBG_TRY(I->materials.upload(md.data(), md.size(), I->stream));
+    BBG_TRY(I->lights.upload(ld.data(), ld.size(), I->stream));
+    BBG_TRY(I->light_func.upload(func.data(), func.size(), I->stream));
+    BBG_TRY(I->light_cdf.upload(cdf.data(), cdf.size(), I->stream));
+    BBG_TRY(I->light_pmf.upload(pmf.data(), pmf.size(), I->stream));
+    BBG_TRY(I->alias_prob.upload(prob.data(), prob.size(), I->stream));
+    BBG_TRY(I->alias_idx.upload(alias.data(), alias.size(), I->stream));
+    BBG_TRY(I->infinite.upload(infinite.data(), infinite.size(), I->stream));
+    BBG_TRY(I->counts.alloc(4));
+    BBG_TRY(I->stats.alloc(2));
+    BBG_TRY(I->wave.alloc(2));
+    BBG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&I->wave_host), 2 * sizeof(int64_t)));
+    BBG_CUDA(cudaStreamSynchronize(I->stream));
+    return BBG_OK;
+}
+
+} // namespace
+
 extern "C" {
-bbg_status bbg_integrator_create(bbg_accel*, const int32_t*, const bbg_material*, int32_t, const bbg_light*, int32_t,
-                                 int32_t, int32_t, int32_t, bbg_integrator** out)
+
+bbg_status bbg_integrator_create(bbg_accel* accel, const int32_t* prim_material, const bbg_material* materials,
+                                 int32_t n_materials, const bbg_light* lights, int32_t n_lights, int32_t max_bounces,
+                                 int32_t rr_min_bounces, int32_t regularize_bsdf, bbg_integrator** out)
 {
-    if (out) *out = nullptr;
-    return Fail(BBG_ERR_UNSUPPORTED, "integrator not built yet");
+    if (!out || !accel || n_materials < 0 || n_lights < 0 || (n_materials > 0 && !materials) ||
+        (n_lights > 0 && !lights) || max_bounces < 0)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_integrator_create: bad argument");
+    }
+    *out = nullptr;
+    if (accel->n_prims == 0)
+    {
+        return Fail(BBG_ERR_UNSUPPORTED, "integrator over an empty scene");
+    }
+    auto* I = new bbg_integrator;
+    I->accel = accel;
+    I->max_bounces = max_bounces;
+    I->rr_min_bounces = rr_min_bounces;
+    I->regularize = regularize_bsdf;
+    bbg_status s = CreateIntegrator(I, accel, prim_material, materials, n_materials, lights, n_lights);
+    if (s != BBG_OK)
+    {
+        delete I;
+        return s;
+    }
+    *out = I;
+    return BBG_OK;
 }
-bbg_status bbg_integrator_destroy(bbg_integrator*) { return BBG_OK; }
-bbg_status bbg_integrator_light_pmf(const bbg_integrator*, float*) { return BBG_ERR_UNSUPPORTED; }
-bbg_status bbg_render(bbg_integrator*, const bbg_camera*, const bbg_render_params*, bbg_film*, bbg_memory,
-                      bbg_render_stats*)
+
+bbg_status bbg_integrator_destroy(bbg_integrator* I)
 {
-    return BBG_ERR_UNSUPPORTED;
+    if (I)
+    {
+        if (I->stream) cudaStreamSynchronize(I->stream);
+        delete I;
+    }
+    return BBG_OK;
 }
-bbg_status bbg_sampler_draws(int32_t, int32_t, int32_t, int32_t, int32_t, float*) { return BBG_ERR_UNSUPPORTED; }
+
+bbg_status bbg_integrator_light_pmf(const bbg_integrator* I, float* pmf_out)
+{
+    if (!I || (!pmf_out && I->n_lights > 0))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_integrator_light_pmf: bad argument");
+    }
+    std::memcpy(pmf_out, I->pmf.data(), sizeof(float) * I->pmf.size());
+    return BBG_OK;
 }
+
+bbg_status bbg_render(bbg_integrator* I, const bbg_camera* camera, const bbg_render_params* params, bbg_film* film,
+                      bbg_memory mem, bbg_render_stats* stats)
+{
+    if (!I)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_render: null integrator");
+    }
+    return Render(I, camera, params, film, mem, stats);
+}
+
+bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out)
+{
+    if (!out || n <= 0 || n > (1 << 20))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_sampler_draws: bad argument");
+    }
+    BBG_TRY(CheckDevice());
+    DevBuf<float> d;
+    BBG_TRY(d.alloc(size_t(n)));
+    SamplerDrawsKernel<<<1, 1>>>(px, py, seed, sample, n, d.p);
+    BBG_CUDA(cudaGetLastError());
+    BBG_CUDA(cudaMemcpy(out, d.p, sizeof(float) * size_t(n), cudaMemcpyDeviceToHost));
+    return BBG_OK;
+}
+
+} // extern "C"

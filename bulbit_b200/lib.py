@@ -169,3 +169,84 @@ def sampler_draws(px, py, seed, sample, n):
     out = np.zeros(n, np.float32)
     check(get_lib().bbg_sampler_draws(px, py, seed, sample, n, _p(out)), "bbg_sampler_draws")
     return out
+
+
+class Film:
+    """Per-pixel film state of a render (what Film::AddSample maintains)."""
+
+    def __init__(self, width, height, spp, path_L=False):
+        self.width, self.height, self.spp = width, height, spp
+        self.rgb_sum = np.zeros((height, width, 3), np.float32)
+        self.count = np.zeros((height, width), np.int32)
+        self.moments = np.zeros((height, width, 2), np.float32)
+        self.path_L = np.zeros((height * width * spp, 3), np.float32) if path_L else None
+        self.stats = abi.RenderStats()
+
+    def struct(self):
+        f = abi.Film()
+        f.rgb_sum = _p(self.rgb_sum)
+        f.count = _p(self.count)
+        f.moments = _p(self.moments)
+        f.path_L = _p(self.path_L)
+        return f
+
+    def image(self):
+        """Film::GetRenderedImage: sum / count (src/reconstruction/film.cpp:80-100)."""
+        with np.errstate(invalid="ignore", divide="ignore"):
+            return self.rgb_sum / self.count[..., None].astype(np.float32)
+
+
+class GpuPathIntegrator:
+    """PathIntegrator(accel, lights, sampler, max_bounces, rr_min_bounces,
+    regularize_bsdf) on the GPU (bbg_integrator_*, bbg_render)."""
+
+    def __init__(self, accel, scene, max_bounces=None, rr_min_bounces=None, regularize=0):
+        self.accel = accel
+        self.scene = scene
+        self._mats = scene.material_array()
+        self._lights = scene.light_array()
+        self._pm = np.ascontiguousarray(scene.prim_material, np.int32)
+        self.h = C.c_void_p()
+        mb = scene.max_bounces if max_bounces is None else max_bounces
+        rr = scene.rr_min_bounces if rr_min_bounces is None else rr_min_bounces
+        check(get_lib().bbg_integrator_create(accel.h, _p(self._pm), C.addressof(self._mats), len(scene.materials),
+                                              C.addressof(self._lights), len(scene.lights), mb, rr, regularize,
+                                              C.byref(self.h)), "bbg_integrator_create")
+
+    def close(self):
+        if self.h:
+            get_lib().bbg_integrator_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def light_pmf(self):
+        out = np.zeros(max(1, len(self.scene.lights)), np.float32)
+        check(get_lib().bbg_integrator_light_pmf(self.h, _p(out)), "bbg_integrator_light_pmf")
+        return out[:len(self.scene.lights)]
+
+    def render(self, spp=None, seed=None, camera_spec=None, wave_paths=0, use_graph=True, light_alias=False,
+               path_L=False):
+        s = self.scene
+        spec = camera_spec or s.camera
+        cam = camera(spec)
+        spp = spp or s.spp
+        p = abi.RenderParams()
+        p.spp = spp
+        p.seed = s.seed if seed is None else seed
+        p.wave_paths = wave_paths
+        p.use_graph = 1 if use_graph else 0
+        p.light_alias = 1 if light_alias else 0
+        film = Film(cam.width, cam.height, spp, path_L=path_L)
+        fs = film.struct()
+        check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(p), C.byref(fs), abi.BBG_MEM_HOST,
+                                   C.byref(film.stats)), "bbg_render")
+        return film
+
+    def render_device(self, cam, params, film_struct, stats):
+        check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(params), C.byref(film_struct),
+                                   abi.BBG_MEM_DEVICE, C.byref(stats)), "bbg_render")
