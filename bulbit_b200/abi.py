@@ -33,6 +33,9 @@ BBG_MAT_CONDUCTOR = 1
 BBG_MAT_DIELECTRIC = 2
 BBG_MAT_METALLIC_ROUGHNESS = 3
 
+BBG_TRAVERSAL_ORDERED = 0
+BBG_TRAVERSAL_REFERENCE = 1
+
 BBG_LIGHT_POINT = 0
 BBG_LIGHT_SPOT = 1
 BBG_LIGHT_UNIFORM_INFINITE = 2
@@ -121,6 +124,7 @@ EXPORTS = [
     ("bbg_accel_export", I32, [P, P, P, P, P]),
     ("bbg_intersect", I32, [P, P, I64, P, I32, P]),
     ("bbg_intersect_any", I32, [P, P, I64, P, I32, P]),
+    ("bbg_accel_set_traversal", I32, [P, I32]),
     ("bbg_accel_set_counting", I32, [P, I32]),
     ("bbg_accel_last_counts", I32, [P, P, P]),
     ("bbg_camera_perspective", I32, [P, P]),

@@ -50,7 +50,8 @@ __global__ void __launch_bounds__(kTraceBlock) TraceKernel(AccelView a, const fl
         float4 r0 = __ldg(rays + 2 * i);
         float4 r1 = __ldg(rays + 2 * i + 1);
         RayQ q = MakeRayQ(V3{ r0.x, r0.y, r0.z }, V3{ r0.w, r1.x, r1.y });
-        TraceResult res = Trace<ANY, COUNT>(a, q, r1.z, r1.w, &nodes, &prims);
+        TraceResult res = COUNT ? TraceReference<ANY, true>(a, q, r1.z, r1.w, &nodes, &prims)
+                                : Trace<ANY>(a, q, r1.z, r1.w);
         if (ANY)
         {
             occluded[i] = res.prim >= 0 ? 1 : 0;
@@ -249,9 +250,10 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
             const float* p0 = g->positions + 3 * size_t(v[0]);
             const float* p1 = g->positions + 3 * size_t(v[1]);
             const float* p2 = g->positions + 3 * size_t(v[2]);
+            // Edges e1 = p1 - p0, e2 = p2 - p0 as Triangle::Intersect computes them.
             r[0] = make_float4(p0[0], p0[1], p0[2], BitsToFloat(uint32_t(prim)));
-            r[1] = make_float4(p1[0], p1[1], p1[2], 0.0f);
-            r[2] = make_float4(p2[0], p2[1], p2[2], 0.0f);
+            r[1] = make_float4(p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2], 0.0f);
+            r[2] = make_float4(p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2], 0.0f);
         }
         else
         {
@@ -260,6 +262,45 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
             r[1] = make_float4(sp.q[0], sp.q[1], sp.q[2], sp.q[3]);
             r[2] = make_float4(sp.s[0], sp.s[1], sp.s[2], sp.radius);
         }
+    }
+    // Child-box layout: one 64-byte record per interior node holding both
+    // children's boxes and references (>= 0 interior record, < 0 ~leaf).
+    {
+        std::vector<int32_t> ref(size_t(a->n_nodes));
+        std::vector<int2> leaves;
+        int32_t n_wide = 0;
+        for (int32_t i = 0; i < a->n_nodes; ++i)
+        {
+            const bbg_bvh_node& nd = a->host_nodes[i];
+            if (nd.count > 0)
+            {
+                ref[i] = ~int32_t(leaves.size());
+                leaves.push_back(make_int2(nd.offset, nd.count));
+            }
+            else
+            {
+                ref[i] = n_wide++;
+            }
+        }
+        std::vector<float4> wide(4 * size_t(std::max(n_wide, 1)));
+        for (int32_t i = 0; i < a->n_nodes; ++i)
+        {
+            const bbg_bvh_node& nd = a->host_nodes[i];
+            if (nd.count > 0)
+            {
+                continue;
+            }
+            const bbg_bvh_node& c0 = a->host_nodes[i + 1];
+            const bbg_bvh_node& c1 = a->host_nodes[nd.offset];
+            float4* w = &wide[4 * size_t(ref[i])];
+            w[0] = make_float4(c0.bmin[0], c0.bmin[1], c0.bmin[2], c0.bmax[0]);
+            w[1] = make_float4(c0.bmax[1], c0.bmax[2], c1.bmin[0], c1.bmin[1]);
+            w[2] = make_float4(c1.bmin[2], c1.bmax[0], c1.bmax[1], c1.bmax[2]);
+            w[3] = make_float4(BitsToFloat(uint32_t(ref[i + 1])), BitsToFloat(uint32_t(ref[nd.offset])), 0.0f, 0.0f);
+        }
+        a->root = ref[0];
+        BBG_TRY(a->wide.upload(wide.data(), wide.size(), a->stream));
+        BBG_TRY(a->leaves.upload(leaves.data(), leaves.size(), a->stream));
     }
     static_assert(sizeof(bbg_bvh_node) == 2 * sizeof(float4), "node layout");
     BBG_TRY(a->nodes.upload(reinterpret_cast<const float4*>(a->host_nodes.data()), 2 * size_t(a->n_nodes), a->stream));
@@ -446,6 +487,16 @@ bbg_status bbg_intersect_any(bbg_accel* a, const bbg_ray* rays, int64_t n, uint8
                              void* stream)
 {
     return Query<true>(a, rays, n, occluded, mem, stream);
+}
+
+bbg_status bbg_accel_set_traversal(bbg_accel* a, int32_t mode)
+{
+    if (!a || (mode != BBG_TRAVERSAL_ORDERED && mode != BBG_TRAVERSAL_REFERENCE))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_set_traversal: bad argument");
+    }
+    a->ordered = mode == BBG_TRAVERSAL_ORDERED;
+    return BBG_OK;
 }
 
 bbg_status bbg_accel_set_counting(bbg_accel* a, int32_t enable)

@@ -18,6 +18,10 @@ struct bbg_accel
     // Traversal data.
     bbg::DevBuf<float4> nodes; // 2 float4 per node
     bbg::DevBuf<float4> slots; // 3 float4 per slot
+    bbg::DevBuf<float4> wide;  // 4 float4 per interior node (child-box layout)
+    bbg::DevBuf<int2> leaves;  // (first slot, count) per leaf
+    int32_t root = 0;
+    bool ordered = true;
 
     // Shading data (the reference Mesh arrays and shapes).
     bbg::DevBuf<int2> prim_shape;     // (kind, index) per primitive
@@ -48,7 +52,7 @@ struct bbg_accel
     bbg::DevBuf<unsigned long long> counters;
     int64_t last_nodes = 0, last_prims = 0;
 
-    bbg::AccelView view() const { return bbg::AccelView{ nodes.p, slots.p, n_nodes }; }
+    bbg::AccelView view() const { return bbg::AccelView{ nodes.p, slots.p, wide.p, leaves.p, root, ordered ? 1 : 0 }; }
 };
 
 namespace bbg

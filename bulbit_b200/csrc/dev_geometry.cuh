@@ -20,9 +20,12 @@ namespace bbg
 
 struct AccelView
 {
-    const float4* nodes; // 2 per node
-    const float4* slots; // 3 per slot
-    int32_t n_nodes;
+    const float4* nodes;  // reference layout: 2 per node
+    const float4* slots;  // 3 per slot
+    const float4* wide;   // child-box layout: 4 per interior node
+    const int2* leaves;   // (first slot, count) per leaf
+    int32_t root;         // child-box layout root reference
+    int32_t ordered;      // 1: nearest-first traversal over the child-box layout
 };
 
 struct RayQ
@@ -84,12 +87,12 @@ __device__ __forceinline__ bool TestRay(const float4& a, const float4& b, const 
 }
 
 // Möller-Trumbore on the normalised direction (src/geometry/triangle.cpp:55-94).
-// Returns true and (t, u, v) on a hit in [t_min, t_max].
-__device__ __forceinline__ bool IntersectTriangle(V3 p0, V3 p1, V3 p2, const RayQ& q, float t_min, float t_max,
+// The edges e1 = p1 - p0 and e2 = p2 - p0 are stored precomputed (the same
+// float values the reference computes per test). Returns true and (t, u, v)
+// on a hit in [t_min, t_max].
+__device__ __forceinline__ bool IntersectTriangle(V3 p0, V3 e1, V3 e2, const RayQ& q, float t_min, float t_max,
                                                   float* t_out, float* u_out, float* v_out)
 {
-    V3 e1 = p1 - p0;
-    V3 e2 = p2 - p0;
     V3 pvec = Cross(q.dn, e2);
     float det = Dot(e1, pvec);
     if (fabsf(det) < kEpsilon)
@@ -177,13 +180,44 @@ struct TraceResult
     float t, u, v;
 };
 
-// Stack traversal of BVH::RayCast. ANY = IntersectAny semantics (stop at the
-// first hit); otherwise Intersect semantics (shrink t_max; a hit at exactly
-// the current t_max replaces the previous one). COUNT accumulates nodes popped
-// and primitive tests.
+// One leaf slot: the primitive's test with the current [t_min, t_max].
+__device__ __forceinline__ bool TestSlot(const AccelView& a, int32_t slot, const RayQ& q, float t_min, float t_max,
+                                         TraceResult* res)
+{
+    const float4* s = a.slots + 3 * size_t(slot);
+    float4 s0 = __ldg(s);
+    float4 s1 = __ldg(s + 1);
+    float4 s2 = __ldg(s + 2);
+    uint32_t tag = __float_as_uint(s0.w);
+    float t, u = 0, v = 0;
+    bool hit;
+    if (tag & kSphereBit)
+    {
+        hit = IntersectSphere(V3{ s0.x, s0.y, s0.z }, s1, V3{ s2.x, s2.y, s2.z }, s2.w, q.o, q.d, t_min, t_max, &t);
+    }
+    else
+    {
+        hit = IntersectTriangle(V3{ s0.x, s0.y, s0.z }, V3{ s1.x, s1.y, s1.z }, V3{ s2.x, s2.y, s2.z }, q, t_min,
+                                t_max, &t, &u, &v);
+    }
+    if (hit)
+    {
+        res->prim = int32_t(tag & ~kSphereBit);
+        res->t = t;
+        res->u = u;
+        res->v = v;
+    }
+    return hit;
+}
+
+// Stack traversal of BVH::RayCast over the reference's own node order. ANY =
+// IntersectAny semantics (stop at the first hit); otherwise Intersect
+// semantics (shrink t_max; a hit at exactly the current t_max replaces the
+// previous one). COUNT accumulates nodes popped and primitive tests.
 template <bool ANY, bool COUNT>
-__device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, float t_min, float t_max,
-                                             uint32_t* nodes_visited = nullptr, uint32_t* prims_tested = nullptr)
+__device__ __forceinline__ TraceResult TraceReference(const AccelView& a, const RayQ& q, float t_min, float t_max,
+                                                      uint32_t* nodes_visited = nullptr,
+                                                      uint32_t* prims_tested = nullptr)
 {
     TraceResult res{ -1, t_max, 0, 0 };
     int32_t stack[kStackCapacity];
@@ -207,38 +241,17 @@ __device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, 
         {
             for (int32_t i = 0; i < count; ++i)
             {
-                const float4* s = a.slots + 3 * size_t(offset + i);
-                float4 s0 = __ldg(s);
-                float4 s1 = __ldg(s + 1);
-                float4 s2 = __ldg(s + 2);
-                uint32_t tag = __float_as_uint(s0.w);
                 if (COUNT) ++*prims_tested;
-                bool hit;
-                float t, u = 0, v = 0;
-                if (tag & kSphereBit)
-                {
-                    hit = IntersectSphere(V3{ s0.x, s0.y, s0.z }, s1, V3{ s2.x, s2.y, s2.z }, s2.w, q.o, q.d, t_min,
-                                          t_max, &t);
-                }
-                else
-                {
-                    hit = IntersectTriangle(V3{ s0.x, s0.y, s0.z }, V3{ s1.x, s1.y, s1.z }, V3{ s2.x, s2.y, s2.z },
-                                            q, t_min, t_max, &t, &u, &v);
-                }
                 // The callback's return value: t_min after an any-hit, the
                 // hit's t after a closest hit, the running t_max on a miss;
                 // RayCast stops when it is <= t_min, else takes it as t_max.
-                if (hit)
+                if (TestSlot(a, offset + i, q, t_min, t_max, &res))
                 {
-                    res.prim = int32_t(tag & ~kSphereBit);
-                    res.t = t;
-                    res.u = u;
-                    res.v = v;
                     if (ANY)
                     {
                         return res;
                     }
-                    t_max = t;
+                    t_max = res.t;
                 }
                 if (t_max <= t_min)
                 {
@@ -264,6 +277,114 @@ __device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, 
         }
     }
     return res;
+}
+
+// Slab test of one child box: [entry, exit] of the ray within the box and
+// within [t_min, t_max], with the reference's per-axis arithmetic
+// (bound - o) * (1/d) (include/bulbit/bounding_box.h:448-480).
+__device__ __forceinline__ bool SlabTest(float lx, float ly, float lz, float hx, float hy, float hz, const RayQ& q,
+                                         float t_min, float t_max, float* entry)
+{
+    float x0 = ((q.neg[0] ? hx : lx) - q.o.x) * q.inv_dir.x;
+    float x1 = ((q.neg[0] ? lx : hx) - q.o.x) * q.inv_dir.x;
+    float y0 = ((q.neg[1] ? hy : ly) - q.o.y) * q.inv_dir.y;
+    float y1 = ((q.neg[1] ? ly : hy) - q.o.y) * q.inv_dir.y;
+    float z0 = ((q.neg[2] ? hz : lz) - q.o.z) * q.inv_dir.z;
+    float z1 = ((q.neg[2] ? lz : hz) - q.o.z) * q.inv_dir.z;
+    float t0 = fmaxf(fmaxf(x0, y0), fmaxf(z0, t_min));
+    float t1 = fminf(fminf(x1, y1), fminf(z1, t_max));
+    *entry = t0;
+    return t0 <= t1;
+}
+
+// Nearest-child-first traversal over the child-box layout: each interior
+// node holds both children's boxes, so one 64-byte fetch tests two boxes; the
+// nearer hit child is visited first, the farther is pushed with its entry
+// distance and skipped on pop once a closer hit is known. The same primitive
+// tests run in a different order than RayCast, so the closest hit is the
+// same primitive and t except where two hits have exactly equal t.
+template <bool ANY>
+__device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const RayQ& q, float t_min, float t_max)
+{
+    TraceResult res{ -1, t_max, 0, 0 };
+    int2 stack[kStackCapacity];
+    int sp = 0;
+    int32_t ref = a.root;
+
+    while (true)
+    {
+        if (ref >= 0)
+        {
+            const float4* n = a.wide + 4 * size_t(ref);
+            float4 f0 = __ldg(n);
+            float4 f1 = __ldg(n + 1);
+            float4 f2 = __ldg(n + 2);
+            int4 f3 = __ldg(reinterpret_cast<const int4*>(n + 3));
+            float e0, e1;
+            bool h0 = SlabTest(f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, q, t_min, t_max, &e0);
+            bool h1 = SlabTest(f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, q, t_min, t_max, &e1);
+            if (h0 && h1)
+            {
+                bool swap = e1 < e0;
+                int32_t near = swap ? f3.y : f3.x;
+                int32_t far = swap ? f3.x : f3.y;
+                float far_entry = swap ? e0 : e1;
+                stack[sp++] = make_int2(far, __float_as_int(far_entry));
+                ref = near;
+                continue;
+            }
+            if (h0 || h1)
+            {
+                ref = h0 ? f3.x : f3.y;
+                continue;
+            }
+        }
+        else
+        {
+            int2 leaf = __ldg(a.leaves + (~ref));
+            for (int32_t i = 0; i < leaf.y; ++i)
+            {
+                if (TestSlot(a, leaf.x + i, q, t_min, t_max, &res))
+                {
+                    if (ANY)
+                    {
+                        return res;
+                    }
+                    t_max = res.t;
+                }
+                if (t_max <= t_min)
+                {
+                    return res;
+                }
+            }
+        }
+        // Pop the next entry that can still hold a closer hit.
+        ref = 0x7fffffff;
+        while (sp > 0)
+        {
+            int2 e = stack[--sp];
+            if (__int_as_float(e.y) <= t_max)
+            {
+                ref = e.x;
+                break;
+            }
+        }
+        if (ref == 0x7fffffff)
+        {
+            break;
+        }
+    }
+    return res;
+}
+
+template <bool ANY>
+__device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, float t_min, float t_max)
+{
+    if (a.ordered)
+    {
+        return TraceOrdered<ANY>(a, q, t_min, t_max);
+    }
+    return TraceReference<ANY, false>(a, q, t_min, t_max);
 }
 
 } // namespace bbg

@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(kBlock) ClosestKernel(SceneDev s, WaveDev w, i
         float4 o = w.o_pdf[slot];
         float4 d = w.d_eta[slot];
         RayQ rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
-        TraceResult r = Trace<false, false>(s.accel, rq, kRayEpsilon, INFINITY);
+        TraceResult r = Trace<false>(s.accel, rq, kRayEpsilon, INFINITY);
         w.hit[slot] = make_float4(__int_as_float(r.prim), r.t, r.u, r.v);
     }
 }
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(kBlock) ShadowKernel(SceneDev s, WaveDev w)
         float4 o = w.sh_o[j];
         float4 d = w.sh_d[j];
         RayQ rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
-        TraceResult r = Trace<true, false>(s.accel, rq, kRayEpsilon, o.w);
+        TraceResult r = Trace<true>(s.accel, rq, kRayEpsilon, o.w);
         if (r.prim < 0)
         {
             int32_t slot = __float_as_int(d.w);

@@ -124,6 +124,10 @@ class GpuAccel:
         check(get_lib().bbg_accel_export(self.h, _p(nodes), _p(slots), None, None), "bbg_accel_export")
         return nodes, slots
 
+    def set_traversal(self, mode):
+        """abi.BBG_TRAVERSAL_ORDERED (default) or abi.BBG_TRAVERSAL_REFERENCE."""
+        check(get_lib().bbg_accel_set_traversal(self.h, mode), "bbg_accel_set_traversal")
+
     def set_counting(self, on):
         check(get_lib().bbg_accel_set_counting(self.h, 1 if on else 0), "bbg_accel_set_counting")
 

@@ -184,9 +184,24 @@ bbg_status bbg_intersect(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_h
 bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
                              bbg_memory mem, void* stream);
 
+/* Traversal order. ORDERED (the default) visits the nearer child first over
+ * a child-box node layout and skips subtrees beyond the closest hit so far;
+ * REFERENCE visits nodes in BVH::RayCast's own order (include/bulbit/bvh.h:
+ * 102-155). Both run the same primitive tests and return the same closest
+ * primitive and t; they can differ only on rays whose two nearest hits have
+ * exactly equal t (the reference keeps the last one it visits). Any-hit
+ * results are identical. */
+enum
+{
+    BBG_TRAVERSAL_ORDERED = 0,
+    BBG_TRAVERSAL_REFERENCE = 1
+};
+bbg_status bbg_accel_set_traversal(bbg_accel* accel, int32_t mode);
+
 /* Traversal statistics of the last bbg_intersect / bbg_intersect_any call on
  * this handle when counting is enabled: nodes popped and slab-tested, and
- * primitive tests, summed over all rays. */
+ * primitive tests, summed over all rays, for a traversal in the reference's
+ * node order (a counting call always uses that order). */
 bbg_status bbg_accel_set_counting(bbg_accel* accel, int32_t enable);
 bbg_status bbg_accel_last_counts(const bbg_accel* accel, int64_t* nodes_visited, int64_t* prims_tested);
 

@@ -8,7 +8,7 @@ where the ids agree, any-hit results identical."""
 import numpy as np
 import pytest
 
-from bulbit_b200 import lib, scenes
+from bulbit_b200 import abi, lib, scenes
 
 pytestmark = pytest.mark.gpu
 
@@ -34,18 +34,23 @@ def run_parity(oracle, scene, closest, anyq, use_ref_tree):
     rs = oracle.RefScene(scene)
     tree = rs.bvh() if use_ref_tree else None
     acc = lib.GpuAccel(scene, bvh=tree)
-    prim, t, _, _ = acc.intersect(closest)
     ref_prim, ref_t, _ = rs.intersect(closest)
-    frac, unexplained, t_bad = compare_closest(rs, closest, prim, t, ref_prim, ref_t)
-    print(f"{scene.name}: closest mismatch fraction {frac:.2e} ({int(frac * len(prim))} rays), "
-          f"hit rate {(ref_prim >= 0).mean():.3f}")
-    assert not unexplained, unexplained[:5]
-    assert t_bad.size == 0
-    occ = acc.intersect_any(anyq)
     ref_occ, _ = rs.intersect_any(anyq)
-    assert np.array_equal(occ, ref_occ)
+    fracs = {}
+    for mode in (abi.BBG_TRAVERSAL_REFERENCE, abi.BBG_TRAVERSAL_ORDERED):
+        acc.set_traversal(mode)
+        prim, t, _, _ = acc.intersect(closest)
+        frac, unexplained, t_bad = compare_closest(rs, closest, prim, t, ref_prim, ref_t)
+        name = "reference-order" if mode == abi.BBG_TRAVERSAL_REFERENCE else "ordered"
+        print(f"{scene.name} [{name}]: closest mismatch fraction {frac:.2e} ({int(round(frac * len(prim)))} rays), "
+              f"hit rate {(ref_prim >= 0).mean():.3f}")
+        assert not unexplained, unexplained[:5]
+        assert t_bad.size == 0
+        occ = acc.intersect_any(anyq)
+        assert np.array_equal(occ, ref_occ)
+        fracs[name] = frac
     acc.close()
-    return frac
+    return fracs
 
 
 @pytest.mark.parametrize("use_ref_tree", [True, False], ids=["reference_tree", "own_tree"])
