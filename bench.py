@@ -199,6 +199,82 @@ def run_e2e(args, acc, closest, anyq, barrier):
     return steps, secs
 
 
+PT_WORKLOAD = ("path tracing: closed Cornell box + displaced gold icosphere (8 subdivisions, 1,310,732 "
+               "triangles), 1024x1024, 64 spp, 16 bounces, IndependentSampler, power light sampler")
+
+
+def run_pt(args, barrier, world):
+    """The path-tracing workload: one step = one full frame (bbg_render)."""
+    import torch
+    from bulbit_b200 import abi, lib, scenes
+    res = args.pt_res
+    scene = scenes.cornell_icosphere(levels=8, width=res, height=res, spp=64, max_bounces=16)
+    t0 = time.perf_counter()
+    acc = lib.GpuAccel(scene)
+    build_s = time.perf_counter() - t0
+    integ = lib.GpuPathIntegrator(acc, scene)
+    cam = lib.camera(scene.camera)
+    params = abi.RenderParams()
+    params.spp, params.seed, params.wave_paths, params.use_graph = 64, 0, args.pt_wave, 1
+    n_pix = res * res
+    rgb = torch.empty((n_pix, 3), dtype=torch.float32, device="cuda")
+    cnt = torch.empty(n_pix, dtype=torch.int32, device="cuda")
+    mom = torch.empty((n_pix, 2), dtype=torch.float32, device="cuda")
+    fs = abi.Film()
+    fs.rgb_sum, fs.count, fs.moments, fs.path_L = rgb.data_ptr(), cnt.data_ptr(), mom.data_ptr(), None
+    stats = abi.RenderStats()
+    for _ in range(max(1, args.warmup)):
+        integ.render_device(cam, params, fs, stats)
+    steps = max(1, args.pt_steps)
+    barrier()
+    dev_ms, rays = 0.0, 0
+    for _ in range(steps):
+        integ.render_device(cam, params, fs, stats)
+        dev_ms += stats.device_ms
+        rays += stats.closest_rays + stats.shadow_rays
+    barrier()
+    # End to end through the C ABI with a host film (copied back in the call).
+    t0 = time.perf_counter()
+    film = integ.render(spp=64)
+    e2e_s = time.perf_counter() - t0
+    paths = stats.paths
+    out = {
+        "value": world * paths * steps / (dev_ms / 1e3), "unit": "paths/s",
+        "mrays_per_s": world * rays / (dev_ms / 1e3) / 1e6, "ms_per_frame": dev_ms / steps,
+        "steps": steps, "closest_rays_per_frame": stats.closest_rays, "shadow_rays_per_frame": stats.shadow_rays,
+        "config": {"workload": PT_WORKLOAD if res == 1024 else f"{PT_WORKLOAD} (reduced to {res}x{res})",
+                   "bvh_build_s": round(build_s, 3), "wave_paths": args.pt_wave or 1 << 22,
+                   "cuda_graph": True},
+        "image_mean": float(np.nanmean(film.image())),
+        "e2e": {"value": world * paths / e2e_s, "unit": "paths/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": n_pix * (12 + 4 + 8)},
+        "gpu_launches_per_frame": None,
+    }
+    integ.close()
+    acc.close()
+    return out, scene
+
+
+def pt_cpu_baseline(scene, res=128):
+    """The reference PathIntegrator (oracle/_ref) rendering the same scene at a
+    reduced resolution on all host threads: Render() + Rendering::Wait()."""
+    from oracle import ref
+    if not ref.available():
+        return None
+    cores = ref.init(0)
+    s = scene
+    s.camera.width = res
+    s.camera.height = res
+    rs = ref.RefScene(s)
+    rs.make_integrator(spp=64)
+    _, _, secs = rs.render()
+    paths = res * res * 64
+    return {"value": paths / secs, "unit": "paths/s", "cores": cores, "kind": "reference",
+            "sample": f"the same scene rendered at {res}x{res}, 64 spp, 16 bounces ({paths} paths) by the "
+                      f"reference Render() + Wait() on {cores} threads; BVH build {rs.build_seconds:.2f} s and "
+                      f"integrator set-up {rs.integrator_seconds:.2f} s excluded"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -208,6 +284,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per query set (smaller cases for profiling)")
+    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt"])
+    ap.add_argument("--pt-res", type=int, default=1024)
+    ap.add_argument("--pt-steps", type=int, default=3)
+    ap.add_argument("--pt-wave", type=int, default=1 << 24)
     args = ap.parse_args()
     rank, world, local = dist_env()
 
@@ -227,6 +307,12 @@ def main():
     def barrier():
         if world > 1:
             dist.barrier()
+
+    if args.workload == "pt":
+        pt, pt_scene = run_pt(args, barrier, world)
+        if rank == 0:
+            print(json.dumps({"path_tracing": pt}))
+        return
 
     n_rays = args.rays
     scene = scenes.triangle_soup(N_TRIS, seed=1)
@@ -323,11 +409,17 @@ def main():
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }
+    acc.close()
+    del dev_c, dev_a, hits, occ
+    if args.workload == "all":
+        pt, pt_scene = run_pt(args, barrier, world)
+        line["path_tracing"] = pt
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene, closest, anyq)
+        if args.workload == "all":
+            line["path_tracing"]["cpu_baseline"] = pt_cpu_baseline(pt_scene)
     if rank == 0:
         print(json.dumps(line))
-    acc.close()
     if world > 1:
         dist.destroy_process_group()
 
