@@ -37,8 +37,9 @@ int PersistentGrid(const void* kernel, int block, size_t smem)
     return sms * std::max(per_sm, 1);
 }
 
-// One thread per ray, grid-stride over the batch. Rays are two float4
-// (o.xyz d.x)(d.yz t_min t_max); hits one float4 (prim bits, t, u, v).
+// Reference-order traversal (and the counting run): one thread per ray,
+// grid-stride over the batch. Rays are two float4 (o.xyz d.x)(d.yz t_min
+// t_max); hits one float4 (prim bits, t, u, v).
 template <bool ANY, bool COUNT>
 __global__ void __launch_bounds__(kTraceBlock) TraceKernel(AccelView a, const float4* __restrict__ rays, int64_t n,
                                                            float4* __restrict__ hits, uint8_t* __restrict__ occluded,
@@ -50,8 +51,7 @@ __global__ void __launch_bounds__(kTraceBlock) TraceKernel(AccelView a, const fl
         float4 r0 = __ldg(rays + 2 * i);
         float4 r1 = __ldg(rays + 2 * i + 1);
         RayQ q = MakeRayQ(V3{ r0.x, r0.y, r0.z }, V3{ r0.w, r1.x, r1.y });
-        TraceResult res = COUNT ? TraceReference<ANY, true>(a, q, r1.z, r1.w, &nodes, &prims)
-                                : Trace<ANY>(a, q, r1.z, r1.w);
+        TraceResult res = TraceReference<ANY, COUNT>(a, q, r1.z, r1.w, &nodes, &prims);
         if (ANY)
         {
             occluded[i] = res.prim >= 0 ? 1 : 0;
@@ -78,6 +78,44 @@ __global__ void __launch_bounds__(kTraceBlock) TraceKernel(AccelView a, const fl
 }
 
 template <bool ANY>
+struct BatchSrc
+{
+    const float4* rays;
+    float4* hits;
+    uint8_t* occluded;
+
+    __device__ __forceinline__ void Load(int32_t i, RayQ* q, float* t_min, float* t_max) const
+    {
+        float4 r0 = __ldg(rays + 2 * size_t(i));
+        float4 r1 = __ldg(rays + 2 * size_t(i) + 1);
+        *q = MakeRayQ(V3{ r0.x, r0.y, r0.z }, V3{ r0.w, r1.x, r1.y });
+        *t_min = r1.z;
+        *t_max = r1.w;
+    }
+    __device__ __forceinline__ void Store(int32_t i, const TraceResult& r) const
+    {
+        if (ANY)
+        {
+            occluded[i] = r.prim >= 0 ? 1 : 0;
+        }
+        else
+        {
+            hits[i] = make_float4(__int_as_float(r.prim), r.t, r.u, r.v);
+        }
+    }
+};
+
+// Ordered traversal: persistent warps pulling rays from a work counter.
+template <bool ANY>
+__global__ void __launch_bounds__(kTraceBlock) PersistentTraceKernel(AccelView a, const float4* __restrict__ rays,
+                                                                     int32_t n, float4* __restrict__ hits,
+                                                                     uint8_t* __restrict__ occluded, int32_t* next)
+{
+    BatchSrc<ANY> src{ rays, hits, occluded };
+    TracePersistent<ANY>(a, n, next, src);
+}
+
+template <bool ANY>
 static bbg_status LaunchTrace(bbg_accel* a, const float4* rays, int64_t n, float4* hits, uint8_t* occ,
                               cudaStream_t stream)
 {
@@ -96,19 +134,26 @@ static bbg_status LaunchTrace(bbg_accel* a, const float4* rays, int64_t n, float
         }
         return Fail(BBG_ERR_UNSUPPORTED, "closest-hit query on an accel with no primitives");
     }
-    if (a->counting)
+    if (a->counting || !a->ordered)
     {
-        auto k = TraceKernel<ANY, true>;
+        auto k = a->counting ? TraceKernel<ANY, true> : TraceKernel<ANY, false>;
         int grid = PersistentGrid(reinterpret_cast<const void*>(k), kTraceBlock);
         grid = int(std::min<int64_t>(grid, (n + kTraceBlock - 1) / kTraceBlock));
         k<<<grid, kTraceBlock, 0, stream>>>(a->view(), rays, n, hits, occ, a->counters.p);
     }
     else
     {
-        auto k = TraceKernel<ANY, false>;
+        auto k = PersistentTraceKernel<ANY>;
         int grid = PersistentGrid(reinterpret_cast<const void*>(k), kTraceBlock);
         grid = int(std::min<int64_t>(grid, (n + kTraceBlock - 1) / kTraceBlock));
-        k<<<grid, kTraceBlock, 0, stream>>>(a->view(), rays, n, hits, occ, nullptr);
+        const int64_t chunk = int64_t(1) << 30;
+        for (int64_t c = 0; c < n; c += chunk)
+        {
+            int32_t m = int32_t(std::min(chunk, n - c));
+            BBG_CUDA(cudaMemsetAsync(a->work.p, 0, sizeof(int32_t), stream));
+            k<<<grid, kTraceBlock, 0, stream>>>(a->view(), rays + 2 * c, m, hits ? hits + c : nullptr,
+                                                occ ? occ + c : nullptr, a->work.p);
+        }
     }
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
@@ -325,6 +370,7 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
         }
     }
     BBG_TRY(a->counters.alloc(2));
+    BBG_TRY(a->work.alloc(1));
     BBG_CUDA(cudaStreamSynchronize(a->stream));
     return BBG_OK;
 }

@@ -50,6 +50,7 @@ struct bbg_accel
     // Traversal counters (nodes, prims) of the last call when enabled.
     bool counting = false;
     bbg::DevBuf<unsigned long long> counters;
+    bbg::DevBuf<int32_t> work; // persistent-kernel work counter
     int64_t last_nodes = 0, last_prims = 0;
 
     bbg::AccelView view() const { return bbg::AccelView{ nodes.p, slots.p, wide.p, leaves.p, root, ordered ? 1 : 0 }; }

@@ -377,6 +377,168 @@ __device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const Ra
     return res;
 }
 
+// Persistent warp-cooperative traversal over the child-box layout (the
+// while-while scheme of Aila & Laine, "Understanding the efficiency of ray
+// traversal on GPUs", HPG 2009, with dynamic ray fetch):
+//   * a warp takes batches of work items from a global counter whenever fewer
+//     than kRefill of its lanes still hold a ray, so lanes that finish early
+//     get new rays instead of idling until the slowest ray of the batch ends;
+//   * each round first walks interior nodes until every busy lane has found a
+//     leaf (a lane that reaches a leaf postpones it and keeps walking), then
+//     tests leaves together, so node and leaf work do not serialise the warp.
+// Per ray the node and primitive tests are exactly those of TraceOrdered.
+// Src supplies Load(item, RayQ*, t_min*, t_max*) and Store(item, result).
+constexpr int32_t kNoNode = int32_t(0x80000000);
+constexpr int kRefill = 16;
+
+template <bool ANY, class Src>
+__device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, int32_t* next, Src& src)
+{
+    const unsigned kFull = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    int32_t item = -1;
+    bool exhausted = false;
+    RayQ q;
+    float t_min = 0, t_max = 0;
+    TraceResult res{ -1, 0, 0, 0 };
+    int2 stack[kStackCapacity];
+    int sp = 0;
+    int32_t node = kNoNode, leaf = kNoNode;
+
+    auto pop = [&]() -> int32_t {
+        while (sp > 0)
+        {
+            int2 e = stack[--sp];
+            if (__int_as_float(e.y) <= t_max)
+            {
+                return e.x;
+            }
+        }
+        return kNoNode;
+    };
+
+    while (true)
+    {
+        __syncwarp();
+        bool busy = item >= 0;
+        unsigned have = __ballot_sync(kFull, busy);
+        if (!exhausted && __popc(have) < kRefill)
+        {
+            unsigned need = ~have;
+            int32_t cnt = __popc(need);
+            int32_t base = 0;
+            if (lane == 0)
+            {
+                base = atomicAdd(next, cnt);
+            }
+            base = __shfl_sync(kFull, base, 0);
+            exhausted = base + cnt >= n;
+            if (!busy)
+            {
+                int32_t r = base + __popc(need & ((1u << lane) - 1u));
+                if (r < n)
+                {
+                    item = r;
+                    src.Load(r, &q, &t_min, &t_max);
+                    res = TraceResult{ -1, t_max, 0, 0 };
+                    sp = 0;
+                    node = a.root;
+                    leaf = kNoNode;
+                    busy = true;
+                }
+            }
+            have = __ballot_sync(kFull, busy);
+        }
+        if (have == 0)
+        {
+            break;
+        }
+        if (busy)
+        {
+            if (node < 0 && node != kNoNode && leaf == kNoNode)
+            {
+                leaf = node;
+                node = pop();
+            }
+            // Node phase.
+            while (node >= 0)
+            {
+                const float4* nd = a.wide + 4 * size_t(node);
+                float4 f0 = __ldg(nd);
+                float4 f1 = __ldg(nd + 1);
+                float4 f2 = __ldg(nd + 2);
+                int4 f3 = __ldg(reinterpret_cast<const int4*>(nd + 3));
+                float e0, e1;
+                bool h0 = SlabTest(f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, q, t_min, t_max, &e0);
+                bool h1 = SlabTest(f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, q, t_min, t_max, &e1);
+                if (h0 && h1)
+                {
+                    bool swap = e1 < e0;
+                    stack[sp++] = make_int2(swap ? f3.x : f3.y, __float_as_int(swap ? e0 : e1));
+                    node = swap ? f3.y : f3.x;
+                }
+                else if (h0 || h1)
+                {
+                    node = h0 ? f3.x : f3.y;
+                }
+                else
+                {
+                    node = pop();
+                }
+                if (node < 0 && node != kNoNode && leaf == kNoNode)
+                {
+                    leaf = node;
+                    node = pop();
+                }
+                if (__all_sync(__activemask(), leaf != kNoNode))
+                {
+                    break;
+                }
+            }
+            // Leaf phase.
+            while (leaf != kNoNode)
+            {
+                int2 lf = __ldg(a.leaves + (~leaf));
+                bool stop = false;
+                for (int32_t i = 0; i < lf.y; ++i)
+                {
+                    if (TestSlot(a, lf.x + i, q, t_min, t_max, &res))
+                    {
+                        if (ANY)
+                        {
+                            stop = true;
+                            break;
+                        }
+                        t_max = res.t;
+                    }
+                    if (t_max <= t_min)
+                    {
+                        stop = true;
+                        break;
+                    }
+                }
+                leaf = kNoNode;
+                if (stop)
+                {
+                    node = kNoNode;
+                    sp = 0;
+                    break;
+                }
+                if (node < 0 && node != kNoNode)
+                {
+                    leaf = node;
+                    node = pop();
+                }
+            }
+            if (node == kNoNode && leaf == kNoNode)
+            {
+                src.Store(item, res);
+                item = -1;
+            }
+        }
+    }
+}
+
 template <bool ANY>
 __device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, float t_min, float t_max)
 {

@@ -73,7 +73,7 @@ struct WaveDev
     float4* sh_o;    // shadow ray origin, t_max
     float4* sh_d;    // shadow ray direction, slot bits
     float4* sh_c;    // contribution
-    int32_t* counts; // [0],[1] ray queues, [2] shadow queue
+    int32_t* counts; // [0],[1] ray queues, [2] shadow queue, [3],[4] work counters
     unsigned long long* stats; // closest rays, shadow rays
     const int64_t* wave;       // [0] first path, [1] paths in wave
 };
@@ -146,22 +146,77 @@ __global__ void __launch_bounds__(kBlock) RaygenKernel(SceneDev s, WaveDev w)
 
 // ---------------------------------------------------------------- intersect
 
+// Work items of the closest-hit pass: queue entry j -> its path's ray.
+struct ClosestSrc
+{
+    const int32_t* q;
+    const float4* o_pdf;
+    const float4* d_eta;
+    float4* hit;
+
+    __device__ __forceinline__ void Load(int32_t j, RayQ* rq, float* t_min, float* t_max) const
+    {
+        int32_t slot = q[j];
+        float4 o = o_pdf[slot];
+        float4 d = d_eta[slot];
+        *rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
+        *t_min = kRayEpsilon;
+        *t_max = INFINITY;
+    }
+    __device__ __forceinline__ void Store(int32_t j, const TraceResult& r) const
+    {
+        hit[q[j]] = make_float4(__int_as_float(r.prim), r.t, r.u, r.v);
+    }
+};
+
+// Work items of the shadow pass: an unoccluded shadow ray adds its
+// contribution to its path's radiance.
+struct ShadowSrc
+{
+    const float4* sh_o;
+    const float4* sh_d;
+    const float4* sh_c;
+    float4* L;
+
+    __device__ __forceinline__ void Load(int32_t j, RayQ* rq, float* t_min, float* t_max) const
+    {
+        float4 o = sh_o[j];
+        float4 d = sh_d[j];
+        *rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
+        *t_min = kRayEpsilon;
+        *t_max = o.w;
+    }
+    __device__ __forceinline__ void Store(int32_t j, const TraceResult& r) const
+    {
+        if (r.prim < 0)
+        {
+            int32_t slot = __float_as_int(sh_d[j].w);
+            float4 c = sh_c[j];
+            float4 l = L[slot];
+            L[slot] = make_float4(l.x + c.x, l.y + c.y, l.z + c.z, 0.0f);
+        }
+    }
+};
+
 __global__ void __launch_bounds__(kBlock) ClosestKernel(SceneDev s, WaveDev w, int parity)
 {
-    const int32_t* q = w.queue[parity];
     const int32_t n = w.counts[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
         atomicAdd(w.stats, (unsigned long long)n);
     }
+    ClosestSrc src{ w.queue[parity], w.o_pdf, w.d_eta, w.hit };
+    if (s.accel.ordered)
+    {
+        TracePersistent<false>(s.accel, n, w.counts + 3, src);
+        return;
+    }
     for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
     {
-        int32_t slot = q[j];
-        float4 o = w.o_pdf[slot];
-        float4 d = w.d_eta[slot];
-        RayQ rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
-        TraceResult r = Trace<false>(s.accel, rq, kRayEpsilon, INFINITY);
-        w.hit[slot] = make_float4(__int_as_float(r.prim), r.t, r.u, r.v);
+        RayQ rq;
+        float t_min, t_max;
+        src.Load(j, &rq, &t_min, &t_max);
+        src.Store(j, TraceReference<false, false>(s.accel, rq, t_min, t_max));
     }
 }
 
@@ -172,19 +227,18 @@ __global__ void __launch_bounds__(kBlock) ShadowKernel(SceneDev s, WaveDev w)
     {
         atomicAdd(w.stats + 1, (unsigned long long)n);
     }
+    ShadowSrc src{ w.sh_o, w.sh_d, w.sh_c, w.L };
+    if (s.accel.ordered)
+    {
+        TracePersistent<true>(s.accel, n, w.counts + 4, src);
+        return;
+    }
     for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
     {
-        float4 o = w.sh_o[j];
-        float4 d = w.sh_d[j];
-        RayQ rq = MakeRayQ(V3{ o.x, o.y, o.z }, V3{ d.x, d.y, d.z });
-        TraceResult r = Trace<true>(s.accel, rq, kRayEpsilon, o.w);
-        if (r.prim < 0)
-        {
-            int32_t slot = __float_as_int(d.w);
-            float4 c = w.sh_c[j];
-            float4 L = w.L[slot];
-            w.L[slot] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, 0.0f);
-        }
+        RayQ rq;
+        float t_min, t_max;
+        src.Load(j, &rq, &t_min, &t_max);
+        src.Store(j, TraceReference<true, false>(s.accel, rq, t_min, t_max));
     }
 }
 
@@ -547,10 +601,14 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int
     }
 }
 
+// Clears the next level's ray queue, the shadow queue and the work counters
+// of the persistent closest-hit and shadow passes.
 __global__ void ResetKernel(WaveDev w, int parity)
 {
     w.counts[parity ^ 1] = 0;
     w.counts[2] = 0;
+    w.counts[3] = 0;
+    w.counts[4] = 0;
 }
 
 // ---------------------------------------------------------------- film
@@ -1033,7 +1091,7 @@ bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim
     BBG_TRY(I->alias_prob.upload(prob.data(), prob.size(), I->stream));
     BBG_TRY(I->alias_idx.upload(alias.data(), alias.size(), I->stream));
     BBG_TRY(I->infinite.upload(infinite.data(), infinite.size(), I->stream));
-    BBG_TRY(I->counts.alloc(4));
+    BBG_TRY(I->counts.alloc(8));
     BBG_TRY(I->stats.alloc(2));
     BBG_TRY(I->wave.alloc(2));
     BBG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&I->wave_host), 2 * sizeof(int64_t)));
