@@ -179,6 +179,20 @@ bbg_status bbg_accel_export(const bbg_accel* accel, bbg_bvh_node* nodes_out, int
 bbg_status bbg_intersect(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem,
                          void* stream);
 
+/* Closest-hit queries for callers that cannot allocate device memory when
+ * they trace (allocation forbidden after start-up, a real-time loop, or device
+ * memory already held by another allocator). No counterpart in the reference:
+ * it exists only for such callers. rays and hits are host buffers; at most
+ * 262,144 rays per call (larger n returns BBG_ERR_INVALID_ARG). The rays and
+ * hits are staged through one fixed device array of about 12 MiB that every
+ * device loading this library holds until the process exits; the call itself
+ * allocates nothing. The first call on a device looks that array's address up
+ * (once per device), so make it before any stream capture. All calls share the
+ * array: calls that overlap on the GPU (from several threads or handles at
+ * once) race and must be serialised by the caller. Results equal
+ * bbg_intersect's for the same accel and traversal mode. */
+bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_hit* hits);
+
 /* Batched BVH::IntersectAny: occluded[i] = 1 if ray i hits anything in
  * [t_min, t_max]. */
 bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
