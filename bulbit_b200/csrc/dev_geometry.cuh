@@ -390,28 +390,62 @@ __device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const Ra
 // Src supplies Load(item, RayQ*, t_min*, t_max*) and Store(item, result).
 constexpr int32_t kNoNode = int32_t(0x80000000);
 constexpr int kRefill = 16;
+// Kernels calling TracePersistent run blocks of this many threads.
+constexpr int kTraversalBlock = 128;
+// Stack entries kept in shared memory per thread; deeper ones go to local
+// memory. The shared part is laid out [depth][thread], so a warp's lanes hit
+// distinct banks whatever depth each lane is at.
+constexpr int kShortStack = 16;
 
 template <bool ANY, class Src>
 __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, int32_t* next, Src& src)
 {
     const unsigned kFull = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x;
     int32_t item = -1;
     bool exhausted = false;
     RayQ q;
     float t_min = 0, t_max = 0;
     TraceResult res{ -1, 0, 0, 0 };
-    int2 stack[kStackCapacity];
+    __shared__ int32_t s_ref[kShortStack * kTraversalBlock];
+    __shared__ float s_entry[kShortStack * kTraversalBlock];
+    int2 spill[kStackCapacity - kShortStack];
     int sp = 0;
     int32_t node = kNoNode, leaf = kNoNode;
 
+    auto push = [&](int32_t ref, float entry) {
+        if (sp < kShortStack)
+        {
+            s_ref[sp * kTraversalBlock + tid] = ref;
+            s_entry[sp * kTraversalBlock + tid] = entry;
+        }
+        else
+        {
+            spill[sp - kShortStack] = make_int2(ref, __float_as_int(entry));
+        }
+        ++sp;
+    };
     auto pop = [&]() -> int32_t {
         while (sp > 0)
         {
-            int2 e = stack[--sp];
-            if (__int_as_float(e.y) <= t_max)
+            --sp;
+            int32_t ref;
+            float entry;
+            if (sp < kShortStack)
             {
-                return e.x;
+                ref = s_ref[sp * kTraversalBlock + tid];
+                entry = s_entry[sp * kTraversalBlock + tid];
+            }
+            else
+            {
+                int2 e = spill[sp - kShortStack];
+                ref = e.x;
+                entry = __int_as_float(e.y);
+            }
+            if (entry <= t_max)
+            {
+                return ref;
             }
         }
         return kNoNode;
@@ -474,7 +508,7 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
                 if (h0 && h1)
                 {
                     bool swap = e1 < e0;
-                    stack[sp++] = make_int2(swap ? f3.x : f3.y, __float_as_int(swap ? e0 : e1));
+                    push(swap ? f3.x : f3.y, swap ? e0 : e1);
                     node = swap ? f3.y : f3.x;
                 }
                 else if (h0 || h1)
