@@ -15,6 +15,10 @@
 #include "bbg_internal.h"
 #include "dev_math.cuh"
 
+#ifndef BBG_SLAB_FMA
+#define BBG_SLAB_FMA 1
+#endif
+
 namespace bbg
 {
 
@@ -34,6 +38,7 @@ struct RayQ
     V3 inv_dir;       // 1 / d per component
     V3 dn;            // d after Vector3::Normalize (triangle test)
     float l;          // length returned by that Normalize
+    V3 oinv;          // o * (1/d), for the fused slab test of the ordered traversal
     int neg[3];       // inv_dir < 0
 };
 
@@ -48,6 +53,7 @@ __device__ __forceinline__ RayQ MakeRayQ(V3 o, V3 d)
     q.neg[2] = q.inv_dir.z < 0;
     q.dn = d;
     q.l = NormalizeInPlace(q.dn);
+    q.oinv = V3{ o.x * q.inv_dir.x, o.y * q.inv_dir.y, o.z * q.inv_dir.z };
     return q;
 }
 
@@ -285,12 +291,25 @@ __device__ __forceinline__ TraceResult TraceReference(const AccelView& a, const 
 __device__ __forceinline__ bool SlabTest(float lx, float ly, float lz, float hx, float hy, float hz, const RayQ& q,
                                          float t_min, float t_max, float* entry)
 {
+#if BBG_SLAB_FMA
+    // bound * (1/d) - o * (1/d) in one fused multiply-add per plane. It may
+    // round differently from the reference's (bound - o) * (1/d); it only
+    // decides which boxes are opened, and triangle boxes are padded by
+    // 10 epsilon (src/geometry/triangle.cpp:42), far beyond that rounding.
+    float x0 = __fmaf_rn(q.neg[0] ? hx : lx, q.inv_dir.x, -q.oinv.x);
+    float x1 = __fmaf_rn(q.neg[0] ? lx : hx, q.inv_dir.x, -q.oinv.x);
+    float y0 = __fmaf_rn(q.neg[1] ? hy : ly, q.inv_dir.y, -q.oinv.y);
+    float y1 = __fmaf_rn(q.neg[1] ? ly : hy, q.inv_dir.y, -q.oinv.y);
+    float z0 = __fmaf_rn(q.neg[2] ? hz : lz, q.inv_dir.z, -q.oinv.z);
+    float z1 = __fmaf_rn(q.neg[2] ? lz : hz, q.inv_dir.z, -q.oinv.z);
+#else
     float x0 = ((q.neg[0] ? hx : lx) - q.o.x) * q.inv_dir.x;
     float x1 = ((q.neg[0] ? lx : hx) - q.o.x) * q.inv_dir.x;
     float y0 = ((q.neg[1] ? hy : ly) - q.o.y) * q.inv_dir.y;
     float y1 = ((q.neg[1] ? ly : hy) - q.o.y) * q.inv_dir.y;
     float z0 = ((q.neg[2] ? hz : lz) - q.o.z) * q.inv_dir.z;
     float z1 = ((q.neg[2] ? lz : hz) - q.o.z) * q.inv_dir.z;
+#endif
     float t0 = fmaxf(fmaxf(x0, y0), fmaxf(z0, t_min));
     float t1 = fminf(fminf(x1, y1), fminf(z1, t_max));
     *entry = t0;
@@ -389,13 +408,20 @@ __device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const Ra
 // Per ray the node and primitive tests are exactly those of TraceOrdered.
 // Src supplies Load(item, RayQ*, t_min*, t_max*) and Store(item, result).
 constexpr int32_t kNoNode = int32_t(0x80000000);
-constexpr int kRefill = 16;
+#ifndef BBG_REFILL
+#define BBG_REFILL 24
+#endif
+#ifndef BBG_SHORT_STACK
+#define BBG_SHORT_STACK 16
+#endif
+// A warp fetches new rays when fewer than kRefill of its lanes are busy.
+constexpr int kRefill = BBG_REFILL;
 // Kernels calling TracePersistent run blocks of this many threads.
 constexpr int kTraversalBlock = 128;
 // Stack entries kept in shared memory per thread; deeper ones go to local
 // memory. The shared part is laid out [depth][thread], so a warp's lanes hit
 // distinct banks whatever depth each lane is at.
-constexpr int kShortStack = 16;
+constexpr int kShortStack = BBG_SHORT_STACK;
 
 template <bool ANY, class Src>
 __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, int32_t* next, Src& src)
