@@ -134,6 +134,13 @@ EXPORTS = [
     ("bbg_integrator_light_pmf", I32, [P, P]),
     ("bbg_render", I32, [P, P, P, P, I32, P]),
     ("bbg_sampler_draws", I32, [I32, I32, I32, I32, I32, P]),
+    ("bbg_guide_create", I32, [P, C.c_uint64, P]),
+    ("bbg_guide_destroy", I32, [P]),
+    ("bbg_guide_get_params", I32, [P, P]),
+    ("bbg_guide_set_params", I32, [P, P]),
+    ("bbg_guide_forward", I32, [P, P, I64, P]),
+    ("bbg_guide_gradient", I32, [P, P, P, P, I64, P, P]),
+    ("bbg_guide_train_step", I32, [P, P, P, P, I64, C.c_float, P]),
     ("bbg_last_error", C.c_char_p, []),
     ("bbg_version", C.c_char_p, []),
 ]

@@ -1,0 +1,286 @@
+// Neural path guiding: a small MLP that maps a shading point to an 8-lobe
+// von Mises-Fisher mixture over directions, sampled in one-sample MIS with the
+// BSDF. No counterpart in the reference renderer; the plain path tracer is
+// its fallback and the judge of its error.
+//
+// Network: 80 inputs -> 64 -> 64 -> 64 (ReLU) -> 40 outputs, BF16 weights and
+// activations, FP32 accumulation (mma.sync m16n8k16), FP32 biases and master
+// weights.
+//   inputs  [0, 72): sin / cos(2^k * pi * p_a) for axis a, k = 0..11, where p
+//                    is the position scaled to [0, 1] by the scene bounds
+//           [72, 75) shading normal, [75, 78) outgoing direction wo,
+//           78 roughness (mean microfacet alpha, 1 for Lambertian), 79 = 1
+//   outputs 5 per lobe j: weight logit, unnormalised mean (3), log kappa
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cstdint>
+
+#include "dev_math.cuh"
+
+namespace bbg
+{
+
+constexpr int kGuideIn = 80;
+constexpr int kGuideHidden = 64;
+constexpr int kGuideOut = 40;
+constexpr int kGuideOutPad = 48; // output rows padded to a multiple of 16 for the backward MMAs
+constexpr int kLobes = 8;
+constexpr int kGuideRaw = 10;    // raw query: p(3), n(3), wo(3), roughness
+
+// Parameter offsets in the FP32 master vector: W0 b0 W1 b1 W2 b2 W3 b3,
+// each W stored [out][in].
+constexpr int kW0 = 0;
+constexpr int kB0 = kW0 + kGuideHidden * kGuideIn;      // 5120
+constexpr int kW1 = kB0 + kGuideHidden;                  // 5184
+constexpr int kB1 = kW1 + kGuideHidden * kGuideHidden;   // 9280
+constexpr int kW2 = kB1 + kGuideHidden;                  // 9344
+constexpr int kB2 = kW2 + kGuideHidden * kGuideHidden;   // 13440
+constexpr int kW3 = kB2 + kGuideHidden;                  // 13504
+constexpr int kB3 = kW3 + kGuideOut * kGuideHidden;      // 16064
+constexpr int kGuideParams = kB3 + kGuideOut;            // 16104
+
+// Biases packed together (as staged in shared memory by the kernels).
+constexpr int kCB0 = 0;
+constexpr int kCB1 = kCB0 + kGuideHidden;
+constexpr int kCB2 = kCB1 + kGuideHidden;
+constexpr int kCB3 = kCB2 + kGuideHidden;
+constexpr int kCBias = kCB3 + kGuideOut; // 232
+
+// BF16 weight images used by the kernels: forward layout [out][in] and the
+// transposed [in][out] layout for the backward pass (W3 transposed padded to
+// 48 columns with zeros).
+constexpr int kBf0 = 0;
+constexpr int kBf1 = kBf0 + kGuideHidden * kGuideIn;
+constexpr int kBf2 = kBf1 + kGuideHidden * kGuideHidden;
+constexpr int kBf3 = kBf2 + kGuideHidden * kGuideHidden;
+constexpr int kBfFwd = kBf3 + kGuideOut * kGuideHidden;  // 15872
+constexpr int kBfT1 = kBfFwd;                            // W1^T [64][64]
+constexpr int kBfT2 = kBfT1 + kGuideHidden * kGuideHidden;
+constexpr int kBfT3 = kBfT2 + kGuideHidden * kGuideHidden; // W3^T [64][48]
+constexpr int kBfAll = kBfT3 + kGuideHidden * kGuideOutPad;
+
+constexpr float kKappaLogMin = -2.0f;
+constexpr float kKappaLogMax = 7.0f;
+
+struct GuideBounds
+{
+    float lo[3];
+    float inv_extent[3];
+};
+
+// Feature f of a raw query (p, n, wo, roughness).
+__device__ __forceinline__ float GuideFeature(int f, const float* raw, const GuideBounds& b)
+{
+    if (f < 72)
+    {
+        int axis = f / 24;
+        int k = (f % 24) >> 1;
+        float pn = (raw[axis] - b.lo[axis]) * b.inv_extent[axis];
+        float x = pn * float(1 << k);
+        return (f & 1) ? cospif(x) : sinpif(x);
+    }
+    if (f < 78)
+    {
+        return raw[f - 72 + 3];
+    }
+    return f == 78 ? raw[9] : 1.0f;
+}
+
+__device__ __forceinline__ uint32_t PackBf16(float lo, float hi)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+// D = A * B + D, m16n8k16, BF16 inputs, FP32 accumulation.
+__device__ __forceinline__ void Mma16816(float* d, const uint32_t* a, uint32_t b0, uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+                 "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// B fragment of an m16n8k16 MMA from a matrix stored [n][k] (k contiguous),
+// row stride ld elements: (k = 2t, 2t+1 | 2t+8, 2t+9; n = g).
+__device__ __forceinline__ void LoadB(const __nv_bfloat16* w, int ld, int n0, int k0, int lane, uint32_t* b0,
+                                      uint32_t* b1)
+{
+    int g = lane >> 2, t = lane & 3;
+    const __nv_bfloat16* row = w + (n0 + g) * ld + k0 + 2 * t;
+    *b0 = *reinterpret_cast<const uint32_t*>(row);
+    *b1 = *reinterpret_cast<const uint32_t*>(row + 8);
+}
+
+// A fragment from a matrix stored [m][k] (k contiguous), row stride ld.
+__device__ __forceinline__ void LoadA(const __nv_bfloat16* x, int ld, int m0, int k0, int lane, uint32_t* a)
+{
+    int g = lane >> 2, t = lane & 3;
+    const __nv_bfloat16* r0 = x + (m0 + g) * ld + k0 + 2 * t;
+    const __nv_bfloat16* r1 = x + (m0 + g + 8) * ld + k0 + 2 * t;
+    a[0] = *reinterpret_cast<const uint32_t*>(r0);
+    a[1] = *reinterpret_cast<const uint32_t*>(r1);
+    a[2] = *reinterpret_cast<const uint32_t*>(r0 + 8);
+    a[3] = *reinterpret_cast<const uint32_t*>(r1 + 8);
+}
+
+// One hidden layer of K inputs -> 64 outputs for the warp's 16 rows: A
+// fragments in, ReLU'd accumulators out (as the next layer's A fragments).
+template <int KT>
+__device__ __forceinline__ void HiddenLayer(const uint32_t (&a)[KT][4], const __nv_bfloat16* w, int ld,
+                                            const float* bias, int lane, float (&acc)[8][4])
+{
+    int t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+    {
+        float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
+        acc[nt][0] = b0;
+        acc[nt][1] = b1;
+        acc[nt][2] = b0;
+        acc[nt][3] = b1;
+    }
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt)
+    {
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+        {
+            uint32_t b0, b1;
+            LoadB(w, ld, nt * 8, kt * 16, lane, &b0, &b1);
+            Mma16816(acc[nt], a[kt], b0, b1);
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+    {
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+        {
+            acc[nt][i] = fmaxf(acc[nt][i], 0.0f);
+        }
+    }
+}
+
+// Accumulators of 64 columns -> A fragments of a K = 64 layer.
+__device__ __forceinline__ void AccToA(const float (&acc)[8][4], uint32_t (&a)[4][4])
+{
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+    {
+        a[kt][0] = PackBf16(acc[2 * kt][0], acc[2 * kt][1]);
+        a[kt][1] = PackBf16(acc[2 * kt][2], acc[2 * kt][3]);
+        a[kt][2] = PackBf16(acc[2 * kt + 1][0], acc[2 * kt + 1][1]);
+        a[kt][3] = PackBf16(acc[2 * kt + 1][2], acc[2 * kt + 1][3]);
+    }
+}
+
+// Output layer 64 -> 40 (no activation).
+__device__ __forceinline__ void OutputLayer(const uint32_t (&a)[4][4], const __nv_bfloat16* w, const float* bias,
+                                            int lane, float (&out)[5][4])
+{
+    int t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 5; ++nt)
+    {
+        float b0 = bias[nt * 8 + 2 * t], b1 = bias[nt * 8 + 2 * t + 1];
+        out[nt][0] = b0;
+        out[nt][1] = b1;
+        out[nt][2] = b0;
+        out[nt][3] = b1;
+    }
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt)
+    {
+#pragma unroll
+        for (int nt = 0; nt < 5; ++nt)
+        {
+            uint32_t b0, b1;
+            LoadB(w, kGuideHidden, nt * 8, kt * 16, lane, &b0, &b1);
+            Mma16816(out[nt], a[kt], b0, b1);
+        }
+    }
+}
+
+// ---------------------------------------------------------------- vMF mixture
+
+struct VmfMixture
+{
+    float logw[kLobes]; // log mixture weight (log-softmax of the logits)
+    V3 mu[kLobes];
+    float kappa[kLobes];
+};
+
+// log of the vMF normalisation kappa / (2 pi (1 - exp(-2 kappa))).
+__device__ __forceinline__ float VmfLogNorm(float kappa)
+{
+    return logf(kappa) - logf(kTwoPi) - log1pf(-expf(-2.0f * kappa));
+}
+
+__device__ __forceinline__ VmfMixture MakeMixture(const float* o)
+{
+    VmfMixture m;
+    float mx = -INFINITY;
+#pragma unroll
+    for (int j = 0; j < kLobes; ++j)
+    {
+        mx = fmaxf(mx, o[5 * j]);
+    }
+    float s = 0;
+#pragma unroll
+    for (int j = 0; j < kLobes; ++j)
+    {
+        s += expf(o[5 * j] - mx);
+    }
+    float lse = mx + logf(s);
+#pragma unroll
+    for (int j = 0; j < kLobes; ++j)
+    {
+        m.logw[j] = o[5 * j] - lse;
+        V3 v{ o[5 * j + 1], o[5 * j + 2], o[5 * j + 3] };
+        float len = fmaxf(Length(v), 1e-6f);
+        m.mu[j] = v / len;
+        m.kappa[j] = expf(Clamp(o[5 * j + 4], kKappaLogMin, kKappaLogMax));
+    }
+    return m;
+}
+
+__device__ __forceinline__ float MixturePdf(const VmfMixture& m, V3 w)
+{
+    float p = 0;
+#pragma unroll
+    for (int j = 0; j < kLobes; ++j)
+    {
+        float k = m.kappa[j];
+        p += expf(m.logw[j] + VmfLogNorm(k) + k * (Dot(m.mu[j], w) - 1.0f));
+    }
+    return p;
+}
+
+// Samples the mixture: lobe by u_lobe, then the vMF lobe with (u1, u2)
+// (W. Jakob, "Numerically stable sampling of the von Mises Fisher
+// distribution on S^2", 2012).
+__device__ __forceinline__ V3 MixtureSample(const VmfMixture& m, float u_lobe, float u1, float u2)
+{
+    int j = kLobes - 1;
+    float c = 0;
+    for (int i = 0; i < kLobes; ++i)
+    {
+        c += expf(m.logw[i]);
+        if (u_lobe < c)
+        {
+            j = i;
+            break;
+        }
+    }
+    float k = m.kappa[j];
+    float w = 1.0f + logf(fmaxf(u1 + (1.0f - u1) * expf(-2.0f * k), 1e-30f)) / k;
+    w = Clamp(w, -1.0f, 1.0f);
+    float r = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+    float phi = kTwoPi * u2;
+    Frame f = FrameFromZ(m.mu[j]);
+    return Normalize(f.FromLocal(V3{ r * cosf(phi), r * sinf(phi), w }));
+}
+
+} // namespace bbg

@@ -1,0 +1,777 @@
+// Neural path guiding on the device: the guide handle, the fused forward
+// (inference) kernel, the fused training kernel (forward, the vMF-mixture
+// negative log-likelihood gradient, and the backward pass through all layers
+// on the tensor cores) and Adam. No counterpart in the reference renderer.
+
+#include "guide.cuh"
+
+#include <cmath>
+#include <cstring>
+#include <random>
+#include <vector>
+
+namespace bbg
+{
+
+namespace
+{
+
+constexpr int kFwdWarps = 8;
+constexpr int kTrainWarps = 2;
+
+// ---------------------------------------------------------------- forward
+
+// Per-warp tile of 16 queries: features -> X (smem, [16][80] bf16) ->
+// 3 hidden layers in registers -> 40 outputs.
+template <class Src>
+__device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_t n, const GuideBounds& bounds,
+                                            const __nv_bfloat16* w, const float* bias, __nv_bfloat16* x, int lane)
+{
+    // Features: two lanes per row, 40 features each.
+    {
+        int row = lane >> 1, half = lane & 1;
+        int64_t item = tile * 16 + row;
+        float raw[kGuideRaw];
+        bool valid = item < n;
+        if (valid)
+        {
+            src.Raw(item, raw);
+        }
+        for (int f = half * 40; f < half * 40 + 40; f += 2)
+        {
+            float v0 = valid ? GuideFeature(f, raw, bounds) : 0.0f;
+            float v1 = valid ? GuideFeature(f + 1, raw, bounds) : 0.0f;
+            *reinterpret_cast<uint32_t*>(x + row * kGuideIn + f) = PackBf16(v0, v1);
+        }
+    }
+    __syncwarp();
+    uint32_t a0[5][4];
+#pragma unroll
+    for (int kt = 0; kt < 5; ++kt)
+    {
+        LoadA(x, kGuideIn, 0, kt * 16, lane, a0[kt]);
+    }
+    float acc[8][4];
+    uint32_t a[4][4];
+    HiddenLayer<5>(a0, w + kBf0, kGuideIn, bias + kCB0, lane, acc);
+    AccToA(acc, a);
+    HiddenLayer<4>(a, w + kBf1, kGuideHidden, bias + kCB1, lane, acc);
+    AccToA(acc, a);
+    HiddenLayer<4>(a, w + kBf2, kGuideHidden, bias + kCB2, lane, acc);
+    AccToA(acc, a);
+    float out[5][4];
+    OutputLayer(a, w + kBf3, bias + kCB3, lane, out);
+    int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int half = 0; half < 2; ++half)
+    {
+        int64_t item = tile * 16 + g + 8 * half;
+        if (item < n)
+        {
+            float* o = src.Out(item);
+#pragma unroll
+            for (int nt = 0; nt < 5; ++nt)
+            {
+                o[nt * 8 + 2 * t] = out[nt][2 * half];
+                o[nt * 8 + 2 * t + 1] = out[nt][2 * half + 1];
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Loads BF16 weights (the first n_bf16 values) and the packed biases into
+// shared memory.
+__device__ __forceinline__ void StageWeights(const __nv_bfloat16* wg, const float* pg, __nv_bfloat16* ws, float* bs,
+                                             int n_bf16)
+{
+    const uint4* src = reinterpret_cast<const uint4*>(wg);
+    uint4* dst = reinterpret_cast<uint4*>(ws);
+    for (int i = threadIdx.x; i < n_bf16 / 8; i += blockDim.x)
+    {
+        dst[i] = src[i];
+    }
+    for (int i = threadIdx.x; i < kCBias; i += blockDim.x)
+    {
+        int src_at = i < kCB1 ? kB0 + i : i < kCB2 ? kB1 + (i - kCB1) : i < kCB3 ? kB2 + (i - kCB2) : kB3 + (i - kCB3);
+        bs[i] = pg[src_at];
+    }
+    __syncthreads();
+}
+
+struct ArraySrc
+{
+    const float* raw;
+    float* out;
+    const int32_t* index; // optional indirection (query i -> record index[i])
+
+    __device__ __forceinline__ int64_t Id(int64_t i) const { return index ? int64_t(index[i]) : i; }
+    __device__ __forceinline__ void Raw(int64_t i, float* r) const
+    {
+        const float* p = raw + kGuideRaw * Id(i);
+        for (int k = 0; k < kGuideRaw; ++k)
+        {
+            r[k] = p[k];
+        }
+    }
+    __device__ __forceinline__ float* Out(int64_t i) const { return out + kGuideOut * Id(i); }
+};
+
+__global__ void __launch_bounds__(32 * kFwdWarps) GuideForwardKernel(const float* raw, const int32_t* index,
+                                                                      const int32_t* n_dev, int64_t n_host,
+                                                                      GuideBounds bounds, const __nv_bfloat16* wg,
+                                                                      const float* pg, float* out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* bs = reinterpret_cast<float*>(smem + kBfFwd * 2);
+    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem + kBfFwd * 2 + kCBias * 4);
+    StageWeights(wg, pg, ws, bs, kBfFwd);
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16* x = xs + warp * 16 * kGuideIn;
+    ArraySrc src{ raw, out, index };
+    const int64_t tiles = (n + 15) / 16;
+    for (int64_t tile = int64_t(blockIdx.x) * kFwdWarps + warp; tile < tiles; tile += int64_t(gridDim.x) * kFwdWarps)
+    {
+        ForwardTile(src, tile, n, bounds, ws, bs, x, lane);
+    }
+}
+
+constexpr size_t kFwdSmem = size_t(kBfFwd) * 2 + size_t(kCBias) * 4 + size_t(kFwdWarps) * 16 * kGuideIn * 2;
+
+// ---------------------------------------------------------------- training
+
+// Gradient of -w log q(dir) w.r.t. the 40 raw outputs of one sample, and the
+// loss term (q: the vMF mixture of MakeMixture).
+__device__ __forceinline__ float MixtureNllGrad(const float* o, V3 dir, float weight, float* g)
+{
+    VmfMixture m = MakeMixture(o);
+    float lp[kLobes];
+    float mx = -INFINITY;
+    for (int j = 0; j < kLobes; ++j)
+    {
+        float k = m.kappa[j];
+        lp[j] = m.logw[j] + VmfLogNorm(k) + k * (Dot(m.mu[j], dir) - 1.0f);
+        mx = fmaxf(mx, lp[j]);
+    }
+    float s = 0;
+    for (int j = 0; j < kLobes; ++j)
+    {
+        s += expf(lp[j] - mx);
+    }
+    float logq = mx + logf(s);
+    for (int j = 0; j < kLobes; ++j)
+    {
+        float gamma = expf(lp[j] - logq); // responsibility
+        float pi = expf(m.logw[j]);
+        float k = m.kappa[j];
+        V3 v{ o[5 * j + 1], o[5 * j + 2], o[5 * j + 3] };
+        float len = fmaxf(Length(v), 1e-6f);
+        float cosm = Dot(m.mu[j], dir);
+        V3 dm = (dir - m.mu[j] * cosm) * (gamma * k / len);
+        g[5 * j] = -weight * (gamma - pi);
+        g[5 * j + 1] = -weight * dm.x;
+        g[5 * j + 2] = -weight * dm.y;
+        g[5 * j + 3] = -weight * dm.z;
+        float r = o[5 * j + 4];
+        float two_k = 2.0f * k;
+        float dlogf_dlogk = 1.0f - two_k / expm1f(two_k) + k * (cosm - 1.0f);
+        bool clamped = r < kKappaLogMin || r > kKappaLogMax;
+        g[5 * j + 4] = clamped ? 0.0f : -weight * gamma * dlogf_dlogk;
+    }
+    return -weight * logq;
+}
+
+struct TrainWarp
+{
+    __nv_bfloat16 x[16 * kGuideIn];      // [sample][feature]
+    __nv_bfloat16 xt[kGuideIn * 16];     // [feature][sample]
+    __nv_bfloat16 h[3][16 * kGuideHidden];   // post-ReLU activations [sample][unit]
+    __nv_bfloat16 ht[3][kGuideHidden * 16];  // [unit][sample]
+    float y[16 * kGuideOut];             // outputs
+    __nv_bfloat16 dy[16 * kGuideOutPad]; // [sample][out], zero padded
+    __nv_bfloat16 dyt[kGuideOutPad * 16];
+    __nv_bfloat16 dh[16 * kGuideHidden];
+    __nv_bfloat16 dht[kGuideHidden * 16];
+};
+
+constexpr size_t kTrainSmem =
+    size_t(kBfAll) * 2 + size_t(kCBias) * 4 + size_t(kGuideParams) * 4 + sizeof(TrainWarp) * kTrainWarps;
+
+// C fragments (16 rows x 64 cols) -> bf16 [16][64] and [64][16].
+__device__ __forceinline__ void StoreActs(const float (&acc)[8][4], __nv_bfloat16* rm, __nv_bfloat16* cm, int lane)
+{
+    int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+    {
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            int row = g + 8 * half;
+            int col = nt * 8 + 2 * t;
+            __nv_bfloat16 v0 = __float2bfloat16_rn(acc[nt][2 * half]);
+            __nv_bfloat16 v1 = __float2bfloat16_rn(acc[nt][2 * half + 1]);
+            rm[row * kGuideHidden + col] = v0;
+            rm[row * kGuideHidden + col + 1] = v1;
+            cm[col * 16 + row] = v0;
+            cm[(col + 1) * 16 + row] = v1;
+        }
+    }
+}
+
+// grad[rows x cols] += A^T B over the warp's 16 samples, where A^T is given
+// [rows][16] (at) and B as [cols][16] (bt); rows and cols multiples of 16/8.
+template <int MT, int NT>
+__device__ __forceinline__ void WeightGrad(const __nv_bfloat16* at, const __nv_bfloat16* bt, float* grad, int ld,
+                                           int rows_valid, int lane)
+{
+    int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+    {
+        uint32_t a[4];
+        LoadA(at, 16, mt * 16, 0, lane, a);
+#pragma unroll
+        for (int nt = 0; nt < NT; ++nt)
+        {
+            uint32_t b0, b1;
+            LoadB(bt, 16, nt * 8, 0, lane, &b0, &b1);
+            float c[4] = { 0, 0, 0, 0 };
+            Mma16816(c, a, b0, b1);
+#pragma unroll
+            for (int half = 0; half < 2; ++half)
+            {
+                int row = mt * 16 + g + 8 * half;
+                int col = nt * 8 + 2 * t;
+                if (row < rows_valid)
+                {
+                    atomicAdd(grad + row * ld + col, c[2 * half]);
+                    atomicAdd(grad + row * ld + col + 1, c[2 * half + 1]);
+                }
+            }
+        }
+    }
+}
+
+// dZ = (dOut . W) masked by the ReLU of the layer's output h: A = dOut
+// [16][K] (ld lda), B = W^T stored [64][K]; writes dZ to dh / dht and adds the
+// column sums to the bias gradient.
+template <int KT>
+__device__ __forceinline__ void BackLayer(const __nv_bfloat16* dout, int lda, const __nv_bfloat16* wt, int ldw,
+                                          const __nv_bfloat16* h, __nv_bfloat16* dh, __nv_bfloat16* dht,
+                                          float* bias_grad, int lane)
+{
+    uint32_t a[KT][4];
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt)
+    {
+        LoadA(dout, lda, 0, kt * 16, lane, a[kt]);
+    }
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+    {
+        acc[nt][0] = acc[nt][1] = acc[nt][2] = acc[nt][3] = 0;
+#pragma unroll
+        for (int kt = 0; kt < KT; ++kt)
+        {
+            uint32_t b0, b1;
+            LoadB(wt, ldw, nt * 8, kt * 16, lane, &b0, &b1);
+            Mma16816(acc[nt], a[kt], b0, b1);
+        }
+    }
+    __syncwarp(); // every lane has read dout before dh is overwritten
+    int g = lane >> 2, t = lane & 3;
+#pragma unroll
+    for (int nt = 0; nt < 8; ++nt)
+    {
+        float colsum0 = 0, colsum1 = 0;
+#pragma unroll
+        for (int half = 0; half < 2; ++half)
+        {
+            int row = g + 8 * half;
+            int col = nt * 8 + 2 * t;
+            float v0 = __bfloat162float(h[row * kGuideHidden + col]) > 0.0f ? acc[nt][2 * half] : 0.0f;
+            float v1 = __bfloat162float(h[row * kGuideHidden + col + 1]) > 0.0f ? acc[nt][2 * half + 1] : 0.0f;
+            colsum0 += v0;
+            colsum1 += v1;
+            __nv_bfloat16 b0 = __float2bfloat16_rn(v0), b1 = __float2bfloat16_rn(v1);
+            dh[row * kGuideHidden + col] = b0;
+            dh[row * kGuideHidden + col + 1] = b1;
+            dht[col * 16 + row] = b0;
+            dht[(col + 1) * 16 + row] = b1;
+        }
+        // Sum over the 8 row groups (lanes with equal t).
+        for (int off = 4; off < 32; off <<= 1)
+        {
+            colsum0 += __shfl_xor_sync(0xffffffffu, colsum0, off);
+            colsum1 += __shfl_xor_sync(0xffffffffu, colsum1, off);
+        }
+        if (g == 0)
+        {
+            atomicAdd(bias_grad + nt * 8 + 2 * t, colsum0);
+            atomicAdd(bias_grad + nt * 8 + 2 * t + 1, colsum1);
+        }
+    }
+    __syncwarp();
+}
+
+__global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float* raw, const float* dirs,
+                                                                      const float* weights, const int32_t* n_dev,
+                                                                      int64_t n_host, GuideBounds bounds,
+                                                                      const __nv_bfloat16* wg, const float* pg,
+                                                                      float* grad_out, float* loss_out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* bs = reinterpret_cast<float*>(smem + size_t(kBfAll) * 2);
+    float* gs = bs + kCBias;
+    TrainWarp* tw = reinterpret_cast<TrainWarp*>(gs + kGuideParams);
+    StageWeights(wg, pg, ws, bs, kBfAll);
+    for (int i = threadIdx.x; i < kGuideParams; i += blockDim.x)
+    {
+        gs[i] = 0;
+    }
+    __syncthreads();
+
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    TrainWarp& W = tw[warp];
+    const int g = lane >> 2, t = lane & 3;
+    float loss = 0;
+    const int64_t tiles = (n + 15) / 16;
+    for (int64_t tile = int64_t(blockIdx.x) * kTrainWarps + warp; tile < tiles;
+         tile += int64_t(gridDim.x) * kTrainWarps)
+    {
+        // Features, both layouts.
+        {
+            int row = lane >> 1, half = lane & 1;
+            int64_t item = tile * 16 + row;
+            bool valid = item < n;
+            float r[kGuideRaw];
+            if (valid)
+            {
+                for (int k = 0; k < kGuideRaw; ++k)
+                {
+                    r[k] = raw[kGuideRaw * item + k];
+                }
+            }
+            for (int f = half * 40; f < half * 40 + 40; ++f)
+            {
+                __nv_bfloat16 v = __float2bfloat16_rn(valid ? GuideFeature(f, r, bounds) : 0.0f);
+                W.x[row * kGuideIn + f] = v;
+                W.xt[f * 16 + row] = v;
+            }
+        }
+        __syncwarp();
+
+        // Forward, keeping activations.
+        uint32_t a0[5][4];
+#pragma unroll
+        for (int kt = 0; kt < 5; ++kt)
+        {
+            LoadA(W.x, kGuideIn, 0, kt * 16, lane, a0[kt]);
+        }
+        float acc[8][4];
+        uint32_t a[4][4];
+        HiddenLayer<5>(a0, ws + kBf0, kGuideIn, bs + kCB0, lane, acc);
+        StoreActs(acc, W.h[0], W.ht[0], lane);
+        AccToA(acc, a);
+        HiddenLayer<4>(a, ws + kBf1, kGuideHidden, bs + kCB1, lane, acc);
+        StoreActs(acc, W.h[1], W.ht[1], lane);
+        AccToA(acc, a);
+        HiddenLayer<4>(a, ws + kBf2, kGuideHidden, bs + kCB2, lane, acc);
+        StoreActs(acc, W.h[2], W.ht[2], lane);
+        AccToA(acc, a);
+        float out[5][4];
+        OutputLayer(a, ws + kBf3, bs + kCB3, lane, out);
+#pragma unroll
+        for (int nt = 0; nt < 5; ++nt)
+        {
+#pragma unroll
+            for (int half = 0; half < 2; ++half)
+            {
+                int row = g + 8 * half;
+                W.y[row * kGuideOut + nt * 8 + 2 * t] = out[nt][2 * half];
+                W.y[row * kGuideOut + nt * 8 + 2 * t + 1] = out[nt][2 * half + 1];
+            }
+        }
+        __syncwarp();
+
+        // Output gradient, one lane per sample.
+        if (lane < 16)
+        {
+            int64_t item = tile * 16 + lane;
+            float gy[kGuideOut];
+            if (item < n)
+            {
+                V3 dir{ dirs[3 * item], dirs[3 * item + 1], dirs[3 * item + 2] };
+                loss += MixtureNllGrad(W.y + lane * kGuideOut, dir, weights[item], gy);
+            }
+            else
+            {
+                for (int k = 0; k < kGuideOut; ++k)
+                {
+                    gy[k] = 0;
+                }
+            }
+            for (int k = 0; k < kGuideOutPad; ++k)
+            {
+                float v = k < kGuideOut ? gy[k] : 0.0f;
+                __nv_bfloat16 b = __float2bfloat16_rn(v);
+                W.dy[lane * kGuideOutPad + k] = b;
+                W.dyt[k * 16 + lane] = b;
+                if (k < kGuideOut && v != 0.0f)
+                {
+                    atomicAdd(gs + kB3 + k, v);
+                }
+            }
+        }
+        __syncwarp();
+
+        // Layer 3: dW3 += dY^T H3, dZ2 = (dY W3) * relu'(H3).
+        WeightGrad<3, 8>(W.dyt, W.ht[2], gs + kW3, kGuideHidden, kGuideOut, lane);
+        BackLayer<3>(W.dy, kGuideOutPad, ws + kBfT3, kGuideOutPad, W.h[2], W.dh, W.dht, gs + kB2, lane);
+        // Layer 2: dW2 += dZ2^T H2, dZ1 = (dZ2 W2) * relu'(H2).
+        WeightGrad<4, 8>(W.dht, W.ht[1], gs + kW2, kGuideHidden, kGuideHidden, lane);
+        BackLayer<4>(W.dh, kGuideHidden, ws + kBfT2, kGuideHidden, W.h[1], W.dh, W.dht, gs + kB1, lane);
+        // Layer 1: dW1 += dZ1^T H1, dZ0 = (dZ1 W1) * relu'(H1).
+        WeightGrad<4, 8>(W.dht, W.ht[0], gs + kW1, kGuideHidden, kGuideHidden, lane);
+        BackLayer<4>(W.dh, kGuideHidden, ws + kBfT1, kGuideHidden, W.h[0], W.dh, W.dht, gs + kB0, lane);
+        // Layer 0: dW0 += dZ0^T X.
+        WeightGrad<4, 10>(W.dht, W.xt, gs + kW0, kGuideIn, kGuideHidden, lane);
+        __syncwarp();
+    }
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        loss += __shfl_xor_sync(0xffffffffu, loss, off);
+    }
+    if (lane == 0 && loss != 0.0f)
+    {
+        atomicAdd(loss_out, loss);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kGuideParams; i += blockDim.x)
+    {
+        float v = gs[i];
+        if (v != 0.0f)
+        {
+            atomicAdd(grad_out + i, v);
+        }
+    }
+}
+
+// Adam on the FP32 master parameters (gradient = grad_sum * inv_n), then the
+// BF16 images (forward and transposed layouts) are refreshed; the gradient
+// accumulator is cleared for the next step.
+__global__ void GuideAdamKernel(float* params, float* m, float* v, float* grad, int step, float lr, float b1, float b2,
+                                float eps, const float* inv_n_dev, float inv_n_host)
+{
+    float inv_n = inv_n_dev ? *inv_n_dev : inv_n_host;
+    float c1 = 1.0f - powf(b1, float(step));
+    float c2 = 1.0f - powf(b2, float(step));
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGuideParams; i += gridDim.x * blockDim.x)
+    {
+        float gi = grad[i] * inv_n;
+        grad[i] = 0;
+        float mi = b1 * m[i] + (1 - b1) * gi;
+        float vi = b2 * v[i] + (1 - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        params[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void GuideConvertKernel(const float* params, __nv_bfloat16* w)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kBfAll; i += gridDim.x * blockDim.x)
+    {
+        float v = 0;
+        if (i < kBf1)
+        {
+            v = params[kW0 + i];
+        }
+        else if (i < kBf2)
+        {
+            v = params[kW1 + (i - kBf1)];
+        }
+        else if (i < kBf3)
+        {
+            v = params[kW2 + (i - kBf2)];
+        }
+        else if (i < kBfFwd)
+        {
+            v = params[kW3 + (i - kBf3)];
+        }
+        else if (i < kBfT2)
+        {
+            int j = i - kBfT1, r = j / kGuideHidden, c = j % kGuideHidden; // W1^T[r][c] = W1[c][r]
+            v = params[kW1 + c * kGuideHidden + r];
+        }
+        else if (i < kBfT3)
+        {
+            int j = i - kBfT2, r = j / kGuideHidden, c = j % kGuideHidden;
+            v = params[kW2 + c * kGuideHidden + r];
+        }
+        else
+        {
+            int j = i - kBfT3, r = j / kGuideOutPad, c = j % kGuideOutPad; // W3^T[r][c] = W3[c][r]
+            v = c < kGuideOut ? params[kW3 + c * kGuideHidden + r] : 0.0f;
+        }
+        w[i] = __float2bfloat16_rn(v);
+    }
+}
+
+} // namespace
+
+// ---------------------------------------------------------------- launches
+
+bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index_dev, const int32_t* n_dev,
+                        int64_t n_host, float* out_dev, cudaStream_t st)
+{
+    int grid = 0;
+    BBG_TRY(GuidePrepare(G, &grid));
+    GuideForwardKernel<<<grid, 32 * kFwdWarps, kFwdSmem, st>>>(raw_dev, index_dev, n_dev, n_host, G->bounds,
+                                                                 G->bf16.p, G->params.p, out_dev);
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
+                           const int32_t* n_dev, int64_t n_host, cudaStream_t st)
+{
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    GuideTrainKernel<<<sms, 32 * kTrainWarps, kTrainSmem, st>>>(raw_dev, dirs_dev, weights_dev, n_dev, n_host,
+                                                                G->bounds, G->bf16.p, G->params.p, G->grad.p,
+                                                                G->loss.p);
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bbg_status GuideApply(bbg_guide* G, float lr, const float* inv_n_dev, float inv_n_host, cudaStream_t st)
+{
+    ++G->step;
+    GuideAdamKernel<<<64, 256, 0, st>>>(G->params.p, G->adam_m.p, G->adam_v.p, G->grad.p, G->step, lr, G->beta1,
+                                        G->beta2, 1e-8f, inv_n_dev, inv_n_host);
+    GuideConvertKernel<<<64, 256, 0, st>>>(G->params.p, G->bf16.p);
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bbg_status GuidePrepare(bbg_guide* G, int* grid)
+{
+    if (!G->smem_set)
+    {
+        BBG_CUDA(cudaFuncSetAttribute(GuideForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFwdSmem)));
+        BBG_CUDA(cudaFuncSetAttribute(GuideTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)));
+        G->smem_set = true;
+    }
+    int sms = 148, per = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideForwardKernel, 32 * kFwdWarps, kFwdSmem);
+    *grid = sms * std::max(per, 1);
+    return BBG_OK;
+}
+
+// Xavier-style uniform initialisation of the hidden layers; the output layer
+// starts near an even mixture of broad lobes toward the 8 cube diagonals.
+void InitGuideParams(uint64_t seed, float* p)
+{
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int at, int fan_out, int fan_in, float scale) {
+        std::uniform_real_distribution<float> u(-scale, scale);
+        for (int i = 0; i < fan_out * fan_in; ++i)
+        {
+            p[at + i] = u(rng);
+        }
+    };
+    fill(kW0, kGuideHidden, kGuideIn, std::sqrt(6.0f / (kGuideIn + kGuideHidden)));
+    fill(kW1, kGuideHidden, kGuideHidden, std::sqrt(6.0f / (2 * kGuideHidden)));
+    fill(kW2, kGuideHidden, kGuideHidden, std::sqrt(6.0f / (2 * kGuideHidden)));
+    fill(kW3, kGuideOut, kGuideHidden, 1e-2f);
+    for (int i = 0; i < kGuideHidden; ++i)
+    {
+        p[kB0 + i] = 0;
+        p[kB1 + i] = 0;
+        p[kB2 + i] = 0;
+    }
+    for (int j = 0; j < kLobes; ++j)
+    {
+        float sx = (j & 1) ? 1.0f : -1.0f, sy = (j & 2) ? 1.0f : -1.0f, sz = (j & 4) ? 1.0f : -1.0f;
+        p[kB3 + 5 * j] = 0;
+        p[kB3 + 5 * j + 1] = sx;
+        p[kB3 + 5 * j + 2] = sy;
+        p[kB3 + 5 * j + 3] = sz;
+        p[kB3 + 5 * j + 4] = std::log(1.5f);
+    }
+}
+
+} // namespace bbg
+
+using namespace bbg;
+
+namespace
+{
+
+bbg_status Create(const float* aabb, uint64_t seed, bbg_guide* G)
+{
+    BBG_TRY(CheckDevice());
+    BBG_CUDA(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
+    for (int a = 0; a < 3; ++a)
+    {
+        float ext = aabb[3 + a] - aabb[a];
+        G->bounds.lo[a] = aabb[a];
+        G->bounds.inv_extent[a] = ext > 0 ? 1.0f / ext : 0.0f;
+    }
+    std::vector<float> p(kGuideParams);
+    InitGuideParams(seed, p.data());
+    BBG_TRY(G->params.upload(p.data(), p.size(), G->stream));
+    std::vector<float> zeros(kGuideParams, 0.0f);
+    BBG_TRY(G->adam_m.upload(zeros.data(), zeros.size(), G->stream));
+    BBG_TRY(G->adam_v.upload(zeros.data(), zeros.size(), G->stream));
+    BBG_TRY(G->grad.upload(zeros.data(), zeros.size(), G->stream));
+    BBG_TRY(G->loss.alloc(1));
+    BBG_TRY(G->bf16.alloc(kBfAll));
+    GuideConvertKernel<<<64, 256, 0, G->stream>>>(G->params.p, G->bf16.p);
+    BBG_CUDA(cudaGetLastError());
+    BBG_CUDA(cudaStreamSynchronize(G->stream));
+    return BBG_OK;
+}
+
+// Host buffers -> device staging.
+bbg_status Stage(bbg_guide* G, const float* raw, const float* dirs, const float* weights, int64_t n)
+{
+    BBG_TRY(G->s_raw.upload(raw, size_t(n) * kGuideRaw, G->stream));
+    if (dirs)
+    {
+        BBG_TRY(G->s_dirs.upload(dirs, size_t(n) * 3, G->stream));
+    }
+    if (weights)
+    {
+        BBG_TRY(G->s_w.upload(weights, size_t(n), G->stream));
+    }
+    return BBG_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+bbg_status bbg_guide_create(const float* scene_aabb, uint64_t seed, bbg_guide** out)
+{
+    if (!scene_aabb || !out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_create: bad argument");
+    }
+    *out = nullptr;
+    auto* G = new bbg_guide;
+    bbg_status s = Create(scene_aabb, seed, G);
+    if (s != BBG_OK)
+    {
+        delete G;
+        return s;
+    }
+    *out = G;
+    return BBG_OK;
+}
+
+bbg_status bbg_guide_destroy(bbg_guide* G)
+{
+    delete G;
+    return BBG_OK;
+}
+
+bbg_status bbg_guide_get_params(bbg_guide* G, float* out)
+{
+    if (!G || !out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_get_params: bad argument");
+    }
+    BBG_CUDA(cudaStreamSynchronize(G->stream));
+    BBG_CUDA(cudaMemcpy(out, G->params.p, sizeof(float) * kGuideParams, cudaMemcpyDeviceToHost));
+    return BBG_OK;
+}
+
+bbg_status bbg_guide_set_params(bbg_guide* G, const float* in)
+{
+    if (!G || !in)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_set_params: bad argument");
+    }
+    BBG_CUDA(cudaMemcpy(G->params.p, in, sizeof(float) * kGuideParams, cudaMemcpyHostToDevice));
+    GuideConvertKernel<<<64, 256, 0, G->stream>>>(G->params.p, G->bf16.p);
+    BBG_CUDA(cudaStreamSynchronize(G->stream));
+    return BBG_OK;
+}
+
+bbg_status bbg_guide_forward(bbg_guide* G, const float* raw, int64_t n, float* out)
+{
+    if (!G || n < 0 || (n > 0 && (!raw || !out)))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_forward: bad argument");
+    }
+    if (n == 0)
+    {
+        return BBG_OK;
+    }
+    BBG_TRY(Stage(G, raw, nullptr, nullptr, n));
+    BBG_TRY(G->s_out.alloc(size_t(n) * kGuideOut));
+    BBG_TRY(GuideForward(G, G->s_raw.p, nullptr, nullptr, n, G->s_out.p, G->stream));
+    BBG_CUDA(cudaMemcpyAsync(out, G->s_out.p, sizeof(float) * size_t(n) * kGuideOut, cudaMemcpyDeviceToHost,
+                             G->stream));
+    BBG_CUDA(cudaStreamSynchronize(G->stream));
+    return BBG_OK;
+}
+
+bbg_status bbg_guide_gradient(bbg_guide* G, const float* raw, const float* dirs, const float* weights, int64_t n,
+                              float* grad_out, float* loss_out)
+{
+    if (!G || n <= 0 || !raw || !dirs || !weights || !grad_out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_gradient: bad argument");
+    }
+    int dummy;
+    BBG_TRY(GuidePrepare(G, &dummy));
+    BBG_TRY(Stage(G, raw, dirs, weights, n));
+    BBG_CUDA(cudaMemsetAsync(G->grad.p, 0, sizeof(float) * kGuideParams, G->stream));
+    BBG_CUDA(cudaMemsetAsync(G->loss.p, 0, sizeof(float), G->stream));
+    BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, G->stream));
+    BBG_CUDA(cudaMemcpyAsync(grad_out, G->grad.p, sizeof(float) * kGuideParams, cudaMemcpyDeviceToHost, G->stream));
+    float loss = 0;
+    BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));
+    BBG_CUDA(cudaMemsetAsync(G->grad.p, 0, sizeof(float) * kGuideParams, G->stream));
+    BBG_CUDA(cudaStreamSynchronize(G->stream));
+    if (loss_out)
+    {
+        *loss_out = loss;
+    }
+    return BBG_OK;
+}
+
+bbg_status bbg_guide_train_step(bbg_guide* G, const float* raw, const float* dirs, const float* weights, int64_t n,
+                                float learning_rate, float* loss_out)
+{
+    if (!G || n <= 0 || !raw || !dirs || !weights)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_train_step: bad argument");
+    }
+    int dummy;
+    BBG_TRY(GuidePrepare(G, &dummy));
+    BBG_TRY(Stage(G, raw, dirs, weights, n));
+    BBG_CUDA(cudaMemsetAsync(G->loss.p, 0, sizeof(float), G->stream));
+    BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, G->stream));
+    BBG_TRY(GuideApply(G, learning_rate, nullptr, 1.0f / float(n), G->stream));
+    float loss = 0;
+    BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));
+    BBG_CUDA(cudaStreamSynchronize(G->stream));
+    if (loss_out)
+    {
+        *loss_out = loss / float(n);
+    }
+    return BBG_OK;
+}
+
+} // extern "C"

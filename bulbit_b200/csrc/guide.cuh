@@ -1,0 +1,43 @@
+// The guide handle (neural path guiding) and its launch helpers.
+#pragma once
+
+#include "cuda_util.cuh"
+#include "dev_guide.cuh"
+
+struct bbg_guide
+{
+    cudaStream_t stream = nullptr;
+    bbg::GuideBounds bounds{};
+    bbg::DevBuf<float> params;  // FP32 master parameters (kGuideParams)
+    bbg::DevBuf<float> adam_m, adam_v, grad, loss;
+    bbg::DevBuf<__nv_bfloat16> bf16; // kBfAll: forward + transposed weight images
+    int step = 0;
+    float beta1 = 0.9f, beta2 = 0.99f;
+    bool smem_set = false;
+    // Staging for host-buffer calls.
+    bbg::DevBuf<float> s_raw, s_dirs, s_w, s_out;
+
+    ~bbg_guide()
+    {
+        if (stream)
+        {
+            cudaStreamSynchronize(stream);
+            cudaStreamDestroy(stream);
+        }
+    }
+};
+
+namespace bbg
+{
+// Sets the kernels' shared-memory limits (once) and returns the forward grid.
+bbg_status GuidePrepare(bbg_guide* G, int* grid);
+// Forward over n queries (raw records of kGuideRaw floats); index (optional)
+// maps query i to record index[i] for both raw and out. n from n_dev if set.
+bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index_dev, const int32_t* n_dev,
+                        int64_t n_host, float* out_dev, cudaStream_t st);
+// Adds the gradient of sum_i -w_i log q_i(dir_i) to the guide's accumulator.
+bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
+                           const int32_t* n_dev, int64_t n_host, cudaStream_t st);
+// One Adam step with gradient = accumulator * inv_n.
+bbg_status GuideApply(bbg_guide* G, float lr, const float* inv_n_dev, float inv_n_host, cudaStream_t st);
+} // namespace bbg

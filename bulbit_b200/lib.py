@@ -254,3 +254,59 @@ class GpuPathIntegrator:
     def render_device(self, cam, params, film_struct, stats):
         check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(params), C.byref(film_struct),
                                    abi.BBG_MEM_DEVICE, C.byref(stats)), "bbg_render")
+
+
+class GpuGuide:
+    """The path-guiding MLP (bbg_guide_*)."""
+
+    N_PARAMS = 16104
+
+    def __init__(self, aabb, seed=1):
+        self._aabb = np.ascontiguousarray(aabb, np.float32)
+        self.h = C.c_void_p()
+        check(get_lib().bbg_guide_create(_p(self._aabb), seed, C.byref(self.h)), "bbg_guide_create")
+
+    def close(self):
+        if self.h:
+            get_lib().bbg_guide_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        out = np.zeros(self.N_PARAMS, np.float32)
+        check(get_lib().bbg_guide_get_params(self.h, _p(out)), "bbg_guide_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        check(get_lib().bbg_guide_set_params(self.h, _p(p)), "bbg_guide_set_params")
+
+    def forward(self, raw):
+        raw = np.ascontiguousarray(raw, np.float32)
+        out = np.zeros((raw.shape[0], 40), np.float32)
+        check(get_lib().bbg_guide_forward(self.h, _p(raw), raw.shape[0], _p(out)), "bbg_guide_forward")
+        return out
+
+    def gradient(self, raw, dirs, weights):
+        raw = np.ascontiguousarray(raw, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        weights = np.ascontiguousarray(weights, np.float32)
+        g = np.zeros(self.N_PARAMS, np.float32)
+        loss = C.c_float()
+        check(get_lib().bbg_guide_gradient(self.h, _p(raw), _p(dirs), _p(weights), raw.shape[0], _p(g),
+                                           C.byref(loss)), "bbg_guide_gradient")
+        return g, loss.value
+
+    def train_step(self, raw, dirs, weights, lr=1e-2):
+        raw = np.ascontiguousarray(raw, np.float32)
+        dirs = np.ascontiguousarray(dirs, np.float32)
+        weights = np.ascontiguousarray(weights, np.float32)
+        loss = C.c_float()
+        check(get_lib().bbg_guide_train_step(self.h, _p(raw), _p(dirs), _p(weights), raw.shape[0], C.c_float(lr),
+                                             C.byref(loss)), "bbg_guide_train_step")
+        return loss.value

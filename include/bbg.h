@@ -367,6 +367,35 @@ bbg_status bbg_render(bbg_integrator* integrator, const bbg_camera* camera, cons
  * StartPixelSample(pixel, sample) with the given seed, computed on the device. */
 bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out);
 
+/* --------------------------------------------------------- path guiding */
+
+/* Neural path guiding (no counterpart in the reference: an added learned
+ * component). A small MLP maps a shading point — raw query of 10 floats:
+ * position (3), shading normal (3), outgoing direction (3), roughness — to an
+ * 8-lobe von Mises-Fisher mixture over incident directions (40 outputs: per
+ * lobe weight logit, unnormalised mean (3), log kappa). Network 80 -> 64 ->
+ * 64 -> 64 -> 40 (ReLU), 16,104 parameters; BF16 weights and activations on
+ * the tensor cores, FP32 accumulation and FP32 master weights; Adam
+ * (betas 0.9 / 0.99). The position is normalised by scene_aabb (min xyz,
+ * max xyz). Host buffers throughout. */
+typedef struct bbg_guide bbg_guide;
+
+bbg_status bbg_guide_create(const float* scene_aabb, uint64_t seed, bbg_guide** out);
+bbg_status bbg_guide_destroy(bbg_guide* guide);
+/* FP32 master parameters, 16,104 floats: W0 b0 W1 b1 W2 b2 W3 b3, W [out][in]. */
+bbg_status bbg_guide_get_params(bbg_guide* guide, float* params_out);
+bbg_status bbg_guide_set_params(bbg_guide* guide, const float* params);
+/* Network outputs (40 per query) for n raw queries. */
+bbg_status bbg_guide_forward(bbg_guide* guide, const float* raw, int64_t n, float* out);
+/* Gradient (16,104 floats) of sum_i -weights[i] * log q_i(dirs[i]) over n
+ * samples (dirs: 3 floats each, unit length), and that sum in *loss_out. */
+bbg_status bbg_guide_gradient(bbg_guide* guide, const float* raw, const float* dirs, const float* weights, int64_t n,
+                              float* grad_out, float* loss_out);
+/* One Adam step on the mean of that loss over the batch; *loss_out = mean loss
+ * before the step. */
+bbg_status bbg_guide_train_step(bbg_guide* guide, const float* raw, const float* dirs, const float* weights, int64_t n,
+                                float learning_rate, float* loss_out);
+
 /* --------------------------------------------------------------- library */
 
 const char* bbg_last_error(void);
