@@ -505,4 +505,20 @@ __device__ __forceinline__ BSDF MakeBSDF(const MaterialDev& m, V3 shading_n, V3 
 
 __device__ __forceinline__ bool IsNonSpecular(int32_t flags) { return (flags & (kFlagDiffuse | kFlagGlossy)) != 0; }
 
+// BSDF::Regularize (include/bulbit/bsdf.h:134): widen the microfacet lobe,
+// then the flags the BxDF reports for the new roughness.
+__device__ __forceinline__ void RegularizeBSDF(BSDF* b)
+{
+    b->mf.Regularize();
+    if (b->type == BBG_MAT_CONDUCTOR)
+    {
+        b->flags = b->mf.EffectivelySmooth() ? (kFlagSpecular | kFlagReflection) : (kFlagGlossy | kFlagReflection);
+    }
+    else if (b->type == BBG_MAT_DIELECTRIC)
+    {
+        int32_t f = (b->eta == 1) ? kFlagTransmission : (kFlagReflection | kFlagTransmission);
+        b->flags = f | (b->mf.EffectivelySmooth() ? kFlagSpecular : kFlagGlossy);
+    }
+}
+
 } // namespace bbg

@@ -463,13 +463,30 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
     }
 }
 
-// Adam on the FP32 master parameters (gradient = grad_sum * inv_n), then the
-// BF16 images (forward and transposed layouts) are refreshed; the gradient
-// accumulator is cleared for the next step.
-__global__ void GuideAdamKernel(float* params, float* m, float* v, float* grad, int step, float lr, float b1, float b2,
-                                float eps, const float* inv_n_dev, float inv_n_host)
+// Counts an Adam step when the batch is not empty. The step number and the
+// batch size live in device memory so a captured graph replays correctly.
+__global__ void GuideStepKernel(int32_t* step, const int32_t* n_dev, int64_t n_host)
 {
-    float inv_n = inv_n_dev ? *inv_n_dev : inv_n_host;
+    int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    if (n > 0)
+    {
+        *step += 1;
+    }
+}
+
+// Adam on the FP32 master parameters (gradient = grad_sum / n), then the
+// BF16 images (forward and transposed layouts) are refreshed; the gradient
+// accumulator is cleared for the next step. An empty batch changes nothing.
+__global__ void GuideAdamKernel(float* params, float* m, float* v, float* grad, const int32_t* step_dev, float lr,
+                                float b1, float b2, float eps, const int32_t* n_dev, int64_t n_host)
+{
+    int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    if (n <= 0)
+    {
+        return;
+    }
+    float inv_n = 1.0f / float(n);
+    int step = *step_dev;
     float c1 = 1.0f - powf(b1, float(step));
     float c2 = 1.0f - powf(b2, float(step));
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kGuideParams; i += gridDim.x * blockDim.x)
@@ -551,11 +568,11 @@ bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs
     return BBG_OK;
 }
 
-bbg_status GuideApply(bbg_guide* G, float lr, const float* inv_n_dev, float inv_n_host, cudaStream_t st)
+bbg_status GuideApply(bbg_guide* G, float lr, const int32_t* n_dev, int64_t n_host, cudaStream_t st)
 {
-    ++G->step;
-    GuideAdamKernel<<<64, 256, 0, st>>>(G->params.p, G->adam_m.p, G->adam_v.p, G->grad.p, G->step, lr, G->beta1,
-                                        G->beta2, 1e-8f, inv_n_dev, inv_n_host);
+    GuideStepKernel<<<1, 1, 0, st>>>(G->step_dev.p, n_dev, n_host);
+    GuideAdamKernel<<<64, 256, 0, st>>>(G->params.p, G->adam_m.p, G->adam_v.p, G->grad.p, G->step_dev.p, lr, G->beta1,
+                                        G->beta2, 1e-8f, n_dev, n_host);
     GuideConvertKernel<<<64, 256, 0, st>>>(G->params.p, G->bf16.p);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
@@ -635,6 +652,8 @@ bbg_status Create(const float* aabb, uint64_t seed, bbg_guide* G)
     BBG_TRY(G->grad.upload(zeros.data(), zeros.size(), G->stream));
     BBG_TRY(G->loss.alloc(1));
     BBG_TRY(G->bf16.alloc(kBfAll));
+    BBG_TRY(G->step_dev.alloc(1));
+    BBG_CUDA(cudaMemsetAsync(G->step_dev.p, 0, sizeof(int32_t), G->stream));
     GuideConvertKernel<<<64, 256, 0, G->stream>>>(G->params.p, G->bf16.p);
     BBG_CUDA(cudaGetLastError());
     BBG_CUDA(cudaStreamSynchronize(G->stream));
@@ -763,7 +782,7 @@ bbg_status bbg_guide_train_step(bbg_guide* G, const float* raw, const float* dir
     BBG_TRY(Stage(G, raw, dirs, weights, n));
     BBG_CUDA(cudaMemsetAsync(G->loss.p, 0, sizeof(float), G->stream));
     BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, G->stream));
-    BBG_TRY(GuideApply(G, learning_rate, nullptr, 1.0f / float(n), G->stream));
+    BBG_TRY(GuideApply(G, learning_rate, nullptr, n, G->stream));
     float loss = 0;
     BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));
     BBG_CUDA(cudaStreamSynchronize(G->stream));

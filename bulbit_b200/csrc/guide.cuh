@@ -11,7 +11,7 @@ struct bbg_guide
     bbg::DevBuf<float> params;  // FP32 master parameters (kGuideParams)
     bbg::DevBuf<float> adam_m, adam_v, grad, loss;
     bbg::DevBuf<__nv_bfloat16> bf16; // kBfAll: forward + transposed weight images
-    int step = 0;
+    bbg::DevBuf<int32_t> step_dev; // Adam step counter
     float beta1 = 0.9f, beta2 = 0.99f;
     bool smem_set = false;
     // Staging for host-buffer calls.
@@ -38,6 +38,7 @@ bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index
 // Adds the gradient of sum_i -w_i log q_i(dir_i) to the guide's accumulator.
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
                            const int32_t* n_dev, int64_t n_host, cudaStream_t st);
-// One Adam step with gradient = accumulator * inv_n.
-bbg_status GuideApply(bbg_guide* G, float lr, const float* inv_n_dev, float inv_n_host, cudaStream_t st);
+// One Adam step with gradient = accumulator / n (n from n_dev if set); an
+// empty batch is skipped.
+bbg_status GuideApply(bbg_guide* G, float lr, const int32_t* n_dev, int64_t n_host, cudaStream_t st);
 } // namespace bbg

@@ -20,6 +20,7 @@
 #include "accel.cuh"
 #include "dev_bsdf.cuh"
 #include "dev_lights.cuh"
+#include "guide.cuh"
 
 #include <algorithm>
 #include <cstring>
@@ -601,14 +602,470 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int
     }
 }
 
-// Clears the next level's ray queue, the shadow queue and the work counters
-// of the persistent closest-hit and shadow passes.
+// ---------------------------------------------------------------- guided shading
+//
+// With a guide, each level shades in two passes around one batched MLP
+// inference: GuidedShadeA does everything up to the BSDF and, at
+// non-specular vertices, queues the guide query; GuidedShadeB (after the
+// inference) does next-event estimation and the continuation with one-sample
+// MIS between the guide and the BSDF (selection probability 1/2). The
+// continuation pdf is the mixture 0.5 q + 0.5 p_bsdf, and both MIS weights
+// (light samples here, emitted light at the next hit) use it, so the
+// estimator stays unbiased whatever the network outputs. Specular vertices
+// continue as in the plain tracer. Training records take (query, direction,
+// pdf, throughput) at sampled vertices and the radiance the rest of the path
+// brings back along that direction.
+
+struct GuideDev
+{
+    float* raw;        // per slot: query (kGuideRaw floats)
+    float* out;        // per slot: network outputs (kGuideOut floats)
+    float4* vtx;       // per slot: (point, material), (sn, front), (st, -), (wo, -)
+    int32_t* queue;    // slots with a guide query this level
+    int32_t* rec_id;   // per slot: open training record or -1
+    float* rec;        // per record: raw (10), dir (3), pdf, beta after the vertex (3), L at next shade (3)
+    int32_t* rec_slot;
+    float* t_raw;      // training batch: raw queries, directions, weights
+    float* t_dir;
+    float* t_w;
+    float* wsum;
+    int32_t rec_cap;
+    int32_t stride;    // paths with index % stride == 0 record training samples
+    int32_t train;
+};
+
+constexpr int kRecFloats = 20;
+
+__device__ __forceinline__ float GuideRoughness(const MaterialDev& m)
+{
+    return m.type == BBG_MAT_DIFFUSE ? 1.0f : sqrtf(m.alpha_x * m.alpha_y);
+}
+
+// Escaped ray: infinite lights with MIS against the previous continuation pdf.
+__device__ __forceinline__ void AddEscaped(const SceneDev& s, Spec beta, int32_t bounce, bool specular_bounce,
+                                           float prev_pdf, Spec* L)
+{
+    for (int32_t k = 0; k < s.n_infinite; ++k)
+    {
+        const LightDev& l = s.lights[s.infinite[k]];
+        Spec Le = l.scale * Spec{ l.L[0], l.L[1], l.L[2] };
+        if (bounce == 0 || specular_bounce)
+        {
+            *L = *L + beta * Le;
+        }
+        else
+        {
+            float light_pdf = kInvFourPi * s.light_pmf[s.infinite[k]];
+            *L = *L + beta * PowerHeuristic(prev_pdf, light_pdf) * Le;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, GuideDev g, int parity)
+{
+    const int32_t* q = w.queue[parity];
+    int32_t* q_next = w.queue[parity ^ 1];
+    const int32_t n = w.counts[parity];
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        int32_t slot = q[j];
+        float4 o4 = w.o_pdf[slot], d4 = w.d_eta[slot], b4 = w.beta[slot], L4 = w.L[slot];
+        float4 hit = w.hit[slot];
+        V3 ro{ o4.x, o4.y, o4.z }, rd{ d4.x, d4.y, d4.z };
+        float prev_pdf = o4.w, eta_scale = d4.w;
+        Spec beta{ b4.x, b4.y, b4.z }, L{ L4.x, L4.y, L4.z };
+        uint64_t rng = w.rng[slot];
+        int32_t fl = w.flags[slot];
+        int32_t bounce = fl & 0xffff;
+        bool specular_bounce = (fl & kSpecularBit) != 0;
+        bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
+
+        if (g.train)
+        {
+            int32_t r = g.rec_id[slot];
+            if (r >= 0)
+            {
+                float* rr = g.rec + size_t(r) * kRecFloats;
+                rr[17] = L.r;
+                rr[18] = L.g;
+                rr[19] = L.b;
+                g.rec_id[slot] = -1;
+            }
+        }
+
+        bool cont = false, guided = false;
+        int32_t prim = __float_as_int(hit.x);
+        if (prim < 0)
+        {
+            AddEscaped(s, beta, bounce, specular_bounce, prev_pdf, &L);
+        }
+        else
+        {
+            int4 info = s.prim_info[prim];
+            Isect is = MakeIsect(s, info, hit, ro, rd);
+            V3 wo = Normalize(-rd);
+            if (info.w >= 0)
+            {
+                const LightDev& l = s.lights[info.w];
+                Spec Le = (is.front_face || l.two_sided) ? Spec{ l.L[0], l.L[1], l.L[2] } : spec(0);
+                if (!IsBlack(Le))
+                {
+                    if (bounce == 0 || specular_bounce)
+                    {
+                        L = L + beta * Le;
+                    }
+                    else
+                    {
+                        float light_pdf = ShapePdf(s, info, is, ro, rd) * s.light_pmf[info.w];
+                        L = L + beta * PowerHeuristic(prev_pdf, light_pdf) * Le;
+                    }
+                }
+            }
+            if (bounce++ >= s.max_bounces)
+            {
+            }
+            else if (info.z < 0)
+            {
+                ro = is.point;
+                rd = -wo;
+                --bounce;
+                cont = true;
+            }
+            else
+            {
+                const MaterialDev& mat = s.materials[info.z];
+                BSDF bsdf = MakeBSDF(mat, is.sn, is.st, is.front_face);
+                if (s.regularize && any_non_specular)
+                {
+                    RegularizeBSDF(&bsdf);
+                }
+                if (IsNonSpecular(bsdf.flags))
+                {
+                    guided = true;
+                    float* r = g.raw + size_t(slot) * kGuideRaw;
+                    r[0] = is.point.x;
+                    r[1] = is.point.y;
+                    r[2] = is.point.z;
+                    r[3] = is.sn.x;
+                    r[4] = is.sn.y;
+                    r[5] = is.sn.z;
+                    r[6] = wo.x;
+                    r[7] = wo.y;
+                    r[8] = wo.z;
+                    r[9] = GuideRoughness(mat);
+                    float4* v = g.vtx + 4 * size_t(slot);
+                    v[0] = make_float4(is.point.x, is.point.y, is.point.z, __int_as_float(info.z));
+                    v[1] = make_float4(is.sn.x, is.sn.y, is.sn.z, is.front_face ? 1.0f : 0.0f);
+                    v[2] = make_float4(is.st.x, is.st.y, is.st.z, 0.0f);
+                    v[3] = make_float4(wo.x, wo.y, wo.z, 0.0f);
+                }
+                else
+                {
+                    P2 u12 = Next2D(rng);
+                    float u0 = Next1D(rng);
+                    BSDFSample bs;
+                    if (bsdf.Sample(&bs, wo, u0, u12))
+                    {
+                        bool spec_sample = (bs.flags & kFlagSpecular) != 0;
+                        specular_bounce = spec_sample;
+                        any_non_specular = any_non_specular || !spec_sample;
+                        if (bs.flags & kFlagTransmission)
+                        {
+                            eta_scale *= Sqr(bs.eta);
+                        }
+                        prev_pdf = bs.pdf;
+                        beta = beta * (bs.f * AbsDot(is.sn, bs.wi) / bs.pdf);
+                        ro = is.point;
+                        rd = bs.wi;
+                        cont = true;
+                        if (bounce > s.rr_min_bounces)
+                        {
+                            float p = MaxComponent(beta) * eta_scale;
+                            if (p < 1)
+                            {
+                                if (Next1D(rng) > p)
+                                {
+                                    cont = false;
+                                }
+                                else
+                                {
+                                    beta = beta / p;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        w.L[slot] = make_float4(L.r, L.g, L.b, 0.0f);
+        if (cont || guided)
+        {
+            w.o_pdf[slot] = make_float4(ro.x, ro.y, ro.z, prev_pdf);
+            w.d_eta[slot] = make_float4(rd.x, rd.y, rd.z, eta_scale);
+            w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
+            w.rng[slot] = rng;
+            w.flags[slot] = bounce | (specular_bounce ? kSpecularBit : 0) | (any_non_specular ? kAnyNonSpecularBit : 0);
+        }
+        int32_t qi = Append(&w.counts[parity ^ 1], cont);
+        if (cont)
+        {
+            q_next[qi] = slot;
+        }
+        int32_t gi = Append(&w.counts[5], guided);
+        if (guided)
+        {
+            g.queue[gi] = slot;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, GuideDev g, int parity)
+{
+    int32_t* q_next = w.queue[parity ^ 1];
+    const int32_t n = w.counts[5];
+    const int64_t wave_base = w.wave[0];
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        int32_t slot = g.queue[j];
+        float4 d4 = w.d_eta[slot], b4 = w.beta[slot];
+        float eta_scale = d4.w;
+        Spec beta{ b4.x, b4.y, b4.z };
+        uint64_t rng = w.rng[slot];
+        int32_t fl = w.flags[slot];
+        int32_t bounce = fl & 0xffff;
+        bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
+        const float4* v = g.vtx + 4 * size_t(slot);
+        float4 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+        V3 point{ v0.x, v0.y, v0.z }, sn{ v1.x, v1.y, v1.z }, st{ v2.x, v2.y, v2.z }, wo{ v3.x, v3.y, v3.z };
+        const MaterialDev& mat = s.materials[__float_as_int(v0.w)];
+        BSDF bsdf = MakeBSDF(mat, sn, st, v1.w != 0.0f);
+        if (s.regularize && any_non_specular)
+        {
+            RegularizeBSDF(&bsdf);
+        }
+        VmfMixture mix = MakeMixture(g.out + size_t(slot) * kGuideOut);
+
+        // Next-event estimation, MIS against the continuation mixture pdf.
+        bool shadow = false;
+        V3 sh_d{};
+        float sh_t = 0;
+        Spec sh_c{};
+        {
+            float u0 = Next1D(rng);
+            P2 u12 = Next2D(rng);
+            if (s.n_lights > 0)
+            {
+                float pmf;
+                int32_t li = SampleLight(s, u0, &pmf);
+                const LightDev& l = s.lights[li];
+                V3 tri[3];
+                const bbg_sphere* sph = nullptr;
+                bool on_tri = false;
+                if (l.type == BBG_LIGHT_DIFFUSE_AREA)
+                {
+                    int4 linfo = s.prim_info[l.prim];
+                    if (linfo.x == BBG_PRIM_TRIANGLE)
+                    {
+                        int32_t vv[3];
+                        TriVerts(s, linfo.y, vv, tri);
+                        on_tri = true;
+                    }
+                    else
+                    {
+                        sph = &s.spheres[linfo.y];
+                    }
+                }
+                LightSampleLi ls;
+                if (SampleLi(l, point, u12, on_tri ? tri : nullptr, sph, &ls))
+                {
+                    float bsdf_pdf = bsdf.PDF(wo, ls.wi);
+                    if (!(IsBlack(ls.Li) || bsdf_pdf == 0))
+                    {
+                        float light_pdf = pmf * ls.pdf;
+                        Spec f_cos = bsdf.F(wo, ls.wi) * AbsDot(sn, ls.wi);
+                        if (IsDeltaLight(l.type))
+                        {
+                            sh_c = beta * ls.Li * f_cos / light_pdf;
+                        }
+                        else
+                        {
+                            float mix_pdf = 0.5f * MixturePdf(mix, ls.wi) + 0.5f * bsdf_pdf;
+                            sh_c = beta * PowerHeuristic(light_pdf, mix_pdf) * ls.Li * f_cos / light_pdf;
+                        }
+                        shadow = true;
+                        sh_d = ls.wi;
+                        sh_t = ls.visibility;
+                    }
+                }
+            }
+        }
+
+        // Continuation: guide or BSDF with probability 1/2 each.
+        bool cont = false;
+        float u_sel = Next1D(rng);
+        P2 u12 = Next2D(rng);
+        float u0 = Next1D(rng);
+        V3 wi;
+        bool have = false;
+        if (u_sel < 0.5f)
+        {
+            wi = MixtureSample(mix, u0, u12.x, u12.y);
+            have = true;
+        }
+        else
+        {
+            BSDFSample bs;
+            have = bsdf.Sample(&bs, wo, u0, u12);
+            wi = bs.wi;
+        }
+        float pdf = 0;
+        if (have)
+        {
+            float pdf_b = bsdf.PDF(wo, wi);
+            pdf = 0.5f * MixturePdf(mix, wi) + 0.5f * pdf_b;
+            Spec f = bsdf.F(wo, wi);
+            float cosv = AbsDot(sn, wi);
+            if (pdf > 0 && !IsBlack(f) && cosv > 0)
+            {
+                if (mat.type == BBG_MAT_DIELECTRIC)
+                {
+                    float cz_o = Dot(wo, sn), cz_i = Dot(wi, sn);
+                    if (cz_o * cz_i < 0)
+                    {
+                        float eta_p = cz_o > 0 ? bsdf.eta : 1 / bsdf.eta;
+                        eta_scale *= Sqr(eta_p);
+                    }
+                }
+                beta = beta * (f * cosv / pdf);
+                cont = true;
+                if (bounce > s.rr_min_bounces)
+                {
+                    float p = MaxComponent(beta) * eta_scale;
+                    if (p < 1)
+                    {
+                        if (Next1D(rng) > p)
+                        {
+                            cont = false;
+                        }
+                        else
+                        {
+                            beta = beta / p;
+                        }
+                    }
+                }
+            }
+        }
+        if (g.train && pdf > 0 && (wave_base + slot) % g.stride == 0)
+        {
+            int32_t r = atomicAdd(&w.counts[6], 1);
+            if (r < g.rec_cap)
+            {
+                float* rr = g.rec + size_t(r) * kRecFloats;
+                const float* raw = g.raw + size_t(slot) * kGuideRaw;
+                for (int k = 0; k < kGuideRaw; ++k)
+                {
+                    rr[k] = raw[k];
+                }
+                rr[10] = wi.x;
+                rr[11] = wi.y;
+                rr[12] = wi.z;
+                rr[13] = pdf;
+                rr[14] = cont ? beta.r : 0.0f;
+                rr[15] = cont ? beta.g : 0.0f;
+                rr[16] = cont ? beta.b : 0.0f;
+                rr[17] = NAN; // filled at the path's next shading pass
+                g.rec_slot[r] = slot;
+                g.rec_id[slot] = cont ? r : -1;
+            }
+        }
+        if (cont)
+        {
+            w.o_pdf[slot] = make_float4(point.x, point.y, point.z, pdf);
+            w.d_eta[slot] = make_float4(wi.x, wi.y, wi.z, eta_scale);
+            w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
+            w.flags[slot] = bounce | kAnyNonSpecularBit;
+        }
+        w.rng[slot] = rng;
+        int32_t qi = Append(&w.counts[parity ^ 1], cont);
+        if (cont)
+        {
+            q_next[qi] = slot;
+        }
+        int32_t si = Append(&w.counts[2], shadow);
+        if (shadow)
+        {
+            w.sh_o[si] = make_float4(point.x, point.y, point.z, sh_t);
+            w.sh_d[si] = make_float4(sh_d.x, sh_d.y, sh_d.z, __int_as_float(slot));
+            w.sh_c[si] = make_float4(sh_c.r, sh_c.g, sh_c.b, 0.0f);
+        }
+    }
+}
+
+// Training targets of the wave's records: the radiance the path brought back
+// along the sampled direction, L(end) - L(at the next shading pass), divided
+// by the throughput after the vertex; weight = its luminance / sampling pdf.
+// Weights are then normalised to mean 1 (GuideNormalizeKernel).
+__global__ void GuideFinalizeKernel(WaveDev w, GuideDev g)
+{
+    int32_t n = min(w.counts[6], g.rec_cap);
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        w.counts[7] = n;
+    }
+    float local = 0;
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    {
+        const float* rr = g.rec + size_t(r) * kRecFloats;
+        float4 Lf = w.L[g.rec_slot[r]];
+        bool started = !isnan(rr[17]);
+        Spec cont = started ? Spec{ Lf.x - rr[17], Lf.y - rr[18], Lf.z - rr[19] } : spec(0);
+        Spec li{ rr[14] > 0 ? cont.r / rr[14] : 0.0f, rr[15] > 0 ? cont.g / rr[15] : 0.0f,
+                 rr[16] > 0 ? cont.b / rr[16] : 0.0f };
+        float wgt = fmaxf(Luminance(li), 0.0f) / rr[13];
+        if (!isfinite(wgt))
+        {
+            wgt = 0;
+        }
+        for (int k = 0; k < kGuideRaw; ++k)
+        {
+            g.t_raw[size_t(r) * kGuideRaw + k] = rr[k];
+        }
+        g.t_dir[3 * size_t(r)] = rr[10];
+        g.t_dir[3 * size_t(r) + 1] = rr[11];
+        g.t_dir[3 * size_t(r) + 2] = rr[12];
+        g.t_w[r] = wgt;
+        local += wgt;
+    }
+    for (int off = 16; off > 0; off >>= 1)
+    {
+        local += __shfl_xor_sync(0xffffffffu, local, off);
+    }
+    if ((threadIdx.x & 31) == 0 && local != 0.0f)
+    {
+        atomicAdd(g.wsum, local);
+    }
+}
+
+__global__ void GuideNormalizeKernel(WaveDev w, GuideDev g)
+{
+    int32_t n = w.counts[7];
+    float sum = *g.wsum;
+    float scale = sum > 0 ? float(n) / sum : 0.0f;
+    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    {
+        g.t_w[r] *= scale;
+    }
+}
+
+// Clears the next level's ray queue, the shadow queue, the work counters of
+// the persistent closest-hit and shadow passes and the guide-query queue.
 __global__ void ResetKernel(WaveDev w, int parity)
 {
     w.counts[parity ^ 1] = 0;
     w.counts[2] = 0;
     w.counts[3] = 0;
     w.counts[4] = 0;
+    w.counts[5] = 0;
 }
 
 // ---------------------------------------------------------------- film
@@ -710,12 +1167,80 @@ struct bbg_integrator
     DevBuf<float> film_rgb, film_moments, film_path_L;
     DevBuf<int32_t> film_count;
 
+    // Guided rendering: per-slot query / output / vertex state, training records.
+    int64_t g_capacity = 0;
+    int32_t g_rec_cap = 0;
+    DevBuf<float> g_raw, g_out, g_rec, g_traw, g_tdir, g_tw, g_wsum;
+    DevBuf<float4> g_vtx;
+    DevBuf<int32_t> g_queue, g_recid, g_recslot;
+
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
     int64_t graph_capacity = -1;
     int graph_iterations = -1;
     FilmDev graph_film{};
     SceneDev graph_scene{};
+    GuideDev graph_guide{};
+    bbg_guide* graph_guide_handle = nullptr;
+    float graph_guide_lr = 0;
+
+    bbg_status ReserveGuide(int64_t n, int32_t rec_cap)
+    {
+        if (n > g_capacity)
+        {
+            size_t m = size_t(n);
+            for (auto* b : { &g_raw, &g_out })
+            {
+                b->reset();
+            }
+            g_vtx.reset();
+            g_queue.reset();
+            g_recid.reset();
+            BBG_TRY(g_raw.alloc(m * kGuideRaw));
+            BBG_TRY(g_out.alloc(m * kGuideOut));
+            BBG_TRY(g_vtx.alloc(4 * m));
+            BBG_TRY(g_queue.alloc(m));
+            BBG_TRY(g_recid.alloc(m));
+            g_capacity = n;
+        }
+        if (rec_cap > g_rec_cap)
+        {
+            size_t r = size_t(rec_cap);
+            for (auto* b : { &g_rec, &g_traw, &g_tdir, &g_tw })
+            {
+                b->reset();
+            }
+            g_recslot.reset();
+            BBG_TRY(g_rec.alloc(r * kRecFloats));
+            BBG_TRY(g_traw.alloc(r * kGuideRaw));
+            BBG_TRY(g_tdir.alloc(r * 3));
+            BBG_TRY(g_tw.alloc(r));
+            BBG_TRY(g_recslot.alloc(r));
+            g_rec_cap = rec_cap;
+        }
+        BBG_TRY(g_wsum.alloc(1));
+        return BBG_OK;
+    }
+
+    GuideDev Guide(int32_t train, int32_t stride) const
+    {
+        GuideDev g{};
+        g.raw = g_raw.p;
+        g.out = g_out.p;
+        g.vtx = g_vtx.p;
+        g.queue = g_queue.p;
+        g.rec_id = g_recid.p;
+        g.rec = g_rec.p;
+        g.rec_slot = g_recslot.p;
+        g.t_raw = g_traw.p;
+        g.t_dir = g_tdir.p;
+        g.t_w = g_tw.p;
+        g.wsum = g_wsum.p;
+        g.rec_cap = g_rec_cap;
+        g.stride = stride;
+        g.train = train;
+        return g;
+    }
 
     ~bbg_integrator()
     {
@@ -771,7 +1296,7 @@ namespace
 
 struct Grids
 {
-    int raygen, closest, shade, shadow, film;
+    int raygen, closest, shade, shadow, film, shade_a, shade_b;
     Grids()
     {
         raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel), kBlock);
@@ -779,29 +1304,85 @@ struct Grids
         shade = PersistentGrid(reinterpret_cast<const void*>(ShadeKernel), kBlock);
         shadow = PersistentGrid(reinterpret_cast<const void*>(ShadowKernel), kBlock);
         film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel), kBlock);
+        shade_a = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeA), kBlock);
+        shade_b = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeB), kBlock);
     }
 };
 
-void EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, int parity, cudaStream_t st)
+// Guided-rendering context of one render (guide == nullptr: plain).
+struct GuideCtx
+{
+    bbg_guide* guide = nullptr;
+    GuideDev dev{};
+    float lr = 0;
+};
+
+__global__ void GuideWaveStartKernel(WaveDev w, GuideDev g)
+{
+    const int64_t n = w.wave[1];
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        g.rec_id[i] = -1;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+    {
+        w.counts[6] = 0;
+        *g.wsum = 0;
+    }
+}
+
+bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, const GuideCtx& gc, int parity,
+                        cudaStream_t st)
 {
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
     ClosestKernel<<<gr.closest, kBlock, 0, st>>>(s, w, parity);
-    ShadeKernel<<<gr.shade, kBlock, 0, st>>>(s, w, parity);
+    if (gc.guide)
+    {
+        GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(s, w, gc.dev, parity);
+        BBG_TRY(GuideForward(gc.guide, gc.dev.raw, gc.dev.queue, w.counts + 5, 0, gc.dev.out, st));
+        GuidedShadeB<<<gr.shade_b, kBlock, 0, st>>>(s, w, gc.dev, parity);
+    }
+    else
+    {
+        ShadeKernel<<<gr.shade, kBlock, 0, st>>>(s, w, parity);
+    }
     ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(s, w);
+    return BBG_OK;
 }
 
-bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const FilmDev& film, int iterations,
-                   cudaStream_t st)
+bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const FilmDev& film, const GuideCtx& gc,
+                   int iterations, cudaStream_t st)
 {
     WaveDev w = I->Wave();
     RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(s, w);
+    if (gc.guide && gc.dev.train)
+    {
+        GuideWaveStartKernel<<<gr.raygen, kBlock, 0, st>>>(w, gc.dev);
+    }
     for (int k = 0; k < iterations; ++k)
     {
-        EnqueueLevel(gr, s, w, k & 1, st);
+        BBG_TRY(EnqueueLevel(gr, s, w, gc, k & 1, st));
     }
     FilmKernel<<<gr.film, kBlock, 0, st>>>(s, w, film);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
+}
+
+// One online training step on the wave's records (after all its levels).
+bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, cudaStream_t st)
+{
+    WaveDev w = I->Wave();
+    GuideFinalizeKernel<<<256, 256, 0, st>>>(w, gc.dev);
+    GuideNormalizeKernel<<<256, 256, 0, st>>>(w, gc.dev);
+    BBG_TRY(GuideAccumulate(gc.guide, gc.dev.t_raw, gc.dev.t_dir, gc.dev.t_w, w.counts + 7, 0, st));
+    BBG_TRY(GuideApply(gc.guide, gc.lr, w.counts + 7, 0, st));
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bool SameGuide(const GuideDev& a, const GuideDev& b)
+{
+    return std::memcmp(&a, &b, sizeof(GuideDev)) == 0;
 }
 
 bool SameScene(const SceneDev& a, const SceneDev& b)
@@ -903,11 +1484,28 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     BBG_CUDA(cudaEventCreate(&e1));
     BBG_CUDA(cudaEventRecord(e0, st));
 
+    GuideCtx gc;
+    if (p->guide)
+    {
+        gc.guide = p->guide;
+        gc.lr = p->guide_lr > 0 ? p->guide_lr : 1e-2f;
+        int32_t batch = p->guide_batch > 0 ? p->guide_batch : (1 << 16);
+        // Record every stride-th path so a wave yields about one batch
+        // (about two guided vertices per path).
+        int32_t stride = int32_t(std::max<int64_t>(1, (2 * wave_paths + batch - 1) / batch));
+        BBG_TRY(I->ReserveGuide(wave_paths, p->guide_train ? batch : 0));
+        gc.dev = I->Guide(p->guide_train ? 1 : 0, stride);
+        int dummy;
+        BBG_TRY(GuidePrepare(gc.guide, &dummy));
+    }
+
     const int iterations = I->max_bounces + 1;
     const Grids gr;
     bool use_graph = p->use_graph != 0;
     if (use_graph && (!I->graph || I->graph_capacity != wave_paths || I->graph_iterations != iterations ||
-                      !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f)))
+                      !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f) ||
+                      I->graph_guide_handle != gc.guide || !SameGuide(I->graph_guide, gc.dev) ||
+                      I->graph_guide_lr != gc.lr))
     {
         if (I->graph)
         {
@@ -916,7 +1514,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         cudaGraph_t g;
         BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        bbg_status es = Enqueue(I, gr, s, f, iterations, st);
+        bbg_status es = Enqueue(I, gr, s, f, gc, iterations, st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         BBG_TRY(es);
         if (ce != cudaSuccess)
@@ -929,6 +1527,9 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         I->graph_iterations = iterations;
         I->graph_scene = s;
         I->graph_film = f;
+        I->graph_guide = gc.dev;
+        I->graph_guide_handle = gc.guide;
+        I->graph_guide_lr = gc.lr;
     }
 
     for (int64_t base = 0; base < n_paths; base += wave_paths)
@@ -944,7 +1545,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         else
         {
-            BBG_TRY(Enqueue(I, gr, s, f, iterations, st));
+            BBG_TRY(Enqueue(I, gr, s, f, gc, iterations, st));
         }
         // Paths still queued after max_bounces + 1 levels only come from
         // material-less surfaces, which do not count a bounce
@@ -960,7 +1561,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
             {
                 return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
             }
-            EnqueueLevel(gr, s, I->Wave(), parity, st);
+            BBG_TRY(EnqueueLevel(gr, s, I->Wave(), gc, parity, st));
             parity ^= 1;
             BBG_CUDA(cudaMemcpyAsync(&left, I->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             BBG_CUDA(cudaStreamSynchronize(st));
@@ -969,6 +1570,10 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         {
             // Re-run the film pass for this wave after the extra levels.
             FilmKernel<<<gr.film, kBlock, 0, st>>>(s, I->Wave(), f);
+        }
+        if (gc.guide && gc.dev.train)
+        {
+            BBG_TRY(EnqueueTraining(I, gc, st));
         }
     }
     BBG_CUDA(cudaEventRecord(e1, st));

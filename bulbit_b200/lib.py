@@ -234,7 +234,7 @@ class GpuPathIntegrator:
         return out[:len(self.scene.lights)]
 
     def render(self, spp=None, seed=None, camera_spec=None, wave_paths=0, use_graph=True, light_alias=False,
-               path_L=False):
+               path_L=False, guide=None, train=False, batch=0, lr=0.0):
         s = self.scene
         spec = camera_spec or s.camera
         cam = camera(spec)
@@ -245,6 +245,10 @@ class GpuPathIntegrator:
         p.wave_paths = wave_paths
         p.use_graph = 1 if use_graph else 0
         p.light_alias = 1 if light_alias else 0
+        p.guide = guide.h if guide is not None else None
+        p.guide_train = 1 if train else 0
+        p.guide_batch = batch
+        p.guide_lr = lr
         film = Film(cam.width, cam.height, spp, path_L=path_L)
         fs = film.struct()
         check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(p), C.byref(fs), abi.BBG_MEM_HOST,

@@ -337,6 +337,14 @@ typedef struct bbg_render_params
     int32_t use_graph;    /* capture the bounce loop of a wave in a CUDA graph */
     int32_t light_alias;  /* 1: sample lights with a Walker alias table (same
                              pmf, different stream) instead of CDF inversion */
+    struct bbg_guide* guide; /* NULL: the reference's estimator. Otherwise, at
+                                non-specular vertices, one-sample MIS between
+                                the guide and the BSDF (probability 1/2 each;
+                                a different random stream, same expectation) */
+    int32_t guide_train;  /* 1: train the guide online on this render's paths,
+                             one Adam step per wave */
+    int32_t guide_batch;  /* training samples per step (0: 65536) */
+    float guide_lr;       /* Adam learning rate (0: 1e-2) */
 } bbg_render_params;
 
 /* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields

@@ -1,0 +1,80 @@
+"""Guided path tracing on the GPU: one-sample MIS between the neural vMF
+guide and the BSDF. The plain path tracer is the judge:
+
+* unbiased: the guided image mean agrees with the plain one within their Monte
+  Carlo standard errors (4 sigma), with an untrained and a trained guide;
+* training helps: against a high-spp plain reference, the relMSE of the same
+  guided estimator is lower with the trained guide than with the untrained one
+  (what the learned network gains over the method without it);
+* the plain renders are unchanged by the presence of guiding code (the parity
+  tests of test_render_gpu.py run without a guide)."""
+import numpy as np
+import pytest
+
+from bulbit_b200 import lib, scenes
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_mse(img, ref):
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def mean_and_se(film):
+    img = film.image()
+    lum = 0.2126 * img[..., 0] + 0.7152 * img[..., 1] + 0.0722 * img[..., 2]
+    n = film.count.astype(np.float64)
+    var = np.maximum(0.0, film.moments[..., 1] - film.moments[..., 0] ** 2) * np.where(n > 1, n / (n - 1), 1)
+    se = np.sqrt(np.sum(var / np.maximum(n, 1))) / lum.size
+    return float(np.nanmean(lum)), float(se)
+
+
+@pytest.fixture(scope="module")
+def setup():
+    scene = scenes.cornell_icosphere(levels=5, width=64, height=64, spp=64, max_bounces=12)
+    acc = lib.GpuAccel(scene)
+    integ = lib.GpuPathIntegrator(acc, scene)
+    return scene, acc, integ
+
+
+def test_guided_estimator_is_unbiased(setup):
+    scene, acc, integ = setup
+    plain = integ.render(spp=512, seed=1)
+    guide = lib.GpuGuide(acc.bounds(), seed=3)
+    untrained = integ.render(spp=512, seed=2, guide=guide)
+    for i in range(20):
+        integ.render(spp=16, seed=100 + i, guide=guide, train=True, wave_paths=1 << 14)
+    trained = integ.render(spp=512, seed=3, guide=guide)
+    mp, sp = mean_and_se(plain)
+    for name, film in (("untrained", untrained), ("trained", trained)):
+        mg, sg = mean_and_se(film)
+        print(f"{name}: guided mean {mg:.5f} +- {sg:.5f}, plain {mp:.5f} +- {sp:.5f}")
+        assert abs(mg - mp) <= 4 * np.hypot(sg, sp)
+
+
+def test_training_lowers_relmse(setup):
+    scene, acc, integ = setup
+    ref = integ.render(spp=8192, seed=7).image()
+    untrained = lib.GpuGuide(acc.bounds(), seed=5)
+    trained = lib.GpuGuide(acc.bounds(), seed=5)
+    losses_seen = 0
+    for i in range(60):
+        integ.render(spp=16, seed=200 + i, guide=trained, train=True, wave_paths=1 << 14)
+        losses_seen += 1
+    e_plain, e_untrained, e_trained = [], [], []
+    for k in range(3):
+        e_plain.append(rel_mse(integ.render(spp=64, seed=50 + k).image(), ref))
+        e_untrained.append(rel_mse(integ.render(spp=64, seed=60 + k, guide=untrained).image(), ref))
+        e_trained.append(rel_mse(integ.render(spp=64, seed=70 + k, guide=trained).image(), ref))
+    p, u, t = np.mean(e_plain), np.mean(e_untrained), np.mean(e_trained)
+    print(f"relMSE at 64 spp: plain {p:.4e}, guided untrained {u:.4e}, guided trained {t:.4e} "
+          f"(trained/plain {t / p:.3f}, trained/untrained {t / u:.3f})")
+    assert t < u
+
+
+def test_guided_render_is_deterministic_and_graph_safe(setup):
+    scene, acc, integ = setup
+    guide = lib.GpuGuide(acc.bounds(), seed=9)
+    a = integ.render(spp=16, seed=4, guide=guide, path_L=True)
+    b = integ.render(spp=16, seed=4, guide=guide, path_L=True, use_graph=False, wave_paths=4096)
+    assert np.array_equal(a.path_L, b.path_L)
