@@ -100,7 +100,8 @@ class Camera(C.Structure):
 class RenderParams(C.Structure):
     _fields_ = [("spp", C.c_int32), ("seed", C.c_int32), ("wave_paths", C.c_int64),
                 ("use_graph", C.c_int32), ("light_alias", C.c_int32), ("guide", C.c_void_p),
-                ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float)]
+                ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float),
+                ("guide_select", C.c_float)]
 
 
 class Film(C.Structure):
@@ -142,6 +143,8 @@ EXPORTS = [
     ("bbg_guide_forward", I32, [P, P, I64, P]),
     ("bbg_guide_gradient", I32, [P, P, P, P, I64, P, P]),
     ("bbg_guide_train_step", I32, [P, P, P, P, I64, C.c_float, P]),
+    ("bbg_guide_mixture_sample", I32, [P, P, I64, P, P]),
+    ("bbg_guide_mixture_pdf", I32, [P, P, I64, P]),
     ("bbg_last_error", C.c_char_p, []),
     ("bbg_version", C.c_char_p, []),
 ]

@@ -5,6 +5,7 @@
 
 #include "guide.cuh"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <random>
@@ -677,7 +678,97 @@ bbg_status Stage(bbg_guide* G, const float* raw, const float* dirs, const float*
 
 } // namespace
 
+namespace bbg
+{
+
+// The vMF mixture of each output row, sampled or evaluated as the guided
+// renderer does (MakeMixture, MixtureSample, MixturePdf).
+__global__ void MixtureSampleKernel(const float* outputs, const float* u, int64_t n, float* dirs, float* pdf)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        VmfMixture m = MakeMixture(outputs + i * kGuideOut);
+        V3 w = MixtureSample(m, u[3 * i], u[3 * i + 1], u[3 * i + 2]);
+        dirs[3 * i] = w.x;
+        dirs[3 * i + 1] = w.y;
+        dirs[3 * i + 2] = w.z;
+        pdf[i] = MixturePdf(m, w);
+    }
+}
+
+__global__ void MixturePdfKernel(const float* outputs, const float* dirs, int64_t n, float* pdf)
+{
+    for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+    {
+        VmfMixture m = MakeMixture(outputs + i * kGuideOut);
+        pdf[i] = MixturePdf(m, V3{ dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2] });
+    }
+}
+
+// Host-buffer driver of the two kernels above: stages outputs and the
+// second input (uniforms or directions), runs one of them, copies back.
+bbg_status MixtureRun(const float* outputs, const float* in, int64_t n, float* dirs_out, float* pdf_out,
+                      cudaStream_t st)
+{
+    DevBuf<float> d_out, d_in, d_dirs, d_pdf;
+    BBG_TRY(d_out.upload(outputs, size_t(n) * kGuideOut, st));
+    BBG_TRY(d_in.upload(in, size_t(n) * 3, st));
+    BBG_TRY(d_pdf.alloc(size_t(n)));
+    int grid = int(std::min<int64_t>((n + 255) / 256, 148 * 16));
+    if (dirs_out)
+    {
+        BBG_TRY(d_dirs.alloc(size_t(n) * 3));
+        MixtureSampleKernel<<<grid, 256, 0, st>>>(d_out.p, d_in.p, n, d_dirs.p, d_pdf.p);
+        BBG_CUDA(cudaGetLastError());
+        BBG_CUDA(cudaMemcpyAsync(dirs_out, d_dirs.p, sizeof(float) * 3 * size_t(n), cudaMemcpyDeviceToHost, st));
+    }
+    else
+    {
+        MixturePdfKernel<<<grid, 256, 0, st>>>(d_out.p, d_in.p, n, d_pdf.p);
+        BBG_CUDA(cudaGetLastError());
+    }
+    BBG_CUDA(cudaMemcpyAsync(pdf_out, d_pdf.p, sizeof(float) * size_t(n), cudaMemcpyDeviceToHost, st));
+    BBG_CUDA(cudaStreamSynchronize(st));
+    return BBG_OK;
+}
+
+bbg_status MixtureCall(const float* outputs, const float* in, int64_t n, float* dirs_out, float* pdf_out)
+{
+    BBG_TRY(CheckDevice());
+    cudaStream_t st;
+    BBG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    bbg_status status = MixtureRun(outputs, in, n, dirs_out, pdf_out, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return status;
+}
+
+} // namespace bbg
+
+namespace
+{
+
+} // namespace
+
 extern "C" {
+
+bbg_status bbg_guide_mixture_sample(const float* outputs, const float* u, int64_t n, float* dirs_out, float* pdf_out)
+{
+    if (n < 0 || (n > 0 && (!outputs || !u || !dirs_out || !pdf_out)))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_mixture_sample: bad argument");
+    }
+    return n == 0 ? BBG_OK : MixtureCall(outputs, u, n, dirs_out, pdf_out);
+}
+
+bbg_status bbg_guide_mixture_pdf(const float* outputs, const float* dirs, int64_t n, float* pdf_out)
+{
+    if (n < 0 || (n > 0 && (!outputs || !dirs || !pdf_out)))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_mixture_pdf: bad argument");
+    }
+    return n == 0 ? BBG_OK : MixtureCall(outputs, dirs, n, nullptr, pdf_out);
+}
 
 bbg_status bbg_guide_create(const float* scene_aabb, uint64_t seed, bbg_guide** out)
 {

@@ -608,13 +608,13 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int
 // inference: GuidedShadeA does everything up to the BSDF and, at
 // non-specular vertices, queues the guide query; GuidedShadeB (after the
 // inference) does next-event estimation and the continuation with one-sample
-// MIS between the guide and the BSDF (selection probability 1/2). The
-// continuation pdf is the mixture 0.5 q + 0.5 p_bsdf, and both MIS weights
-// (light samples here, emitted light at the next hit) use it, so the
-// estimator stays unbiased whatever the network outputs. Specular vertices
-// continue as in the plain tracer. Training records take (query, direction,
-// pdf, throughput) at sampled vertices and the radiance the rest of the path
-// brings back along that direction.
+// MIS between the guide and the BSDF (guide selection probability s, 1/2 by
+// default). The continuation pdf is the mixture s q + (1 - s) p_bsdf, and
+// both MIS weights (light samples here, emitted light at the next hit) use
+// it, so the estimator stays unbiased whatever the network outputs. Specular
+// vertices continue as in the plain tracer. Training records take (query,
+// direction, pdf, throughput) at sampled vertices and the radiance the rest
+// of the path brings back along that direction.
 
 struct GuideDev
 {
@@ -623,7 +623,8 @@ struct GuideDev
     float4* vtx;       // per slot: (point, material), (sn, front), (st, -), (wo, -)
     int32_t* queue;    // slots with a guide query this level
     int32_t* rec_id;   // per slot: open training record or -1
-    float* rec;        // per record: raw (10), dir (3), pdf, beta after the vertex (3), L at next shade (3)
+    float* rec;        // per record: raw (10), unit dir (3), pdf, throughput into the vertex over the
+                       // RR survival probability (3), L at the next shading pass (3)
     int32_t* rec_slot;
     float* t_raw;      // training batch: raw queries, directions, weights
     float* t_dir;
@@ -632,6 +633,7 @@ struct GuideDev
     int32_t rec_cap;
     int32_t stride;    // paths with index % stride == 0 record training samples
     int32_t train;
+    float select;      // probability of sampling the guide rather than the BSDF
 };
 
 constexpr int kRecFloats = 20;
@@ -889,7 +891,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
                         }
                         else
                         {
-                            float mix_pdf = 0.5f * MixturePdf(mix, ls.wi) + 0.5f * bsdf_pdf;
+                            float mix_pdf = g.select * MixturePdf(mix, ls.wi) + (1.0f - g.select) * bsdf_pdf;
                             sh_c = beta * PowerHeuristic(light_pdf, mix_pdf) * ls.Li * f_cos / light_pdf;
                         }
                         shadow = true;
@@ -900,62 +902,79 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
             }
         }
 
-        // Continuation: guide or BSDF with probability 1/2 each.
+        // Continuation: the guide with probability g.select, else the BSDF.
+        // A BSDF sample is weighted with its own f and pdf, as the plain
+        // tracer does: where the shading frame is not orthonormal (normals
+        // and tangents are interpolated independently, see MakeIsect) those
+        // differ from f() and PDF() at the world direction, and only the
+        // sample's own values keep the plain estimator's expectation. A
+        // specular sample is a discrete mass the guide cannot produce; its
+        // probability is (1 - select) times the BSDF's.
         bool cont = false;
         float u_sel = Next1D(rng);
         P2 u12 = Next2D(rng);
         float u0 = Next1D(rng);
-        V3 wi;
-        bool have = false;
-        if (u_sel < 0.5f)
+        V3 wi{}, wdir{};
+        Spec f{};
+        float pdf = 0, cosv = 0, eta_sample = 1, rr_p = 1;
+        bool spec_sample = false, transmit = false;
+        const Spec beta_in = beta;
+        if (u_sel < g.select)
         {
             wi = MixtureSample(mix, u0, u12.x, u12.y);
-            have = true;
+            wdir = wi;
+            f = bsdf.F(wo, wi);
+            pdf = g.select * MixturePdf(mix, wi) + (1.0f - g.select) * bsdf.PDF(wo, wi);
+            cosv = AbsDot(sn, wi);
+            if (mat.type == BBG_MAT_DIELECTRIC)
+            {
+                float cz_o = Dot(wo, sn), cz_i = Dot(wi, sn);
+                transmit = cz_o * cz_i < 0;
+                eta_sample = cz_o > 0 ? bsdf.eta : 1 / bsdf.eta;
+            }
         }
         else
         {
             BSDFSample bs;
-            have = bsdf.Sample(&bs, wo, u0, u12);
-            wi = bs.wi;
-        }
-        float pdf = 0;
-        if (have)
-        {
-            float pdf_b = bsdf.PDF(wo, wi);
-            pdf = 0.5f * MixturePdf(mix, wi) + 0.5f * pdf_b;
-            Spec f = bsdf.F(wo, wi);
-            float cosv = AbsDot(sn, wi);
-            if (pdf > 0 && !IsBlack(f) && cosv > 0)
+            if (bsdf.Sample(&bs, wo, u0, u12))
             {
-                if (mat.type == BBG_MAT_DIELECTRIC)
+                wi = bs.wi;
+                wdir = Normalize(wi);
+                f = bs.f;
+                spec_sample = (bs.flags & kFlagSpecular) != 0;
+                pdf = spec_sample ? (1.0f - g.select) * bs.pdf
+                                  : g.select * MixturePdf(mix, wdir) + (1.0f - g.select) * bs.pdf;
+                cosv = AbsDot(sn, wi);
+                transmit = (bs.flags & kFlagTransmission) != 0;
+                eta_sample = bs.eta;
+            }
+        }
+        if (pdf > 0 && !IsBlack(f) && cosv > 0)
+        {
+            if (transmit)
+            {
+                eta_scale *= Sqr(eta_sample);
+            }
+            beta = beta * (f * cosv / pdf);
+            cont = true;
+            if (bounce > s.rr_min_bounces)
+            {
+                float p = MaxComponent(beta) * eta_scale;
+                if (p < 1)
                 {
-                    float cz_o = Dot(wo, sn), cz_i = Dot(wi, sn);
-                    if (cz_o * cz_i < 0)
+                    if (Next1D(rng) > p)
                     {
-                        float eta_p = cz_o > 0 ? bsdf.eta : 1 / bsdf.eta;
-                        eta_scale *= Sqr(eta_p);
+                        cont = false;
                     }
-                }
-                beta = beta * (f * cosv / pdf);
-                cont = true;
-                if (bounce > s.rr_min_bounces)
-                {
-                    float p = MaxComponent(beta) * eta_scale;
-                    if (p < 1)
+                    else
                     {
-                        if (Next1D(rng) > p)
-                        {
-                            cont = false;
-                        }
-                        else
-                        {
-                            beta = beta / p;
-                        }
+                        beta = beta / p;
+                        rr_p = p;
                     }
                 }
             }
         }
-        if (g.train && pdf > 0 && (wave_base + slot) % g.stride == 0)
+        if (g.train && pdf > 0 && !spec_sample && (wave_base + slot) % g.stride == 0)
         {
             int32_t r = atomicAdd(&w.counts[6], 1);
             if (r < g.rec_cap)
@@ -966,13 +985,13 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
                 {
                     rr[k] = raw[k];
                 }
-                rr[10] = wi.x;
-                rr[11] = wi.y;
-                rr[12] = wi.z;
+                rr[10] = wdir.x;
+                rr[11] = wdir.y;
+                rr[12] = wdir.z;
                 rr[13] = pdf;
-                rr[14] = cont ? beta.r : 0.0f;
-                rr[15] = cont ? beta.g : 0.0f;
-                rr[16] = cont ? beta.b : 0.0f;
+                rr[14] = cont ? beta_in.r / rr_p : 0.0f;
+                rr[15] = cont ? beta_in.g / rr_p : 0.0f;
+                rr[16] = cont ? beta_in.b / rr_p : 0.0f;
                 rr[17] = NAN; // filled at the path's next shading pass
                 g.rec_slot[r] = slot;
                 g.rec_id[slot] = cont ? r : -1;
@@ -983,7 +1002,8 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
             w.o_pdf[slot] = make_float4(point.x, point.y, point.z, pdf);
             w.d_eta[slot] = make_float4(wi.x, wi.y, wi.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
-            w.flags[slot] = bounce | kAnyNonSpecularBit;
+            w.flags[slot] = bounce | (spec_sample ? kSpecularBit : 0) |
+                            ((any_non_specular || !spec_sample) ? kAnyNonSpecularBit : 0);
         }
         w.rng[slot] = rng;
         int32_t qi = Append(&w.counts[parity ^ 1], cont);
@@ -1001,10 +1021,15 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
     }
 }
 
-// Training targets of the wave's records: the radiance the path brought back
-// along the sampled direction, L(end) - L(at the next shading pass), divided
-// by the throughput after the vertex; weight = its luminance / sampling pdf.
-// Weights are then normalised to mean 1 (GuideNormalizeKernel).
+// Training targets of the wave's records: the integrand's product f cos L_i
+// over the sampling pdf (the target of Mueller et al. 2019, "Neural
+// Importance Sampling"). The radiance the path gathered after the vertex is
+// dL = L(end) - L(at the next shading pass) = beta_in f cos L_i / (pdf p_rr),
+// so the weight f cos L_i / pdf = luminance(dL p_rr / beta_in). The next
+// hit's emission enters with its MIS weight, so on diffuse surfaces, where
+// NEE takes nearly all of it, the guide mostly learns indirect light, and on
+// glossy ones it learns the reflected light too. Weights are then
+// normalised to mean 1 (GuideNormalizeKernel).
 __global__ void GuideFinalizeKernel(WaveDev w, GuideDev g)
 {
     int32_t n = min(w.counts[6], g.rec_cap);
@@ -1019,9 +1044,9 @@ __global__ void GuideFinalizeKernel(WaveDev w, GuideDev g)
         float4 Lf = w.L[g.rec_slot[r]];
         bool started = !isnan(rr[17]);
         Spec cont = started ? Spec{ Lf.x - rr[17], Lf.y - rr[18], Lf.z - rr[19] } : spec(0);
-        Spec li{ rr[14] > 0 ? cont.r / rr[14] : 0.0f, rr[15] > 0 ? cont.g / rr[15] : 0.0f,
-                 rr[16] > 0 ? cont.b / rr[16] : 0.0f };
-        float wgt = fmaxf(Luminance(li), 0.0f) / rr[13];
+        Spec prod{ rr[14] > 0 ? cont.r / rr[14] : 0.0f, rr[15] > 0 ? cont.g / rr[15] : 0.0f,
+                   rr[16] > 0 ? cont.b / rr[16] : 0.0f };
+        float wgt = fmaxf(Luminance(prod), 0.0f);
         if (!isfinite(wgt))
         {
             wgt = 0;
@@ -1495,6 +1520,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         int32_t stride = int32_t(std::max<int64_t>(1, (2 * wave_paths + batch - 1) / batch));
         BBG_TRY(I->ReserveGuide(wave_paths, p->guide_train ? batch : 0));
         gc.dev = I->Guide(p->guide_train ? 1 : 0, stride);
+        gc.dev.select = (p->guide_select > 0 && p->guide_select <= 1) ? p->guide_select : 0.5f;
         int dummy;
         BBG_TRY(GuidePrepare(gc.guide, &dummy));
     }

@@ -234,7 +234,7 @@ class GpuPathIntegrator:
         return out[:len(self.scene.lights)]
 
     def render(self, spp=None, seed=None, camera_spec=None, wave_paths=0, use_graph=True, light_alias=False,
-               path_L=False, guide=None, train=False, batch=0, lr=0.0):
+               path_L=False, guide=None, train=False, batch=0, lr=0.0, select=0.0):
         s = self.scene
         spec = camera_spec or s.camera
         cam = camera(spec)
@@ -249,6 +249,7 @@ class GpuPathIntegrator:
         p.guide_train = 1 if train else 0
         p.guide_batch = batch
         p.guide_lr = lr
+        p.guide_select = select
         film = Film(cam.width, cam.height, spp, path_L=path_L)
         fs = film.struct()
         check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(p), C.byref(fs), abi.BBG_MEM_HOST,
@@ -314,3 +315,24 @@ class GpuGuide:
         check(get_lib().bbg_guide_train_step(self.h, _p(raw), _p(dirs), _p(weights), raw.shape[0], C.c_float(lr),
                                              C.byref(loss)), "bbg_guide_train_step")
         return loss.value
+
+
+def mixture_sample(outputs, u):
+    """Sample the vMF mixtures that network output rows (n, 40) describe, with
+    uniforms u (n, 3) -> (unit directions (n, 3), mixture density (n,))."""
+    outputs = np.ascontiguousarray(outputs, np.float32)
+    u = np.ascontiguousarray(u, np.float32)
+    n = outputs.shape[0]
+    d = np.zeros((n, 3), np.float32)
+    pdf = np.zeros(n, np.float32)
+    check(get_lib().bbg_guide_mixture_sample(_p(outputs), _p(u), n, _p(d), _p(pdf)), "bbg_guide_mixture_sample")
+    return d, pdf
+
+
+def mixture_pdf(outputs, dirs):
+    """Density of the mixtures (n, 40) at unit directions (n, 3)."""
+    outputs = np.ascontiguousarray(outputs, np.float32)
+    dirs = np.ascontiguousarray(dirs, np.float32)
+    pdf = np.zeros(outputs.shape[0], np.float32)
+    check(get_lib().bbg_guide_mixture_pdf(_p(outputs), _p(dirs), outputs.shape[0], _p(pdf)), "bbg_guide_mixture_pdf")
+    return pdf

@@ -339,12 +339,14 @@ typedef struct bbg_render_params
                              pmf, different stream) instead of CDF inversion */
     struct bbg_guide* guide; /* NULL: the reference's estimator. Otherwise, at
                                 non-specular vertices, one-sample MIS between
-                                the guide and the BSDF (probability 1/2 each;
-                                a different random stream, same expectation) */
+                                the guide and the BSDF (a different random
+                                stream, same expectation) */
     int32_t guide_train;  /* 1: train the guide online on this render's paths,
                              one Adam step per wave */
     int32_t guide_batch;  /* training samples per step (0: 65536) */
     float guide_lr;       /* Adam learning rate (0: 1e-2) */
+    float guide_select;   /* probability of sampling the guide rather than the
+                             BSDF, in (0, 1] (0: 1/2) */
 } bbg_render_params;
 
 /* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields
@@ -403,6 +405,13 @@ bbg_status bbg_guide_gradient(bbg_guide* guide, const float* raw, const float* d
  * before the step. */
 bbg_status bbg_guide_train_step(bbg_guide* guide, const float* raw, const float* dirs, const float* weights, int64_t n,
                                 float learning_rate, float* loss_out);
+
+/* The vMF mixture a network output row describes (40 floats), evaluated on
+ * the device exactly as the guided renderer does: sample n directions with
+ * uniforms u (3 per row; pdf_out receives the mixture density of each), or
+ * evaluate the density at n unit directions. Host buffers. */
+bbg_status bbg_guide_mixture_sample(const float* outputs, const float* u, int64_t n, float* dirs_out, float* pdf_out);
+bbg_status bbg_guide_mixture_pdf(const float* outputs, const float* dirs, int64_t n, float* pdf_out);
 
 /* --------------------------------------------------------------- library */
 
