@@ -609,12 +609,18 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int
 // non-specular vertices, queues the guide query; GuidedShadeB (after the
 // inference) does next-event estimation and the continuation with one-sample
 // MIS between the guide and the BSDF (guide selection probability s, 1/2 by
-// default). The continuation pdf is the mixture s q + (1 - s) p_bsdf, and
-// both MIS weights (light samples here, emitted light at the next hit) use
-// it, so the estimator stays unbiased whatever the network outputs. Specular
-// vertices continue as in the plain tracer. Training records take (query,
-// direction, pdf, throughput) at sampled vertices and the radiance the rest
-// of the path brings back along that direction.
+// default): the continuation's density is the mixture s q + (1 - s) p_bsdf.
+// Light sampling and the continuation are combined with the plain tracer's
+// weights, the power heuristic on the light and BSDF pdfs: any weights that
+// sum to one at every direction keep the estimator unbiased, whatever the
+// network outputs, and these leave next-event estimation exactly as in the
+// plain tracer (the mixture density in them would raise the weight of light
+// samples on glossy surfaces, where they are noisy, up to fourfold) and
+// bound a continuation sample's weight by 1/(1 - s) times the plain one.
+// Specular vertices, and those whose shading frame is not orthonormal
+// (kGuideFrameSkew), continue as in the plain tracer. Training records take
+// (query, direction, pdf, throughput) at sampled vertices and the radiance
+// the rest of the path brings back along that direction.
 
 struct GuideDev
 {
@@ -637,6 +643,17 @@ struct GuideDev
 };
 
 constexpr int kRecFloats = 20;
+
+// Largest |n . t| of a shading frame at which a vertex is guided. The BSDF
+// frame is built from the interpolated normal and tangent without
+// orthogonalising them (Frame::FromXZ, include/bulbit/frame.h:139-142); when
+// they are not orthogonal, the directions the BSDF samples (mapped to world
+// space by the skewed frame) and the values f() and PDF() give for a world
+// direction (mapped back by dot products) describe different measures, so a
+// guide direction, which only f() and PDF() can weigh, would shift the pixel
+// estimates. Such vertices use the plain tracer's BSDF sampling. The bound
+// keeps the angular error far below the narrowest lobe the materials have.
+constexpr float kGuideFrameSkew = 1e-3f;
 
 __device__ __forceinline__ float GuideRoughness(const MaterialDev& m)
 {
@@ -661,6 +678,63 @@ __device__ __forceinline__ void AddEscaped(const SceneDev& s, Spec beta, int32_t
             *L = *L + beta * PowerHeuristic(prev_pdf, light_pdf) * Le;
         }
     }
+}
+
+// Next-event estimation at a non-specular vertex (PathIntegrator's
+// SampleDirectLight, as in ShadeKernel: u0 then u12 drawn, power heuristic
+// on the light and BSDF pdfs). Returns whether a shadow ray was made.
+__device__ __forceinline__ bool DirectLight(const SceneDev& s, const BSDF& bsdf, V3 point, V3 sn, V3 wo, Spec beta,
+                                            uint64_t& rng, V3* sh_d, float* sh_t, Spec* sh_c)
+{
+    float u0 = Next1D(rng);
+    P2 u12 = Next2D(rng);
+    if (s.n_lights <= 0)
+    {
+        return false;
+    }
+    float pmf;
+    int32_t li = SampleLight(s, u0, &pmf);
+    const LightDev& l = s.lights[li];
+    V3 tri[3];
+    const bbg_sphere* sph = nullptr;
+    bool on_tri = false;
+    if (l.type == BBG_LIGHT_DIFFUSE_AREA)
+    {
+        int4 linfo = s.prim_info[l.prim];
+        if (linfo.x == BBG_PRIM_TRIANGLE)
+        {
+            int32_t vv[3];
+            TriVerts(s, linfo.y, vv, tri);
+            on_tri = true;
+        }
+        else
+        {
+            sph = &s.spheres[linfo.y];
+        }
+    }
+    LightSampleLi ls;
+    if (!SampleLi(l, point, u12, on_tri ? tri : nullptr, sph, &ls))
+    {
+        return false;
+    }
+    float bsdf_pdf = bsdf.PDF(wo, ls.wi);
+    if (IsBlack(ls.Li) || bsdf_pdf == 0)
+    {
+        return false;
+    }
+    float light_pdf = pmf * ls.pdf;
+    Spec f_cos = bsdf.F(wo, ls.wi) * AbsDot(sn, ls.wi);
+    if (IsDeltaLight(l.type))
+    {
+        *sh_c = beta * ls.Li * f_cos / light_pdf;
+    }
+    else
+    {
+        *sh_c = beta * PowerHeuristic(light_pdf, bsdf_pdf) * ls.Li * f_cos / light_pdf;
+    }
+    *sh_d = ls.wi;
+    *sh_t = ls.visibility;
+    return true;
 }
 
 __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, GuideDev g, int parity)
@@ -695,7 +769,10 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
             }
         }
 
-        bool cont = false, guided = false;
+        bool cont = false, guided = false, shadow = false;
+        V3 sh_o{}, sh_d{};
+        float sh_t = 0;
+        Spec sh_c{};
         int32_t prim = __float_as_int(hit.x);
         if (prim < 0)
         {
@@ -741,7 +818,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
                 {
                     RegularizeBSDF(&bsdf);
                 }
-                if (IsNonSpecular(bsdf.flags))
+                if (IsNonSpecular(bsdf.flags) && fabsf(Dot(is.sn, is.st)) <= kGuideFrameSkew)
                 {
                     guided = true;
                     float* r = g.raw + size_t(slot) * kGuideRaw;
@@ -763,6 +840,13 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
                 }
                 else
                 {
+                    // Specular, or a skewed shading frame: the plain
+                    // tracer's next-event estimation and BSDF sampling.
+                    if (IsNonSpecular(bsdf.flags))
+                    {
+                        shadow = DirectLight(s, bsdf, is.point, is.sn, wo, beta, rng, &sh_d, &sh_t, &sh_c);
+                        sh_o = is.point;
+                    }
                     P2 u12 = Next2D(rng);
                     float u0 = Next1D(rng);
                     BSDFSample bs;
@@ -818,6 +902,13 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
         {
             g.queue[gi] = slot;
         }
+        int32_t si = Append(&w.counts[2], shadow);
+        if (shadow)
+        {
+            w.sh_o[si] = make_float4(sh_o.x, sh_o.y, sh_o.z, sh_t);
+            w.sh_d[si] = make_float4(sh_d.x, sh_d.y, sh_d.z, __int_as_float(slot));
+            w.sh_c[si] = make_float4(sh_c.r, sh_c.g, sh_c.b, 0.0f);
+        }
     }
 }
 
@@ -847,60 +938,11 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
         }
         VmfMixture mix = MakeMixture(g.out + size_t(slot) * kGuideOut);
 
-        // Next-event estimation, MIS against the continuation mixture pdf.
-        bool shadow = false;
+        // Next-event estimation with the plain tracer's weights.
         V3 sh_d{};
         float sh_t = 0;
         Spec sh_c{};
-        {
-            float u0 = Next1D(rng);
-            P2 u12 = Next2D(rng);
-            if (s.n_lights > 0)
-            {
-                float pmf;
-                int32_t li = SampleLight(s, u0, &pmf);
-                const LightDev& l = s.lights[li];
-                V3 tri[3];
-                const bbg_sphere* sph = nullptr;
-                bool on_tri = false;
-                if (l.type == BBG_LIGHT_DIFFUSE_AREA)
-                {
-                    int4 linfo = s.prim_info[l.prim];
-                    if (linfo.x == BBG_PRIM_TRIANGLE)
-                    {
-                        int32_t vv[3];
-                        TriVerts(s, linfo.y, vv, tri);
-                        on_tri = true;
-                    }
-                    else
-                    {
-                        sph = &s.spheres[linfo.y];
-                    }
-                }
-                LightSampleLi ls;
-                if (SampleLi(l, point, u12, on_tri ? tri : nullptr, sph, &ls))
-                {
-                    float bsdf_pdf = bsdf.PDF(wo, ls.wi);
-                    if (!(IsBlack(ls.Li) || bsdf_pdf == 0))
-                    {
-                        float light_pdf = pmf * ls.pdf;
-                        Spec f_cos = bsdf.F(wo, ls.wi) * AbsDot(sn, ls.wi);
-                        if (IsDeltaLight(l.type))
-                        {
-                            sh_c = beta * ls.Li * f_cos / light_pdf;
-                        }
-                        else
-                        {
-                            float mix_pdf = g.select * MixturePdf(mix, ls.wi) + (1.0f - g.select) * bsdf_pdf;
-                            sh_c = beta * PowerHeuristic(light_pdf, mix_pdf) * ls.Li * f_cos / light_pdf;
-                        }
-                        shadow = true;
-                        sh_d = ls.wi;
-                        sh_t = ls.visibility;
-                    }
-                }
-            }
-        }
+        bool shadow = DirectLight(s, bsdf, point, sn, wo, beta, rng, &sh_d, &sh_t, &sh_c);
 
         // Continuation: the guide with probability g.select, else the BSDF.
         // A BSDF sample is weighted with its own f and pdf, as the plain
@@ -916,7 +958,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
         float u0 = Next1D(rng);
         V3 wi{}, wdir{};
         Spec f{};
-        float pdf = 0, cosv = 0, eta_sample = 1, rr_p = 1;
+        float pdf = 0, pdf_b = 0, cosv = 0, eta_sample = 1, rr_p = 1;
         bool spec_sample = false, transmit = false;
         const Spec beta_in = beta;
         if (u_sel < g.select)
@@ -924,7 +966,8 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
             wi = MixtureSample(mix, u0, u12.x, u12.y);
             wdir = wi;
             f = bsdf.F(wo, wi);
-            pdf = g.select * MixturePdf(mix, wi) + (1.0f - g.select) * bsdf.PDF(wo, wi);
+            pdf_b = bsdf.PDF(wo, wi);
+            pdf = g.select * MixturePdf(mix, wi) + (1.0f - g.select) * pdf_b;
             cosv = AbsDot(sn, wi);
             if (mat.type == BBG_MAT_DIELECTRIC)
             {
@@ -941,6 +984,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
                 wi = bs.wi;
                 wdir = Normalize(wi);
                 f = bs.f;
+                pdf_b = bs.pdf;
                 spec_sample = (bs.flags & kFlagSpecular) != 0;
                 pdf = spec_sample ? (1.0f - g.select) * bs.pdf
                                   : g.select * MixturePdf(mix, wdir) + (1.0f - g.select) * bs.pdf;
@@ -999,7 +1043,9 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
         }
         if (cont)
         {
-            w.o_pdf[slot] = make_float4(point.x, point.y, point.z, pdf);
+            // The emission MIS at the next hit weighs the BSDF pdf against
+            // the light's (see above); the throughput carries the mixture's.
+            w.o_pdf[slot] = make_float4(point.x, point.y, point.z, pdf_b);
             w.d_eta[slot] = make_float4(wi.x, wi.y, wi.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
             w.flags[slot] = bounce | (spec_sample ? kSpecularBit : 0) |

@@ -54,24 +54,42 @@ def train(integ, guide, iterations, seed0=200):
         integ.render(spp=16, seed=seed0 + i, guide=guide, train=True, wave_paths=1 << 14)
 
 
+def pixel_stats(film):
+    """Per-pixel luminance mean and its standard error."""
+    img = film.image()
+    lum = 0.2126 * img[..., 0] + 0.7152 * img[..., 1] + 0.0722 * img[..., 2]
+    n = film.count.astype(np.float64)
+    var = np.maximum(0.0, film.moments[..., 1] - film.moments[..., 0] ** 2) * np.where(n > 1, n / (n - 1), 1)
+    return lum, np.sqrt(var / np.maximum(n, 1))
+
+
 def check_unbiased(plain, film, label):
+    """Image mean within 4 standard errors, and per pixel: the mean of z^2
+    over pixels (z = difference / combined standard error) near 1, so that
+    no bias hides in pixels whose errors cancel in the image mean."""
     mp, sp = mean_and_se(plain)
     mg, sg = mean_and_se(film)
-    print(f"{label}: guided mean {mg:.5f} +- {sg:.5f}, plain {mp:.5f} +- {sp:.5f}")
+    lp, ep = pixel_stats(plain)
+    lg, eg = pixel_stats(film)
+    se = np.hypot(ep, eg)
+    ok = se > 0
+    z2 = float(np.mean(((lg - lp)[ok] / se[ok]) ** 2))
+    print(f"{label}: guided mean {mg:.5f} +- {sg:.5f}, plain {mp:.5f} +- {sp:.5f}, per-pixel mean z^2 {z2:.3f}")
     assert abs(mg - mp) <= 4 * np.hypot(sg, sp)
+    assert z2 < 1.25
 
 
 def test_guided_estimator_is_unbiased(setup, smooth):
-    """Untrained guide on the displaced icosphere; untrained and trained guide
-    on the smooth one. On the displaced sphere the shading frame (interpolated
+    """Untrained and trained guide on the displaced icosphere and on the
+    smooth one. On the displaced sphere the shading frame (interpolated
     tangent and normal, not orthogonalised, as in the reference) is far from
-    orthonormal, so the BSDF's sampling disagrees with its own f()/PDF(); a
-    sharp trained guide, which must use f()/PDF() for its directions, then
-    shifts the mean there by about 2 %: a property of that frame."""
+    orthonormal, and such vertices are traced as by the plain tracer."""
     scene, acc, integ = setup
     plain = integ.render(spp=512, seed=1)
     guide = lib.GpuGuide(acc.bounds(), seed=3)
     check_unbiased(plain, integ.render(spp=512, seed=2, guide=guide), "displaced, untrained")
+    train(integ, guide, 200)
+    check_unbiased(plain, integ.render(spp=512, seed=3, guide=guide), "displaced, trained")
     scene, acc, integ = smooth
     plain = integ.render(spp=512, seed=1)
     guide = lib.GpuGuide(acc.bounds(), seed=3)
@@ -80,24 +98,26 @@ def test_guided_estimator_is_unbiased(setup, smooth):
     check_unbiased(plain, integ.render(spp=512, seed=3, guide=guide), "smooth, trained")
 
 
-@pytest.mark.parametrize("which", ["setup", "smooth"])
-def test_training_lowers_relmse(request, which):
+@pytest.mark.parametrize("which,bound", [("setup", 1.0), ("smooth", 0.8)])
+def test_training_lowers_relmse(request, which, bound):
     """What the learned network gains over the same estimator without it:
-    relMSE against an 8192-spp plain render, trained vs untrained guide."""
+    relMSE against an 8192-spp plain render, trained vs untrained guide. On
+    the displaced icosphere most vertices of the sphere are traced unguided
+    (skewed shading frames), so the gain there is smaller."""
     scene, acc, integ = request.getfixturevalue(which)
     ref = integ.render(spp=8192, seed=7).image()
     untrained = lib.GpuGuide(acc.bounds(), seed=5)
     trained = lib.GpuGuide(acc.bounds(), seed=5)
     train(integ, trained, 200)
     e_plain, e_untrained, e_trained = [], [], []
-    for k in range(3):
+    for k in range(5):
         e_plain.append(rel_mse(integ.render(spp=64, seed=50 + k).image(), ref))
         e_untrained.append(rel_mse(integ.render(spp=64, seed=60 + k, guide=untrained).image(), ref))
         e_trained.append(rel_mse(integ.render(spp=64, seed=70 + k, guide=trained).image(), ref))
     p, u, t = np.mean(e_plain), np.mean(e_untrained), np.mean(e_trained)
     print(f"{which} relMSE at 64 spp: plain {p:.4e}, guided untrained {u:.4e}, guided trained {t:.4e} "
           f"(trained/plain {t / p:.3f}, trained/untrained {t / u:.3f})")
-    assert t < 0.8 * u
+    assert t < bound * u
 
 
 def test_guided_render_is_deterministic_and_graph_safe(setup):
