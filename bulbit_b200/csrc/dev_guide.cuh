@@ -50,6 +50,12 @@ constexpr int kCBias = kCB3 + kGuideOut; // 232
 // BF16 weight images used by the kernels: forward layout [out][in] and the
 // transposed [in][out] layout for the backward pass (W3 transposed padded to
 // 48 columns with zeros).
+// The forward image (W0..W3, offsets kBf0..kBf3) is stored in MMA fragment
+// order, so a B fragment is one conflict-free 8-byte shared-memory load: for
+// a layer of N outputs (NT = N/8 tiles) and K inputs, element
+// ((kt * NT + nt) * 32 + lane) * 4 + e holds W[n][k] with n = nt*8 + lane/4
+// and k = kt*16 + 2*(lane%4) + {0, 1, 8, 9}[e]. The transposed images
+// (kBfT1..kBfT3, backward pass) are row-major.
 constexpr int kBf0 = 0;
 constexpr int kBf1 = kBf0 + kGuideHidden * kGuideIn;
 constexpr int kBf2 = kBf1 + kGuideHidden * kGuideHidden;
@@ -113,6 +119,19 @@ __device__ __forceinline__ void LoadB(const __nv_bfloat16* w, int ld, int n0, in
     *b1 = *reinterpret_cast<const uint32_t*>(row + 8);
 }
 
+// B fragment (b0, b1) of tile (nt, kt) from a fragment-ordered image.
+__device__ __forceinline__ void LoadBFrag(const __nv_bfloat16* w, int n_tiles, int nt, int kt, int lane, uint32_t* b0,
+                                          uint32_t* b1)
+{
+    uint2 v = *reinterpret_cast<const uint2*>(w + ((kt * n_tiles + nt) * 32 + lane) * 4);
+    *b0 = v.x;
+    *b1 = v.y;
+}
+
+// Row stride (elements) of the [16][80] feature tiles in shared memory:
+// 44 words, so the 8 rows an A-fragment load touches fall in distinct banks.
+constexpr int kXLd = 88;
+
 // A fragment from a matrix stored [m][k] (k contiguous), row stride ld.
 __device__ __forceinline__ void LoadA(const __nv_bfloat16* x, int ld, int m0, int k0, int lane, uint32_t* a)
 {
@@ -128,8 +147,8 @@ __device__ __forceinline__ void LoadA(const __nv_bfloat16* x, int ld, int m0, in
 // One hidden layer of K inputs -> 64 outputs for the warp's 16 rows: A
 // fragments in, ReLU'd accumulators out (as the next layer's A fragments).
 template <int KT>
-__device__ __forceinline__ void HiddenLayer(const uint32_t (&a)[KT][4], const __nv_bfloat16* w, int ld,
-                                            const float* bias, int lane, float (&acc)[8][4])
+__device__ __forceinline__ void HiddenLayer(const uint32_t (&a)[KT][4], const __nv_bfloat16* w, const float* bias,
+                                            int lane, float (&acc)[8][4])
 {
     int t = lane & 3;
 #pragma unroll
@@ -148,7 +167,7 @@ __device__ __forceinline__ void HiddenLayer(const uint32_t (&a)[KT][4], const __
         for (int nt = 0; nt < 8; ++nt)
         {
             uint32_t b0, b1;
-            LoadB(w, ld, nt * 8, kt * 16, lane, &b0, &b1);
+            LoadBFrag(w, 8, nt, kt, lane, &b0, &b1);
             Mma16816(acc[nt], a[kt], b0, b1);
         }
     }
@@ -197,7 +216,7 @@ __device__ __forceinline__ void OutputLayer(const uint32_t (&a)[4][4], const __n
         for (int nt = 0; nt < 5; ++nt)
         {
             uint32_t b0, b1;
-            LoadB(w, kGuideHidden, nt * 8, kt * 16, lane, &b0, &b1);
+            LoadBFrag(w, 5, nt, kt, lane, &b0, &b1);
             Mma16816(out[nt], a[kt], b0, b1);
         }
     }

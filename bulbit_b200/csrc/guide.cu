@@ -42,7 +42,7 @@ __device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_
         {
             float v0 = valid ? GuideFeature(f, raw, bounds) : 0.0f;
             float v1 = valid ? GuideFeature(f + 1, raw, bounds) : 0.0f;
-            *reinterpret_cast<uint32_t*>(x + row * kGuideIn + f) = PackBf16(v0, v1);
+            *reinterpret_cast<uint32_t*>(x + row * kXLd + f) = PackBf16(v0, v1);
         }
     }
     __syncwarp();
@@ -50,15 +50,15 @@ __device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_
 #pragma unroll
     for (int kt = 0; kt < 5; ++kt)
     {
-        LoadA(x, kGuideIn, 0, kt * 16, lane, a0[kt]);
+        LoadA(x, kXLd, 0, kt * 16, lane, a0[kt]);
     }
     float acc[8][4];
     uint32_t a[4][4];
-    HiddenLayer<5>(a0, w + kBf0, kGuideIn, bias + kCB0, lane, acc);
+    HiddenLayer<5>(a0, w + kBf0, bias + kCB0, lane, acc);
     AccToA(acc, a);
-    HiddenLayer<4>(a, w + kBf1, kGuideHidden, bias + kCB1, lane, acc);
+    HiddenLayer<4>(a, w + kBf1, bias + kCB1, lane, acc);
     AccToA(acc, a);
-    HiddenLayer<4>(a, w + kBf2, kGuideHidden, bias + kCB2, lane, acc);
+    HiddenLayer<4>(a, w + kBf2, bias + kCB2, lane, acc);
     AccToA(acc, a);
     float out[5][4];
     OutputLayer(a, w + kBf3, bias + kCB3, lane, out);
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(32 * kFwdWarps) GuideForwardKernel(const float
     StageWeights(wg, pg, ws, bs, kBfFwd);
     const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* x = xs + warp * 16 * kGuideIn;
+    __nv_bfloat16* x = xs + warp * 16 * kXLd;
     ArraySrc src{ raw, out, index };
     const int64_t tiles = (n + 15) / 16;
     for (int64_t tile = int64_t(blockIdx.x) * kFwdWarps + warp; tile < tiles; tile += int64_t(gridDim.x) * kFwdWarps)
@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(32 * kFwdWarps) GuideForwardKernel(const float
     }
 }
 
-constexpr size_t kFwdSmem = size_t(kBfFwd) * 2 + size_t(kCBias) * 4 + size_t(kFwdWarps) * 16 * kGuideIn * 2;
+constexpr size_t kFwdSmem = size_t(kBfFwd) * 2 + size_t(kCBias) * 4 + size_t(kFwdWarps) * 16 * kXLd * 2;
 
 // ---------------------------------------------------------------- training
 
@@ -186,7 +186,7 @@ __device__ __forceinline__ float MixtureNllGrad(const float* o, V3 dir, float we
 
 struct TrainWarp
 {
-    __nv_bfloat16 x[16 * kGuideIn];      // [sample][feature]
+    __nv_bfloat16 x[16 * kXLd];          // [sample][feature], padded rows
     __nv_bfloat16 xt[kGuideIn * 16];     // [feature][sample]
     __nv_bfloat16 h[3][16 * kGuideHidden];   // post-ReLU activations [sample][unit]
     __nv_bfloat16 ht[3][kGuideHidden * 16];  // [unit][sample]
@@ -362,7 +362,7 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
             for (int f = half * 40; f < half * 40 + 40; ++f)
             {
                 __nv_bfloat16 v = __float2bfloat16_rn(valid ? GuideFeature(f, r, bounds) : 0.0f);
-                W.x[row * kGuideIn + f] = v;
+                W.x[row * kXLd + f] = v;
                 W.xt[f * 16 + row] = v;
             }
         }
@@ -373,17 +373,17 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
 #pragma unroll
         for (int kt = 0; kt < 5; ++kt)
         {
-            LoadA(W.x, kGuideIn, 0, kt * 16, lane, a0[kt]);
+            LoadA(W.x, kXLd, 0, kt * 16, lane, a0[kt]);
         }
         float acc[8][4];
         uint32_t a[4][4];
-        HiddenLayer<5>(a0, ws + kBf0, kGuideIn, bs + kCB0, lane, acc);
+        HiddenLayer<5>(a0, ws + kBf0, bs + kCB0, lane, acc);
         StoreActs(acc, W.h[0], W.ht[0], lane);
         AccToA(acc, a);
-        HiddenLayer<4>(a, ws + kBf1, kGuideHidden, bs + kCB1, lane, acc);
+        HiddenLayer<4>(a, ws + kBf1, bs + kCB1, lane, acc);
         StoreActs(acc, W.h[1], W.ht[1], lane);
         AccToA(acc, a);
-        HiddenLayer<4>(a, ws + kBf2, kGuideHidden, bs + kCB2, lane, acc);
+        HiddenLayer<4>(a, ws + kBf2, bs + kCB2, lane, acc);
         StoreActs(acc, W.h[2], W.ht[2], lane);
         AccToA(acc, a);
         float out[5][4];
@@ -507,21 +507,17 @@ __global__ void GuideConvertKernel(const float* params, __nv_bfloat16* w)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kBfAll; i += gridDim.x * blockDim.x)
     {
         float v = 0;
-        if (i < kBf1)
+        if (i < kBfFwd)
         {
-            v = params[kW0 + i];
-        }
-        else if (i < kBf2)
-        {
-            v = params[kW1 + (i - kBf1)];
-        }
-        else if (i < kBf3)
-        {
-            v = params[kW2 + (i - kBf2)];
-        }
-        else if (i < kBfFwd)
-        {
-            v = params[kW3 + (i - kBf3)];
+            // Fragment order (see kBf0): locate layer, tile, lane, element.
+            int base = i < kBf1 ? kBf0 : i < kBf2 ? kBf1 : i < kBf3 ? kBf2 : kBf3;
+            int src = i < kBf1 ? kW0 : i < kBf2 ? kW1 : i < kBf3 ? kW2 : kW3;
+            int n_in = i < kBf1 ? kGuideIn : kGuideHidden;
+            int n_tiles = i < kBf3 ? kGuideHidden / 8 : kGuideOut / 8;
+            int j = i - base, e = j & 3, lane = (j >> 2) & 31, tile = j >> 7;
+            int n = (tile % n_tiles) * 8 + (lane >> 2);
+            int k = (tile / n_tiles) * 16 + 2 * (lane & 3) + (e & 1) + 8 * (e >> 1);
+            v = params[src + n * n_in + k];
         }
         else if (i < kBfT2)
         {
