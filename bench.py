@@ -8,8 +8,10 @@ closest-hit rays and 16,777,216 any-hit rays (t_max = 0.5 x distance to the
 target) from the sphere of radius 3 toward U[-1,1]^3; seeded synthetic data.
 value = (closest + any-hit rays traced by all ranks) / max-over-ranks device
 time, in Mrays/s. The path-tracing workload (Cornell box with a displaced
-gold icosphere) is reported beside it as paths/s when the integrator is
-available.
+gold icosphere, 1024x1024, 64 spp) is reported beside it as paths/s and
+Mrays/s, and neural-guided against plain path tracing as the ratio of their
+relMSE at equal device time (the same scene at 256x256 against a 16384-spp
+plain render).
 
 Each rank is an independent replica (the path does not shard across GPUs);
 ranks only meet at barriers and the max-reduction of their timings.
@@ -255,6 +257,67 @@ def run_pt(args, barrier, world):
     return out, scene
 
 
+def rel_mse(img, ref):
+    """mean over pixels and channels of (x - ref)^2 / (ref^2 + 1e-2)."""
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def run_guided(args):
+    """Neural path guiding against the plain tracer at equal device time.
+
+    Scene: the path-tracing workload's Cornell box at a reduced resolution
+    (args.guided_res). Reference: a 16384-spp plain render. Plain arm: 64 spp.
+    Guided arm: a fresh guide trained online while it renders (train on every
+    wave, guide_steps Adam steps of 2^16 samples each, lr 1e-2, guide/BSDF
+    selection 1/2); its spp is chosen from a probe render so its device time
+    matches the plain arm's; every sample, the training ones included, counts
+    toward its image."""
+    from bulbit_b200 import lib, scenes
+    res, wave, steps = args.guided_res, 1 << 21, 8
+    scene = scenes.cornell_icosphere(levels=8, width=res, height=res, spp=64, max_bounces=16)
+    acc = lib.GpuAccel(scene)
+    integ = lib.GpuPathIntegrator(acc, scene)
+    ref_film = integ.render(spp=16384, seed=7)
+    ref = ref_film.image()
+    integ.render(spp=64, seed=1)  # graph capture for this shape
+    plain = integ.render(spp=64, seed=2)
+    t_plain = plain.stats.device_ms
+    e_plain = rel_mse(plain.image(), ref)
+
+    def guided(spp, seed, gseed):
+        g = lib.GpuGuide(acc.bounds(), seed=gseed)
+        f = integ.render(spp=spp, seed=seed, guide=g, train=True, wave_paths=wave, steps=steps, lr=1e-2)
+        return f, g
+
+    probe, _ = guided(64, 3, 5)
+    spp_eq = max(1, int(64 * t_plain / probe.stats.device_ms))
+    gf, g = guided(spp_eq, 4, 6)
+    if gf.stats.device_ms > 1.05 * t_plain and spp_eq > 1:  # time is not linear in spp (whole waves)
+        spp_eq = max(1, int(spp_eq * t_plain / gf.stats.device_ms))
+        gf, g = guided(spp_eq, 4, 6)
+    t_guided = gf.stats.device_ms
+    e_guided = rel_mse(gf.image(), ref)
+    same_spp = integ.render(spp=64, seed=8, guide=g)  # the trained guide, no more training
+    e_same = rel_mse(same_spp.image(), ref)
+    # Monte Carlo error falls as 1/time, so relMSE x time compares the two at
+    # exactly equal time; the raw ratio at the matched spp is reported too.
+    out = {
+        "metric": "relMSE at equal time, guided / plain", "value": (e_guided * t_guided) / (e_plain * t_plain),
+        "higher_is_better": False, "raw_relmse_ratio": e_guided / e_plain,
+        "plain": {"spp": 64, "device_ms": t_plain, "relMSE": e_plain},
+        "guided": {"spp": spp_eq, "device_ms": t_guided, "relMSE": e_guided,
+                   "trained_guide_64spp_relMSE": e_same, "trained_guide_64spp_device_ms": same_spp.stats.device_ms},
+        "reference": {"spp": 16384, "device_ms": ref_film.stats.device_ms},
+        "config": {"workload": f"Cornell box + displaced gold icosphere (1,310,720 triangles) at {res}x{res}, "
+                               "16 bounces; relMSE against a 16384-spp plain render",
+                   "wave_paths": wave, "guide_steps_per_wave": steps, "guide_batch": 1 << 16, "guide_lr": 1e-2,
+                   "guide_select": 0.5, "time": "device time of each render call (CUDA events)"},
+    }
+    integ.close()
+    acc.close()
+    return out
+
+
 def pt_cpu_baseline(scene, res=128):
     """The reference PathIntegrator (oracle/_ref) rendering the same scene at a
     reduced resolution on all host threads: Render() + Rendering::Wait()."""
@@ -284,7 +347,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per query set (smaller cases for profiling)")
-    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt"])
+    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided"])
+    ap.add_argument("--guided-res", type=int, default=256)
     ap.add_argument("--pt-res", type=int, default=1024)
     ap.add_argument("--pt-steps", type=int, default=3)
     ap.add_argument("--pt-wave", type=int, default=1 << 24)
@@ -312,6 +376,10 @@ def main():
         pt, pt_scene = run_pt(args, barrier, world)
         if rank == 0:
             print(json.dumps({"path_tracing": pt}))
+        return
+    if args.workload == "guided":
+        if rank == 0:
+            print(json.dumps({"guided_path_tracing": run_guided(args)}))
         return
 
     n_rays = args.rays
@@ -414,6 +482,9 @@ def main():
     if args.workload == "all":
         pt, pt_scene = run_pt(args, barrier, world)
         line["path_tracing"] = pt
+        if rank == 0:
+            line["guided_path_tracing"] = run_guided(args)
+        barrier()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene, closest, anyq)
         if args.workload == "all":

@@ -101,7 +101,7 @@ class RenderParams(C.Structure):
     _fields_ = [("spp", C.c_int32), ("seed", C.c_int32), ("wave_paths", C.c_int64),
                 ("use_graph", C.c_int32), ("light_alias", C.c_int32), ("guide", C.c_void_p),
                 ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float),
-                ("guide_select", C.c_float)]
+                ("guide_select", C.c_float), ("guide_steps", C.c_int32)]
 
 
 class Film(C.Structure):

@@ -1243,7 +1243,7 @@ struct bbg_integrator
     int32_t g_rec_cap = 0;
     DevBuf<float> g_raw, g_out, g_rec, g_traw, g_tdir, g_tw, g_wsum;
     DevBuf<float4> g_vtx;
-    DevBuf<int32_t> g_queue, g_recid, g_recslot;
+    DevBuf<int32_t> g_queue, g_recid, g_recslot, g_slice;
 
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -1255,7 +1255,7 @@ struct bbg_integrator
     bbg_guide* graph_guide_handle = nullptr;
     float graph_guide_lr = 0;
 
-    bbg_status ReserveGuide(int64_t n, int32_t rec_cap)
+    bbg_status ReserveGuide(int64_t n, int32_t rec_cap, int32_t steps)
     {
         if (n > g_capacity)
         {
@@ -1290,6 +1290,7 @@ struct bbg_integrator
             g_rec_cap = rec_cap;
         }
         BBG_TRY(g_wsum.alloc(1));
+        BBG_TRY(g_slice.alloc(size_t(std::max(1, steps))));
         return BBG_OK;
     }
 
@@ -1386,7 +1387,20 @@ struct GuideCtx
     bbg_guide* guide = nullptr;
     GuideDev dev{};
     float lr = 0;
+    int32_t batch = 0;  // training samples per Adam step
+    int32_t steps = 1;  // Adam steps per wave
+    int32_t* slice = nullptr; // per step: its number of samples (device)
 };
+
+// Splits the wave's training samples into gc.steps batches of gc.batch.
+__global__ void GuideSliceKernel(WaveDev w, int32_t* slice, int32_t batch, int32_t steps)
+{
+    int32_t n = w.counts[7];
+    for (int32_t k = threadIdx.x; k < steps; k += blockDim.x)
+    {
+        slice[k] = max(0, min(batch, n - k * batch));
+    }
+}
 
 __global__ void GuideWaveStartKernel(WaveDev w, GuideDev g)
 {
@@ -1445,8 +1459,14 @@ bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, cudaStream_t s
     WaveDev w = I->Wave();
     GuideFinalizeKernel<<<256, 256, 0, st>>>(w, gc.dev);
     GuideNormalizeKernel<<<256, 256, 0, st>>>(w, gc.dev);
-    BBG_TRY(GuideAccumulate(gc.guide, gc.dev.t_raw, gc.dev.t_dir, gc.dev.t_w, w.counts + 7, 0, st));
-    BBG_TRY(GuideApply(gc.guide, gc.lr, w.counts + 7, 0, st));
+    GuideSliceKernel<<<1, 32, 0, st>>>(w, gc.slice, gc.batch, gc.steps);
+    for (int32_t k = 0; k < gc.steps; ++k)
+    {
+        size_t off = size_t(k) * size_t(gc.batch);
+        BBG_TRY(GuideAccumulate(gc.guide, gc.dev.t_raw + off * kGuideRaw, gc.dev.t_dir + off * 3, gc.dev.t_w + off,
+                                gc.slice + k, 0, st));
+        BBG_TRY(GuideApply(gc.guide, gc.lr, gc.slice + k, 0, st));
+    }
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
 }
@@ -1553,7 +1573,6 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     cudaEvent_t e0, e1;
     BBG_CUDA(cudaEventCreate(&e0));
     BBG_CUDA(cudaEventCreate(&e1));
-    BBG_CUDA(cudaEventRecord(e0, st));
 
     GuideCtx gc;
     if (p->guide)
@@ -1561,11 +1580,21 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         gc.guide = p->guide;
         gc.lr = p->guide_lr > 0 ? p->guide_lr : 1e-2f;
         int32_t batch = p->guide_batch > 0 ? p->guide_batch : (1 << 16);
-        // Record every stride-th path so a wave yields about one batch
+        int32_t steps = p->guide_steps > 0 ? p->guide_steps : 1;
+        if (p->guide_train && int64_t(batch) * steps > (int64_t(1) << 28))
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "guide_batch x guide_steps exceeds 2^28 training samples per wave");
+        }
+        // Record every stride-th path so a wave yields about steps batches
         // (about two guided vertices per path).
-        int32_t stride = int32_t(std::max<int64_t>(1, (2 * wave_paths + batch - 1) / batch));
-        BBG_TRY(I->ReserveGuide(wave_paths, p->guide_train ? batch : 0));
+        int64_t samples = int64_t(batch) * steps;
+        int32_t stride = int32_t(std::max<int64_t>(1, (2 * wave_paths + samples - 1) / samples));
+        BBG_TRY(I->ReserveGuide(wave_paths, p->guide_train ? int32_t(samples) : 0, steps));
+        gc.batch = batch;
+        gc.steps = steps;
         gc.dev = I->Guide(p->guide_train ? 1 : 0, stride);
+        gc.dev.rec_cap = p->guide_train ? int32_t(samples) : 0;
+        gc.slice = I->g_slice.p;
         gc.dev.select = (p->guide_select > 0 && p->guide_select <= 1) ? p->guide_select : 0.5f;
         int dummy;
         BBG_TRY(GuidePrepare(gc.guide, &dummy));
@@ -1604,6 +1633,9 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         I->graph_guide_lr = gc.lr;
     }
 
+    // Device time of the render itself: buffer set-up and graph capture
+    // (once per configuration) are not included.
+    BBG_CUDA(cudaEventRecord(e0, st));
     for (int64_t base = 0; base < n_paths; base += wave_paths)
     {
         int64_t count = std::min(wave_paths, n_paths - base);

@@ -234,7 +234,7 @@ class GpuPathIntegrator:
         return out[:len(self.scene.lights)]
 
     def render(self, spp=None, seed=None, camera_spec=None, wave_paths=0, use_graph=True, light_alias=False,
-               path_L=False, guide=None, train=False, batch=0, lr=0.0, select=0.0):
+               path_L=False, guide=None, train=False, batch=0, lr=0.0, select=0.0, steps=0):
         s = self.scene
         spec = camera_spec or s.camera
         cam = camera(spec)
@@ -250,6 +250,7 @@ class GpuPathIntegrator:
         p.guide_batch = batch
         p.guide_lr = lr
         p.guide_select = select
+        p.guide_steps = steps
         film = Film(cam.width, cam.height, spp, path_L=path_L)
         fs = film.struct()
         check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(p), C.byref(fs), abi.BBG_MEM_HOST,

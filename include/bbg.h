@@ -347,6 +347,8 @@ typedef struct bbg_render_params
     float guide_lr;       /* Adam learning rate (0: 1e-2) */
     float guide_select;   /* probability of sampling the guide rather than the
                              BSDF, in (0, 1] (0: 1/2) */
+    int32_t guide_steps;  /* Adam steps per wave when training, each on its own
+                             batch of guide_batch training samples (0: 1) */
 } bbg_render_params;
 
 /* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields
@@ -367,7 +369,9 @@ typedef struct bbg_render_stats
     int64_t paths;
     int64_t closest_rays;   /* closest-hit rays traced */
     int64_t shadow_rays;    /* shadow rays traced */
-    double device_ms;       /* device time of the render, CUDA events */
+    double device_ms;       /* device time of the render's waves, CUDA events
+                               (buffer set-up and graph capture, once per
+                               configuration, excluded) */
 } bbg_render_stats;
 
 bbg_status bbg_render(bbg_integrator* integrator, const bbg_camera* camera, const bbg_render_params* params,
