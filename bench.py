@@ -318,6 +318,74 @@ def run_guided(args):
     return out
 
 
+def run_batch(args):
+    """The batched uneven multi-scene workload: 16 Cornell-box variants
+    (seeds 0-15: displaced geodesic sphere of 10^4-2x10^6 triangles drawn
+    log-uniform, Lambertian / dielectric / conductor, 256^2-1024^2), 32 spp,
+    12 bounces. Each scene is rendered alone and then all 16 as one batch
+    (every wavefront stage launched once per level for all scenes); paths/s
+    and Mrays/s of both, per-scene Mrays/s, and a bit-exact check of the
+    batch's film of one scene against its own render. Guided vs plain: per
+    scene at 96x96, relMSE against a 4096-spp plain render, guided (trained
+    while rendering) vs plain at 32 spp, and relMSE x time."""
+    from bulbit_b200 import lib, scenes
+    t0 = time.perf_counter()
+    sc = [scenes.cornell_batch_variant(seed) for seed in range(16)]
+    gen_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    accs = [lib.GpuAccel(s) for s in sc]
+    build_s = time.perf_counter() - t0
+    integs = [lib.GpuPathIntegrator(a, s) for a, s in zip(accs, sc)]
+    per_scene, alone_ms, alone_rays = [], 0.0, 0
+    for s, it in zip(sc, integs):
+        it.render(spp=32, seed=0)  # capture
+        f = it.render(spp=32, seed=0)
+        rays = f.stats.closest_rays + f.stats.shadow_rays
+        alone_ms += f.stats.device_ms
+        alone_rays += rays
+        per_scene.append({"scene": s.name, "triangles": s.n_prims, "paths": f.stats.paths, "rays": rays,
+                          "alone_ms": f.stats.device_ms, "alone_mrays_per_s": rays / f.stats.device_ms / 1e3})
+    b = lib.GpuBatch()
+    b.render(integs, spp=32, seeds=[0] * 16)  # capture
+    films, st = b.render(integs, spp=32, seeds=[0] * 16)
+    batch_rays = st.closest_rays + st.shadow_rays
+    k = int(np.argmin([s.n_prims for s in sc]))
+    alone = integs[k].render(spp=32, seed=0)
+    exact = bool(np.array_equal(alone.rgb_sum, films[k].rgb_sum) and np.array_equal(alone.count, films[k].count))
+    # Guided vs plain per scene at a reduced resolution.
+    for s, row in zip(sc, per_scene):
+        s.camera.width = s.camera.height = 96
+        a = lib.GpuAccel(s)
+        it = lib.GpuPathIntegrator(a, s)
+        ref = it.render(spp=4096, seed=7).image()
+        it.render(spp=32, seed=1)
+        pf = it.render(spp=32, seed=2)
+        g = lib.GpuGuide(a.bounds(), seed=5)
+        gf = it.render(spp=32, seed=3, guide=g, train=True, wave_paths=1 << 17, steps=4)
+        ep, eg = rel_mse(pf.image(), ref), rel_mse(gf.image(), ref)
+        row["guided_vs_plain_96px_32spp"] = {"plain_relMSE": ep, "guided_relMSE": eg, "relMSE_ratio": eg / ep,
+                                             "plain_ms": pf.stats.device_ms, "guided_ms": gf.stats.device_ms,
+                                             "equal_time_ratio": eg * gf.stats.device_ms / (ep * pf.stats.device_ms)}
+        it.close()
+        a.close()
+    out = {
+        "metric": "paths/s", "value": st.paths / (st.device_ms / 1e3), "unit": "paths/s",
+        "mrays_per_s": batch_rays / st.device_ms / 1e3, "batch_ms": st.device_ms,
+        "sequential": {"ms": alone_ms, "paths_per_s": st.paths / (alone_ms / 1e3),
+                       "mrays_per_s": alone_rays / alone_ms / 1e3},
+        "speedup_vs_sequential": alone_ms / st.device_ms,
+        "batch_film_equals_alone": exact, "per_scene": per_scene,
+        "config": {"workload": "16 uneven Cornell-box variants (seeds 0-15), 32 spp, 12 bounces, one batch",
+                   "total_triangles": int(sum(s.n_prims for s in sc)), "paths": st.paths,
+                   "scene_generation_s": round(gen_s, 2), "bvh_build_s": round(build_s, 2)},
+    }
+    b.close()
+    for it, a in zip(integs, accs):
+        it.close()
+        a.close()
+    return out
+
+
 def pt_cpu_baseline(scene, res=128):
     """The reference PathIntegrator (oracle/_ref) rendering the same scene at a
     reduced resolution on all host threads: Render() + Rendering::Wait()."""
@@ -347,7 +415,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per query set (smaller cases for profiling)")
-    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided"])
+    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided", "batch"])
     ap.add_argument("--guided-res", type=int, default=256)
     ap.add_argument("--pt-res", type=int, default=1024)
     ap.add_argument("--pt-steps", type=int, default=3)
@@ -380,6 +448,10 @@ def main():
     if args.workload == "guided":
         if rank == 0:
             print(json.dumps({"guided_path_tracing": run_guided(args)}))
+        return
+    if args.workload == "batch":
+        if rank == 0:
+            print(json.dumps({"batched_scenes": run_batch(args)}))
         return
 
     n_rays = args.rays

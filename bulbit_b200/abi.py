@@ -136,6 +136,9 @@ EXPORTS = [
     ("bbg_integrator_light_pmf", I32, [P, P]),
     ("bbg_render", I32, [P, P, P, P, I32, P]),
     ("bbg_sampler_draws", I32, [I32, I32, I32, I32, I32, P]),
+    ("bbg_batch_create", I32, [P]),
+    ("bbg_batch_destroy", I32, [P]),
+    ("bbg_batch_render", I32, [P, I32, P, P, P, P, I32, P]),
     ("bbg_guide_create", I32, [P, C.c_uint64, P]),
     ("bbg_guide_destroy", I32, [P]),
     ("bbg_guide_get_params", I32, [P, P]),

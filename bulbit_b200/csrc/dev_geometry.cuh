@@ -439,6 +439,9 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
     int2 spill[kStackCapacity - kShortStack];
     int sp = 0;
     int32_t node = kNoNode, leaf = kNoNode;
+    // The tree a ray is traced in: the one given, or, when the work source
+    // names one per item (several scenes in one launch), that one.
+    AccelView av = a;
 
     auto push = [&](int32_t ref, float entry) {
         if (sp < kShortStack)
@@ -500,9 +503,13 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
                 {
                     item = r;
                     src.Load(r, &q, &t_min, &t_max);
+                    if constexpr (requires { src.View(r); })
+                    {
+                        av = src.View(r);
+                    }
                     res = TraceResult{ -1, t_max, 0, 0 };
                     sp = 0;
-                    node = a.root;
+                    node = av.root;
                     leaf = kNoNode;
                     busy = true;
                 }
@@ -523,7 +530,7 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
             // Node phase.
             while (node >= 0)
             {
-                const float4* nd = a.wide + 4 * size_t(node);
+                const float4* nd = av.wide + 4 * size_t(node);
                 float4 f0 = __ldg(nd);
                 float4 f1 = __ldg(nd + 1);
                 float4 f2 = __ldg(nd + 2);
@@ -558,11 +565,11 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
             // Leaf phase.
             while (leaf != kNoNode)
             {
-                int2 lf = __ldg(a.leaves + (~leaf));
+                int2 lf = __ldg(av.leaves + (~leaf));
                 bool stop = false;
                 for (int32_t i = 0; i < lf.y; ++i)
                 {
-                    if (TestSlot(a, lf.x + i, q, t_min, t_max, &res))
+                    if (TestSlot(av, lf.x + i, q, t_min, t_max, &res))
                     {
                         if (ANY)
                         {

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 namespace bbg
@@ -81,6 +82,70 @@ struct WaveDev
 
 constexpr int32_t kSpecularBit = 1 << 16;
 constexpr int32_t kAnyNonSpecularBit = 1 << 17;
+// flags bits 20-30: the path's scene within a batch of scenes.
+constexpr int32_t kSceneShift = 20;
+constexpr int32_t kSceneMask = 0x7ff << kSceneShift;
+constexpr int32_t kMaxBatchScenes = 0x800;
+
+struct FilmDev
+{
+    float* rgb_sum;
+    int32_t* count;
+    float* moments;
+    float* path_L; // optional
+};
+
+// The scenes a render's kernels see. OneScene: a single scene, passed as
+// kernel parameters (every path's scene bits are 0). SceneTable: several
+// scenes rendered together; per-scene descriptors and films live in device
+// memory, the batch's pixels are the scenes' pixels one scene after another
+// (pixel_start: prefix sums), and every scene has the same spp.
+struct OneScene
+{
+    SceneDev s;
+    FilmDev f;
+    __device__ __forceinline__ const SceneDev& Scene(int32_t) const { return s; }
+    __device__ __forceinline__ const FilmDev& Film(int32_t) const { return f; }
+    __device__ __forceinline__ int32_t Spp() const { return s.spp; }
+    __device__ __forceinline__ int32_t Locate(int64_t pixel, int64_t* local) const
+    {
+        *local = pixel;
+        return 0;
+    }
+};
+
+struct SceneTable
+{
+    const SceneDev* scenes;
+    const FilmDev* films;
+    const int64_t* pixel_start; // n + 1 entries
+    int32_t n;
+    int32_t spp;
+    __device__ __forceinline__ const SceneDev& Scene(int32_t i) const { return scenes[i]; }
+    __device__ __forceinline__ const FilmDev& Film(int32_t i) const { return films[i]; }
+    __device__ __forceinline__ int32_t Spp() const { return spp; }
+    __device__ __forceinline__ int32_t Locate(int64_t pixel, int64_t* local) const
+    {
+        int32_t lo = 0, hi = n - 1;
+        while (lo < hi)
+        {
+            int32_t mid = (lo + hi + 1) >> 1;
+            if (pixel_start[mid] <= pixel)
+            {
+                lo = mid;
+            }
+            else
+            {
+                hi = mid - 1;
+            }
+        }
+        *local = pixel - pixel_start[lo];
+        return lo;
+    }
+};
+
+template <class Scenes>
+constexpr bool kIsBatch = std::is_same_v<Scenes, SceneTable>;
 
 // Warp-aggregated append of `pred` lanes to a queue counter.
 __device__ __forceinline__ int32_t Append(int32_t* counter, bool pred)
@@ -102,16 +167,20 @@ __device__ __forceinline__ int32_t Append(int32_t* counter, bool pred)
 
 // Render loop body (src/integrator/integrator.cpp:185-190) and
 // PerspectiveCamera::SampleRay (src/camera/perspective_camera.cpp:40-52).
-__global__ void __launch_bounds__(kBlock) RaygenKernel(SceneDev s, WaveDev w)
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock) RaygenKernel(Scenes sc, WaveDev w)
 {
     const int64_t base = w.wave[0];
     const int64_t n = w.wave[1];
-    const CameraDev& c = s.camera;
+    const int32_t spp = sc.Spp();
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
     {
         int64_t path = base + i;
-        int32_t sample = int32_t(path % s.spp);
-        int64_t pixel = path / s.spp;
+        int32_t sample = int32_t(path % spp);
+        int64_t pixel;
+        int32_t scene = sc.Locate(path / spp, &pixel);
+        const SceneDev& s = sc.Scene(scene);
+        const CameraDev& c = s.camera;
         int32_t px = int32_t(pixel % c.width);
         int32_t py = int32_t(pixel / c.width);
         uint64_t rng = SamplerStart(px, py, s.seed, sample);
@@ -134,7 +203,7 @@ __global__ void __launch_bounds__(kBlock) RaygenKernel(SceneDev s, WaveDev w)
         w.beta[i] = make_float4(1, 1, 1, 0);
         w.L[i] = make_float4(0, 0, 0, 0);
         w.rng[i] = rng;
-        w.flags[i] = 0;
+        w.flags[i] = scene << kSceneShift;
         w.queue[0][i] = int32_t(i);
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -146,6 +215,8 @@ __global__ void __launch_bounds__(kBlock) RaygenKernel(SceneDev s, WaveDev w)
 }
 
 // ---------------------------------------------------------------- intersect
+//
+// In a batch, each work item is traced in its own scene's tree (View).
 
 // Work items of the closest-hit pass: queue entry j -> its path's ray.
 struct ClosestSrc
@@ -199,12 +270,38 @@ struct ShadowSrc
     }
 };
 
-__global__ void __launch_bounds__(kBlock) ClosestKernel(SceneDev s, WaveDev w, int parity)
+struct ClosestBatchSrc : ClosestSrc
+{
+    const int32_t* flags;
+    const SceneDev* scenes;
+    __device__ __forceinline__ AccelView View(int32_t j) const { return scenes[flags[q[j]] >> kSceneShift].accel; }
+};
+
+struct ShadowBatchSrc : ShadowSrc
+{
+    const int32_t* flags;
+    const SceneDev* scenes;
+    __device__ __forceinline__ AccelView View(int32_t j) const
+    {
+        return scenes[flags[__float_as_int(sh_d[j].w)] >> kSceneShift].accel;
+    }
+};
+
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock) ClosestKernel(Scenes sc, WaveDev w, int parity)
 {
     const int32_t n = w.counts[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
         atomicAdd(w.stats, (unsigned long long)n);
+    }
+    const SceneDev& s = sc.Scene(0);
+    if constexpr (kIsBatch<Scenes>)
+    {
+        // Every scene of a batch uses the child-box layout (checked on the host).
+        ClosestBatchSrc src{ { w.queue[parity], w.o_pdf, w.d_eta, w.hit }, w.flags, sc.scenes };
+        TracePersistent<false>(s.accel, n, w.counts + 3, src);
+        return;
     }
     ClosestSrc src{ w.queue[parity], w.o_pdf, w.d_eta, w.hit };
     if (s.accel.ordered)
@@ -221,12 +318,20 @@ __global__ void __launch_bounds__(kBlock) ClosestKernel(SceneDev s, WaveDev w, i
     }
 }
 
-__global__ void __launch_bounds__(kBlock) ShadowKernel(SceneDev s, WaveDev w)
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock) ShadowKernel(Scenes sc, WaveDev w)
 {
     const int32_t n = w.counts[2];
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
         atomicAdd(w.stats + 1, (unsigned long long)n);
+    }
+    const SceneDev& s = sc.Scene(0);
+    if constexpr (kIsBatch<Scenes>)
+    {
+        ShadowBatchSrc src{ { w.sh_o, w.sh_d, w.sh_c, w.L }, w.flags, sc.scenes };
+        TracePersistent<true>(s.accel, n, w.counts + 4, src);
+        return;
     }
     ShadowSrc src{ w.sh_o, w.sh_d, w.sh_c, w.L };
     if (s.accel.ordered)
@@ -383,7 +488,8 @@ __device__ __forceinline__ int32_t SampleLight(const SceneDev& s, float u, float
     return offset;
 }
 
-__global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int parity)
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock) ShadeKernel(Scenes sc, WaveDev w, int parity)
 {
     const int32_t* q = w.queue[parity];
     int32_t* q_next = w.queue[parity ^ 1];
@@ -399,6 +505,7 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int
         Spec beta{ b4.x, b4.y, b4.z }, L{ L4.x, L4.y, L4.z };
         uint64_t rng = w.rng[slot];
         int32_t fl = w.flags[slot];
+        const SceneDev& s = sc.Scene(fl >> kSceneShift);
         int32_t bounce = fl & 0xffff;
         bool specular_bounce = (fl & kSpecularBit) != 0;
         bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
@@ -585,7 +692,8 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(SceneDev s, WaveDev w, int
             w.d_eta[slot] = make_float4(rd.x, rd.y, rd.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
             w.rng[slot] = rng;
-            w.flags[slot] = bounce | (specular_bounce ? kSpecularBit : 0) | (any_non_specular ? kAnyNonSpecularBit : 0);
+            w.flags[slot] = (fl & kSceneMask) | bounce | (specular_bounce ? kSpecularBit : 0) |
+                            (any_non_specular ? kAnyNonSpecularBit : 0);
         }
         int32_t qi = Append(&w.counts[parity ^ 1], cont);
         if (cont)
@@ -1141,33 +1249,30 @@ __global__ void ResetKernel(WaveDev w, int parity)
 
 // ---------------------------------------------------------------- film
 
-struct FilmDev
-{
-    float* rgb_sum;
-    int32_t* count;
-    float* moments;
-    float* path_L; // optional
-};
 
 // Film::AddSample over each pixel's samples in order (src/reconstruction/film.cpp:26-37).
-__global__ void __launch_bounds__(kBlock) FilmKernel(SceneDev s, WaveDev w, FilmDev f)
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock) FilmKernel(Scenes sc, WaveDev w)
 {
     const int64_t base = w.wave[0];
-    const int64_t n_pixels = w.wave[1] / s.spp;
-    const int64_t pixel0 = base / s.spp;
+    const int32_t spp = sc.Spp();
+    const int64_t n_pixels = w.wave[1] / spp;
+    const int64_t pixel0 = base / spp;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n_pixels; i += int64_t(gridDim.x) * blockDim.x)
     {
+        int64_t p;
+        const FilmDev& f = sc.Film(sc.Locate(pixel0 + i, &p));
         Spec sum = spec(0);
         int32_t count = 0;
         float m0 = 0, m1 = 0;
-        for (int32_t k = 0; k < s.spp; ++k)
+        for (int32_t k = 0; k < spp; ++k)
         {
-            int64_t slot = i * s.spp + k;
+            int64_t slot = i * spp + k;
             float4 L4 = w.L[slot];
             Spec L{ L4.x, L4.y, L4.z };
             if (f.path_L)
             {
-                float* dst = f.path_L + 3 * (base + slot);
+                float* dst = f.path_L + 3 * (p * spp + k);
                 dst[0] = L.r;
                 dst[1] = L.g;
                 dst[2] = L.b;
@@ -1183,7 +1288,6 @@ __global__ void __launch_bounds__(kBlock) FilmKernel(SceneDev s, WaveDev w, Film
             m0 = m0 * (1 - alpha) + l * alpha;
             m1 = m1 * (1 - alpha) + (l * l) * alpha;
         }
-        int64_t p = pixel0 + i;
         f.rgb_sum[3 * p] = sum.r;
         f.rgb_sum[3 * p + 1] = sum.g;
         f.rgb_sum[3 * p + 2] = sum.b;
@@ -1366,20 +1470,23 @@ struct bbg_integrator
 namespace
 {
 
-struct Grids
+// Persistent grid sizes of the stage kernels for one kind of scene set.
+template <class Scenes>
+struct GridsT
 {
     int raygen, closest, shade, shadow, film, shade_a, shade_b;
-    Grids()
+    GridsT()
     {
-        raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel), kBlock);
-        closest = PersistentGrid(reinterpret_cast<const void*>(ClosestKernel), kBlock);
-        shade = PersistentGrid(reinterpret_cast<const void*>(ShadeKernel), kBlock);
-        shadow = PersistentGrid(reinterpret_cast<const void*>(ShadowKernel), kBlock);
-        film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel), kBlock);
+        raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel<Scenes>), kBlock);
+        closest = PersistentGrid(reinterpret_cast<const void*>(ClosestKernel<Scenes>), kBlock);
+        shade = PersistentGrid(reinterpret_cast<const void*>(ShadeKernel<Scenes>), kBlock);
+        shadow = PersistentGrid(reinterpret_cast<const void*>(ShadowKernel<Scenes>), kBlock);
+        film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel<Scenes>), kBlock);
         shade_a = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeA), kBlock);
         shade_b = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeB), kBlock);
     }
 };
+using Grids = GridsT<OneScene>;
 
 // Guided-rendering context of one render (guide == nullptr: plain).
 struct GuideCtx
@@ -1419,8 +1526,9 @@ __global__ void GuideWaveStartKernel(WaveDev w, GuideDev g)
 bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, const GuideCtx& gc, int parity,
                         cudaStream_t st)
 {
+    const OneScene one{ s, FilmDev{} };
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
-    ClosestKernel<<<gr.closest, kBlock, 0, st>>>(s, w, parity);
+    ClosestKernel<<<gr.closest, kBlock, 0, st>>>(one, w, parity);
     if (gc.guide)
     {
         GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(s, w, gc.dev, parity);
@@ -1429,9 +1537,9 @@ bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, co
     }
     else
     {
-        ShadeKernel<<<gr.shade, kBlock, 0, st>>>(s, w, parity);
+        ShadeKernel<<<gr.shade, kBlock, 0, st>>>(one, w, parity);
     }
-    ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(s, w);
+    ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(one, w);
     return BBG_OK;
 }
 
@@ -1439,7 +1547,8 @@ bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const 
                    int iterations, cudaStream_t st)
 {
     WaveDev w = I->Wave();
-    RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(s, w);
+    const OneScene one{ s, film };
+    RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(one, w);
     if (gc.guide && gc.dev.train)
     {
         GuideWaveStartKernel<<<gr.raygen, kBlock, 0, st>>>(w, gc.dev);
@@ -1448,7 +1557,7 @@ bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const 
     {
         BBG_TRY(EnqueueLevel(gr, s, w, gc, k & 1, st));
     }
-    FilmKernel<<<gr.film, kBlock, 0, st>>>(s, w, film);
+    FilmKernel<<<gr.film, kBlock, 0, st>>>(one, w);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
 }
@@ -1486,29 +1595,10 @@ bool SameFilm(const FilmDev& a, const FilmDev& b)
     return std::memcmp(&a, &b, sizeof(FilmDev)) == 0;
 }
 
-bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p, bbg_film* film, bbg_memory mem,
-                  bbg_render_stats* stats)
+// The kernels' view of one scene: its accel, shading data, lights and camera.
+SceneDev MakeSceneDev(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p)
 {
-    if (!cam || !p || !film || !film->rgb_sum || !film->count || !film->moments || p->spp <= 0 || cam->width <= 0 ||
-        cam->height <= 0 || (mem != BBG_MEM_HOST && mem != BBG_MEM_DEVICE))
-    {
-        return Fail(BBG_ERR_INVALID_ARG, "bbg_render: bad argument");
-    }
     bbg_accel* a = I->accel;
-    const int64_t n_pixels = int64_t(cam->width) * cam->height;
-    const int64_t n_paths = n_pixels * p->spp;
-
-    // Wave size: whole pixels, at most the requested (or default) paths.
-    int64_t want = p->wave_paths > 0 ? p->wave_paths : (int64_t(1) << 22);
-    int64_t px_per_wave = std::max<int64_t>(1, want / p->spp);
-    px_per_wave = std::min(px_per_wave, n_pixels);
-    const int64_t wave_paths = px_per_wave * p->spp;
-    if (wave_paths > (int64_t(1) << 30))
-    {
-        return Fail(BBG_ERR_INVALID_ARG, "wave of %lld paths exceeds 2^30", (long long)wave_paths);
-    }
-    BBG_TRY(I->Reserve(wave_paths));
-
     SceneDev s{};
     s.accel = a->view();
     s.prim_info = I->prim_info.p;
@@ -1544,6 +1634,32 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     std::memcpy(s.camera.v, cam->v, sizeof(float) * 3);
     s.camera.lens_radius = cam->lens_radius;
     s.camera.filter_extent = cam->filter_extent;
+    return s;
+}
+
+bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p, bbg_film* film, bbg_memory mem,
+                  bbg_render_stats* stats)
+{
+    if (!cam || !p || !film || !film->rgb_sum || !film->count || !film->moments || p->spp <= 0 || cam->width <= 0 ||
+        cam->height <= 0 || (mem != BBG_MEM_HOST && mem != BBG_MEM_DEVICE))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_render: bad argument");
+    }
+    const int64_t n_pixels = int64_t(cam->width) * cam->height;
+    const int64_t n_paths = n_pixels * p->spp;
+
+    // Wave size: whole pixels, at most the requested (or default) paths.
+    int64_t want = p->wave_paths > 0 ? p->wave_paths : (int64_t(1) << 22);
+    int64_t px_per_wave = std::max<int64_t>(1, want / p->spp);
+    px_per_wave = std::min(px_per_wave, n_pixels);
+    const int64_t wave_paths = px_per_wave * p->spp;
+    if (wave_paths > (int64_t(1) << 30))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "wave of %lld paths exceeds 2^30", (long long)wave_paths);
+    }
+    BBG_TRY(I->Reserve(wave_paths));
+
+    SceneDev s = MakeSceneDev(I, cam, p);
 
     FilmDev f{};
     if (mem == BBG_MEM_DEVICE)
@@ -1673,7 +1789,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         if (extra > 0)
         {
             // Re-run the film pass for this wave after the extra levels.
-            FilmKernel<<<gr.film, kBlock, 0, st>>>(s, I->Wave(), f);
+            FilmKernel<<<gr.film, kBlock, 0, st>>>(OneScene{ s, f }, I->Wave());
         }
         if (gc.guide && gc.dev.train)
         {
@@ -1707,6 +1823,17 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         stats->shadow_rays = int64_t(c[1]);
         stats->device_ms = ms;
     }
+    return BBG_OK;
+}
+
+// Queue counters, statistics and the pinned wave record of a wave engine
+// (an integrator, or the engine of a batch); the stream must exist.
+bbg_status InitWaveEngine(bbg_integrator* I)
+{
+    BBG_TRY(I->counts.alloc(8));
+    BBG_TRY(I->stats.alloc(2));
+    BBG_TRY(I->wave.alloc(2));
+    BBG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&I->wave_host), 2 * sizeof(int64_t)));
     return BBG_OK;
 }
 
@@ -1800,11 +1927,228 @@ bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim
     BBG_TRY(I->alias_prob.upload(prob.data(), prob.size(), I->stream));
     BBG_TRY(I->alias_idx.upload(alias.data(), alias.size(), I->stream));
     BBG_TRY(I->infinite.upload(infinite.data(), infinite.size(), I->stream));
-    BBG_TRY(I->counts.alloc(8));
-    BBG_TRY(I->stats.alloc(2));
-    BBG_TRY(I->wave.alloc(2));
-    BBG_CUDA(cudaMallocHost(reinterpret_cast<void**>(&I->wave_host), 2 * sizeof(int64_t)));
+    BBG_TRY(InitWaveEngine(I));
     BBG_CUDA(cudaStreamSynchronize(I->stream));
+    return BBG_OK;
+}
+
+
+// ---------------------------------------------------------------- batches of scenes
+
+using BatchGrids = GridsT<SceneTable>;
+
+bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int parity, cudaStream_t st)
+{
+    ResetKernel<<<1, 1, 0, st>>>(w, parity);
+    ClosestKernel<<<gr.closest, kBlock, 0, st>>>(t, w, parity);
+    ShadeKernel<<<gr.shade, kBlock, 0, st>>>(t, w, parity);
+    ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(t, w);
+    return BBG_OK;
+}
+
+bbg_status EnqueueBatch(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int iterations, cudaStream_t st)
+{
+    RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(t, w);
+    for (int k = 0; k < iterations; ++k)
+    {
+        BBG_TRY(EnqueueBatchLevel(gr, t, w, k & 1, st));
+    }
+    FilmKernel<<<gr.film, kBlock, 0, st>>>(t, w);
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+} // namespace
+
+struct bbg_batch
+{
+    bbg_integrator engine; // wave buffers, stream and graph of the batch
+    bbg::DevBuf<bbg::SceneDev> scenes;
+    bbg::DevBuf<bbg::FilmDev> films;
+    bbg::DevBuf<int64_t> pixel_start;
+    std::vector<bbg::SceneDev> host_scenes;
+    std::vector<bbg::FilmDev> host_films;
+    std::vector<int64_t> host_pixel_start;
+    // Graph of one wave, valid while these stay the same (the tables are read
+    // from device memory at run time, so their contents may change).
+    int64_t graph_capacity = -1;
+    int graph_iterations = -1;
+    bbg::SceneTable graph_table{};
+};
+
+namespace
+{
+
+bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrators, const bbg_camera* cams,
+                       const bbg_render_params* params, bbg_film* films, bbg_memory mem, bbg_render_stats* stats)
+{
+    if (n <= 0 || n > kMaxBatchScenes || !integrators || !cams || !params || !films ||
+        (mem != BBG_MEM_HOST && mem != BBG_MEM_DEVICE))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: bad argument");
+    }
+    const int32_t spp = params[0].spp;
+    int iterations = 0;
+    B->host_scenes.resize(size_t(n));
+    B->host_films.resize(size_t(n));
+    B->host_pixel_start.assign(size_t(n) + 1, 0);
+    for (int32_t i = 0; i < n; ++i)
+    {
+        bbg_integrator* I = integrators[i];
+        const bbg_camera* cam = &cams[i];
+        const bbg_film* film = &films[i];
+        if (!I || params[i].spp != spp || spp <= 0 || params[i].guide || cam->width <= 0 || cam->height <= 0 ||
+            !film->rgb_sum || !film->count || !film->moments)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: scene %d: bad argument (spp must match, no guide)",
+                        int(i));
+        }
+        if (!I->accel->ordered)
+        {
+            return Fail(BBG_ERR_UNSUPPORTED, "bbg_batch_render: scene %d uses the reference-order traversal", int(i));
+        }
+        const int64_t n_pixels = int64_t(cam->width) * cam->height;
+        B->host_scenes[i] = MakeSceneDev(I, cam, &params[i]);
+        FilmDev f{};
+        if (mem == BBG_MEM_DEVICE)
+        {
+            f = FilmDev{ film->rgb_sum, film->count, film->moments, film->path_L };
+        }
+        else
+        {
+            BBG_TRY(I->film_rgb.alloc(3 * size_t(n_pixels)));
+            BBG_TRY(I->film_count.alloc(size_t(n_pixels)));
+            BBG_TRY(I->film_moments.alloc(2 * size_t(n_pixels)));
+            f = FilmDev{ I->film_rgb.p, I->film_count.p, I->film_moments.p, nullptr };
+            if (film->path_L)
+            {
+                BBG_TRY(I->film_path_L.alloc(3 * size_t(n_pixels) * size_t(spp)));
+                f.path_L = I->film_path_L.p;
+            }
+        }
+        B->host_films[i] = f;
+        B->host_pixel_start[i + 1] = B->host_pixel_start[i] + n_pixels;
+        iterations = std::max(iterations, I->max_bounces + 1);
+    }
+    const int64_t total_pixels = B->host_pixel_start[size_t(n)];
+    const int64_t n_paths = total_pixels * spp;
+
+    bbg_integrator* E = &B->engine;
+    cudaStream_t st = E->stream;
+    BBG_TRY(B->scenes.upload(B->host_scenes.data(), B->host_scenes.size(), st));
+    BBG_TRY(B->films.upload(B->host_films.data(), B->host_films.size(), st));
+    BBG_TRY(B->pixel_start.upload(B->host_pixel_start.data(), B->host_pixel_start.size(), st));
+    const SceneTable table{ B->scenes.p, B->films.p, B->pixel_start.p, n, spp };
+
+    int64_t want = params[0].wave_paths > 0 ? params[0].wave_paths : (int64_t(1) << 22);
+    const int64_t px_per_wave = std::min(std::max<int64_t>(1, want / spp), total_pixels);
+    const int64_t wave_paths = px_per_wave * spp;
+    if (wave_paths > (int64_t(1) << 30))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "wave of %lld paths exceeds 2^30", (long long)wave_paths);
+    }
+    BBG_TRY(E->Reserve(wave_paths));
+    const BatchGrids gr;
+    const bool use_graph = params[0].use_graph != 0;
+    if (use_graph && (!E->graph || B->graph_capacity != wave_paths || B->graph_iterations != iterations ||
+                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0))
+    {
+        if (E->graph)
+        {
+            cudaGraphExecDestroy(E->graph);
+            E->graph = nullptr;
+        }
+        cudaGraph_t g;
+        BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        bbg_status es = EnqueueBatch(gr, table, E->Wave(), iterations, st);
+        cudaError_t ce = cudaStreamEndCapture(st, &g);
+        BBG_TRY(es);
+        if (ce != cudaSuccess)
+        {
+            return Fail(BBG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(ce));
+        }
+        BBG_CUDA(cudaGraphInstantiate(&E->graph, g, 0));
+        cudaGraphDestroy(g);
+        B->graph_capacity = wave_paths;
+        B->graph_iterations = iterations;
+        B->graph_table = table;
+    }
+
+    BBG_CUDA(cudaMemsetAsync(E->stats.p, 0, 2 * sizeof(unsigned long long), st));
+    cudaEvent_t e0, e1;
+    BBG_CUDA(cudaEventCreate(&e0));
+    BBG_CUDA(cudaEventCreate(&e1));
+    BBG_CUDA(cudaEventRecord(e0, st));
+    for (int64_t base = 0; base < n_paths; base += wave_paths)
+    {
+        int64_t count = std::min(wave_paths, n_paths - base);
+        BBG_CUDA(cudaStreamSynchronize(st)); // the pinned wave record is reused
+        E->wave_host[0] = base;
+        E->wave_host[1] = count;
+        BBG_CUDA(cudaMemcpyAsync(E->wave.p, E->wave_host, 2 * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+        if (use_graph)
+        {
+            BBG_CUDA(cudaGraphLaunch(E->graph, st));
+        }
+        else
+        {
+            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), iterations, st));
+        }
+        // Paths still queued come from material-less surfaces (no bounce
+        // counted): drain them level by level, then redo the film pass.
+        int32_t left = 0;
+        int parity = iterations & 1;
+        BBG_CUDA(cudaMemcpyAsync(&left, E->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        BBG_CUDA(cudaStreamSynchronize(st));
+        int extra = 0;
+        while (left > 0)
+        {
+            if (++extra > 4096)
+            {
+                return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
+            }
+            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), parity, st));
+            parity ^= 1;
+            BBG_CUDA(cudaMemcpyAsync(&left, E->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            BBG_CUDA(cudaStreamSynchronize(st));
+        }
+        if (extra > 0)
+        {
+            FilmKernel<<<gr.film, kBlock, 0, st>>>(table, E->Wave());
+        }
+    }
+    BBG_CUDA(cudaEventRecord(e1, st));
+    BBG_CUDA(cudaStreamSynchronize(st));
+    BBG_CUDA(cudaGetLastError());
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (mem == BBG_MEM_HOST)
+    {
+        for (int32_t i = 0; i < n; ++i)
+        {
+            const FilmDev& f = B->host_films[i];
+            const size_t np = size_t(B->host_pixel_start[i + 1] - B->host_pixel_start[i]);
+            BBG_CUDA(cudaMemcpy(films[i].rgb_sum, f.rgb_sum, 3 * sizeof(float) * np, cudaMemcpyDeviceToHost));
+            BBG_CUDA(cudaMemcpy(films[i].count, f.count, sizeof(int32_t) * np, cudaMemcpyDeviceToHost));
+            BBG_CUDA(cudaMemcpy(films[i].moments, f.moments, 2 * sizeof(float) * np, cudaMemcpyDeviceToHost));
+            if (films[i].path_L)
+            {
+                BBG_CUDA(cudaMemcpy(films[i].path_L, f.path_L, 3 * sizeof(float) * np * size_t(spp),
+                                    cudaMemcpyDeviceToHost));
+            }
+        }
+    }
+    if (stats)
+    {
+        unsigned long long c[2];
+        BBG_CUDA(cudaMemcpy(c, E->stats.p, sizeof(c), cudaMemcpyDeviceToHost));
+        stats->paths = n_paths;
+        stats->closest_rays = int64_t(c[0]);
+        stats->shadow_rays = int64_t(c[1]);
+        stats->device_ms = ms;
+    }
     return BBG_OK;
 }
 
@@ -1884,6 +2228,47 @@ bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sampl
     BBG_CUDA(cudaGetLastError());
     BBG_CUDA(cudaMemcpy(out, d.p, sizeof(float) * size_t(n), cudaMemcpyDeviceToHost));
     return BBG_OK;
+}
+
+bbg_status bbg_batch_create(bbg_batch** out)
+{
+    if (!out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_create: bad argument");
+    }
+    *out = nullptr;
+    BBG_TRY(CheckDevice());
+    auto* B = new bbg_batch;
+    cudaError_t e = cudaStreamCreateWithFlags(&B->engine.stream, cudaStreamNonBlocking);
+    bbg_status s = e == cudaSuccess ? InitWaveEngine(&B->engine)
+                                    : Fail(BBG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    if (s != BBG_OK)
+    {
+        delete B;
+        return s;
+    }
+    *out = B;
+    return BBG_OK;
+}
+
+bbg_status bbg_batch_destroy(bbg_batch* B)
+{
+    if (B)
+    {
+        if (B->engine.stream) cudaStreamSynchronize(B->engine.stream);
+        delete B;
+    }
+    return BBG_OK;
+}
+
+bbg_status bbg_batch_render(bbg_batch* B, int32_t n, bbg_integrator* const* integrators, const bbg_camera* cameras,
+                            const bbg_render_params* params, bbg_film* films, bbg_memory mem, bbg_render_stats* stats)
+{
+    if (!B)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: null batch");
+    }
+    return RenderBatch(B, n, integrators, cameras, params, films, mem, stats);
 }
 
 } // extern "C"

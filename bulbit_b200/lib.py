@@ -318,6 +318,48 @@ class GpuGuide:
         return loss.value
 
 
+class GpuBatch:
+    """Several scenes rendered together (bbg_batch_*)."""
+
+    def __init__(self):
+        self.h = C.c_void_p()
+        check(get_lib().bbg_batch_create(C.byref(self.h)), "bbg_batch_create")
+
+    def close(self):
+        if self.h:
+            get_lib().bbg_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def render(self, integrators, spp, seeds=None, wave_paths=0, use_graph=True, path_L=False):
+        """Render each GpuPathIntegrator's scene (its own camera) at spp ->
+        (list of Film, batch RenderStats)."""
+        n = len(integrators)
+        seeds = [it.scene.seed for it in integrators] if seeds is None else seeds
+        ints = (C.c_void_p * n)(*[it.h.value for it in integrators])
+        cams = (abi.Camera * n)(*[camera(it.scene.camera) for it in integrators])
+        params = (abi.RenderParams * n)()
+        films, fstructs = [], (abi.Film * n)()
+        spps = [spp] * n if isinstance(spp, int) else list(spp)
+        for i, it in enumerate(integrators):
+            params[i].spp = spps[i]
+            params[i].seed = seeds[i]
+            params[i].wave_paths = wave_paths
+            params[i].use_graph = 1 if use_graph else 0
+            film = Film(cams[i].width, cams[i].height, spps[i], path_L=path_L)
+            films.append(film)
+            fstructs[i] = film.struct()
+        stats = abi.RenderStats()
+        check(get_lib().bbg_batch_render(self.h, n, ints, cams, params, fstructs, abi.BBG_MEM_HOST, C.byref(stats)),
+              "bbg_batch_render")
+        return films, stats
+
+
 def mixture_sample(outputs, u):
     """Sample the vMF mixtures that network output rows (n, 40) describe, with
     uniforms u (n, 3) -> (unit directions (n, 3), mixture density (n,))."""

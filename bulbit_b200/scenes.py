@@ -353,6 +353,38 @@ def icosphere(levels):
     return v, f.astype(np.int32)
 
 
+def geodesic_sphere(freq):
+    """Unit geodesic sphere of any frequency: every icosahedron face divided
+    into freq^2 triangles on a barycentric grid, points pushed to the sphere
+    (20 freq^2 triangles, 10 freq^2 + 2 vertices). Returns (vertices float64,
+    faces int32)."""
+    v0, f0 = icosphere(0)
+    n = int(freq)
+    ii, jj = np.meshgrid(np.arange(n + 1), np.arange(n + 1), indexing="ij")
+    keep = ii + jj <= n
+    ii, jj = ii[keep], jj[keep]
+    local = -np.ones((n + 1, n + 1), np.int64)
+    local[ii, jj] = np.arange(ii.size)
+    # Triangles of one face in grid indices (both orientations of cells).
+    ti, tj = np.meshgrid(np.arange(n), np.arange(n), indexing="ij")
+    up = ti + tj < n
+    dn = ti + tj < n - 1
+    tri_up = np.stack([local[ti[up], tj[up]], local[ti[up] + 1, tj[up]], local[ti[up], tj[up] + 1]], 1)
+    tri_dn = np.stack([local[ti[dn] + 1, tj[dn]], local[ti[dn] + 1, tj[dn] + 1], local[ti[dn], tj[dn] + 1]], 1)
+    tris = np.concatenate([tri_up, tri_dn], 0)
+    pts, faces = [], []
+    for k, (a, b, c) in enumerate(f0):
+        p = v0[a] + (v0[b] - v0[a]) * (ii[:, None] / n) + (v0[c] - v0[a]) * (jj[:, None] / n)
+        pts.append(p / np.linalg.norm(p, axis=1)[:, None])
+        faces.append(tris + k * ii.size)
+    pts = np.concatenate(pts, 0)
+    faces = np.concatenate(faces, 0)
+    # Merge the copies of points on shared edges and corners.
+    key = np.round(pts * 1e9).astype(np.int64)
+    _, first, inv = np.unique(key, axis=0, return_index=True, return_inverse=True)
+    return pts[first], inv.reshape(-1)[faces].astype(np.int32)
+
+
 def _vertex_normals(pos, faces):
     p = pos.astype(np.float64)
     fn = np.cross(p[faces[:, 1]] - p[faces[:, 0]], p[faces[:, 2]] - p[faces[:, 0]])
@@ -374,7 +406,7 @@ CORNELL_GREEN = (0.14, 0.45, 0.091)
 CORNELL_WHITE = (0.725, 0.71, 0.68)
 
 
-def cornell_icosphere(levels=8, width=1024, height=1024, spp=64, max_bounces=16, seed=3,
+def cornell_icosphere(levels=8, width=1024, height=1024, spp=64, max_bounces=16, seed=3, freq=None,
                       displacement=0.02, sphere_material=None, light_emission=(17.0, 12.0, 4.0)):
     """Closed Cornell box [-1,1]^3 (12 triangles: left wall red, right wall
     green, floor/ceiling/back/front white), a 0.5x0.5 one-sided diffuse area
@@ -383,7 +415,7 @@ def cornell_icosphere(levels=8, width=1024, height=1024, spp=64, max_bounces=16,
     subdivisions, each vertex displaced radially by N(0, displacement^2),
     gold conductor of roughness 0.2 unless sphere_material is given. The
     camera sits inside the box near the front wall, looking at the back wall."""
-    s = SceneData(name=f"cornell_ico{levels}")
+    s = SceneData(name=f"cornell_ico{levels}" if freq is None else f"cornell_geo{freq}")
     mats = [diffuse(CORNELL_RED), diffuse(CORNELL_GREEN), diffuse(CORNELL_WHITE),
             sphere_material or conductor(GOLD_ETA, GOLD_K, 0.2)]
     RED, GREEN, WHITE, SPHERE = 0, 1, 2, 3
@@ -429,7 +461,7 @@ def cornell_icosphere(levels=8, width=1024, height=1024, spp=64, max_bounces=16,
     box_tri = np.array(tri, np.int64)
 
     # Icosphere.
-    v, f = icosphere(levels)
+    v, f = icosphere(levels) if freq is None else geodesic_sphere(freq)
     rng = PCG32Streams(seed, np.arange(v.shape[0], dtype=np.uint64))
     g, _ = _gaussian_pairs(rng, displacement)
     radius = 0.5 + g.astype(np.float64)
@@ -464,4 +496,32 @@ def cornell_icosphere(levels=8, width=1024, height=1024, spp=64, max_bounces=16,
     s.camera = camera_spec((0.0, 0.0, 0.98), (0.0, 0.0, -1.0), (0.0, 1.0, 0.0), 70.0, 0.0, 1.0,
                            width, height)
     s.spp, s.seed, s.max_bounces = spp, 0, max_bounces
+    return s
+
+
+BATCH_RESOLUTIONS = (256, 512, 768, 1024)
+
+
+def cornell_batch_variant(seed, spp=32, max_bounces=12, resolution=None):
+    """One of the uneven Cornell-box variants rendered as a batch: the sphere
+    is a displaced geodesic sphere whose triangle count is drawn log-uniform
+    in [10^4, 2x10^6] (frequency round(sqrt(count / 20))), its material drawn
+    uniformly from {Lambertian albedo U(0.2, 0.9) per channel, smooth
+    dielectric IOR 1.5, gold conductor roughness U(0.05, 0.5)}, and the
+    resolution from 256^2 .. 1024^2; all draws from numpy's generator seeded
+    with `seed`, the displacement from PCG32 seeded with it."""
+    rng = np.random.default_rng(seed)
+    count = math.exp(rng.uniform(math.log(1e4), math.log(2e6)))
+    freq = max(1, int(round(math.sqrt(count / 20))))
+    kind = int(rng.integers(3))
+    if kind == 0:
+        mat = diffuse(tuple(float(x) for x in rng.uniform(0.2, 0.9, 3)))
+    elif kind == 1:
+        mat = dielectric(1.5)
+    else:
+        mat = conductor(GOLD_ETA, GOLD_K, float(rng.uniform(0.05, 0.5)))
+    res = int(rng.choice(BATCH_RESOLUTIONS)) if resolution is None else resolution
+    s = cornell_icosphere(width=res, height=res, spp=spp, max_bounces=max_bounces, seed=seed, freq=freq,
+                          sphere_material=mat)
+    s.name = f"variant{seed}:geo{freq}:{['lambertian', 'dielectric', 'conductor'][kind]}:{res}"
     return s

@@ -377,6 +377,31 @@ typedef struct bbg_render_stats
 bbg_status bbg_render(bbg_integrator* integrator, const bbg_camera* camera, const bbg_render_params* params,
                       bbg_film* film, bbg_memory mem, bbg_render_stats* stats);
 
+/* --------------------------------------------------- batches of scenes */
+
+/* Several scenes rendered together (no counterpart in the reference, whose
+ * Render() takes one scene). Each stage of the wavefront — ray generation,
+ * closest hit, shading, shadow rays, film — runs once per bounce level over
+ * the paths of all scenes: every path is traced in its own scene's tree and
+ * shaded with its own materials and lights, so scenes of very different
+ * sizes share the GPU instead of leaving it idle in turn. Every path keeps
+ * the sampler stream and arithmetic of its scene's own bbg_render, so each
+ * scene's film equals rendering that scene alone. */
+typedef struct bbg_batch bbg_batch;
+
+bbg_status bbg_batch_create(bbg_batch** out);
+bbg_status bbg_batch_destroy(bbg_batch* batch);
+/* Renders n scenes (1 <= n <= 2048): integrators[i] seen through cameras[i]
+ * with params[i] into films[i] (host or device memory as mem says). Every
+ * params[i].spp must be equal and params[i].guide NULL; every accel must use
+ * the default traversal (BBG_TRAVERSAL_ORDERED). The wave size and CUDA-graph
+ * choice come from params[0]. stats (optional) receives the batch's totals.
+ * Calls on one batch must not overlap, nor overlap renders of the same
+ * integrators (their film buffers are reused for host-memory films). */
+bbg_status bbg_batch_render(bbg_batch* batch, int32_t n, bbg_integrator* const* integrators,
+                            const bbg_camera* cameras, const bbg_render_params* params, bbg_film* films,
+                            bbg_memory mem, bbg_render_stats* stats);
+
 /* The first n uniform draws of IndependentSampler after
  * StartPixelSample(pixel, sample) with the given seed, computed on the device. */
 bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out);
