@@ -104,6 +104,11 @@ class RenderParams(C.Structure):
                 ("guide_select", C.c_float), ("guide_steps", C.c_int32)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("block", C.c_int32), ("short_stack", C.c_int32), ("wave_paths", C.c_int64),
+                ("probe_ms", C.c_double), ("from_cache", C.c_int32)]
+
+
 class Film(C.Structure):
     _fields_ = [("rgb_sum", C.c_void_p), ("count", C.c_void_p), ("moments", C.c_void_p),
                 ("path_L", C.c_void_p)]
@@ -139,6 +144,9 @@ EXPORTS = [
     ("bbg_batch_create", I32, [P]),
     ("bbg_batch_destroy", I32, [P]),
     ("bbg_batch_render", I32, [P, I32, P, P, P, P, I32, P]),
+    ("bbg_integrator_autotune", I32, [P, P, P, P]),
+    ("bbg_integrator_set_tuning", I32, [P, P]),
+    ("bbg_batch_autotune", I32, [P, I32, P, P, P, P]),
     ("bbg_guide_create", I32, [P, C.c_uint64, P]),
     ("bbg_guide_destroy", I32, [P]),
     ("bbg_guide_get_params", I32, [P, P]),

@@ -423,7 +423,9 @@ constexpr int kTraversalBlock = 128;
 // distinct banks whatever depth each lane is at.
 constexpr int kShortStack = BBG_SHORT_STACK;
 
-template <bool ANY, class Src>
+// BLOCK: threads per block of the launch; SHORT: stack entries kept in
+// shared memory per thread (0: the whole stack in local memory).
+template <bool ANY, class Src, int BLOCK = kTraversalBlock, int SHORT = kShortStack>
 __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, int32_t* next, Src& src)
 {
     const unsigned kFull = 0xffffffffu;
@@ -434,9 +436,9 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
     RayQ q;
     float t_min = 0, t_max = 0;
     TraceResult res{ -1, 0, 0, 0 };
-    __shared__ int32_t s_ref[kShortStack * kTraversalBlock];
-    __shared__ float s_entry[kShortStack * kTraversalBlock];
-    int2 spill[kStackCapacity - kShortStack];
+    __shared__ int32_t s_ref[(SHORT > 0 ? SHORT : 1) * BLOCK];
+    __shared__ float s_entry[(SHORT > 0 ? SHORT : 1) * BLOCK];
+    int2 spill[kStackCapacity - SHORT];
     int sp = 0;
     int32_t node = kNoNode, leaf = kNoNode;
     // The tree a ray is traced in: the one given, or, when the work source
@@ -444,14 +446,14 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
     AccelView av = a;
 
     auto push = [&](int32_t ref, float entry) {
-        if (sp < kShortStack)
+        if (sp < SHORT)
         {
-            s_ref[sp * kTraversalBlock + tid] = ref;
-            s_entry[sp * kTraversalBlock + tid] = entry;
+            s_ref[sp * BLOCK + tid] = ref;
+            s_entry[sp * BLOCK + tid] = entry;
         }
         else
         {
-            spill[sp - kShortStack] = make_int2(ref, __float_as_int(entry));
+            spill[sp - SHORT] = make_int2(ref, __float_as_int(entry));
         }
         ++sp;
     };
@@ -461,14 +463,14 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
             --sp;
             int32_t ref;
             float entry;
-            if (sp < kShortStack)
+            if (sp < SHORT)
             {
-                ref = s_ref[sp * kTraversalBlock + tid];
-                entry = s_entry[sp * kTraversalBlock + tid];
+                ref = s_ref[sp * BLOCK + tid];
+                entry = s_entry[sp * BLOCK + tid];
             }
             else
             {
-                int2 e = spill[sp - kShortStack];
+                int2 e = spill[sp - SHORT];
                 ref = e.x;
                 entry = __int_as_float(e.y);
             }

@@ -24,6 +24,9 @@
 
 #include <algorithm>
 #include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -287,8 +290,19 @@ struct ShadowBatchSrc : ShadowSrc
     }
 };
 
-template <class Scenes>
-__global__ void __launch_bounds__(kBlock) ClosestKernel(Scenes sc, WaveDev w, int parity)
+// Launch shapes of the traversal passes the autotuner chooses from: threads
+// per block and stack entries per thread kept in shared memory (0: the
+// whole traversal stack in local memory).
+struct TraversalShape
+{
+    int block;
+    int short_stack;
+};
+constexpr int kNumShapes = 4;
+constexpr TraversalShape kShapes[kNumShapes] = { { 128, 16 }, { 128, 0 }, { 128, 8 }, { 256, 16 } };
+
+template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack>
+__global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int parity)
 {
     const int32_t n = w.counts[parity];
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -300,13 +314,13 @@ __global__ void __launch_bounds__(kBlock) ClosestKernel(Scenes sc, WaveDev w, in
     {
         // Every scene of a batch uses the child-box layout (checked on the host).
         ClosestBatchSrc src{ { w.queue[parity], w.o_pdf, w.d_eta, w.hit }, w.flags, sc.scenes };
-        TracePersistent<false>(s.accel, n, w.counts + 3, src);
+        TracePersistent<false, ClosestBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
         return;
     }
     ClosestSrc src{ w.queue[parity], w.o_pdf, w.d_eta, w.hit };
     if (s.accel.ordered)
     {
-        TracePersistent<false>(s.accel, n, w.counts + 3, src);
+        TracePersistent<false, ClosestSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
         return;
     }
     for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
@@ -318,8 +332,8 @@ __global__ void __launch_bounds__(kBlock) ClosestKernel(Scenes sc, WaveDev w, in
     }
 }
 
-template <class Scenes>
-__global__ void __launch_bounds__(kBlock) ShadowKernel(Scenes sc, WaveDev w)
+template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack>
+__global__ void __launch_bounds__(BLOCK) ShadowKernel(Scenes sc, WaveDev w)
 {
     const int32_t n = w.counts[2];
     if (blockIdx.x == 0 && threadIdx.x == 0)
@@ -330,13 +344,13 @@ __global__ void __launch_bounds__(kBlock) ShadowKernel(Scenes sc, WaveDev w)
     if constexpr (kIsBatch<Scenes>)
     {
         ShadowBatchSrc src{ { w.sh_o, w.sh_d, w.sh_c, w.L }, w.flags, sc.scenes };
-        TracePersistent<true>(s.accel, n, w.counts + 4, src);
+        TracePersistent<true, ShadowBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
         return;
     }
     ShadowSrc src{ w.sh_o, w.sh_d, w.sh_c, w.L };
     if (s.accel.ordered)
     {
-        TracePersistent<true>(s.accel, n, w.counts + 4, src);
+        TracePersistent<true, ShadowSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
         return;
     }
     for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
@@ -1358,6 +1372,11 @@ struct bbg_integrator
     GuideDev graph_guide{};
     bbg_guide* graph_guide_handle = nullptr;
     float graph_guide_lr = 0;
+    int graph_shape = -1;
+    // Launch shape of the traversal passes (index into kShapes) and wave size
+    // for renders that do not name one (0: 2^22 paths); set by the autotuner.
+    int32_t shape = 0;
+    int64_t tuned_wave = 0;
 
     bbg_status ReserveGuide(int64_t n, int32_t rec_cap, int32_t steps)
     {
@@ -1474,19 +1493,59 @@ namespace
 template <class Scenes>
 struct GridsT
 {
-    int raygen, closest, shade, shadow, film, shade_a, shade_b;
+    int raygen, closest[kNumShapes], shade, shadow[kNumShapes], film, shade_a, shade_b;
     GridsT()
     {
         raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel<Scenes>), kBlock);
-        closest = PersistentGrid(reinterpret_cast<const void*>(ClosestKernel<Scenes>), kBlock);
+        Shape<0>();
+        Shape<1>();
+        Shape<2>();
+        Shape<3>();
         shade = PersistentGrid(reinterpret_cast<const void*>(ShadeKernel<Scenes>), kBlock);
-        shadow = PersistentGrid(reinterpret_cast<const void*>(ShadowKernel<Scenes>), kBlock);
         film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel<Scenes>), kBlock);
         shade_a = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeA), kBlock);
         shade_b = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeB), kBlock);
     }
+    template <int K>
+    void Shape()
+    {
+        constexpr TraversalShape t = kShapes[K];
+        closest[K] = PersistentGrid(
+            reinterpret_cast<const void*>(ClosestKernel<Scenes, t.block, t.short_stack>), t.block);
+        shadow[K] = PersistentGrid(
+            reinterpret_cast<const void*>(ShadowKernel<Scenes, t.block, t.short_stack>), t.block);
+    }
 };
 using Grids = GridsT<OneScene>;
+
+template <int K, class Scenes>
+void LaunchTraceShape(const GridsT<Scenes>& gr, const Scenes& sc, const WaveDev& w, int parity, bool shadow,
+                      cudaStream_t st)
+{
+    constexpr TraversalShape t = kShapes[K];
+    if (shadow)
+    {
+        ShadowKernel<Scenes, t.block, t.short_stack><<<gr.shadow[K], t.block, 0, st>>>(sc, w);
+    }
+    else
+    {
+        ClosestKernel<Scenes, t.block, t.short_stack><<<gr.closest[K], t.block, 0, st>>>(sc, w, parity);
+    }
+}
+
+// The closest-hit (shadow = false) or shadow pass with launch shape `shape`.
+template <class Scenes>
+void LaunchTrace(int shape, const GridsT<Scenes>& gr, const Scenes& sc, const WaveDev& w, int parity, bool shadow,
+                 cudaStream_t st)
+{
+    switch (shape)
+    {
+    case 1: LaunchTraceShape<1>(gr, sc, w, parity, shadow, st); break;
+    case 2: LaunchTraceShape<2>(gr, sc, w, parity, shadow, st); break;
+    case 3: LaunchTraceShape<3>(gr, sc, w, parity, shadow, st); break;
+    default: LaunchTraceShape<0>(gr, sc, w, parity, shadow, st); break;
+    }
+}
 
 // Guided-rendering context of one render (guide == nullptr: plain).
 struct GuideCtx
@@ -1524,11 +1583,11 @@ __global__ void GuideWaveStartKernel(WaveDev w, GuideDev g)
 }
 
 bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, const GuideCtx& gc, int parity,
-                        cudaStream_t st)
+                        int shape, cudaStream_t st)
 {
     const OneScene one{ s, FilmDev{} };
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
-    ClosestKernel<<<gr.closest, kBlock, 0, st>>>(one, w, parity);
+    LaunchTrace(shape, gr, one, w, parity, false, st);
     if (gc.guide)
     {
         GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(s, w, gc.dev, parity);
@@ -1539,12 +1598,12 @@ bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, co
     {
         ShadeKernel<<<gr.shade, kBlock, 0, st>>>(one, w, parity);
     }
-    ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(one, w);
+    LaunchTrace(shape, gr, one, w, parity, true, st);
     return BBG_OK;
 }
 
 bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const FilmDev& film, const GuideCtx& gc,
-                   int iterations, cudaStream_t st)
+                   int iterations, int shape, cudaStream_t st)
 {
     WaveDev w = I->Wave();
     const OneScene one{ s, film };
@@ -1555,7 +1614,7 @@ bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const 
     }
     for (int k = 0; k < iterations; ++k)
     {
-        BBG_TRY(EnqueueLevel(gr, s, w, gc, k & 1, st));
+        BBG_TRY(EnqueueLevel(gr, s, w, gc, k & 1, shape, st));
     }
     FilmKernel<<<gr.film, kBlock, 0, st>>>(one, w);
     BBG_CUDA(cudaGetLastError());
@@ -1648,8 +1707,8 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     const int64_t n_pixels = int64_t(cam->width) * cam->height;
     const int64_t n_paths = n_pixels * p->spp;
 
-    // Wave size: whole pixels, at most the requested (or default) paths.
-    int64_t want = p->wave_paths > 0 ? p->wave_paths : (int64_t(1) << 22);
+    // Wave size: whole pixels, at most the requested (or tuned, or default) paths.
+    int64_t want = p->wave_paths > 0 ? p->wave_paths : I->tuned_wave > 0 ? I->tuned_wave : (int64_t(1) << 22);
     int64_t px_per_wave = std::max<int64_t>(1, want / p->spp);
     px_per_wave = std::min(px_per_wave, n_pixels);
     const int64_t wave_paths = px_per_wave * p->spp;
@@ -1722,7 +1781,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     if (use_graph && (!I->graph || I->graph_capacity != wave_paths || I->graph_iterations != iterations ||
                       !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f) ||
                       I->graph_guide_handle != gc.guide || !SameGuide(I->graph_guide, gc.dev) ||
-                      I->graph_guide_lr != gc.lr))
+                      I->graph_guide_lr != gc.lr || I->graph_shape != I->shape))
     {
         if (I->graph)
         {
@@ -1731,7 +1790,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         cudaGraph_t g;
         BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        bbg_status es = Enqueue(I, gr, s, f, gc, iterations, st);
+        bbg_status es = Enqueue(I, gr, s, f, gc, iterations, I->shape, st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         BBG_TRY(es);
         if (ce != cudaSuccess)
@@ -1747,6 +1806,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         I->graph_guide = gc.dev;
         I->graph_guide_handle = gc.guide;
         I->graph_guide_lr = gc.lr;
+        I->graph_shape = I->shape;
     }
 
     // Device time of the render itself: buffer set-up and graph capture
@@ -1765,7 +1825,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         else
         {
-            BBG_TRY(Enqueue(I, gr, s, f, gc, iterations, st));
+            BBG_TRY(Enqueue(I, gr, s, f, gc, iterations, I->shape, st));
         }
         // Paths still queued after max_bounces + 1 levels only come from
         // material-less surfaces, which do not count a bounce
@@ -1781,7 +1841,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
             {
                 return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
             }
-            BBG_TRY(EnqueueLevel(gr, s, I->Wave(), gc, parity, st));
+            BBG_TRY(EnqueueLevel(gr, s, I->Wave(), gc, parity, I->shape, st));
             parity ^= 1;
             BBG_CUDA(cudaMemcpyAsync(&left, I->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             BBG_CUDA(cudaStreamSynchronize(st));
@@ -1937,21 +1997,23 @@ bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim
 
 using BatchGrids = GridsT<SceneTable>;
 
-bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int parity, cudaStream_t st)
+bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int parity, int shape,
+                             cudaStream_t st)
 {
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
-    ClosestKernel<<<gr.closest, kBlock, 0, st>>>(t, w, parity);
+    LaunchTrace(shape, gr, t, w, parity, false, st);
     ShadeKernel<<<gr.shade, kBlock, 0, st>>>(t, w, parity);
-    ShadowKernel<<<gr.shadow, kBlock, 0, st>>>(t, w);
+    LaunchTrace(shape, gr, t, w, parity, true, st);
     return BBG_OK;
 }
 
-bbg_status EnqueueBatch(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int iterations, cudaStream_t st)
+bbg_status EnqueueBatch(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int iterations, int shape,
+                        cudaStream_t st)
 {
     RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(t, w);
     for (int k = 0; k < iterations; ++k)
     {
-        BBG_TRY(EnqueueBatchLevel(gr, t, w, k & 1, st));
+        BBG_TRY(EnqueueBatchLevel(gr, t, w, k & 1, shape, st));
     }
     FilmKernel<<<gr.film, kBlock, 0, st>>>(t, w);
     BBG_CUDA(cudaGetLastError());
@@ -1974,6 +2036,9 @@ struct bbg_batch
     int64_t graph_capacity = -1;
     int graph_iterations = -1;
     bbg::SceneTable graph_table{};
+    int graph_shape = -1;
+    int32_t shape = 0;      // as bbg_integrator::shape, for the batch
+    int64_t tuned_wave = 0; // as bbg_integrator::tuned_wave
 };
 
 namespace
@@ -2040,7 +2105,9 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     BBG_TRY(B->pixel_start.upload(B->host_pixel_start.data(), B->host_pixel_start.size(), st));
     const SceneTable table{ B->scenes.p, B->films.p, B->pixel_start.p, n, spp };
 
-    int64_t want = params[0].wave_paths > 0 ? params[0].wave_paths : (int64_t(1) << 22);
+    int64_t want = params[0].wave_paths > 0 ? params[0].wave_paths
+                   : B->tuned_wave > 0      ? B->tuned_wave
+                                            : (int64_t(1) << 22);
     const int64_t px_per_wave = std::min(std::max<int64_t>(1, want / spp), total_pixels);
     const int64_t wave_paths = px_per_wave * spp;
     if (wave_paths > (int64_t(1) << 30))
@@ -2051,7 +2118,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     const BatchGrids gr;
     const bool use_graph = params[0].use_graph != 0;
     if (use_graph && (!E->graph || B->graph_capacity != wave_paths || B->graph_iterations != iterations ||
-                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0))
+                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != B->shape))
     {
         if (E->graph)
         {
@@ -2060,7 +2127,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         cudaGraph_t g;
         BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        bbg_status es = EnqueueBatch(gr, table, E->Wave(), iterations, st);
+        bbg_status es = EnqueueBatch(gr, table, E->Wave(), iterations, B->shape, st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         BBG_TRY(es);
         if (ce != cudaSuccess)
@@ -2072,6 +2139,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         B->graph_capacity = wave_paths;
         B->graph_iterations = iterations;
         B->graph_table = table;
+        B->graph_shape = B->shape;
     }
 
     BBG_CUDA(cudaMemsetAsync(E->stats.p, 0, 2 * sizeof(unsigned long long), st));
@@ -2092,7 +2160,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         else
         {
-            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), iterations, st));
+            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), iterations, B->shape, st));
         }
         // Paths still queued come from material-less surfaces (no bounce
         // counted): drain them level by level, then redo the film pass.
@@ -2107,7 +2175,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             {
                 return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
             }
-            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), parity, st));
+            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), parity, B->shape, st));
             parity ^= 1;
             BBG_CUDA(cudaMemcpyAsync(&left, E->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             BBG_CUDA(cudaStreamSynchronize(st));
@@ -2149,6 +2217,191 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         stats->shadow_rays = int64_t(c[1]);
         stats->device_ms = ms;
     }
+    return BBG_OK;
+}
+
+
+// ---------------------------------------------------------------- autotuning
+
+// One probe render of a candidate: launch shape, wave size, spp -> its
+// device time and paths.
+using ProbeFn = std::function<bbg_status(int shape, int64_t wave, int32_t spp, double* ms, int64_t* paths)>;
+
+std::mutex g_tune_mutex;
+std::map<std::vector<int64_t>, bbg_tuning> g_tune_cache;
+
+bbg_tuning TuningOf(int shape, int64_t wave, double per_mpath)
+{
+    bbg_tuning t{};
+    t.block = kShapes[shape].block;
+    t.short_stack = kShapes[shape].short_stack;
+    t.wave_paths = wave;
+    t.probe_ms = per_mpath;
+    return t;
+}
+
+int ShapeOf(int32_t block, int32_t short_stack)
+{
+    for (int k = 0; k < kNumShapes; ++k)
+    {
+        if (kShapes[k].block == block && kShapes[k].short_stack == short_stack)
+        {
+            return k;
+        }
+    }
+    return -1;
+}
+
+// Times each launch shape at the default wave size, then each wave size the
+// render can fill with the best shape; every candidate twice, the faster
+// run counting, compared per path. A probe of wave w renders enough samples
+// per pixel for about two waves (at most the render's spp).
+bbg_status Tune(const std::vector<int64_t>& key, int64_t pixels, int32_t spp, const ProbeFn& probe, bbg_tuning* out)
+{
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end())
+        {
+            *out = it->second;
+            out->from_cache = 1;
+            return BBG_OK;
+        }
+    }
+    const int64_t total = pixels * spp;
+    auto measure = [&](int shape, int64_t wave, double* per_mpath) -> bbg_status {
+        int32_t ps = int32_t(std::min<int64_t>(spp, std::max<int64_t>(1, (2 * wave + pixels - 1) / pixels)));
+        double best = 1e300;
+        for (int r = 0; r < 2; ++r)
+        {
+            double ms = 0;
+            int64_t paths = 0;
+            BBG_TRY(probe(shape, wave, ps, &ms, &paths));
+            best = std::min(best, ms / (double(paths) / 1e6));
+        }
+        *per_mpath = best;
+        return BBG_OK;
+    };
+    const int64_t w0 = std::min<int64_t>(int64_t(1) << 22, total);
+    int best_shape = 0;
+    int64_t best_wave = w0;
+    double best_t = 1e300;
+    for (int k = 0; k < kNumShapes; ++k)
+    {
+        double t;
+        BBG_TRY(measure(k, w0, &t));
+        if (t < best_t)
+        {
+            best_t = t;
+            best_shape = k;
+        }
+    }
+    for (int e = 20; e <= 23; ++e)
+    {
+        int64_t wave = int64_t(1) << e;
+        if (wave == w0 || wave > total)
+        {
+            continue;
+        }
+        double t;
+        BBG_TRY(measure(best_shape, wave, &t));
+        if (t < best_t)
+        {
+            best_t = t;
+            best_wave = wave;
+        }
+    }
+    *out = TuningOf(best_shape, best_wave, best_t);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = *out;
+    return BBG_OK;
+}
+
+std::vector<int64_t> SceneKey(const bbg_integrator* I, const bbg_camera* cam, int32_t spp)
+{
+    const bbg_accel* a = I->accel;
+    return { a->n_prims, a->n_nodes, a->max_depth, cam->width, cam->height, spp, I->max_bounces };
+}
+
+bbg_status AutotuneIntegrator(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p, bbg_tuning* out)
+{
+    if (!cam || !p || !out || p->spp <= 0 || p->guide || cam->width <= 0 || cam->height <= 0)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_integrator_autotune: bad argument");
+    }
+    const int64_t pixels = int64_t(cam->width) * cam->height;
+    std::vector<float> rgb(3 * static_cast<size_t>(pixels)), mom(2 * static_cast<size_t>(pixels));
+    std::vector<int32_t> cnt(static_cast<size_t>(pixels));
+    ProbeFn probe = [&](int shape, int64_t wave, int32_t spp, double* ms, int64_t* paths) -> bbg_status {
+        const int saved = I->shape;
+        I->shape = shape;
+        bbg_render_params q = *p;
+        q.spp = spp;
+        q.wave_paths = wave;
+        q.use_graph = 1;
+        bbg_film f{ rgb.data(), cnt.data(), mom.data(), nullptr };
+        bbg_render_stats st{};
+        bbg_status s = Render(I, cam, &q, &f, BBG_MEM_HOST, &st);
+        I->shape = saved;
+        *ms = st.device_ms;
+        *paths = st.paths;
+        return s;
+    };
+    std::vector<int64_t> key = SceneKey(I, cam, p->spp);
+    key.insert(key.begin(), 0);
+    BBG_TRY(Tune(key, pixels, p->spp, probe, out));
+    I->shape = ShapeOf(out->block, out->short_stack);
+    I->tuned_wave = out->wave_paths;
+    return BBG_OK;
+}
+
+bbg_status AutotuneBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrators, const bbg_camera* cams,
+                         const bbg_render_params* params, bbg_tuning* out)
+{
+    if (n <= 0 || n > kMaxBatchScenes || !integrators || !cams || !params || !out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_autotune: bad argument");
+    }
+    std::vector<int64_t> key{ 1, n };
+    int64_t pixels = 0;
+    std::vector<std::vector<float>> rgb(static_cast<size_t>(n)), mom(static_cast<size_t>(n));
+    std::vector<std::vector<int32_t>> cnt(static_cast<size_t>(n));
+    std::vector<bbg_film> films(static_cast<size_t>(n));
+    for (int32_t i = 0; i < n; ++i)
+    {
+        if (!integrators[i] || cams[i].width <= 0 || cams[i].height <= 0)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_autotune: scene %d: bad argument", int(i));
+        }
+        std::vector<int64_t> k = SceneKey(integrators[i], &cams[i], params[i].spp);
+        key.insert(key.end(), k.begin(), k.end());
+        const int64_t px = int64_t(cams[i].width) * cams[i].height;
+        pixels += px;
+        rgb[i].resize(3 * size_t(px));
+        mom[i].resize(2 * size_t(px));
+        cnt[i].resize(size_t(px));
+        films[i] = bbg_film{ rgb[i].data(), cnt[i].data(), mom[i].data(), nullptr };
+    }
+    ProbeFn probe = [&](int shape, int64_t wave, int32_t spp, double* ms, int64_t* paths) -> bbg_status {
+        const int saved = B->shape;
+        B->shape = shape;
+        std::vector<bbg_render_params> q(params, params + n);
+        for (auto& r : q)
+        {
+            r.spp = spp;
+            r.wave_paths = wave;
+            r.use_graph = 1;
+        }
+        bbg_render_stats st{};
+        bbg_status s = RenderBatch(B, n, integrators, cams, q.data(), films.data(), BBG_MEM_HOST, &st);
+        B->shape = saved;
+        *ms = st.device_ms;
+        *paths = st.paths;
+        return s;
+    };
+    BBG_TRY(Tune(key, pixels, params[0].spp, probe, out));
+    B->shape = ShapeOf(out->block, out->short_stack);
+    B->tuned_wave = out->wave_paths;
     return BBG_OK;
 }
 
@@ -2269,6 +2522,37 @@ bbg_status bbg_batch_render(bbg_batch* B, int32_t n, bbg_integrator* const* inte
         return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: null batch");
     }
     return RenderBatch(B, n, integrators, cameras, params, films, mem, stats);
+}
+
+bbg_status bbg_integrator_autotune(bbg_integrator* I, const bbg_camera* camera, const bbg_render_params* params,
+                                   bbg_tuning* out)
+{
+    if (!I)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_integrator_autotune: null integrator");
+    }
+    return AutotuneIntegrator(I, camera, params, out);
+}
+
+bbg_status bbg_integrator_set_tuning(bbg_integrator* I, const bbg_tuning* t)
+{
+    if (!I || !t || ShapeOf(t->block, t->short_stack) < 0 || t->wave_paths < 0 || t->wave_paths > (int64_t(1) << 30))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_integrator_set_tuning: not a supported configuration");
+    }
+    I->shape = ShapeOf(t->block, t->short_stack);
+    I->tuned_wave = t->wave_paths;
+    return BBG_OK;
+}
+
+bbg_status bbg_batch_autotune(bbg_batch* B, int32_t n, bbg_integrator* const* integrators, const bbg_camera* cameras,
+                              const bbg_render_params* params, bbg_tuning* out)
+{
+    if (!B)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_autotune: null batch");
+    }
+    return AutotuneBatch(B, n, integrators, cameras, params, out);
 }
 
 } // extern "C"

@@ -257,6 +257,22 @@ class GpuPathIntegrator:
                                    C.byref(film.stats)), "bbg_render")
         return film
 
+    def autotune(self, spp=None, seed=None, camera_spec=None):
+        """bbg_integrator_autotune for renders at spp -> abi.Tuning."""
+        cam = camera(camera_spec or self.scene.camera)
+        p = abi.RenderParams()
+        p.spp = spp or self.scene.spp
+        p.seed = self.scene.seed if seed is None else seed
+        out = abi.Tuning()
+        check(get_lib().bbg_integrator_autotune(self.h, C.byref(cam), C.byref(p), C.byref(out)),
+              "bbg_integrator_autotune")
+        return out
+
+    def set_tuning(self, block=128, short_stack=16, wave_paths=0):
+        t = abi.Tuning()
+        t.block, t.short_stack, t.wave_paths = block, short_stack, wave_paths
+        check(get_lib().bbg_integrator_set_tuning(self.h, C.byref(t)), "bbg_integrator_set_tuning")
+
     def render_device(self, cam, params, film_struct, stats):
         check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(params), C.byref(film_struct),
                                    abi.BBG_MEM_DEVICE, C.byref(stats)), "bbg_render")
@@ -335,6 +351,19 @@ class GpuBatch:
             self.close()
         except Exception:
             pass
+
+    def autotune(self, integrators, spp, seeds=None):
+        n = len(integrators)
+        seeds = [it.scene.seed for it in integrators] if seeds is None else seeds
+        ints = (C.c_void_p * n)(*[it.h.value for it in integrators])
+        cams = (abi.Camera * n)(*[camera(it.scene.camera) for it in integrators])
+        params = (abi.RenderParams * n)()
+        for i in range(n):
+            params[i].spp = spp
+            params[i].seed = seeds[i]
+        out = abi.Tuning()
+        check(get_lib().bbg_batch_autotune(self.h, n, ints, cams, params, C.byref(out)), "bbg_batch_autotune")
+        return out
 
     def render(self, integrators, spp, seeds=None, wave_paths=0, use_graph=True, path_L=False):
         """Render each GpuPathIntegrator's scene (its own camera) at spp ->

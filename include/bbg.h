@@ -402,6 +402,38 @@ bbg_status bbg_batch_render(bbg_batch* batch, int32_t n, bbg_integrator* const* 
                             const bbg_camera* cameras, const bbg_render_params* params, bbg_film* films,
                             bbg_memory mem, bbg_render_stats* stats);
 
+/* ------------------------------------------------------------ autotuning */
+
+/* Launch configuration of a render: the traversal passes' threads per block
+ * and traversal-stack entries per thread kept in shared memory (0: the whole
+ * stack in local memory), and the wave size (paths in flight, which sizes
+ * every queue). No counterpart in the reference. */
+typedef struct bbg_tuning
+{
+    int32_t block;        /* 128 or 256 */
+    int32_t short_stack;  /* 0, 8 or 16 (16 only with block 128 or 256) */
+    int64_t wave_paths;
+    double probe_ms;      /* device time per million paths of the chosen probe */
+    int32_t from_cache;   /* 1: reused from an identical scene, nothing timed */
+} bbg_tuning;
+
+/* Chooses the configuration for renders of this scene, camera size, spp and
+ * bounce limit by timing short probe renders (first each launch shape at the
+ * default wave size, then each wave size from 2^20 to 2^23 paths that the
+ * render can fill), keeps it for the integrator's later renders that leave
+ * wave_paths at 0, and caches it per scene signature (primitive and node
+ * counts, tree depth, image size, spp, bounces) for the process, so a later
+ * identical scene is not timed again. params: spp and seed of the renders to
+ * tune for (guide must be NULL). */
+bbg_status bbg_integrator_autotune(bbg_integrator* integrator, const bbg_camera* camera,
+                                   const bbg_render_params* params, bbg_tuning* out);
+/* Sets the configuration directly (block/short_stack must be one of the
+ * combinations above; wave_paths 0 = default). */
+bbg_status bbg_integrator_set_tuning(bbg_integrator* integrator, const bbg_tuning* tuning);
+/* The same for a batch of scenes (the arguments of bbg_batch_render). */
+bbg_status bbg_batch_autotune(bbg_batch* batch, int32_t n, bbg_integrator* const* integrators,
+                              const bbg_camera* cameras, const bbg_render_params* params, bbg_tuning* out);
+
 /* The first n uniform draws of IndependentSampler after
  * StartPixelSample(pixel, sample) with the given seed, computed on the device. */
 bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out);
