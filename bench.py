@@ -225,16 +225,28 @@ def run_pt(args, barrier, world):
     fs = abi.Film()
     fs.rgb_sum, fs.count, fs.moments, fs.path_L = rgb.data_ptr(), cnt.data_ptr(), mom.data_ptr(), None
     stats = abi.RenderStats()
-    for _ in range(max(1, args.warmup)):
-        integ.render_device(cam, params, fs, stats)
     steps = max(1, args.pt_steps)
-    barrier()
-    dev_ms, rays = 0.0, 0
-    for _ in range(steps):
-        integ.render_device(cam, params, fs, stats)
-        dev_ms += stats.device_ms
-        rays += stats.closest_rays + stats.shadow_rays
-    barrier()
+
+    def timed():
+        for _ in range(max(1, args.warmup)):
+            integ.render_device(cam, params, fs, stats)
+        barrier()
+        ms, r = 0.0, 0
+        for _ in range(steps):
+            integ.render_device(cam, params, fs, stats)
+            ms += stats.device_ms
+            r += stats.closest_rays + stats.shadow_rays
+        barrier()
+        return ms, r
+
+    # Default launch configuration, then the autotuned one (which the
+    # reported value uses; params.wave_paths = 0 lets the tuned wave apply).
+    default_ms, _ = timed()
+    t0 = time.perf_counter()
+    tuning = integ.autotune(spp=64, seed=0)
+    tune_s = time.perf_counter() - t0
+    params.wave_paths = 0
+    dev_ms, rays = timed()
     # End to end through the C ABI with a host film (copied back in the call).
     t0 = time.perf_counter()
     film = integ.render(spp=64)
@@ -244,13 +256,16 @@ def run_pt(args, barrier, world):
         "value": world * paths * steps / (dev_ms / 1e3), "unit": "paths/s",
         "mrays_per_s": world * rays / (dev_ms / 1e3) / 1e6, "ms_per_frame": dev_ms / steps,
         "steps": steps, "closest_rays_per_frame": stats.closest_rays, "shadow_rays_per_frame": stats.shadow_rays,
+        "default_config_ms_per_frame": default_ms / steps,
         "config": {"workload": PT_WORKLOAD if res == 1024 else f"{PT_WORKLOAD} (reduced to {res}x{res})",
-                   "bvh_build_s": round(build_s, 3), "wave_paths": args.pt_wave or 1 << 22,
+                   "bvh_build_s": round(build_s, 3), "default_wave_paths": args.pt_wave,
+                   "tuned": {"block": tuning.block, "short_stack": tuning.short_stack,
+                             "wave_paths": tuning.wave_paths, "autotune_s": round(tune_s, 2)},
                    "cuda_graph": True},
         "image_mean": float(np.nanmean(film.image())),
         "e2e": {"value": world * paths / e2e_s, "unit": "paths/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": n_pix * (12 + 4 + 8)},
-        "gpu_launches_per_frame": None,
+        "gpu_launches_per_frame": -(-paths // (tuning.wave_paths - tuning.wave_paths % 64)) * (2 + 4 * 17),
     }
     integ.close()
     acc.close()
@@ -324,7 +339,8 @@ def run_batch(args):
     log-uniform, Lambertian / dielectric / conductor, 256^2-1024^2), 32 spp,
     12 bounces. Each scene is rendered alone and then all 16 as one batch
     (every wavefront stage launched once per level for all scenes); paths/s
-    and Mrays/s of both, per-scene Mrays/s, and a bit-exact check of the
+    and Mrays/s of both (each autotuned: the batch as a whole, every scene
+    alone for itself), per-scene Mrays/s, and a bit-exact check of the
     batch's film of one scene against its own render. Guided vs plain: per
     scene at 96x96, relMSE against a 4096-spp plain render, guided (trained
     while rendering) vs plain at 32 spp, and relMSE x time."""
@@ -337,6 +353,10 @@ def run_batch(args):
     build_s = time.perf_counter() - t0
     integs = [lib.GpuPathIntegrator(a, s) for a, s in zip(accs, sc)]
     per_scene, alone_ms, alone_rays = [], 0.0, 0
+    t0 = time.perf_counter()
+    for it in integs:
+        it.autotune(spp=32, seed=0)
+    tune_alone_s = time.perf_counter() - t0
     for s, it in zip(sc, integs):
         it.render(spp=32, seed=0)  # capture
         f = it.render(spp=32, seed=0)
@@ -346,6 +366,11 @@ def run_batch(args):
         per_scene.append({"scene": s.name, "triangles": s.n_prims, "paths": f.stats.paths, "rays": rays,
                           "alone_ms": f.stats.device_ms, "alone_mrays_per_s": rays / f.stats.device_ms / 1e3})
     b = lib.GpuBatch()
+    b.render(integs, spp=32, seeds=[0] * 16)  # capture
+    _, st_default = b.render(integs, spp=32, seeds=[0] * 16)
+    t0 = time.perf_counter()
+    bt = b.autotune(integs, spp=32, seeds=[0] * 16)
+    tune_batch_s = time.perf_counter() - t0
     b.render(integs, spp=32, seeds=[0] * 16)  # capture
     films, st = b.render(integs, spp=32, seeds=[0] * 16)
     batch_rays = st.closest_rays + st.shadow_rays
@@ -374,6 +399,9 @@ def run_batch(args):
         "sequential": {"ms": alone_ms, "paths_per_s": st.paths / (alone_ms / 1e3),
                        "mrays_per_s": alone_rays / alone_ms / 1e3},
         "speedup_vs_sequential": alone_ms / st.device_ms,
+        "batch_default_config_ms": st_default.device_ms,
+        "tuning": {"batch": {"block": bt.block, "short_stack": bt.short_stack, "wave_paths": bt.wave_paths},
+                   "batch_autotune_s": round(tune_batch_s, 2), "per_scene_autotune_s": round(tune_alone_s, 2)},
         "batch_film_equals_alone": exact, "per_scene": per_scene,
         "config": {"workload": "16 uneven Cornell-box variants (seeds 0-15), 32 spp, 12 bounces, one batch",
                    "total_triangles": int(sum(s.n_prims for s in sc)), "paths": st.paths,

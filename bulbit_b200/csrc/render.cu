@@ -2252,8 +2252,8 @@ int ShapeOf(int32_t block, int32_t short_stack)
     return -1;
 }
 
-// Times each launch shape at the default wave size, then each wave size the
-// render can fill with the best shape; every candidate twice, the faster
+// Times each launch shape at the default wave size, then each wave size
+// (2^20 .. 2^24 paths) the render can fill with the best shape; every candidate twice, the faster
 // run counting, compared per path. A probe of wave w renders enough samples
 // per pixel for about two waves (at most the render's spp).
 bbg_status Tune(const std::vector<int64_t>& key, int64_t pixels, int32_t spp, const ProbeFn& probe, bbg_tuning* out)
@@ -2296,7 +2296,7 @@ bbg_status Tune(const std::vector<int64_t>& key, int64_t pixels, int32_t spp, co
             best_shape = k;
         }
     }
-    for (int e = 20; e <= 23; ++e)
+    for (int e = 20; e <= 24; ++e)
     {
         int64_t wave = int64_t(1) << e;
         if (wave == w0 || wave > total)

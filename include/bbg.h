@@ -419,7 +419,7 @@ typedef struct bbg_tuning
 
 /* Chooses the configuration for renders of this scene, camera size, spp and
  * bounce limit by timing short probe renders (first each launch shape at the
- * default wave size, then each wave size from 2^20 to 2^23 paths that the
+ * default wave size, then each wave size from 2^20 to 2^24 paths that the
  * render can fill), keeps it for the integrator's later renders that leave
  * wave_paths at 0, and caches it per scene signature (primitive and node
  * counts, tree depth, image size, spp, bounces) for the process, so a later
