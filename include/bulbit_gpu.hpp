@@ -1,0 +1,119 @@
+// C++ drop-in for the reference renderer's ray-query and path-tracing path
+// (Sopiro/Bulbit), on top of the C ABI in bbg.h.
+//
+// A program written against the reference library changes two lines:
+//
+//     BVH accel(scene.GetPrimitives());                       // unchanged
+//     bulbit_gpu::GpuBVH gpu_accel(accel);                     // + GPU copy of that tree
+//     bulbit_gpu::GpuPathIntegrator integrator(&gpu_accel, scene.GetLights(), &sampler, max_bounces);
+//     Rendering* rendering = integrator.Render(alloc, &camera); // same call, same Rendering/Film
+//
+// GpuBVH is an Intersectable beside BVH (include/bulbit/bvh.h:11-75): it
+// takes the reference-built SAH tree node for node (or builds the same tree
+// itself from the primitives) and answers Intersect / IntersectAny
+// (include/bulbit/intersectable.h:37-45) on the GPU, one ray at a time
+// through the batched kernel, or in batches through IntersectBatch /
+// OccludedBatch. GpuPathIntegrator is an Integrator with PathIntegrator's
+// constructor (include/bulbit/integrators.h:92-114): the base constructor
+// preprocesses the lights exactly as the reference does, and Render()
+// returns at once a Rendering whose job renders on the GPU and fills its Film
+// through Film::AddSample, sample by sample in the reference's order, so the
+// Film state (sums, counts, luminance moments) is the one the reference's
+// Render() would leave, up to the per-path tolerance of the GPU arithmetic.
+//
+// Supported scene content (checked in the constructors, which throw
+// std::runtime_error otherwise): Triangle and Sphere shapes; DiffuseMaterial,
+// ConductorMaterial, DielectricMaterial and MetallicRoughnessMaterial with
+// constant textures, no normal or alpha maps and energy_compensation off;
+// PointLight, SpotLight, UniformInfiniteLight, DiffuseAreaLight with a
+// constant emission; PerspectiveCamera with a BoxFilter; IndependentSampler.
+// Primitives without a material are passed through as the reference does.
+//
+// Build: compile bulbit_b200/cpp/bulbit_gpu.cpp with the reference's include
+// directory and flags, link libbulbit_b200.so and the reference library.
+#pragma once
+
+#include "bbg.h"
+
+#include "bulbit/bulbit.h"
+#include "bulbit/bvh.h"
+#include "bulbit/cameras.h"
+#include "bulbit/integrator.h"
+#include "bulbit/lights.h"
+#include "bulbit/materials.h"
+#include "bulbit/progress.h"
+#include "bulbit/samplers.h"
+#include "bulbit/shapes.h"
+
+#include <atomic>
+#include <cstdint>
+#include <unordered_map>
+#include <vector>
+
+namespace bulbit_gpu
+{
+
+class GpuBVH : public bulbit::Intersectable
+{
+public:
+    // The reference's own tree (BVH::nodes, BVH::primitives), node for node.
+    explicit GpuBVH(const bulbit::BVH& bvh);
+    // The same SAH tree built by the library (bbg_bvh_build) from the
+    // primitives, in the order given (primitive index = position).
+    explicit GpuBVH(const std::vector<bulbit::Primitive*>& primitives);
+    ~GpuBVH() override;
+
+    GpuBVH(const GpuBVH&) = delete;
+    GpuBVH& operator=(const GpuBVH&) = delete;
+
+    bulbit::AABB GetAABB() const override;
+    // One ray through the GPU kernel; the hit's record (point, normals, uv,
+    // front face) is completed by the hit primitive's own Intersect, so it is
+    // the record the reference's BVH::Intersect returns for that primitive.
+    bool Intersect(bulbit::Intersection* out_isect, const bulbit::Ray& ray, ::Float t_min,
+                   ::Float t_max) const override;
+    bool IntersectAny(const bulbit::Ray& ray, ::Float t_min, ::Float t_max) const override;
+
+    // Batched queries, host buffers: closest hits (hit.prim indexes
+    // Primitives(), -1 on a miss) and occlusion flags.
+    void IntersectBatch(const bbg_ray* rays, int64_t n, bbg_hit* hits) const;
+    void OccludedBatch(const bbg_ray* rays, int64_t n, uint8_t* occluded) const;
+
+    const std::vector<const bulbit::Primitive*>& Primitives() const { return prims_; }
+    int32_t IndexOf(const bulbit::Primitive* p) const;
+    bbg_accel* Handle() const { return accel_; }
+
+private:
+    void Upload(const bbg_bvh* tree);
+
+    std::vector<const bulbit::Primitive*> prims_;
+    std::unordered_map<const bulbit::Primitive*, int32_t> index_;
+    bbg_accel* accel_ = nullptr;
+    bulbit::AABB bounds_;
+};
+
+class GpuPathIntegrator : public bulbit::Integrator
+{
+public:
+    // PathIntegrator(accel, lights, sampler, max_bounces, rr_min_bounces,
+    // regularize_bsdf) with the GPU accel in place of the BVH.
+    GpuPathIntegrator(const GpuBVH* accel, std::vector<bulbit::Light*> lights, const bulbit::Sampler* sampler,
+                      ::int32 max_bounces, ::int32 rr_min_bounces = 1, bool regularize_bsdf = false);
+    ~GpuPathIntegrator() override;
+
+    // Returns at once; the Rendering's job renders on the GPU. Wait() /
+    // WaitAndLogProgress() and GetFilm() behave as for the reference.
+    bulbit::Rendering* Render(::Allocator& alloc, const bulbit::Camera* camera) override;
+
+    // Device time and ray counts of the last finished render.
+    const bbg_render_stats& LastStats() const { return stats_; }
+    bbg_integrator* Handle() const { return integrator_; }
+
+private:
+    const GpuBVH* gpu_;
+    const bulbit::Sampler* sampler_;
+    bbg_integrator* integrator_ = nullptr;
+    bbg_render_stats stats_{};
+};
+
+} // namespace bulbit_gpu
