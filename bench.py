@@ -241,12 +241,17 @@ def run_pt(args, barrier, world):
 
     # Default launch configuration, then the autotuned one (which the
     # reported value uses; params.wave_paths = 0 lets the tuned wave apply).
-    default_ms, _ = timed()
-    t0 = time.perf_counter()
-    tuning = integ.autotune(spp=64, seed=0)
-    tune_s = time.perf_counter() - t0
-    params.wave_paths = 0
-    dev_ms, rays = timed()
+    default_ms, default_rays = timed()
+    if args.no_autotune:
+        tuning = abi.Tuning(128, 16, args.pt_wave, 0.0, 0)
+        tune_s = 0.0
+        dev_ms, rays = default_ms, default_rays
+    else:
+        t0 = time.perf_counter()
+        tuning = integ.autotune(spp=64, seed=0)
+        tune_s = time.perf_counter() - t0
+        params.wave_paths = 0
+        dev_ms, rays = timed()
     # End to end through the C ABI with a host film (copied back in the call).
     t0 = time.perf_counter()
     film = integ.render(spp=64)
@@ -443,7 +448,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per query set (smaller cases for profiling)")
-    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided", "batch"])
+    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided", "batch", "guided-frame"])
+    ap.add_argument("--no-autotune", action="store_true", help="path tracing: default launch configuration only")
     ap.add_argument("--guided-res", type=int, default=256)
     ap.add_argument("--pt-res", type=int, default=1024)
     ap.add_argument("--pt-steps", type=int, default=3)
@@ -476,6 +482,21 @@ def main():
     if args.workload == "guided":
         if rank == 0:
             print(json.dumps({"guided_path_tracing": run_guided(args)}))
+        return
+    if args.workload == "guided-frame":
+        # One guided frame with online training (a profiling case): the
+        # path-tracing scene at --guided-res, 64 spp, waves of 2^20 paths.
+        from bulbit_b200 import lib, scenes
+        sc = scenes.cornell_icosphere(levels=8, width=args.guided_res, height=args.guided_res, spp=64,
+                                      max_bounces=16)
+        acc = lib.GpuAccel(sc)
+        integ = lib.GpuPathIntegrator(acc, sc)
+        f = integ.render(spp=64, seed=3, guide=lib.GpuGuide(acc.bounds(), seed=5), train=True, wave_paths=1 << 20,
+                         steps=8)
+        if rank == 0:
+            print(json.dumps({"guided_frame": {"device_ms": f.stats.device_ms, "paths": f.stats.paths,
+                                               "closest_rays": f.stats.closest_rays,
+                                               "shadow_rays": f.stats.shadow_rays}}))
         return
     if args.workload == "batch":
         if rank == 0:

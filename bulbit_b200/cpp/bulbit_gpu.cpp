@@ -464,7 +464,10 @@ bool GpuBVH::Intersect(Intersection* out_isect, const Ray& ray, Float t_min, Flo
 {
     bbg_ray r = ToRay(ray, t_min, t_max);
     bbg_hit h{};
-    Check(bbg_intersect(accel_, &r, 1, &h, BBG_MEM_HOST, nullptr), "bbg_intersect");
+    {
+        std::lock_guard<std::mutex> lock(mutex_);
+        Check(bbg_intersect(accel_, &r, 1, &h, BBG_MEM_HOST, nullptr), "bbg_intersect");
+    }
     if (h.prim < 0)
     {
         return false;
@@ -476,17 +479,20 @@ bool GpuBVH::IntersectAny(const Ray& ray, Float t_min, Float t_max) const
 {
     bbg_ray r = ToRay(ray, t_min, t_max);
     uint8_t occluded = 0;
+    std::lock_guard<std::mutex> lock(mutex_);
     Check(bbg_intersect_any(accel_, &r, 1, &occluded, BBG_MEM_HOST, nullptr), "bbg_intersect_any");
     return occluded != 0;
 }
 
 void GpuBVH::IntersectBatch(const bbg_ray* rays, int64_t n, bbg_hit* hits) const
 {
+    std::lock_guard<std::mutex> lock(mutex_);
     Check(bbg_intersect(accel_, rays, n, hits, BBG_MEM_HOST, nullptr), "bbg_intersect");
 }
 
 void GpuBVH::OccludedBatch(const bbg_ray* rays, int64_t n, uint8_t* occluded) const
 {
+    std::lock_guard<std::mutex> lock(mutex_);
     Check(bbg_intersect_any(accel_, rays, n, occluded, BBG_MEM_HOST, nullptr), "bbg_intersect_any");
 }
 

@@ -47,6 +47,7 @@
 
 #include <atomic>
 #include <cstdint>
+#include <mutex>
 #include <unordered_map>
 #include <vector>
 
@@ -75,7 +76,9 @@ public:
     bool IntersectAny(const bulbit::Ray& ray, ::Float t_min, ::Float t_max) const override;
 
     // Batched queries, host buffers: closest hits (hit.prim indexes
-    // Primitives(), -1 on a miss) and occlusion flags.
+    // Primitives(), -1 on a miss) and occlusion flags. All queries of one
+    // GpuBVH are serialised (the reference calls Intersect from every pool
+    // thread; one call at a time uses the accel's staging buffers).
     void IntersectBatch(const bbg_ray* rays, int64_t n, bbg_hit* hits) const;
     void OccludedBatch(const bbg_ray* rays, int64_t n, uint8_t* occluded) const;
 
@@ -90,6 +93,7 @@ private:
     std::unordered_map<const bulbit::Primitive*, int32_t> index_;
     bbg_accel* accel_ = nullptr;
     bulbit::AABB bounds_;
+    mutable std::mutex mutex_;
 };
 
 class GpuPathIntegrator : public bulbit::Integrator
