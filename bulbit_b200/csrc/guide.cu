@@ -18,7 +18,7 @@ namespace
 {
 
 constexpr int kFwdWarps = 8;
-constexpr int kTrainWarps = 2;
+constexpr int kTrainWarps = 6;
 
 // ---------------------------------------------------------------- forward
 
@@ -197,8 +197,30 @@ struct TrainWarp
     __nv_bfloat16 dht[kGuideHidden * 16];
 };
 
-constexpr size_t kTrainSmem =
-    size_t(kBfAll) * 2 + size_t(kCBias) * 4 + size_t(kGuideParams) * 4 + sizeof(TrainWarp) * kTrainWarps;
+// Shared memory: weights (all images), packed biases, packed bias-gradient
+// accumulators, then one TrainWarp per warp.
+constexpr size_t kTrainSmem = size_t(kBfAll) * 2 + 2 * size_t(kCBias) * 4 + sizeof(TrainWarp) * kTrainWarps;
+static_assert((size_t(kBfAll) * 2 + 2 * size_t(kCBias) * 4) % 16 == 0, "TrainWarp alignment");
+
+// Training scratch (global, bf16, one column per sample, row stride = the
+// batch capacity): the transposed layer inputs and output gradients that the
+// weight-gradient GEMMs read. Rows: X^T 80, H0^T 64, H1^T 64, H2^T 64,
+// dY^T 48 (40 + zero padding), dZ2^T 64, dZ1^T 64, dZ0^T 64.
+constexpr int kRowX = 0, kRowH0 = 80, kRowH1 = 144, kRowH2 = 208, kRowDY = 272, kRowDZ2 = 320, kRowDZ1 = 384,
+              kRowDZ0 = 448, kScratchRows = 512;
+
+// Copies a warp's [rows][16] bf16 block (16 samples) into scratch rows
+// row0.. at sample column col0 (16-byte stores).
+__device__ __forceinline__ void StoreColumns(const __nv_bfloat16* src, int rows, __nv_bfloat16* scratch, int64_t ld,
+                                             int row0, int64_t col0, int lane)
+{
+    for (int i = lane; i < 2 * rows; i += 32)
+    {
+        int r = i >> 1, half = i & 1;
+        uint4 v = *reinterpret_cast<const uint4*>(src + r * 16 + half * 8);
+        *reinterpret_cast<uint4*>(scratch + (int64_t(row0) + r) * ld + col0 + half * 8) = v;
+    }
+}
 
 // C fragments (16 rows x 64 cols) -> bf16 [16][64] and [64][16].
 __device__ __forceinline__ void StoreActs(const float (&acc)[8][4], __nv_bfloat16* rm, __nv_bfloat16* cm, int lane)
@@ -218,40 +240,6 @@ __device__ __forceinline__ void StoreActs(const float (&acc)[8][4], __nv_bfloat1
             rm[row * kGuideHidden + col + 1] = v1;
             cm[col * 16 + row] = v0;
             cm[(col + 1) * 16 + row] = v1;
-        }
-    }
-}
-
-// grad[rows x cols] += A^T B over the warp's 16 samples, where A^T is given
-// [rows][16] (at) and B as [cols][16] (bt); rows and cols multiples of 16/8.
-template <int MT, int NT>
-__device__ __forceinline__ void WeightGrad(const __nv_bfloat16* at, const __nv_bfloat16* bt, float* grad, int ld,
-                                           int rows_valid, int lane)
-{
-    int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int mt = 0; mt < MT; ++mt)
-    {
-        uint32_t a[4];
-        LoadA(at, 16, mt * 16, 0, lane, a);
-#pragma unroll
-        for (int nt = 0; nt < NT; ++nt)
-        {
-            uint32_t b0, b1;
-            LoadB(bt, 16, nt * 8, 0, lane, &b0, &b1);
-            float c[4] = { 0, 0, 0, 0 };
-            Mma16816(c, a, b0, b1);
-#pragma unroll
-            for (int half = 0; half < 2; ++half)
-            {
-                int row = mt * 16 + g + 8 * half;
-                int col = nt * 8 + 2 * t;
-                if (row < rows_valid)
-                {
-                    atomicAdd(grad + row * ld + col, c[2 * half]);
-                    atomicAdd(grad + row * ld + col + 1, c[2 * half + 1]);
-                }
-            }
         }
     }
 }
@@ -323,17 +311,18 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
                                                                       const float* weights, const int32_t* n_dev,
                                                                       int64_t n_host, GuideBounds bounds,
                                                                       const __nv_bfloat16* wg, const float* pg,
+                                                                      __nv_bfloat16* scratch, int64_t ld,
                                                                       float* grad_out, float* loss_out)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smem);
     float* bs = reinterpret_cast<float*>(smem + size_t(kBfAll) * 2);
-    float* gs = bs + kCBias;
-    TrainWarp* tw = reinterpret_cast<TrainWarp*>(gs + kGuideParams);
+    float* bgs = bs + kCBias; // bias gradients, packed like bs
+    TrainWarp* tw = reinterpret_cast<TrainWarp*>(bgs + kCBias);
     StageWeights(wg, pg, ws, bs, kBfAll);
-    for (int i = threadIdx.x; i < kGuideParams; i += blockDim.x)
+    for (int i = threadIdx.x; i < kCBias; i += blockDim.x)
     {
-        gs[i] = 0;
+        bgs[i] = 0;
     }
     __syncthreads();
 
@@ -426,23 +415,32 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
                 W.dyt[k * 16 + lane] = b;
                 if (k < kGuideOut && v != 0.0f)
                 {
-                    atomicAdd(gs + kB3 + k, v);
+                    atomicAdd(bgs + kCB3 + k, v);
                 }
             }
         }
         __syncwarp();
 
         // Layer 3: dW3 += dY^T H3, dZ2 = (dY W3) * relu'(H3).
-        WeightGrad<3, 8>(W.dyt, W.ht[2], gs + kW3, kGuideHidden, kGuideOut, lane);
-        BackLayer<3>(W.dy, kGuideOutPad, ws + kBfT3, kGuideOutPad, W.h[2], W.dh, W.dht, gs + kB2, lane);
-        // Layer 2: dW2 += dZ2^T H2, dZ1 = (dZ2 W2) * relu'(H2).
-        WeightGrad<4, 8>(W.dht, W.ht[1], gs + kW2, kGuideHidden, kGuideHidden, lane);
-        BackLayer<4>(W.dh, kGuideHidden, ws + kBfT2, kGuideHidden, W.h[1], W.dh, W.dht, gs + kB1, lane);
-        // Layer 1: dW1 += dZ1^T H1, dZ0 = (dZ1 W1) * relu'(H1).
-        WeightGrad<4, 8>(W.dht, W.ht[0], gs + kW1, kGuideHidden, kGuideHidden, lane);
-        BackLayer<4>(W.dh, kGuideHidden, ws + kBfT1, kGuideHidden, W.h[0], W.dh, W.dht, gs + kB0, lane);
-        // Layer 0: dW0 += dZ0^T X.
-        WeightGrad<4, 10>(W.dht, W.xt, gs + kW0, kGuideIn, kGuideHidden, lane);
+        // The layer inputs and output gradients, transposed, go to the
+        // scratch columns of these 16 samples; the weight gradients are the
+        // GEMMs dW = dZ^T A over the whole batch (GuideWeightGradKernel).
+        const int64_t col0 = tile * 16;
+        StoreColumns(W.xt, kGuideIn, scratch, ld, kRowX, col0, lane);
+        StoreColumns(W.ht[0], kGuideHidden, scratch, ld, kRowH0, col0, lane);
+        StoreColumns(W.ht[1], kGuideHidden, scratch, ld, kRowH1, col0, lane);
+        StoreColumns(W.ht[2], kGuideHidden, scratch, ld, kRowH2, col0, lane);
+        StoreColumns(W.dyt, kGuideOutPad, scratch, ld, kRowDY, col0, lane);
+        // dZ2 = (dY W3) * relu'(H2), then dZ1, dZ0 likewise.
+        BackLayer<3>(W.dy, kGuideOutPad, ws + kBfT3, kGuideOutPad, W.h[2], W.dh, W.dht, bgs + kCB2, lane);
+        __syncwarp();
+        StoreColumns(W.dht, kGuideHidden, scratch, ld, kRowDZ2, col0, lane);
+        BackLayer<4>(W.dh, kGuideHidden, ws + kBfT2, kGuideHidden, W.h[1], W.dh, W.dht, bgs + kCB1, lane);
+        __syncwarp();
+        StoreColumns(W.dht, kGuideHidden, scratch, ld, kRowDZ1, col0, lane);
+        BackLayer<4>(W.dh, kGuideHidden, ws + kBfT1, kGuideHidden, W.h[0], W.dh, W.dht, bgs + kCB0, lane);
+        __syncwarp();
+        StoreColumns(W.dht, kGuideHidden, scratch, ld, kRowDZ0, col0, lane);
         __syncwarp();
     }
     for (int off = 16; off > 0; off >>= 1)
@@ -454,12 +452,122 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
         atomicAdd(loss_out, loss);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kGuideParams; i += blockDim.x)
+    for (int i = threadIdx.x; i < kCBias; i += blockDim.x)
     {
-        float v = gs[i];
+        float v = bgs[i];
         if (v != 0.0f)
         {
-            atomicAdd(grad_out + i, v);
+            int dst = i < kCB1 ? kB0 + i : i < kCB2 ? kB1 + (i - kCB1) : i < kCB3 ? kB2 + (i - kCB2) : kB3 + (i - kCB3);
+            atomicAdd(grad_out + dst, v);
+        }
+    }
+}
+
+// Weight gradients dW_L[m][n] = sum over the batch of dZ_L[s][m] A_L[s][n]
+// (A_L: the layer's input), from the training scratch. Work items: (layer,
+// 16-row tile of dW, chunk of kGradChunk samples); each warp runs the chunk's
+// MMAs with FP32 accumulators in registers and stores its 16 x n block as the
+// chunk's partial sum; GuideGradReduceKernel adds the chunks' partial sums to
+// the gradient (no atomics, a fixed summation order). Samples past the batch
+// are zero in the dZ rows.
+constexpr int kGradChunk = 256;
+constexpr int kGradWarps = 8;
+
+struct GradLayer
+{
+    int dz_row, a_row, m, n, w_off;
+};
+__constant__ GradLayer kGradLayers[4] = { { kRowDZ0, kRowX, kGuideHidden, kGuideIn, kW0 },
+                                          { kRowDZ1, kRowH0, kGuideHidden, kGuideHidden, kW1 },
+                                          { kRowDZ2, kRowH1, kGuideHidden, kGuideHidden, kW2 },
+                                          { kRowDY, kRowH2, kGuideOut, kGuideHidden, kW3 } };
+constexpr int kGradTiles = 4 + 4 + 4 + 3; // 16-row tiles over the four layers
+
+// grad[w] += sum over chunks of partial[chunk][w], for the weight entries.
+__global__ void GuideGradReduceKernel(const float* partial, const int32_t* n_dev, int64_t n_host, float* grad)
+{
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    const int64_t chunks = ((n + 15) / 16 * 16 + kGradChunk - 1) / kGradChunk;
+    constexpr int kWeights = kGuideParams - kCBias;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kWeights; i += gridDim.x * blockDim.x)
+    {
+        // The i-th weight entry: W0 b0 W1 b1 W2 b2 W3 b3, biases skipped.
+        int w = i < kB0 - kW0 ? kW0 + i
+                : i < kB0 - kW0 + (kB1 - kW1) ? kW1 + (i - (kB0 - kW0))
+                : i < kB0 - kW0 + (kB1 - kW1) + (kB2 - kW2) ? kW2 + (i - (kB0 - kW0) - (kB1 - kW1))
+                : kW3 + (i - (kB0 - kW0) - (kB1 - kW1) - (kB2 - kW2));
+        float s = 0;
+        for (int64_t c = 0; c < chunks; ++c)
+        {
+            s += partial[c * kGuideParams + w];
+        }
+        grad[w] += s;
+    }
+}
+
+__global__ void __launch_bounds__(32 * kGradWarps) GuideWeightGradKernel(const __nv_bfloat16* scratch, int64_t ld,
+                                                                           const int32_t* n_dev, int64_t n_host,
+                                                                           float* partial)
+{
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    const int64_t n_pad = (n + 15) / 16 * 16;
+    const int64_t chunks = (n_pad + kGradChunk - 1) / kGradChunk;
+    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int64_t items = chunks * kGradTiles;
+    for (int64_t item = int64_t(blockIdx.x) * kGradWarps + (threadIdx.x >> 5); item < items;
+         item += int64_t(gridDim.x) * kGradWarps)
+    {
+        int tile = int(item % kGradTiles);
+        int64_t chunk = item / kGradTiles;
+        int layer = tile < 4 ? 0 : tile < 8 ? 1 : tile < 12 ? 2 : 3;
+        int mt = tile - 4 * layer;
+        const GradLayer L = kGradLayers[layer];
+        const int n_tiles = L.n / 8;
+        float acc[10][4];
+#pragma unroll
+        for (int j = 0; j < 10; ++j)
+        {
+            acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0;
+        }
+        const int64_t k_end = min(n_pad, (chunk + 1) * kGradChunk);
+#pragma unroll 4
+        for (int64_t k = chunk * kGradChunk; k < k_end; k += 16)
+        {
+            uint32_t a[4];
+            const __nv_bfloat16* ar = scratch + (int64_t(L.dz_row) + mt * 16) * ld + k;
+            a[0] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g) * ld + 2 * t);
+            a[1] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g + 8) * ld + 2 * t);
+            a[2] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g) * ld + 2 * t + 8);
+            a[3] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g + 8) * ld + 2 * t + 8);
+#pragma unroll
+            for (int j = 0; j < 10; ++j)
+            {
+                if (j < n_tiles)
+                {
+                    const __nv_bfloat16* br = scratch + (int64_t(L.a_row) + j * 8 + g) * ld + k + 2 * t;
+                    uint32_t b0 = *reinterpret_cast<const uint32_t*>(br);
+                    uint32_t b1 = *reinterpret_cast<const uint32_t*>(br + 8);
+                    Mma16816(acc[j], a, b0, b1);
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 10; ++j)
+        {
+            if (j < n_tiles)
+            {
+#pragma unroll
+                for (int half = 0; half < 2; ++half)
+                {
+                    int row = mt * 16 + g + 8 * half;
+                    int col = j * 8 + 2 * t;
+                    if (row < L.m)
+                    {
+                        *reinterpret_cast<float2*>(partial + chunk * kGuideParams + L.w_off + row * L.n + col) =
+                            make_float2(acc[j][2 * half], acc[j][2 * half + 1]);
+                    }
+                }
+            }
         }
     }
 }
@@ -554,13 +662,21 @@ bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index
 }
 
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
-                           const int32_t* n_dev, int64_t n_host, cudaStream_t st)
+                           const int32_t* n_dev, int64_t n_host, int64_t capacity, cudaStream_t st)
 {
+    const int64_t ld = std::max<int64_t>(16, (capacity + 15) / 16 * 16);
+    BBG_TRY(G->scratch.alloc(size_t(kScratchRows) * size_t(ld)));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
     GuideTrainKernel<<<sms, 32 * kTrainWarps, kTrainSmem, st>>>(raw_dev, dirs_dev, weights_dev, n_dev, n_host,
-                                                                G->bounds, G->bf16.p, G->params.p, G->grad.p,
-                                                                G->loss.p);
+                                                                G->bounds, G->bf16.p, G->params.p, G->scratch.p, ld,
+                                                                G->grad.p, G->loss.p);
+    const int64_t chunks = (ld + kGradChunk - 1) / kGradChunk;
+    BBG_TRY(G->partial.alloc(size_t(chunks) * kGuideParams));
+    const int64_t items = chunks * kGradTiles;
+    const int grid = int(std::max<int64_t>(1, std::min<int64_t>((items + kGradWarps - 1) / kGradWarps, 8 * sms)));
+    GuideWeightGradKernel<<<grid, 32 * kGradWarps, 0, st>>>(G->scratch.p, ld, n_dev, n_host, G->partial.p);
+    GuideGradReduceKernel<<<(kGuideParams + 255) / 256, 256, 0, st>>>(G->partial.p, n_dev, n_host, G->grad.p);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
 }
@@ -844,7 +960,7 @@ bbg_status bbg_guide_gradient(bbg_guide* G, const float* raw, const float* dirs,
     BBG_TRY(Stage(G, raw, dirs, weights, n));
     BBG_CUDA(cudaMemsetAsync(G->grad.p, 0, sizeof(float) * kGuideParams, G->stream));
     BBG_CUDA(cudaMemsetAsync(G->loss.p, 0, sizeof(float), G->stream));
-    BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, G->stream));
+    BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, n, G->stream));
     BBG_CUDA(cudaMemcpyAsync(grad_out, G->grad.p, sizeof(float) * kGuideParams, cudaMemcpyDeviceToHost, G->stream));
     float loss = 0;
     BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));
@@ -868,7 +984,7 @@ bbg_status bbg_guide_train_step(bbg_guide* G, const float* raw, const float* dir
     BBG_TRY(GuidePrepare(G, &dummy));
     BBG_TRY(Stage(G, raw, dirs, weights, n));
     BBG_CUDA(cudaMemsetAsync(G->loss.p, 0, sizeof(float), G->stream));
-    BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, G->stream));
+    BBG_TRY(GuideAccumulate(G, G->s_raw.p, G->s_dirs.p, G->s_w.p, nullptr, n, n, G->stream));
     BBG_TRY(GuideApply(G, learning_rate, nullptr, n, G->stream));
     float loss = 0;
     BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));

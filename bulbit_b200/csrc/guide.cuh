@@ -12,6 +12,8 @@ struct bbg_guide
     bbg::DevBuf<float> adam_m, adam_v, grad, loss;
     bbg::DevBuf<__nv_bfloat16> bf16; // kBfAll: forward + transposed weight images
     bbg::DevBuf<int32_t> step_dev; // Adam step counter
+    bbg::DevBuf<__nv_bfloat16> scratch; // training: transposed activations and gradients
+    bbg::DevBuf<float> partial;         // training: per-chunk weight-gradient partial sums
     float beta1 = 0.9f, beta2 = 0.99f;
     bool smem_set = false;
     // Staging for host-buffer calls.
@@ -35,9 +37,10 @@ bbg_status GuidePrepare(bbg_guide* G, int* grid);
 // maps query i to record index[i] for both raw and out. n from n_dev if set.
 bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index_dev, const int32_t* n_dev,
                         int64_t n_host, float* out_dev, cudaStream_t st);
-// Adds the gradient of sum_i -w_i log q_i(dir_i) to the guide's accumulator.
+// Adds the gradient of sum_i -w_i log q_i(dir_i) to the guide's accumulator;
+// capacity bounds n (n from n_dev if set) and sizes the training scratch.
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
-                           const int32_t* n_dev, int64_t n_host, cudaStream_t st);
+                           const int32_t* n_dev, int64_t n_host, int64_t capacity, cudaStream_t st);
 // One Adam step with gradient = accumulator / n (n from n_dev if set); an
 // empty batch is skipped.
 bbg_status GuideApply(bbg_guide* G, float lr, const int32_t* n_dev, int64_t n_host, cudaStream_t st);

@@ -1632,7 +1632,7 @@ bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, cudaStream_t s
     {
         size_t off = size_t(k) * size_t(gc.batch);
         BBG_TRY(GuideAccumulate(gc.guide, gc.dev.t_raw + off * kGuideRaw, gc.dev.t_dir + off * 3, gc.dev.t_w + off,
-                                gc.slice + k, 0, st));
+                                gc.slice + k, 0, gc.batch, st));
         BBG_TRY(GuideApply(gc.guide, gc.lr, gc.slice + k, 0, st));
     }
     BBG_CUDA(cudaGetLastError());
