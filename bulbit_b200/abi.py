@@ -76,7 +76,8 @@ class Hit(C.Structure):
 
 class Material(C.Structure):
     _fields_ = [("type", C.c_int32), ("conductor_from_r", C.c_int32), ("reflectance", f3),
-                ("eta", f3), ("k", f3), ("roughness", C.c_float * 2), ("metallic", C.c_float)]
+                ("eta", f3), ("k", f3), ("roughness", C.c_float * 2), ("metallic", C.c_float),
+                ("energy_compensation", C.c_int32)]
 
 
 class Light(C.Structure):
@@ -141,6 +142,7 @@ EXPORTS = [
     ("bbg_integrator_light_pmf", I32, [P, P]),
     ("bbg_render", I32, [P, P, P, P, I32, P]),
     ("bbg_sampler_draws", I32, [I32, I32, I32, I32, I32, P]),
+    ("bbg_ggx_energy_tables", I32, [P, P]),
     ("bbg_batch_create", I32, [P]),
     ("bbg_batch_destroy", I32, [P]),
     ("bbg_batch_render", I32, [P, I32, P, P, P, P, I32, P]),

@@ -153,10 +153,6 @@ bbg_material TranslateMaterial(const Material* m)
     else if (m->Is<ConductorMaterial>())
     {
         const ConductorMaterial* c = m->Cast<ConductorMaterial>();
-        if (c->*Get(CondEc{}))
-        {
-            Unsupported("ConductorMaterial with energy_compensation = true");
-        }
         if (c->*Get(CondNormal{}) || c->*Get(CondAlpha{}))
         {
             Unsupported("ConductorMaterial with normal or alpha textures");
@@ -173,6 +169,7 @@ bbg_material TranslateMaterial(const Material* m)
         PutSpec(out.reflectance, refl ? ConstSpectrum(refl, "ConductorMaterial reflectance") : Spectrum(1));
         out.roughness[0] = ConstScalar(c->*Get(CondU{}), "ConductorMaterial roughness");
         out.roughness[1] = ConstScalar(c->*Get(CondV{}), "ConductorMaterial roughness");
+        out.energy_compensation = (c->*Get(CondEc{})) ? 1 : 0;
     }
     else if (m->Is<DielectricMaterial>())
     {

@@ -49,6 +49,7 @@ struct MaterialDev
     float alpha_x;    // microfacet alpha (after RoughnessToAlpha)
     float alpha_y;
     float metallic;
+    int32_t ms;       // conductor: energy compensation (ConductorMultiScatteringBxDF)
 };
 
 // BxDF_Flags values (include/bulbit/bxdf.h:8-22).

@@ -18,11 +18,52 @@ namespace bbg
 
 // ---------------------------------------------------------------- microfacet
 
+// Energy tables of the GGX distribution with F = 1, in the reference's layout
+// (TrowbridgeReitzDistribution::PrepareReflectanceTexture,
+// src/bxdf/microfacet.cpp:28-70): E(cos theta_o, alpha) 32 x 32 (x: cos theta,
+// y: alpha) and E_avg(alpha) 32 x 1. Filled on the device by
+// GgxEnergyTablesKernel (render.cu) before any energy-compensated material is
+// shaded.
+constexpr int kEnergyTableSize = 32;
+static __device__ float g_ggx_e[kEnergyTableSize * kEnergyTableSize];
+static __device__ float g_ggx_e_avg[kEnergyTableSize];
+
+// ImageTexture<Float>::Evaluate: bilinear, texel coordinates clamped
+// (include/bulbit/textures.h:55-87).
+__device__ __forceinline__ float TableBilinear(const float* img, int w, int h, float u, float v)
+{
+    float x = u * float(w) - 0.5f;
+    float y = v * float(h) - 0.5f;
+    float fx = floorf(x), fy = floorf(y);
+    int i0 = int(fx), i1 = i0 + 1;
+    int j0 = int(fy), j1 = j0 + 1;
+    i0 = min(max(i0, 0), w - 1);
+    j0 = min(max(j0, 0), h - 1);
+    i1 = min(max(i1, 0), w - 1);
+    j1 = min(max(j1, 0), h - 1);
+    float fu = x - fx;
+    float fv = y - fy;
+    float v00 = img[i0 + j0 * w], v10 = img[i1 + j0 * w];
+    float v01 = img[i0 + j1 * w], v11 = img[i1 + j1 * w];
+    return (1 - fu) * (1 - fv) * v00 + (1 - fu) * fv * v01 + fu * (1 - fv) * v10 + fu * fv * v11;
+}
+
 struct TrowbridgeReitz
 {
     float alpha_x, alpha_y;
 
     __device__ __forceinline__ bool EffectivelySmooth() const { return SMax(alpha_x, alpha_y) < 1e-3f; }
+
+    // E(wo), E_avg (include/bulbit/microfacet.h:133-145).
+    __device__ __forceinline__ float MeanAlpha() const { return sqrtf(alpha_x * alpha_y); }
+    __device__ __forceinline__ float E(V3 wo) const
+    {
+        return TableBilinear(g_ggx_e, kEnergyTableSize, kEnergyTableSize, wo.z, MeanAlpha());
+    }
+    __device__ __forceinline__ float EAvg() const
+    {
+        return TableBilinear(g_ggx_e_avg, kEnergyTableSize, 1, MeanAlpha(), 0.0f);
+    }
 
     __device__ __forceinline__ float D(V3 wm) const
     {
@@ -193,6 +234,7 @@ struct BSDF
     const float* ck;
     TrowbridgeReitz mf;
     float metallic;
+    int32_t ms;      // conductor: energy compensation (multiple-scattering lobe)
 
     // ---- Lambertian (src/bxdf/lambertian_bxdf.cpp)
     __device__ Spec LambertF(V3 wo, V3 wi) const
@@ -256,6 +298,82 @@ struct BSDF
         Spec F = FresnelComplex(AbsDot(wo, wm), ceta, ck);
         Spec f = F * mf.D(wm) * mf.G(wo, wi) / (4 * cos_theta_i * cos_theta_o);
         *s = BSDFSample{ r * f, wi, pdf, kFlagGlossy | kFlagReflection, 1 };
+        return true;
+    }
+
+    // ---- Energy-compensated conductor (src/bxdf/conductor_multi_scattering_bxdf.cpp):
+    // the single-scattering lobe plus a diffuse-like multiple-scattering lobe
+    // scaled by the lost energy (1 - E(wo)) (1 - E(wi)).
+    __device__ Spec ConductorMsLobe(V3 wo, V3 wi) const
+    {
+        float E_avg = mf.EAvg();
+        Spec F0 = FresnelComplex(1, ceta, ck);
+        Spec F90 = FresnelComplex(0, ceta, ck);
+        Spec fresnel_avg = (20 * F0 + F90) / 21.0f; // FresnelConductorAverage (scattering.h:174-185)
+        Spec fresnel_ms = fresnel_avg * fresnel_avg * E_avg / (spec(1) - fresnel_avg * (1 - E_avg));
+        return fresnel_ms * ((1 - mf.E(wo)) * (1 - mf.E(wi))) / (kPi * (1 - E_avg));
+    }
+    __device__ Spec ConductorMsF(V3 wo, V3 wi) const
+    {
+        if (!SameHemisphere(wo, wi) || mf.EffectivelySmooth()) return spec(0);
+        float cos_theta_o = AbsCosTheta(wo);
+        float cos_theta_i = AbsCosTheta(wi);
+        if (cos_theta_i == 0 || cos_theta_o == 0) return spec(0);
+        V3 wm = wo + wi;
+        if (Length2(wm) == 0) return spec(0);
+        NormalizeInPlace(wm);
+        Spec F = FresnelComplex(AbsDot(wo, wm), ceta, ck);
+        Spec f_ss = F * mf.D(wm) * mf.G(wo, wi) / (4 * cos_theta_i * cos_theta_o);
+        return r * (f_ss + ConductorMsLobe(wo, wi));
+    }
+    __device__ float ConductorMsPDF(V3 wo, V3 wi) const
+    {
+        if (!SameHemisphere(wo, wi) || mf.EffectivelySmooth()) return 0;
+        V3 wm = wo + wi;
+        if (Length2(wm) == 0) return 0;
+        NormalizeInPlace(wm);
+        if (DotZ(wm) < 0) wm = -wm;
+        float pdf_ss = mf.PDF(wo, wm) / (4 * AbsDot(wo, wm));
+        float pdf_ms = wi.z * kInvPi; // CosineHemispherePDF(wi.z)
+        float e = mf.E(wo);
+        return pdf_ms * (1 - e) + pdf_ss * e; // Lerp(pdf_ms, pdf_ss, E(wo))
+    }
+    __device__ bool ConductorMsSample(BSDFSample* s, V3 wo, float u0, P2 u12) const
+    {
+        if (mf.EffectivelySmooth())
+        {
+            V3 wi{ -wo.x, -wo.y, wo.z };
+            Spec f = FresnelComplex(AbsCosTheta(wi), ceta, ck) / AbsCosTheta(wi);
+            *s = BSDFSample{ r * f, wi, 1, kFlagSpecular | kFlagReflection, 1 };
+            return true;
+        }
+        if (wo.z == 0) return false;
+        V3 wm, wi;
+        int32_t flag;
+        float e = mf.E(wo);
+        if (u0 < e)
+        {
+            wm = mf.SampleWm(wo, u12);
+            wi = Reflect(wo, wm);
+            flag = kFlagGlossy | kFlagReflection;
+        }
+        else
+        {
+            wi = SampleCosineHemisphere(u12);
+            wm = Normalize(wo + wi);
+            flag = kFlagDiffuse | kFlagReflection;
+        }
+        if (!SameHemisphere(wo, wi)) return false;
+        float cos_theta_o = AbsCosTheta(wo);
+        float cos_theta_i = AbsCosTheta(wi);
+        if (cos_theta_i == 0 || cos_theta_o == 0) return false;
+        Spec F = FresnelComplex(AbsDot(wo, wm), ceta, ck);
+        Spec f_ss = F * mf.D(wm) * mf.G(wo, wi) / (4 * cos_theta_i * cos_theta_o);
+        Spec f_ms = ConductorMsLobe(wo, wi);
+        float pdf_ss = mf.PDF(wo, wm) / (4 * AbsDot(wo, wm));
+        float pdf_ms = wi.z * kInvPi;
+        float pdf = pdf_ms * (1 - e) + pdf_ss * e;
+        *s = BSDFSample{ r * (f_ss + f_ms), wi, pdf, flag, 1 };
         return true;
     }
 
@@ -442,7 +560,7 @@ struct BSDF
         switch (type)
         {
         case BBG_MAT_DIFFUSE: return LambertF(wo, wi);
-        case BBG_MAT_CONDUCTOR: return ConductorF(wo, wi);
+        case BBG_MAT_CONDUCTOR: return ms ? ConductorMsF(wo, wi) : ConductorF(wo, wi);
         case BBG_MAT_DIELECTRIC: return DielectricF(wo, wi);
         default: return MRF(wo, wi);
         }
@@ -455,7 +573,7 @@ struct BSDF
         switch (type)
         {
         case BBG_MAT_DIFFUSE: return LambertPDF(wo, wi);
-        case BBG_MAT_CONDUCTOR: return ConductorPDF(wo, wi);
+        case BBG_MAT_CONDUCTOR: return ms ? ConductorMsPDF(wo, wi) : ConductorPDF(wo, wi);
         case BBG_MAT_DIELECTRIC: return DielectricPDF(wo, wi);
         default: return MRPDF(wo, wi);
         }
@@ -468,7 +586,7 @@ struct BSDF
         switch (type)
         {
         case BBG_MAT_DIFFUSE: ok = LambertSample(s, wo, u12); break;
-        case BBG_MAT_CONDUCTOR: ok = ConductorSample(s, wo, u12); break;
+        case BBG_MAT_CONDUCTOR: ok = ms ? ConductorMsSample(s, wo, u0, u12) : ConductorSample(s, wo, u12); break;
         case BBG_MAT_DIELECTRIC: ok = DielectricSample(s, wo, u0, u12); break;
         default: ok = MRSample(s, wo, u0, u12); break;
         }
@@ -491,6 +609,7 @@ __device__ __forceinline__ BSDF MakeBSDF(const MaterialDev& m, V3 shading_n, V3 
     b.metallic = m.metallic;
     b.ceta = m.eta;
     b.ck = m.k;
+    b.ms = m.ms;
     b.eta = 1;
     b.flags = m.flags;
     if (m.type == BBG_MAT_DIELECTRIC)

@@ -550,7 +550,7 @@ bbg_status MakeMaterial(const bbg_material& m, MaterialDev* out)
     case BBG_MAT_CONDUCTOR:
     {
         // ConductorMaterial::GetBSDF (src/material/conductor_material.cpp:52-99),
-        // energy_compensation = false -> ConductorBxDF (include/bulbit/bxdfs.h:249-300).
+        // ConductorBxDF (include/bulbit/bxdfs.h:249-300).
         out->alpha_x = m.roughness[0] * m.roughness[0];
         out->alpha_y = m.roughness[1] * m.roughness[1];
         std::memcpy(out->r, m.reflectance, sizeof(out->r));
@@ -573,10 +573,17 @@ bbg_status MakeMaterial(const bbg_material& m, MaterialDev* out)
         }
         bool smooth = std::max(out->alpha_x, out->alpha_y) < 1e-3f;
         out->flags = smooth ? (kFlagSpecular | kFlagReflection) : (kFlagGlossy | kFlagReflection);
+        // energy_compensation = true -> ConductorMultiScatteringBxDF (same
+        // flags, include/bulbit/bxdfs.h:303-357).
+        out->ms = m.energy_compensation ? 1 : 0;
         return BBG_OK;
     }
     case BBG_MAT_DIELECTRIC:
     {
+        if (m.energy_compensation)
+        {
+            return Fail(BBG_ERR_UNSUPPORTED, "energy-compensated dielectric materials are not supported");
+        }
         // DielectricMaterial::GetBSDF (src/material/dielectric_material.cpp:28-52);
         // DielectricBxDF stores Sqrt(r) (include/bulbit/bxdfs.h:85-90). The
         // relative eta and the flags depend on the hit side and are set per hit.

@@ -1311,6 +1311,114 @@ __global__ void __launch_bounds__(kBlock) FilmKernel(Scenes sc, WaveDev w)
     }
 }
 
+// ---------------------------------------------------------------- GGX energy tables
+
+// PermutationElement (include/bulbit/hash.h:129-159): Kensler's hashed
+// permutation of [0, l) ("Correlated Multi-Jittered Sampling", 2013).
+__device__ __forceinline__ uint32_t PermutationElement(uint32_t i, uint32_t l, uint32_t p)
+{
+    uint32_t w = l - 1;
+    w |= w >> 1;
+    w |= w >> 2;
+    w |= w >> 4;
+    w |= w >> 8;
+    w |= w >> 16;
+    do
+    {
+        i ^= p;
+        i *= 0xe170893du;
+        i ^= p >> 16;
+        i ^= (i & w) >> 4;
+        i ^= p >> 8;
+        i *= 0x0929eb3fu;
+        i ^= p >> 23;
+        i ^= (i & w) >> 1;
+        i *= 1u | p >> 27;
+        i *= 0x6935fa69u;
+        i ^= (i & w) >> 11;
+        i *= 0x74dcb303u;
+        i ^= (i & w) >> 2;
+        i *= 0x9e501cc3u;
+        i ^= (i & w) >> 2;
+        i *= 0xc860a3dfu;
+        i &= w;
+        i ^= i >> 5;
+    } while (i >= l);
+    return (i + p) % l;
+}
+
+constexpr int kEnergySamples = 1024; // 32 x 32 strata, PrepareReflectanceTextures(32, 1024)
+
+// The stratified samples of PrepareReflectanceTextures (src/bxdf/microfacet.cpp:239-275):
+// RNG(3); per sample a permuted 1-D stratum (u0, drawn but unused by GGX) and
+// a permuted 2-D stratum, in that draw order. One thread.
+__global__ void GgxEnergySamplesKernel(P2* u12)
+{
+    uint64_t st = 0; // RNG(3): Seed(initstate = 3, initseq = 1)
+    PcgNext(st);
+    st += 3;
+    PcgNext(st);
+    for (int i = 0; i < kEnergySamples; ++i)
+    {
+        int32_t s0 = int32_t(PermutationElement(uint32_t(i), kEnergySamples, 1));
+        float u0 = (float(s0) + Next1D(st)) / float(kEnergySamples);
+        (void)u0;
+        int32_t s1 = int32_t(PermutationElement(uint32_t(i), kEnergySamples, 2));
+        int32_t x = s1 % 32, y = s1 / 32;
+        float a = Next1D(st);
+        float b = Next1D(st);
+        u12[i] = P2{ (float(x) + a) / 32.0f, (float(y) + b) / 32.0f };
+    }
+}
+
+// E(cos theta, alpha) = rho(wo) of TrowbridgeReitzDistribution(alpha, alpha)
+// (include/bulbit/microfacet.h:109-130), one thread per table entry, samples
+// summed in order; then E_avg(alpha) = 2 sum_i E cos theta d.
+__global__ void GgxEnergyTablesKernel(const P2* u12)
+{
+    const float d = 1.0f / kEnergyTableSize;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e < kEnergyTableSize * kEnergyTableSize)
+    {
+        int i = e % kEnergyTableSize, j = e / kEnergyTableSize;
+        float a = d / 2 + d * float(j);
+        float cos_theta = d / 2 + d * float(i);
+        float sin_theta = sqrtf(1 - cos_theta * cos_theta);
+        V3 wo{ sin_theta, 0, cos_theta };
+        TrowbridgeReitz mf{ a, a };
+        float r = 0;
+        for (int k = 0; k < kEnergySamples; ++k)
+        {
+            V3 wm = mf.SampleWm(wo, u12[k]);
+            V3 wi = Reflect(wo, wm);
+            if (!SameHemisphere(wo, wi))
+            {
+                continue;
+            }
+            float pdf = mf.PDF(wo, wm) / (4 * AbsDot(wo, wm));
+            float f = mf.D(wm) * mf.G(wo, wi) / (4 * AbsCosTheta(wo) * AbsCosTheta(wi));
+            r += f * AbsCosTheta(wi) / pdf;
+        }
+        g_ggx_e[e] = r / float(kEnergySamples);
+    }
+}
+
+__global__ void GgxEnergyAverageKernel()
+{
+    const float d = 1.0f / kEnergyTableSize;
+    int j = threadIdx.x;
+    if (j < kEnergyTableSize)
+    {
+        float r_sum = 0;
+        for (int i = 0; i < kEnergyTableSize; ++i)
+        {
+            float cos_theta = d / 2 + d * float(i);
+            r_sum += g_ggx_e[i + kEnergyTableSize * j] * cos_theta * d;
+        }
+        g_ggx_e_avg[j] = 2 * r_sum;
+    }
+}
+
 // ---------------------------------------------------------------- sampler probe
 
 __global__ void SamplerDrawsKernel(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out)
@@ -1897,6 +2005,34 @@ bbg_status InitWaveEngine(bbg_integrator* I)
     return BBG_OK;
 }
 
+// Fills the GGX energy tables on the current device, once per process and
+// device (they depend on nothing but the reference's fixed sample set).
+bbg_status EnsureGgxTables()
+{
+    static std::mutex mutex;
+    static std::vector<bool> done;
+    int dev = 0;
+    BBG_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mutex);
+    if (size_t(dev) < done.size() && done[dev])
+    {
+        return BBG_OK;
+    }
+    DevBuf<P2> u12;
+    BBG_TRY(u12.alloc(kEnergySamples));
+    GgxEnergySamplesKernel<<<1, 1>>>(u12.p);
+    GgxEnergyTablesKernel<<<(kEnergyTableSize * kEnergyTableSize + 127) / 128, 128>>>(u12.p);
+    GgxEnergyAverageKernel<<<1, kEnergyTableSize>>>();
+    BBG_CUDA(cudaGetLastError());
+    BBG_CUDA(cudaDeviceSynchronize());
+    if (done.size() <= size_t(dev))
+    {
+        done.resize(size_t(dev) + 1, false);
+    }
+    done[dev] = true;
+    return BBG_OK;
+}
+
 bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim_material, const bbg_material* mats,
                             int32_t n_mats, const bbg_light* lights, int32_t n_lights)
 {
@@ -1908,6 +2044,10 @@ bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim
     for (int32_t i = 0; i < n_mats; ++i)
     {
         BBG_TRY(MakeMaterial(mats[i], &md[i]));
+        if (md[i].ms)
+        {
+            BBG_TRY(EnsureGgxTables());
+        }
     }
     std::vector<int4> info(size_t(a->n_prims));
     for (int32_t i = 0; i < a->n_prims; ++i)
@@ -2466,6 +2606,19 @@ bbg_status bbg_render(bbg_integrator* I, const bbg_camera* camera, const bbg_ren
         return Fail(BBG_ERR_INVALID_ARG, "bbg_render: null integrator");
     }
     return Render(I, camera, params, film, mem, stats);
+}
+
+bbg_status bbg_ggx_energy_tables(float* e_out, float* e_avg_out)
+{
+    if (!e_out || !e_avg_out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_ggx_energy_tables: bad argument");
+    }
+    BBG_TRY(CheckDevice());
+    BBG_TRY(EnsureGgxTables());
+    BBG_CUDA(cudaMemcpyFromSymbol(e_out, g_ggx_e, sizeof(g_ggx_e)));
+    BBG_CUDA(cudaMemcpyFromSymbol(e_avg_out, g_ggx_e_avg, sizeof(g_ggx_e_avg)));
+    return BBG_OK;
 }
 
 bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out)

@@ -389,6 +389,14 @@ class GpuBatch:
         return films, stats
 
 
+def ggx_energy_tables():
+    """bbg_ggx_energy_tables: (E 32x32 indexed [alpha][cos], E_avg 32)."""
+    e = np.zeros(32 * 32, np.float32)
+    a = np.zeros(32, np.float32)
+    check(get_lib().bbg_ggx_energy_tables(_p(e), _p(a)), "bbg_ggx_energy_tables")
+    return e.reshape(32, 32), a
+
+
 def mixture_sample(outputs, u):
     """Sample the vMF mixtures that network output rows (n, 40) describe, with
     uniforms u (n, 3) -> (unit directions (n, 3), mixture density (n,))."""

@@ -160,13 +160,14 @@ def diffuse(rgb):
     return m
 
 
-def conductor(eta, k, roughness, reflectance=(1.0, 1.0, 1.0)):
+def conductor(eta, k, roughness, reflectance=(1.0, 1.0, 1.0), energy_compensation=False):
     m = abi.Material()
     m.type = abi.BBG_MAT_CONDUCTOR
     m.eta[:] = list(eta)
     m.k[:] = list(k)
     m.roughness[:] = [roughness, roughness]
     m.reflectance[:] = list(reflectance)
+    m.energy_compensation = 1 if energy_compensation else 0
     return m
 
 

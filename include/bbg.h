@@ -248,6 +248,9 @@ typedef struct bbg_material
     float k[3];
     float roughness[2];
     float metallic;
+    int32_t energy_compensation; /* conductor: ConductorMaterial's energy_compensation
+                                    (multiple-scattering lobe from the GGX energy
+                                    tables); dielectrics support only 0 */
 } bbg_material;
 
 enum
@@ -401,6 +404,13 @@ bbg_status bbg_batch_destroy(bbg_batch* batch);
 bbg_status bbg_batch_render(bbg_batch* batch, int32_t n, bbg_integrator* const* integrators,
                             const bbg_camera* cameras, const bbg_render_params* params, bbg_film* films,
                             bbg_memory mem, bbg_render_stats* stats);
+
+/* The GGX energy tables the energy-compensated conductor uses, as the
+ * reference computes them (TrowbridgeReitzDistribution::
+ * PrepareReflectanceTexture, src/bxdf/microfacet.cpp:28-70; samples from
+ * PrepareReflectanceTextures, :239-275): e_out 32 x 32 (index cos_i + 32 *
+ * alpha_j), e_avg_out 32. Computed on the device once per process. */
+bbg_status bbg_ggx_energy_tables(float* e_out, float* e_avg_out);
 
 /* ------------------------------------------------------------ autotuning */
 

@@ -23,8 +23,9 @@
 //
 // Supported scene content (checked in the constructors, which throw
 // std::runtime_error otherwise): Triangle and Sphere shapes; DiffuseMaterial,
-// ConductorMaterial, DielectricMaterial and MetallicRoughnessMaterial with
-// constant textures, no normal or alpha maps and energy_compensation off;
+// ConductorMaterial (energy compensation on or off), DielectricMaterial
+// (energy compensation off) and MetallicRoughnessMaterial with constant
+// textures and no normal or alpha maps;
 // PointLight, SpotLight, UniformInfiniteLight, DiffuseAreaLight with a
 // constant emission; PerspectiveCamera with a BoxFilter; IndependentSampler.
 // Primitives without a material are passed through as the reference does.

@@ -22,6 +22,8 @@
 #include "bulbit/integrators.h"
 #include "bulbit/lights.h"
 #include "bulbit/materials.h"
+#include "bulbit/microfacet.h"
+#include "bulbit/textures.h"
 #include "bulbit/parallel_for.h"
 #include "bulbit/samplers.h"
 #include "bulbit/scene.h"
@@ -62,6 +64,9 @@ BBREF_STEAL(CamVertical, &PerspectiveCamera::vertical)
 BBREF_STEAL(CamU, &PerspectiveCamera::u)
 BBREF_STEAL(CamV, &PerspectiveCamera::v)
 BBREF_STEAL(CamLensRadius, &PerspectiveCamera::lens_radius)
+BBREF_STEAL(GgxE, &TrowbridgeReitzDistribution::E_texture)
+BBREF_STEAL(GgxEAvg, &TrowbridgeReitzDistribution::E_avg_texture)
+BBREF_STEAL(FloatTexImage, &ImageTexture<Float>::image)
 
 namespace
 {
@@ -130,12 +135,12 @@ Material* MakeMaterial(Scene& scene, const bbg_material& m)
         {
             return scene.CreateMaterial<ConductorMaterial>(SpecTex(scene, m.k), FloatTex(scene, m.roughness[0]),
                                                            FloatTex(scene, m.roughness[1]),
-                                                           SpecTex(scene, m.reflectance), false);
+                                                           SpecTex(scene, m.reflectance), m.energy_compensation != 0);
         }
         return scene.CreateMaterial<ConductorMaterial>(SpecTex(scene, m.eta), SpecTex(scene, m.k),
                                                        FloatTex(scene, m.roughness[0]),
                                                        FloatTex(scene, m.roughness[1]), SpecTex(scene, m.reflectance),
-                                                       false);
+                                                       m.energy_compensation != 0);
     case BBG_MAT_DIELECTRIC:
         return scene.CreateMaterial<DielectricMaterial>(m.eta[0], FloatTex(scene, m.roughness[0]),
                                                         FloatTex(scene, m.roughness[1]), SpecTex(scene, m.reflectance),
@@ -555,6 +560,27 @@ int bbref_light_pmf(void* handle, float* pmf_out)
 }
 
 // The first n draws of IndependentSampler after StartPixelSample.
+// The reference's GGX energy tables after PrepareReflectanceTextures(32, 1024)
+// (what every Integrator constructor runs): E 32 x 32, E_avg 32.
+int bbref_ggx_energy_tables(float* e_out, float* e_avg_out)
+{
+    EnsurePool(0);
+    PrepareReflectanceTextures(32, 1024);
+    const auto& e = *(*Get(GgxE{}));
+    const auto& e_avg = *(*Get(GgxEAvg{}));
+    const auto& ei = e.*Get(FloatTexImage{});
+    const auto& ai = e_avg.*Get(FloatTexImage{});
+    for (int32 i = 0; i < 32 * 32; ++i)
+    {
+        e_out[i] = ei[i];
+    }
+    for (int32 i = 0; i < 32; ++i)
+    {
+        e_avg_out[i] = ai[i];
+    }
+    return 0;
+}
+
 int bbref_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out)
 {
     IndependentSampler s(1, seed);

@@ -44,6 +44,7 @@ def lib():
             "bbref_render": (C.c_double, [P, P, P, P]),
             "bbref_light_pmf": (I32, [P, P]),
             "bbref_sampler_draws": (I32, [I32, I32, I32, I32, I32, P]),
+            "bbref_ggx_energy_tables": (I32, [P, P]),
             "bbref_pcg32": (I32, [C.c_uint64, C.c_uint64, I32, P]),
             "bbref_hash_pixel_sample": (C.c_uint64, [I32, I32, I32, I32]),
         }
@@ -171,6 +172,14 @@ def sampler_draws(px, py, seed, sample, n):
     out = np.zeros(n, np.float32)
     lib().bbref_sampler_draws(px, py, seed, sample, n, _p(out))
     return out
+
+
+def ggx_energy_tables():
+    """The reference's GGX energy tables: (E 32x32 indexed [alpha][cos], E_avg 32)."""
+    e = np.zeros(32 * 32, np.float32)
+    a = np.zeros(32, np.float32)
+    lib().bbref_ggx_energy_tables(_p(e), _p(a))
+    return e.reshape(32, 32), a
 
 
 def pcg32(initstate, initseq, n):

@@ -90,11 +90,11 @@ void MeshScene(Scene& scene)
                             Point3(-0.5f, 2.99f, 0.5f) });
     auto* white = scene.CreateMaterial<DiffuseMaterial>(
         scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(0.7f, 0.7f, 0.65f)));
+    // Gold with the library default (energy_compensation = true).
     auto* gold = scene.CreateMaterial<ConductorMaterial>(
         scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(0.161f, 0.492f, 1.426f)),
         scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(4.08769f, 2.32625f, 1.846f)),
-        scene.CreateTexture<ConstantTexture, Float>(0.3f), scene.CreateTexture<ConstantTexture, Float>(0.3f),
-        scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(1.0f)), false);
+        scene.CreateTexture<ConstantTexture, Float>(0.3f), scene.CreateTexture<ConstantTexture, Float>(0.3f));
     auto* glass = scene.CreateMaterial<DielectricMaterial>(
         1.5f, scene.CreateTexture<ConstantTexture, Float>(0.0f), scene.CreateTexture<ConstantTexture, Float>(0.0f),
         scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(1.0f)), false);

@@ -93,15 +93,33 @@ def test_cornell_paths(oracle):
     check_paths("cornell_gold", film.path_L, ref_L)
 
 
+def test_ggx_energy_tables_match_reference(oracle):
+    """The energy-compensated conductor's tables (E, E_avg), computed on the
+    device from the reference's stratified sample set, agree with the
+    reference's PrepareReflectanceTextures(32, 1024) output to 2e-6 relative
+    (the VNDF sampler's sin/cos may differ from glibc's by an ulp)."""
+    e, a = lib.ggx_energy_tables()
+    re, ra = oracle.ggx_energy_tables()
+    print(f"E: {np.mean(e == re):.4f} of entries bit-identical, max |diff| {np.abs(e - re).max():.2e}; "
+          f"E_avg: {np.mean(a == ra):.4f} bit-identical")
+    assert np.allclose(e, re, rtol=2e-6, atol=0)
+    assert np.allclose(a, ra, rtol=2e-6, atol=0)
+
+
 @pytest.mark.parametrize("mat", ["dielectric_smooth", "dielectric_rough", "metallic_roughness", "conductor_smooth",
-                                 "conductor_from_r"])
+                                 "conductor_from_r", "conductor_energy_compensated",
+                                 "conductor_from_r_energy_compensated"])
 def test_materials_paths(oracle, mat):
     m = {"dielectric_smooth": scenes.dielectric(1.5, 0.0),
          "dielectric_rough": scenes.dielectric(1.5, 0.3),
          "metallic_roughness": scenes.metallic_roughness((0.8, 0.5, 0.3), 0.4, 0.35),
          "conductor_smooth": scenes.conductor(scenes.GOLD_ETA, scenes.GOLD_K, 0.0),
-         "conductor_from_r": scenes.conductor((0, 0, 0), (0.9, 0.6, 0.3), 0.25)}[mat]
-    if mat == "conductor_from_r":
+         "conductor_from_r": scenes.conductor((0, 0, 0), (0.9, 0.6, 0.3), 0.25),
+         "conductor_energy_compensated": scenes.conductor(scenes.GOLD_ETA, scenes.GOLD_K, 0.35,
+                                                          energy_compensation=True),
+         "conductor_from_r_energy_compensated": scenes.conductor((0, 0, 0), (0.9, 0.6, 0.3), 0.5,
+                                                                 energy_compensation=True)}[mat]
+    if mat.startswith("conductor_from_r"):
         m.conductor_from_r = 1
     scene = scenes.cornell_icosphere(levels=3, width=40, height=40, spp=8, max_bounces=12, sphere_material=m)
     rs, acc, integ, film, ref_L = render_both(oracle, scene)
