@@ -36,6 +36,13 @@ BBG_MAT_METALLIC_ROUGHNESS = 3
 BBG_TRAVERSAL_ORDERED = 0
 BBG_TRAVERSAL_REFERENCE = 1
 
+BBG_FILTER_BOX = 0
+BBG_FILTER_TENT = 1
+BBG_FILTER_GAUSSIAN = 2
+
+BBG_SAMPLER_INDEPENDENT = 0
+BBG_SAMPLER_STRATIFIED = 1
+
 BBG_LIGHT_POINT = 0
 BBG_LIGHT_SPOT = 1
 BBG_LIGHT_UNIFORM_INFINITE = 2
@@ -89,20 +96,23 @@ class Light(C.Structure):
 class CameraSpec(C.Structure):
     _fields_ = [("position", f3), ("target", f3), ("up", f3), ("vfov_deg", C.c_float),
                 ("aperture_radius", C.c_float), ("focus_distance", C.c_float),
-                ("width", C.c_int32), ("height", C.c_int32), ("filter_extent", C.c_float)]
+                ("width", C.c_int32), ("height", C.c_int32), ("filter_extent", C.c_float),
+                ("filter_type", C.c_int32), ("filter_sigma", C.c_float)]
 
 
 class Camera(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("origin", f3), ("lower_left", f3),
                 ("horizontal", f3), ("vertical", f3), ("u", f3), ("v", f3),
-                ("lens_radius", C.c_float), ("filter_extent", C.c_float)]
+                ("lens_radius", C.c_float), ("filter_extent", C.c_float),
+                ("filter_type", C.c_int32), ("filter_sigma", C.c_float)]
 
 
 class RenderParams(C.Structure):
     _fields_ = [("spp", C.c_int32), ("seed", C.c_int32), ("wave_paths", C.c_int64),
                 ("use_graph", C.c_int32), ("light_alias", C.c_int32), ("guide", C.c_void_p),
                 ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float),
-                ("guide_select", C.c_float), ("guide_steps", C.c_int32)]
+                ("guide_select", C.c_float), ("guide_steps", C.c_int32),
+                ("sampler", C.c_int32), ("x_samples", C.c_int32), ("jitter", C.c_int32)]
 
 
 class Tuning(C.Structure):

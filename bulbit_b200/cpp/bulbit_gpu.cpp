@@ -54,6 +54,9 @@ BULBIT_GPU_STEAL(CamU, &PerspectiveCamera::u)
 BULBIT_GPU_STEAL(CamV, &PerspectiveCamera::v)
 BULBIT_GPU_STEAL(CamLensRadius, &PerspectiveCamera::lens_radius)
 BULBIT_GPU_STEAL(SamplerSeed, &IndependentSampler::seed)
+BULBIT_GPU_STEAL(StratSeed, &StratifiedSampler::seed)
+BULBIT_GPU_STEAL(StratX, &StratifiedSampler::x_samples)
+BULBIT_GPU_STEAL(StratJitter, &StratifiedSampler::jitter)
 BULBIT_GPU_STEAL(ConstSpec, &ConstantTexture<Spectrum>::value)
 BULBIT_GPU_STEAL(ConstFloat, &ConstantTexture<Float>::value)
 BULBIT_GPU_STEAL(CondEta, &ConductorMaterial::eta)
@@ -501,9 +504,9 @@ GpuPathIntegrator::GpuPathIntegrator(const GpuBVH* accel, std::vector<Light*> li
     , gpu_{ accel }
     , sampler_{ sampler }
 {
-    if (!dynamic_cast<const IndependentSampler*>(sampler))
+    if (!dynamic_cast<const IndependentSampler*>(sampler) && !dynamic_cast<const StratifiedSampler*>(sampler))
     {
-        Unsupported("sampler (supported: IndependentSampler)");
+        Unsupported("sampler (supported: IndependentSampler, StratifiedSampler)");
     }
     // Materials, deduplicated, and each primitive's index among them.
     std::vector<bbg_material> materials;
@@ -547,10 +550,25 @@ GpuPathIntegrator::~GpuPathIntegrator()
 Rendering* GpuPathIntegrator::Render(Allocator& alloc, const Camera* camera)
 {
     auto* pc = dynamic_cast<const PerspectiveCamera*>(camera);
-    auto* box = pc ? dynamic_cast<const BoxFilter*>(pc->GetFilter()) : nullptr;
-    if (!pc || !box)
+    const Filter* filter = pc ? pc->GetFilter() : nullptr;
+    int32_t filter_type = -1;
+    float filter_sigma = 0;
+    if (dynamic_cast<const BoxFilter*>(filter))
     {
-        Unsupported("camera (supported: PerspectiveCamera with a BoxFilter)");
+        filter_type = BBG_FILTER_BOX;
+    }
+    else if (dynamic_cast<const TentFilter*>(filter))
+    {
+        filter_type = BBG_FILTER_TENT;
+    }
+    else if (auto* gf = dynamic_cast<const GaussianFilter*>(filter))
+    {
+        filter_type = BBG_FILTER_GAUSSIAN;
+        filter_sigma = gf->sigma;
+    }
+    if (!pc || filter_type < 0)
+    {
+        Unsupported("camera (supported: PerspectiveCamera with a Box, Tent or Gaussian filter)");
     }
     bbg_camera cam{};
     const Point2i res = pc->GetScreenResolution();
@@ -563,12 +581,24 @@ Rendering* GpuPathIntegrator::Render(Allocator& alloc, const Camera* camera)
     Put3(cam.u, pc->*Get(CamU{}));
     Put3(cam.v, pc->*Get(CamV{}));
     cam.lens_radius = pc->*Get(CamLensRadius{});
-    cam.filter_extent = box->extent;
+    cam.filter_extent = filter->extent;
+    cam.filter_type = filter_type;
+    cam.filter_sigma = filter_sigma;
 
     bbg_render_params params{};
     params.spp = sampler_->samples_per_pixel;
-    params.seed = static_cast<const IndependentSampler*>(sampler_)->*Get(SamplerSeed{});
     params.use_graph = 1;
+    if (auto* st = dynamic_cast<const StratifiedSampler*>(sampler_))
+    {
+        params.sampler = BBG_SAMPLER_STRATIFIED;
+        params.seed = st->*Get(StratSeed{});
+        params.x_samples = st->*Get(StratX{});
+        params.jitter = (st->*Get(StratJitter{})) ? 1 : 0;
+    }
+    else
+    {
+        params.seed = static_cast<const IndependentSampler*>(sampler_)->*Get(SamplerSeed{});
+    }
 
     GpuRendering* progress = alloc.new_object<GpuRendering>(camera);
     bbg_integrator* handle = integrator_;

@@ -86,7 +86,14 @@ struct CameraDev
     float origin[3], lower_left[3], horizontal[3], vertical[3], u[3], v[3];
     float lens_radius;
     float filter_extent;
+    int32_t filter_type;     // BBG_FILTER_*
+    const float* filter_cdf; // Gaussian: GaussianFilterCdf tables (device)
 };
+
+// Gaussian filter table resolution (GaussianFilter: 32 x 32 samples).
+constexpr int32_t kFilterTable = 32;
+constexpr int32_t kFilterCdfFloats = (kFilterTable + 1) * (kFilterTable + 1);
+void GaussianFilterCdf(float sigma, float extent, float* cdf_out);
 
 // ---- host helpers (host_build.cpp) -----------------------------------------
 

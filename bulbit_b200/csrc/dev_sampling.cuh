@@ -82,6 +82,89 @@ __device__ __forceinline__ P2 Next2D(uint64_t& state)
     return P2{ a, b };
 }
 
+// PermutationElement (include/bulbit/hash.h:129-159): Kensler's hashed
+// permutation of [0, l) ("Correlated Multi-Jittered Sampling", 2013).
+__device__ __forceinline__ uint32_t PermutationElement(uint32_t i, uint32_t l, uint32_t p)
+{
+    uint32_t w = l - 1;
+    w |= w >> 1;
+    w |= w >> 2;
+    w |= w >> 4;
+    w |= w >> 8;
+    w |= w >> 16;
+    do
+    {
+        i ^= p;
+        i *= 0xe170893du;
+        i ^= p >> 16;
+        i ^= (i & w) >> 4;
+        i ^= p >> 8;
+        i *= 0x0929eb3fu;
+        i ^= p >> 23;
+        i ^= (i & w) >> 1;
+        i *= 1u | p >> 27;
+        i *= 0x6935fa69u;
+        i ^= (i & w) >> 11;
+        i *= 0x74dcb303u;
+        i ^= (i & w) >> 2;
+        i *= 0x9e501cc3u;
+        i ^= (i & w) >> 2;
+        i *= 0xc860a3dfu;
+        i &= w;
+        i ^= i >> 5;
+    } while (i >= l);
+    return (i + p) % l;
+}
+
+// The per-path sampler: IndependentSampler (src/sampler/independent_sampler.cpp)
+// or StratifiedSampler (src/sampler/stratified_sampler.cpp:16-58). Both seed
+// the same PCG32 stream from the pixel and sample; the stratified one places
+// each draw of dimension d in a stratum chosen by a permutation hashed from
+// (seed, pixel, d), jittered by the stream.
+struct PathSampler
+{
+    uint64_t state;
+    int32_t dim;        // stratified: next dimension
+    int32_t stratified; // 0: independent
+    int32_t px, py, sample, seed, spp, x_samples, jitter;
+};
+
+__device__ __forceinline__ uint32_t StratumHash(const PathSampler& s)
+{
+    // Hash(seed, current_pixel, dimension): 16 bytes, little-endian.
+    uint64_t k0 = uint64_t(uint32_t(s.seed)) | (uint64_t(uint32_t(s.px)) << 32);
+    uint64_t k1 = uint64_t(uint32_t(s.py)) | (uint64_t(uint32_t(s.dim)) << 32);
+    return uint32_t(Murmur64A_16(k0, k1));
+}
+
+__device__ __forceinline__ float Next1D(PathSampler& s)
+{
+    if (!s.stratified)
+    {
+        return Next1D(s.state);
+    }
+    int32_t stratum = int32_t(PermutationElement(uint32_t(s.sample), uint32_t(s.spp), StratumHash(s)));
+    s.dim += 1;
+    float delta = s.jitter ? Next1D(s.state) : 0.5f;
+    return (float(stratum) + delta) / float(s.spp);
+}
+
+__device__ __forceinline__ P2 Next2D(PathSampler& s)
+{
+    if (!s.stratified)
+    {
+        return Next2D(s.state);
+    }
+    int32_t stratum = int32_t(PermutationElement(uint32_t(s.sample), uint32_t(s.spp), StratumHash(s)));
+    s.dim += 2;
+    int32_t x = stratum % s.x_samples;
+    int32_t y = stratum / s.x_samples;
+    float dx = s.jitter ? Next1D(s.state) : 0.5f;
+    float dy = s.jitter ? Next1D(s.state) : 0.5f;
+    int32_t y_samples = s.spp / s.x_samples;
+    return P2{ (float(x) + dx) / float(s.x_samples), (float(y) + dy) / float(y_samples) };
+}
+
 // PowerHeuristic(1, f, 1, g) (include/bulbit/sampling.h:42-48).
 __device__ __forceinline__ float PowerHeuristic(float pdf_f, float pdf_g)
 {

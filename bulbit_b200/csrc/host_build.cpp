@@ -528,6 +528,8 @@ void CameraFromSpec(const bbg_camera_spec& s, bbg_camera* out)
     Store3(out->v, v);
     out->lens_radius = s.aperture_radius;
     out->filter_extent = s.filter_extent;
+    out->filter_type = s.filter_type;
+    out->filter_sigma = s.filter_sigma;
 }
 
 // ---------------------------------------------------------------- materials
@@ -754,6 +756,38 @@ void BuildDistribution(const float* f, int32_t n, float* func, float* cdf, float
             cdf[i] /= *func_integral;
         }
     }
+}
+
+// GaussianFilter's tabulated distribution (src/reconstruction/gaussian_filter.cpp:8-28):
+// 32 x 32 values Gaussian(p.x) Gaussian(p.y) at the cell centres of
+// [-extent/2, extent/2]^2, then Distribution2D (include/bulbit/sampling.h:426-446).
+// Only the CDFs are kept (SampleContinuous reads nothing else): cdf_out[0..33)
+// the marginal, then row v's conditional at 33 + 33 v.
+void GaussianFilterCdf(float sigma, float extent, float* cdf_out)
+{
+    constexpr int32_t n = kFilterTable;
+    const float two_pi = float(2 * 3.14159265358979323846);
+    auto gaussian = [&](float x) {
+        return 1 / std::sqrt(two_pi * sigma * sigma) * std::exp(-((x - 0) * (x - 0)) / (2 * sigma * sigma));
+    };
+    float values[n * n];
+    float half_extent = extent / 2;
+    for (int32_t y = 0; y < n; ++y)
+    {
+        for (int32_t x = 0; x < n; ++x)
+        {
+            float px = ((float(x) + 0.5f) / float(n)) * extent - half_extent;
+            float py = ((float(y) + 0.5f) / float(n)) * extent - half_extent;
+            values[y * n + x] = gaussian(px) * gaussian(py);
+        }
+    }
+    float func[n], integral[n];
+    for (int32_t v = 0; v < n; ++v)
+    {
+        BuildDistribution(&values[v * n], n, func, cdf_out + (n + 1) * (v + 1), &integral[v]);
+    }
+    float marginal_integral;
+    BuildDistribution(integral, n, func, cdf_out, &marginal_integral);
 }
 
 // Vose's alias method over the pmf (exact in double, stored in float).

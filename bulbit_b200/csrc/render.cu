@@ -61,6 +61,9 @@ struct SceneDev
     int32_t regularize;
     int32_t spp;
     int32_t seed;
+    int32_t sampler_kind; // BBG_SAMPLER_*
+    int32_t x_samples;    // stratified: strata along x
+    int32_t jitter;       // stratified: jitter within strata
     CameraDev camera;
 };
 
@@ -81,6 +84,7 @@ struct WaveDev
     int32_t* counts; // [0],[1] ray queues, [2] shadow queue, [3],[4] work counters
     unsigned long long* stats; // closest rays, shadow rays
     const int64_t* wave;       // [0] first path, [1] paths in wave
+    int32_t* dim;              // stratified sampler: next dimension per slot
 };
 
 constexpr int32_t kSpecularBit = 1 << 16;
@@ -166,6 +170,88 @@ __device__ __forceinline__ int32_t Append(int32_t* counter, bool pred)
     return base + __popc(m & ((1u << lane) - 1u));
 }
 
+// The sampler of the path in `slot` (PathSampler), and its write-back. A
+// stratified sampler needs the path's pixel and sample (single-scene renders).
+__device__ __forceinline__ PathSampler LoadSampler(const SceneDev& s, const WaveDev& w, int32_t slot)
+{
+    PathSampler p{};
+    p.state = w.rng[slot];
+    p.stratified = s.sampler_kind == BBG_SAMPLER_STRATIFIED;
+    if (p.stratified)
+    {
+        int64_t path = w.wave[0] + slot;
+        int64_t pixel = path / s.spp;
+        p.sample = int32_t(path % s.spp);
+        p.px = int32_t(pixel % s.camera.width);
+        p.py = int32_t(pixel / s.camera.width);
+        p.dim = w.dim[slot];
+        p.seed = s.seed;
+        p.spp = s.spp;
+        p.x_samples = s.x_samples;
+        p.jitter = s.jitter;
+    }
+    return p;
+}
+
+__device__ __forceinline__ void StoreSampler(const WaveDev& w, int32_t slot, const PathSampler& p)
+{
+    w.rng[slot] = p.state;
+    if (p.stratified)
+    {
+        w.dim[slot] = p.dim;
+    }
+}
+
+// Distribution1D::SampleContinuous over a CDF of n + 1 entries
+// (include/bulbit/sampling.h:375-393): FindInterval, then the linear offset.
+__device__ __forceinline__ float CdfSampleContinuous(const float* cdf, int32_t n, float u, int32_t* off)
+{
+    int32_t size = n + 1;
+    int32_t first = 0, len = size;
+    while (len > 0)
+    {
+        int32_t half = len >> 1, middle = first + half;
+        if (cdf[middle] <= u)
+        {
+            first = middle + 1;
+            len -= half + 1;
+        }
+        else
+        {
+            len = half;
+        }
+    }
+    int32_t offset = first - 1;
+    offset = offset < 0 ? 0 : (offset > size - 2 ? size - 2 : offset);
+    *off = offset;
+    float du = (u - cdf[offset]) / (cdf[offset + 1] - cdf[offset]);
+    return (float(offset) + du) / float(n);
+}
+
+// Filter::Sample for the camera's filter (src/reconstruction/box_filter.cpp:17-21,
+// tent_filter.cpp:21-29, gaussian_filter.cpp:40-43: Distribution2D::SampleContinuous,
+// the marginal over rows first).
+__device__ __forceinline__ P2 FilterSample(const CameraDev& c, P2 u)
+{
+    const float e = c.filter_extent;
+    if (c.filter_type == BBG_FILTER_GAUSSIAN)
+    {
+        int32_t v, dummy;
+        float d1 = CdfSampleContinuous(c.filter_cdf, kFilterTable, u.y, &v);
+        float d0 = CdfSampleContinuous(c.filter_cdf + (kFilterTable + 1) * (v + 1), kFilterTable, u.x, &dummy);
+        return P2{ d0 * e - e / 2, d1 * e - e / 2 };
+    }
+    if (c.filter_type == BBG_FILTER_TENT)
+    {
+        float h = e / 2;
+        float x = u.x < 0.5f ? h * (sqrtf(2 * u.x) - 1) : h * (1 - sqrtf(1 - 2 * (u.x - 0.5f)));
+        float y = u.y < 0.5f ? h * (sqrtf(2 * u.y) - 1) : h * (1 - sqrtf(1 - 2 * (u.y - 0.5f)));
+        return P2{ x, y };
+    }
+    // BoxFilter: (2u - 1) * extent / 2.
+    return P2{ (u.x * 2 - 1) * e / 2, (u.y * 2 - 1) * e / 2 };
+}
+
 // ---------------------------------------------------------------- raygen
 
 // Render loop body (src/integrator/integrator.cpp:185-190) and
@@ -186,12 +272,21 @@ __global__ void __launch_bounds__(kBlock) RaygenKernel(Scenes sc, WaveDev w)
         const CameraDev& c = s.camera;
         int32_t px = int32_t(pixel % c.width);
         int32_t py = int32_t(pixel / c.width);
-        uint64_t rng = SamplerStart(px, py, s.seed, sample);
+        PathSampler rng{};
+        rng.state = SamplerStart(px, py, s.seed, sample);
+        rng.stratified = s.sampler_kind == BBG_SAMPLER_STRATIFIED;
+        rng.px = px;
+        rng.py = py;
+        rng.sample = sample;
+        rng.seed = s.seed;
+        rng.spp = s.spp;
+        rng.x_samples = s.x_samples;
+        rng.jitter = s.jitter;
         P2 u1 = Next2D(rng); // lens sample: the right-hand argument, drawn first
         P2 u0 = Next2D(rng); // filter sample
 
-        // BoxFilter::Sample: (2u - 1) * extent / 2, then + 0.5.
-        P2 f{ (u0.x * 2 - 1) * c.filter_extent / 2, (u0.y * 2 - 1) * c.filter_extent / 2 };
+        // pixel offset = filter->Sample(u0) + 0.5.
+        P2 f = FilterSample(c, u0);
         P2 off{ f.x + 0.5f, f.y + 0.5f };
         V3 pixel_center = load3(c.lower_left) + load3(c.horizontal) * (px + off.x) / float(c.width) +
                           load3(c.vertical) * (py + off.y) / float(c.height);
@@ -205,7 +300,11 @@ __global__ void __launch_bounds__(kBlock) RaygenKernel(Scenes sc, WaveDev w)
         w.d_eta[i] = make_float4(d.x, d.y, d.z, 1.0f);
         w.beta[i] = make_float4(1, 1, 1, 0);
         w.L[i] = make_float4(0, 0, 0, 0);
-        w.rng[i] = rng;
+        w.rng[i] = rng.state;
+        if (rng.stratified)
+        {
+            w.dim[i] = rng.dim;
+        }
         w.flags[i] = scene << kSceneShift;
         w.queue[0][i] = int32_t(i);
     }
@@ -517,9 +616,9 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(Scenes sc, WaveDev w, int 
         V3 ro{ o4.x, o4.y, o4.z }, rd{ d4.x, d4.y, d4.z };
         float prev_bsdf_pdf = o4.w, eta_scale = d4.w;
         Spec beta{ b4.x, b4.y, b4.z }, L{ L4.x, L4.y, L4.z };
-        uint64_t rng = w.rng[slot];
         int32_t fl = w.flags[slot];
         const SceneDev& s = sc.Scene(fl >> kSceneShift);
+        PathSampler rng = LoadSampler(s, w, slot);
         int32_t bounce = fl & 0xffff;
         bool specular_bounce = (fl & kSpecularBit) != 0;
         bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
@@ -705,7 +804,7 @@ __global__ void __launch_bounds__(kBlock) ShadeKernel(Scenes sc, WaveDev w, int 
             w.o_pdf[slot] = make_float4(ro.x, ro.y, ro.z, prev_bsdf_pdf);
             w.d_eta[slot] = make_float4(rd.x, rd.y, rd.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
-            w.rng[slot] = rng;
+            StoreSampler(w, slot, rng);
             w.flags[slot] = (fl & kSceneMask) | bounce | (specular_bounce ? kSpecularBit : 0) |
                             (any_non_specular ? kAnyNonSpecularBit : 0);
         }
@@ -806,7 +905,7 @@ __device__ __forceinline__ void AddEscaped(const SceneDev& s, Spec beta, int32_t
 // SampleDirectLight, as in ShadeKernel: u0 then u12 drawn, power heuristic
 // on the light and BSDF pdfs). Returns whether a shadow ray was made.
 __device__ __forceinline__ bool DirectLight(const SceneDev& s, const BSDF& bsdf, V3 point, V3 sn, V3 wo, Spec beta,
-                                            uint64_t& rng, V3* sh_d, float* sh_t, Spec* sh_c)
+                                            PathSampler& rng, V3* sh_d, float* sh_t, Spec* sh_c)
 {
     float u0 = Next1D(rng);
     P2 u12 = Next2D(rng);
@@ -872,7 +971,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
         V3 ro{ o4.x, o4.y, o4.z }, rd{ d4.x, d4.y, d4.z };
         float prev_pdf = o4.w, eta_scale = d4.w;
         Spec beta{ b4.x, b4.y, b4.z }, L{ L4.x, L4.y, L4.z };
-        uint64_t rng = w.rng[slot];
+        PathSampler rng = LoadSampler(s, w, slot);
         int32_t fl = w.flags[slot];
         int32_t bounce = fl & 0xffff;
         bool specular_bounce = (fl & kSpecularBit) != 0;
@@ -1011,7 +1110,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
             w.o_pdf[slot] = make_float4(ro.x, ro.y, ro.z, prev_pdf);
             w.d_eta[slot] = make_float4(rd.x, rd.y, rd.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
-            w.rng[slot] = rng;
+            StoreSampler(w, slot, rng);
             w.flags[slot] = bounce | (specular_bounce ? kSpecularBit : 0) | (any_non_specular ? kAnyNonSpecularBit : 0);
         }
         int32_t qi = Append(&w.counts[parity ^ 1], cont);
@@ -1045,7 +1144,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
         float4 d4 = w.d_eta[slot], b4 = w.beta[slot];
         float eta_scale = d4.w;
         Spec beta{ b4.x, b4.y, b4.z };
-        uint64_t rng = w.rng[slot];
+        PathSampler rng = LoadSampler(s, w, slot);
         int32_t fl = w.flags[slot];
         int32_t bounce = fl & 0xffff;
         bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
@@ -1173,7 +1272,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, Gu
             w.flags[slot] = bounce | (spec_sample ? kSpecularBit : 0) |
                             ((any_non_specular || !spec_sample) ? kAnyNonSpecularBit : 0);
         }
-        w.rng[slot] = rng;
+        StoreSampler(w, slot, rng);
         int32_t qi = Append(&w.counts[parity ^ 1], cont);
         if (cont)
         {
@@ -1313,40 +1412,6 @@ __global__ void __launch_bounds__(kBlock) FilmKernel(Scenes sc, WaveDev w)
 
 // ---------------------------------------------------------------- GGX energy tables
 
-// PermutationElement (include/bulbit/hash.h:129-159): Kensler's hashed
-// permutation of [0, l) ("Correlated Multi-Jittered Sampling", 2013).
-__device__ __forceinline__ uint32_t PermutationElement(uint32_t i, uint32_t l, uint32_t p)
-{
-    uint32_t w = l - 1;
-    w |= w >> 1;
-    w |= w >> 2;
-    w |= w >> 4;
-    w |= w >> 8;
-    w |= w >> 16;
-    do
-    {
-        i ^= p;
-        i *= 0xe170893du;
-        i ^= p >> 16;
-        i ^= (i & w) >> 4;
-        i ^= p >> 8;
-        i *= 0x0929eb3fu;
-        i ^= p >> 23;
-        i ^= (i & w) >> 1;
-        i *= 1u | p >> 27;
-        i *= 0x6935fa69u;
-        i ^= (i & w) >> 11;
-        i *= 0x74dcb303u;
-        i ^= (i & w) >> 2;
-        i *= 0x9e501cc3u;
-        i ^= (i & w) >> 2;
-        i *= 0xc860a3dfu;
-        i &= w;
-        i ^= i >> 5;
-    } while (i >= l);
-    return (i + p) % l;
-}
-
 constexpr int kEnergySamples = 1024; // 32 x 32 strata, PrepareReflectanceTextures(32, 1024)
 
 // The stratified samples of PrepareReflectanceTextures (src/bxdf/microfacet.cpp:239-275):
@@ -1455,11 +1520,14 @@ struct bbg_integrator
     int64_t capacity = 0;
     DevBuf<float4> o_pdf, d_eta, beta, L, hit, sh_o, sh_d, sh_c;
     DevBuf<uint64_t> rng;
-    DevBuf<int32_t> flags, queue0, queue1, counts;
+    DevBuf<int32_t> flags, queue0, queue1, counts, dim;
     DevBuf<unsigned long long> stats;
     DevBuf<int64_t> wave;
     int64_t* wave_host = nullptr; // pinned
 
+    // Gaussian filter table of the last camera that used one (sigma, extent).
+    DevBuf<float> filter_cdf;
+    float filter_key[2] = { -1, -1 };
     // Film (device copies for host-memory renders).
     DevBuf<float> film_rgb, film_moments, film_path_L;
     DevBuf<int32_t> film_count;
@@ -1570,6 +1638,7 @@ struct bbg_integrator
         w.counts = counts.p;
         w.stats = stats.p;
         w.wave = wave.p;
+        w.dim = dim.p;
         return w;
     }
 
@@ -1584,7 +1653,7 @@ struct bbg_integrator
         }
         rng.reset();
         BBG_TRY(rng.alloc(m));
-        for (auto* b : { &flags, &queue0, &queue1 })
+        for (auto* b : { &flags, &queue0, &queue1, &dim })
         {
             b->reset();
             BBG_TRY(b->alloc(m));
@@ -1762,6 +1831,35 @@ bool SameFilm(const FilmDev& a, const FilmDev& b)
     return std::memcmp(&a, &b, sizeof(FilmDev)) == 0;
 }
 
+// Checks a render's sampler and filter choice and prepares the Gaussian
+// filter's table (once per sigma and extent) for MakeSceneDev.
+bbg_status PrepareSamplerAndFilter(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p)
+{
+    if (p->sampler != BBG_SAMPLER_INDEPENDENT &&
+        (p->sampler != BBG_SAMPLER_STRATIFIED || p->x_samples <= 0 || p->spp % p->x_samples != 0))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "sampler %d with x_samples %d does not divide spp %d", p->sampler,
+                    p->x_samples, p->spp);
+    }
+    if (cam->filter_type < BBG_FILTER_BOX || cam->filter_type > BBG_FILTER_GAUSSIAN ||
+        (cam->filter_type == BBG_FILTER_GAUSSIAN && !(cam->filter_sigma > 0 && cam->filter_extent > 0)))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "filter type %d (sigma %g, extent %g)", cam->filter_type,
+                    double(cam->filter_sigma), double(cam->filter_extent));
+    }
+    if (cam->filter_type == BBG_FILTER_GAUSSIAN &&
+        (I->filter_key[0] != cam->filter_sigma || I->filter_key[1] != cam->filter_extent || !I->filter_cdf.p))
+    {
+        std::vector<float> cdf(kFilterCdfFloats);
+        GaussianFilterCdf(cam->filter_sigma, cam->filter_extent, cdf.data());
+        BBG_TRY(I->filter_cdf.upload(cdf.data(), cdf.size(), I->stream));
+        BBG_CUDA(cudaStreamSynchronize(I->stream));
+        I->filter_key[0] = cam->filter_sigma;
+        I->filter_key[1] = cam->filter_extent;
+    }
+    return BBG_OK;
+}
+
 // The kernels' view of one scene: its accel, shading data, lights and camera.
 SceneDev MakeSceneDev(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p)
 {
@@ -1791,6 +1889,11 @@ SceneDev MakeSceneDev(bbg_integrator* I, const bbg_camera* cam, const bbg_render
     s.regularize = I->regularize;
     s.spp = p->spp;
     s.seed = p->seed;
+    s.sampler_kind = p->sampler;
+    s.x_samples = p->x_samples;
+    s.jitter = p->jitter ? 1 : 0;
+    s.camera.filter_type = cam->filter_type;
+    s.camera.filter_cdf = cam->filter_type == BBG_FILTER_GAUSSIAN ? I->filter_cdf.p : nullptr;
     s.camera.width = cam->width;
     s.camera.height = cam->height;
     std::memcpy(s.camera.origin, cam->origin, sizeof(float) * 3);
@@ -1825,6 +1928,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         return Fail(BBG_ERR_INVALID_ARG, "wave of %lld paths exceeds 2^30", (long long)wave_paths);
     }
     BBG_TRY(I->Reserve(wave_paths));
+    BBG_TRY(PrepareSamplerAndFilter(I, cam, p));
 
     SceneDev s = MakeSceneDev(I, cam, p);
 
@@ -2213,6 +2317,12 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             return Fail(BBG_ERR_UNSUPPORTED, "bbg_batch_render: scene %d uses the reference-order traversal", int(i));
         }
         const int64_t n_pixels = int64_t(cam->width) * cam->height;
+        if (params[i].sampler != BBG_SAMPLER_INDEPENDENT)
+        {
+            return Fail(BBG_ERR_UNSUPPORTED, "bbg_batch_render: scene %d: batches use the independent sampler",
+                        int(i));
+        }
+        BBG_TRY(PrepareSamplerAndFilter(I, cam, &params[i]));
         B->host_scenes[i] = MakeSceneDev(I, cam, &params[i]);
         FilmDev f{};
         if (mem == BBG_MEM_DEVICE)

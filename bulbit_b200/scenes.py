@@ -193,7 +193,8 @@ GOLD_ETA = (0.161, 0.492, 1.426)
 GOLD_K = (4.08769, 2.32625, 1.846)
 
 
-def camera_spec(position, target, up, vfov, aperture, focus, width, height, filter_extent=1.0):
+def camera_spec(position, target, up, vfov, aperture, focus, width, height, filter_extent=1.0,
+                filter_type=abi.BBG_FILTER_BOX, filter_sigma=0.5):
     c = abi.CameraSpec()
     c.position[:] = list(position)
     c.target[:] = list(target)
@@ -204,6 +205,8 @@ def camera_spec(position, target, up, vfov, aperture, focus, width, height, filt
     c.width = width
     c.height = height
     c.filter_extent = filter_extent
+    c.filter_type = filter_type
+    c.filter_sigma = filter_sigma
     return c
 
 

@@ -284,6 +284,15 @@ typedef struct bbg_light
 
 /* PerspectiveCamera inputs (src/camera/perspective_camera.cpp:8) with a
  * Transform::LookAt(position, target, up) pose and a BoxFilter(extent). */
+/* Reconstruction filters (src/reconstruction/{box,tent,gaussian}_filter.cpp):
+ * the filter's Sample(u) places each camera sample in its pixel. */
+enum
+{
+    BBG_FILTER_BOX = 0,
+    BBG_FILTER_TENT = 1,
+    BBG_FILTER_GAUSSIAN = 2
+};
+
 typedef struct bbg_camera_spec
 {
     float position[3];
@@ -295,6 +304,8 @@ typedef struct bbg_camera_spec
     int32_t width;
     int32_t height;
     float filter_extent;
+    int32_t filter_type;  /* BBG_FILTER_* (0: box) */
+    float filter_sigma;   /* Gaussian standard deviation (GaussianFilter(sigma, extent)) */
 } bbg_camera_spec;
 
 /* The derived state PerspectiveCamera::SampleRay reads
@@ -311,6 +322,8 @@ typedef struct bbg_camera
     float v[3];
     float lens_radius;
     float filter_extent;
+    int32_t filter_type;
+    float filter_sigma;
 } bbg_camera;
 
 bbg_status bbg_camera_perspective(const bbg_camera_spec* spec, bbg_camera* out);
@@ -352,7 +365,18 @@ typedef struct bbg_render_params
                              BSDF, in (0, 1] (0: 1/2) */
     int32_t guide_steps;  /* Adam steps per wave when training, each on its own
                              batch of guide_batch training samples (0: 1) */
+    int32_t sampler;      /* BBG_SAMPLER_INDEPENDENT (0) or BBG_SAMPLER_STRATIFIED:
+                             StratifiedSampler(x_samples, spp / x_samples, jitter,
+                             seed), src/sampler/stratified_sampler.cpp */
+    int32_t x_samples;    /* stratified: strata along x (spp must be a multiple) */
+    int32_t jitter;       /* stratified: jitter within strata */
 } bbg_render_params;
+
+enum
+{
+    BBG_SAMPLER_INDEPENDENT = 0,
+    BBG_SAMPLER_STRATIFIED = 1
+};
 
 /* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields
  * are those Film::AddSample maintains (src/reconstruction/film.cpp:26-37):

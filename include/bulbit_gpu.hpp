@@ -27,7 +27,8 @@
 // (energy compensation off) and MetallicRoughnessMaterial with constant
 // textures and no normal or alpha maps;
 // PointLight, SpotLight, UniformInfiniteLight, DiffuseAreaLight with a
-// constant emission; PerspectiveCamera with a BoxFilter; IndependentSampler.
+// constant emission; PerspectiveCamera with a Box, Tent or Gaussian filter;
+// IndependentSampler or StratifiedSampler.
 // Primitives without a material are passed through as the reference does.
 //
 // Build: compile bulbit_b200/cpp/bulbit_gpu.cpp with the reference's include

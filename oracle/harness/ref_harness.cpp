@@ -82,19 +82,51 @@ struct RefScene
     int32 n_prims = 0;
 };
 
+std::unique_ptr<Filter> MakeFilter(const bbg_camera_spec& s)
+{
+    switch (s.filter_type)
+    {
+    case BBG_FILTER_TENT:
+        return std::make_unique<TentFilter>(s.filter_extent);
+    case BBG_FILTER_GAUSSIAN:
+        return std::make_unique<GaussianFilter>(s.filter_sigma, s.filter_extent);
+    default:
+        return std::make_unique<BoxFilter>(s.filter_extent);
+    }
+}
+
 struct RefCamera
 {
-    BoxFilter filter;
+    std::unique_ptr<Filter> filter;
     PerspectiveCamera camera;
 
     RefCamera(const bbg_camera_spec& s)
-        : filter(s.filter_extent)
+        : filter(MakeFilter(s))
         , camera(Transform::LookAt(Point3(s.position[0], s.position[1], s.position[2]),
                                    Point3(s.target[0], s.target[1], s.target[2]), Vec3(s.up[0], s.up[1], s.up[2])),
-                 s.vfov_deg, s.aperture_radius, s.focus_distance, Point2i(s.width, s.height), nullptr, &filter)
+                 s.vfov_deg, s.aperture_radius, s.focus_distance, Point2i(s.width, s.height), nullptr, filter.get())
     {
     }
 };
+
+// The sampler the next integrator and path traces use: IndependentSampler, or
+// StratifiedSampler(x_samples, spp / x_samples, jitter, seed).
+struct SamplerChoice
+{
+    int32_t kind = BBG_SAMPLER_INDEPENDENT;
+    int32_t x_samples = 1;
+    int32_t jitter = 1;
+};
+SamplerChoice g_sampler;
+
+Sampler* NewSampler(int32_t spp, int32_t seed)
+{
+    if (g_sampler.kind == BBG_SAMPLER_STRATIFIED)
+    {
+        return new StratifiedSampler(g_sampler.x_samples, spp / g_sampler.x_samples, g_sampler.jitter != 0, seed);
+    }
+    return new IndependentSampler(spp, seed);
+}
 
 void EnsurePool(int32 threads)
 {
@@ -282,8 +314,7 @@ int bbref_integrator_create(void* handle, int32_t spp, int32_t seed, int32_t max
                             int32_t regularize, double* seconds)
 {
     auto* rs = static_cast<RefScene*>(handle);
-    static thread_local std::unique_ptr<IndependentSampler> keep;
-    auto* sampler = new IndependentSampler(spp, seed); // owned for the process lifetime (non-owning in the API)
+    Sampler* sampler = NewSampler(spp, seed); // owned for the process lifetime (non-owning in the API)
     auto t0 = std::chrono::steady_clock::now();
     InScratchDir([&] {
         rs->integrator = std::make_unique<PathIntegrator>(rs->bvh.get(), rs->lights, sampler, max_bounces,
@@ -470,6 +501,8 @@ int bbref_camera(const bbg_camera_spec* spec, bbg_camera* out)
     put(out->v, c.*Get(CamV{}));
     out->lens_radius = c.*Get(CamLensRadius{});
     out->filter_extent = spec->filter_extent;
+    out->filter_type = spec->filter_type;
+    out->filter_sigma = spec->filter_sigma;
     return 0;
 }
 
@@ -486,12 +519,12 @@ double bbref_trace_paths(void* handle, const bbg_camera_spec* spec, int32_t spp,
     const Camera* camera = &rc.camera;
     const PathIntegrator* integrator = rs->integrator.get();
     auto t0 = std::chrono::steady_clock::now();
+    std::unique_ptr<Sampler> proto(NewSampler(spp, seed));
     ParallelFor(0, int32(n), [&](int32 b, int32 e) {
-        IndependentSampler proto(spp, seed);
-        int8 mem[64];
+        int8 mem[128];
         BufferResource buffer(mem, sizeof(mem));
         Allocator alloc(&buffer);
-        Sampler* sampler = proto.Clone(alloc);
+        Sampler* sampler = proto->Clone(alloc);
         for (int32 i = b; i < e; ++i)
         {
             int64 id = path_ids ? path_ids[i] : i;
@@ -560,6 +593,11 @@ int bbref_light_pmf(void* handle, float* pmf_out)
 }
 
 // The first n draws of IndependentSampler after StartPixelSample.
+void bbref_set_sampler(int32_t kind, int32_t x_samples, int32_t jitter)
+{
+    g_sampler = SamplerChoice{ kind, x_samples, jitter };
+}
+
 // The reference's GGX energy tables after PrepareReflectanceTextures(32, 1024)
 // (what every Integrator constructor runs): E 32 x 32, E_avg 32.
 int bbref_ggx_energy_tables(float* e_out, float* e_avg_out)

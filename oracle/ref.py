@@ -45,6 +45,7 @@ def lib():
             "bbref_light_pmf": (I32, [P, P]),
             "bbref_sampler_draws": (I32, [I32, I32, I32, I32, I32, P]),
             "bbref_ggx_energy_tables": (I32, [P, P]),
+            "bbref_set_sampler": (None, [I32, I32, I32]),
             "bbref_pcg32": (I32, [C.c_uint64, C.c_uint64, I32, P]),
             "bbref_hash_pixel_sample": (C.c_uint64, [I32, I32, I32, I32]),
         }
@@ -172,6 +173,11 @@ def sampler_draws(px, py, seed, sample, n):
     out = np.zeros(n, np.float32)
     lib().bbref_sampler_draws(px, py, seed, sample, n, _p(out))
     return out
+
+
+def set_sampler(kind=0, x_samples=1, jitter=1):
+    """Sampler for later integrators and path traces: 0 independent, 1 stratified."""
+    lib().bbref_set_sampler(kind, x_samples, jitter)
 
 
 def ggx_energy_tables():

@@ -203,10 +203,9 @@ void CompareQueries(const BVH& bvh, const bulbit_gpu::GpuBVH& gpu, Point3 center
     r->Expect(same_single >= n_single - 2 && same_any >= n_single - 2 && same_batch >= n_batch - 20, tag + "_queries_ok");
 }
 
-void CompareRender(Scene& scene, const BVH& bvh, const bulbit_gpu::GpuBVH& gpu, const Camera& camera, int32 spp,
-                   int32 bounces, Result* r, const std::string& tag)
+void CompareRender(Scene& scene, const BVH& bvh, const bulbit_gpu::GpuBVH& gpu, const Camera& camera,
+                   const Sampler& sampler, int32 bounces, Result* r, const std::string& tag)
 {
-    IndependentSampler sampler(spp);
     Allocator alloc;
     PathIntegrator cpu(&bvh, scene.GetLights(), &sampler, bounces);
     Rendering* a = cpu.Render(alloc, &camera);
@@ -259,7 +258,8 @@ int main()
             Point3 camera_pos(3.0f, 2.0f, 5.0f), sphere_pos(0.0f, 1.0f, 0.0f);
             PerspectiveCamera camera(Transform::LookAt(camera_pos, sphere_pos, y_axis), 35, 0.01f,
                                      Dist(camera_pos, sphere_pos), Point2i(160, 90), nullptr, &filter);
-            CompareRender(scene, bvh, gpu, camera, 16, 8, &r, "readme");
+            IndependentSampler sampler(16);
+            CompareRender(scene, bvh, gpu, camera, sampler, 8, &r, "readme");
         }
         {
             Scene scene;
@@ -269,11 +269,13 @@ int main()
             bulbit_gpu::GpuBVH gpu_own(scene.GetPrimitives()); // the library's own build of the same tree
             CompareQueries(bvh, gpu, Point3(0, 1.2f, 0), 2.5f, &r, "mesh");
             CompareQueries(bvh, gpu_own, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_own_tree");
-            BoxFilter filter;
+            // The camera's default filter (GaussianFilter) and a stratified sampler.
+            GaussianFilter filter;
             Point3 eye(0.0f, 1.5f, 5.0f), at(0.0f, 1.2f, 0.0f);
             PerspectiveCamera camera(Transform::LookAt(eye, at, y_axis), 50, 0.0f, Dist(eye, at), Point2i(96, 72),
                                      nullptr, &filter);
-            CompareRender(scene, bvh, gpu, camera, 32, 12, &r, "mesh");
+            StratifiedSampler sampler(8, 4, true, 3);
+            CompareRender(scene, bvh, gpu, camera, sampler, 12, &r, "mesh");
         }
     }
     catch (const std::exception& e)

@@ -126,6 +126,38 @@ def test_materials_paths(oracle, mat):
     check_paths(mat, film.path_L, ref_L)
 
 
+@pytest.mark.parametrize("x_samples,jitter", [(4, True), (2, False)])
+def test_stratified_sampler_paths(oracle, x_samples, jitter):
+    """StratifiedSampler(x, spp / x, jitter, seed): every draw's stratum comes
+    from a permutation hashed from (seed, pixel, dimension)."""
+    scene = scenes.readme_sphere(width=64, height=36, spp=8)
+    scene.seed = 5
+    oracle.set_sampler(abi.BBG_SAMPLER_STRATIFIED, x_samples, 1 if jitter else 0)
+    try:
+        rs = oracle.RefScene(scene)
+        rs.make_integrator()
+        ref_L, _ = rs.trace_paths()
+    finally:
+        oracle.set_sampler()
+    acc = lib.GpuAccel(scene)
+    integ = lib.GpuPathIntegrator(acc, scene)
+    film = integ.render(path_L=True, sampler=abi.BBG_SAMPLER_STRATIFIED, x_samples=x_samples, jitter=jitter)
+    check_paths(f"stratified x{x_samples} jitter {jitter}", film.path_L, ref_L)
+
+
+@pytest.mark.parametrize("filt", ["tent", "gaussian"])
+def test_filter_paths(oracle, filt):
+    """TentFilter and GaussianFilter (tabulated Distribution2D) offsets of the
+    camera samples; the README scene's lens makes every offset visible."""
+    scene = scenes.readme_sphere(width=64, height=36, spp=8)
+    if filt == "tent":
+        scene.camera.filter_type, scene.camera.filter_extent = abi.BBG_FILTER_TENT, 2.0
+    else:
+        scene.camera.filter_type, scene.camera.filter_extent, scene.camera.filter_sigma = abi.BBG_FILTER_GAUSSIAN, 3.0, 0.5
+    rs, acc, integ, film, ref_L = render_both(oracle, scene)
+    check_paths(filt, film.path_L, ref_L)
+
+
 def test_point_and_sphere_area_lights_and_passthrough(oracle):
     """Point light, a spherical diffuse area light (two-sided), and a
     material-less sphere that paths cross without a bounce."""
