@@ -587,7 +587,7 @@ def main():
                    "parallelism": f"replicas x{world}", "bvh_build_s": round(build_s, 3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "TraceKernel<closest> (bulbit_b200/csrc/accel.cu)",
+                     "kernel": "PersistentTraceKernel<closest> (bulbit_b200/csrc/accel.cu)",
                      "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_closest,
                      "per_ray": {"nodes": nodes_c / n_rays, "prims": prims_c / n_rays,
@@ -598,6 +598,27 @@ def main():
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }
+    acc.close()
+    # The same soup and rays over the tree built on the device (linear BVH):
+    # its build time beside the host SAH build, and its closest + any-hit
+    # throughput (untimed in the headline; same event method).
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    acc = lib.GpuAccel(scene, device_build=True)
+    device_build_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    ev_d = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(max(1, args.steps))]
+    for k in range(len(ev_d)):
+        step(ev_d[k])
+    torch.cuda.synchronize()
+    dev_ms = sum(e[0].elapsed_time(e[2]) for e in ev_d)
+    line["device_built_tree"] = {
+        "build_ms": device_build_s * 1e3, "host_sah_build_ms": build_s * 1e3,
+        "mrays_per_s": rays_per_step * len(ev_d) / (dev_ms / 1e3) / 1e6,
+        "closest_ms": statistics.mean(e[0].elapsed_time(e[1]) for e in ev_d),
+        "any_ms": statistics.mean(e[1].elapsed_time(e[2]) for e in ev_d)}
     acc.close()
     del dev_c, dev_a, hits, occ
     if args.workload == "all":

@@ -217,7 +217,30 @@ bbg_status CheckGeometry(const bbg_geometry* g)
     return BBG_OK;
 }
 
-bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
+// Shading data (the reference Mesh arrays and shapes).
+bbg_status UploadShading(bbg_accel* a, const bbg_geometry* g)
+{
+    BBG_TRY(a->prim_shape.upload(a->host_prim_shape.data(), a->host_prim_shape.size(), a->stream));
+    BBG_TRY(a->tri_indices.upload(g->tri_indices, 3 * size_t(g->n_triangles), a->stream));
+    BBG_TRY(a->positions.upload(g->positions, 3 * size_t(g->n_vertices), a->stream));
+    if (g->n_spheres)
+    {
+        BBG_TRY(a->spheres.upload(g->spheres, size_t(g->n_spheres), a->stream));
+    }
+    a->has_shading = g->n_triangles == 0 || (g->normals && g->tangents);
+    if (g->normals && g->tangents)
+    {
+        BBG_TRY(a->normals.upload(g->normals, 3 * size_t(g->n_vertices), a->stream));
+        BBG_TRY(a->tangents.upload(g->tangents, 3 * size_t(g->n_vertices), a->stream));
+        if (g->uvs)
+        {
+            BBG_TRY(a->uvs.upload(g->uvs, 2 * size_t(g->n_vertices), a->stream));
+        }
+    }
+    return BBG_OK;
+}
+
+bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, bool device_build = false)
 {
     // Host-side checks and the tree come first: a malformed scene or tree is
     // rejected before any device work.
@@ -241,8 +264,14 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
         return BBG_OK;
     }
 
-    // Tree: given (the reference-built one, flattened) or built here.
-    if (bvh)
+    // Tree: given (the reference-built one, flattened), built on the host, or
+    // (device_build) built on the device after the geometry is uploaded.
+    if (device_build)
+    {
+        a->device_built = true;
+        a->ordered = true;
+    }
+    else if (bvh)
     {
         if (!bvh->nodes || !bvh->slot_prims || bvh->n_nodes <= 0 || bvh->n_slots != g->n_prims)
         {
@@ -261,18 +290,21 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
         BBG_TRY(BuildBvh(aabbs.data(), g->n_prims, a->host_nodes.data(), a->host_slots.data(), &n_nodes));
         a->host_nodes.resize(size_t(n_nodes));
     }
-    a->n_nodes = int32_t(a->host_nodes.size());
-    a->n_slots = int32_t(a->host_slots.size());
-    BBG_TRY(ValidateBvh(a->host_nodes.data(), a->n_nodes, a->n_slots, g->n_prims, a->host_slots.data(),
-                        &a->max_depth));
-    if (a->max_depth > kStackCapacity)
+    if (!device_build)
     {
-        return Fail(BBG_ERR_STACK_OVERFLOW, "tree depth %d exceeds the traversal stack (%d)", a->max_depth,
-                    kStackCapacity);
+        a->n_nodes = int32_t(a->host_nodes.size());
+        a->n_slots = int32_t(a->host_slots.size());
+        BBG_TRY(ValidateBvh(a->host_nodes.data(), a->n_nodes, a->n_slots, g->n_prims, a->host_slots.data(),
+                            &a->max_depth));
+        if (a->max_depth > kStackCapacity)
+        {
+            return Fail(BBG_ERR_STACK_OVERFLOW, "tree depth %d exceeds the traversal stack (%d)", a->max_depth,
+                        kStackCapacity);
+        }
+        const bbg_bvh_node& root = a->host_nodes[0];
+        std::memcpy(a->bounds, root.bmin, 3 * sizeof(float));
+        std::memcpy(a->bounds + 3, root.bmax, 3 * sizeof(float));
     }
-    const bbg_bvh_node& root = a->host_nodes[0];
-    std::memcpy(a->bounds, root.bmin, 3 * sizeof(float));
-    std::memcpy(a->bounds + 3, root.bmax, 3 * sizeof(float));
 
     BBG_TRY(CheckDevice());
     BBG_CUDA(cudaSetDevice(0));
@@ -281,6 +313,16 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
     {
         BBG_CUDA(cudaStreamCreateWithFlags(&a->copy_stream[s], cudaStreamNonBlocking));
         BBG_CUDA(cudaEventCreateWithFlags(&a->stage_done[s], cudaEventDisableTiming));
+    }
+
+    if (device_build)
+    {
+        BBG_TRY(UploadShading(a, g));
+        BBG_TRY(BuildLbvh(a, g));
+        BBG_TRY(a->counters.alloc(2));
+        BBG_TRY(a->work.alloc(1));
+        BBG_CUDA(cudaStreamSynchronize(a->stream));
+        return BBG_OK;
     }
 
     // Slot records in leaf order.
@@ -351,24 +393,7 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a)
     BBG_TRY(a->nodes.upload(reinterpret_cast<const float4*>(a->host_nodes.data()), 2 * size_t(a->n_nodes), a->stream));
     BBG_TRY(a->slots.upload(slot_rec.data(), slot_rec.size(), a->stream));
 
-    // Shading data.
-    BBG_TRY(a->prim_shape.upload(a->host_prim_shape.data(), a->host_prim_shape.size(), a->stream));
-    BBG_TRY(a->tri_indices.upload(g->tri_indices, 3 * size_t(g->n_triangles), a->stream));
-    BBG_TRY(a->positions.upload(g->positions, 3 * size_t(g->n_vertices), a->stream));
-    if (g->n_spheres)
-    {
-        BBG_TRY(a->spheres.upload(g->spheres, size_t(g->n_spheres), a->stream));
-    }
-    a->has_shading = g->n_triangles == 0 || (g->normals && g->tangents);
-    if (g->normals && g->tangents)
-    {
-        BBG_TRY(a->normals.upload(g->normals, 3 * size_t(g->n_vertices), a->stream));
-        BBG_TRY(a->tangents.upload(g->tangents, 3 * size_t(g->n_vertices), a->stream));
-        if (g->uvs)
-        {
-            BBG_TRY(a->uvs.upload(g->uvs, 2 * size_t(g->n_vertices), a->stream));
-        }
-    }
+    BBG_TRY(UploadShading(a, g));
     BBG_TRY(a->counters.alloc(2));
     BBG_TRY(a->work.alloc(1));
     BBG_CUDA(cudaStreamSynchronize(a->stream));
@@ -455,6 +480,24 @@ bbg_status Query(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out, bbg_me
 
 extern "C" {
 
+bbg_status bbg_accel_create_device_build(const bbg_geometry* geometry, bbg_accel** out)
+{
+    if (!out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_create_device_build: out is NULL");
+    }
+    *out = nullptr;
+    auto* a = new bbg_accel;
+    bbg_status s = CreateAccel(geometry, nullptr, a, true);
+    if (s != BBG_OK)
+    {
+        bbg_accel_destroy(a);
+        return s;
+    }
+    *out = a;
+    return BBG_OK;
+}
+
 bbg_status bbg_accel_create(const bbg_geometry* geometry, const bbg_bvh* bvh, bbg_accel** out)
 {
     if (!out)
@@ -517,6 +560,10 @@ bbg_status bbg_accel_export(const bbg_accel* a, bbg_bvh_node* nodes_out, int32_t
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_export: null accel");
     }
+    if (a->device_built)
+    {
+        return Fail(BBG_ERR_UNSUPPORTED, "bbg_accel_export: the tree was built on the device (no reference layout)");
+    }
     if (n_nodes_out) *n_nodes_out = a->n_nodes;
     if (n_slots_out) *n_slots_out = a->n_slots;
     if (nodes_out) std::memcpy(nodes_out, a->host_nodes.data(), a->host_nodes.size() * sizeof(bbg_bvh_node));
@@ -541,6 +588,10 @@ bbg_status bbg_accel_set_traversal(bbg_accel* a, int32_t mode)
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_set_traversal: bad argument");
     }
+    if (a->device_built && mode != BBG_TRAVERSAL_ORDERED)
+    {
+        return Fail(BBG_ERR_UNSUPPORTED, "a tree built on the device has only the child-box layout");
+    }
     a->ordered = mode == BBG_TRAVERSAL_ORDERED;
     return BBG_OK;
 }
@@ -550,6 +601,10 @@ bbg_status bbg_accel_set_counting(bbg_accel* a, int32_t enable)
     if (!a)
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_set_counting: null accel");
+    }
+    if (a->device_built && enable)
+    {
+        return Fail(BBG_ERR_UNSUPPORTED, "counting needs the reference-order traversal (not for device-built trees)");
     }
     a->counting = enable != 0;
     return BBG_OK;

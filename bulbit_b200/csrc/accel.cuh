@@ -22,6 +22,7 @@ struct bbg_accel
     bbg::DevBuf<int2> leaves;  // (first slot, count) per leaf
     int32_t root = 0;
     bool ordered = true;
+    bool device_built = false; // tree built on the device (child-box layout only)
 
     // Shading data (the reference Mesh arrays and shapes).
     bbg::DevBuf<int2> prim_shape;     // (kind, index) per primitive
@@ -61,4 +62,7 @@ namespace bbg
 // Launches the batched traversal kernel on device-resident rays.
 bbg_status LaunchIntersect(bbg_accel* a, const float4* rays, int64_t n, float4* hits, cudaStream_t stream);
 bbg_status LaunchIntersectAny(bbg_accel* a, const float4* rays, int64_t n, uint8_t* occluded, cudaStream_t stream);
+// Builds a linear BVH on the device (lbvh.cu) over the uploaded geometry:
+// fills slots, the child-box layout, leaves, root, bounds and depth.
+bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g);
 } // namespace bbg

@@ -82,10 +82,14 @@ NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("offset", "<i4")
 class GpuAccel:
     """The GPU accel beside the reference BVH (bbg_accel_*)."""
 
-    def __init__(self, scene, bvh=None):
+    def __init__(self, scene, bvh=None, device_build=False):
         self.scene = scene
         self._g = scene.geometry()
         self.h = C.c_void_p()
+        if device_build:
+            check(get_lib().bbg_accel_create_device_build(C.byref(self._g), C.byref(self.h)),
+                  "bbg_accel_create_device_build")
+            return
         bvh_arg = None
         if bvh is not None:
             nodes, slots = bvh

@@ -158,3 +158,62 @@ def test_closest_and_any_agree_at_full_size():
     t = hits[:, 1]
     expect = (prim >= 0) & (t <= ra[:, 7])
     assert torch.equal(expect.to(torch.uint8), occ)
+
+
+def classify_against_brute_force(rs, rays, prim, t, ref_prim, ref_t):
+    """Mismatches between two trees' closest hits, classified with a brute-force
+    test of every primitive: near-ties, and rays one tree would let through (its
+    slab test, without a robustness margin as in the reference, missing a box
+    that contains the true closest hit). Returns (ties, leaks_ref, leaks_dev,
+    unexplained)."""
+    ties = leaks_ref = leaks_dev = 0
+    unexplained = []
+    for i in np.nonzero(prim != ref_prim)[0]:
+        prims, ts = rs.intersect_all(rays[i])
+        if len(ts) >= 2 and (ts[1] - ts[0]) <= NEAR_TIE_REL * abs(ts[0]):
+            ties += 1
+        elif len(ts) and prim[i] == prims[0] and t[i] == ts[0]:
+            leaks_ref += 1
+        elif len(ts) and ref_prim[i] == prims[0] and ref_t[i] == ts[0]:
+            leaks_dev += 1
+        else:
+            unexplained.append((int(i), int(prim[i]), int(ref_prim[i]), float(t[i]), float(ref_t[i])))
+    return ties, leaks_ref, leaks_dev, unexplained
+
+
+def test_device_built_tree_parity(oracle):
+    """The linear BVH built on the device: closest hits agree with the
+    reference BVH except near-ties (or rays that one tree's boxes would let
+    through, counted separately: none were seen), any-hit agrees on the soup;
+    the tree has no reference layout (reference traversal, counting and export
+    are refused)."""
+    soup = scenes.triangle_soup(200_000, seed=1)
+    closest, anyq = scenes.soup_rays(1 << 19, seed=2)
+    cornell = scenes.cornell_icosphere(levels=6, width=8, height=8)
+    rng = np.random.default_rng(4)
+    n = 200_000
+    crays = np.zeros((n, 8), np.float32)
+    crays[:, :3] = rng.uniform(-0.95, 0.95, (n, 3))
+    d = rng.normal(size=(n, 3))
+    crays[:, 3:6] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    crays[:, 6], crays[:, 7] = 1e-4, np.inf
+    for scene, rays, anyq in ((soup, closest, anyq), (cornell, crays, None)):
+        rs = oracle.RefScene(scene)
+        acc = lib.GpuAccel(scene, device_build=True)
+        ref_prim, ref_t, _ = rs.intersect(rays)
+        prim, t, _, _ = acc.intersect(rays)
+        ties, leaks_ref, leaks_dev, unexplained = classify_against_brute_force(rs, rays, prim, t, ref_prim, ref_t)
+        print(f"device-built tree, {scene.name}: {len(rays)} rays, mismatches: {ties} near-ties, "
+              f"{leaks_ref} through the reference tree, {leaks_dev} through the device tree")
+        assert not unexplained, unexplained[:5]
+        assert leaks_ref + leaks_dev <= 1e-3 * len(rays)
+        same = (prim == ref_prim) & (ref_prim >= 0)
+        assert np.array_equal(t[same].view(np.uint32), ref_t[same].view(np.uint32))
+        if anyq is not None:
+            ref_occ, _ = rs.intersect_any(anyq)
+            assert np.array_equal(acc.intersect_any(anyq), ref_occ)
+    for call in (lambda: acc.set_traversal(abi.BBG_TRAVERSAL_REFERENCE), lambda: acc.set_counting(True),
+                 lambda: acc.export()):
+        with pytest.raises(lib.BbgError) as e:
+            call()
+        assert e.value.status == abi.BBG_ERR_UNSUPPORTED
