@@ -177,10 +177,6 @@ bbg_material TranslateMaterial(const Material* m)
     else if (m->Is<DielectricMaterial>())
     {
         const DielectricMaterial* d = m->Cast<DielectricMaterial>();
-        if (d->*Get(DielEc{}))
-        {
-            Unsupported("DielectricMaterial with energy_compensation = true");
-        }
         if (d->*Get(DielNormal{}))
         {
             Unsupported("DielectricMaterial with a normal texture");
@@ -192,6 +188,7 @@ bbg_material TranslateMaterial(const Material* m)
         PutSpec(out.reflectance, refl ? ConstSpectrum(refl, "DielectricMaterial reflectance") : Spectrum(1));
         out.roughness[0] = ConstScalar(d->*Get(DielU{}), "DielectricMaterial roughness");
         out.roughness[1] = ConstScalar(d->*Get(DielV{}), "DielectricMaterial roughness");
+        out.energy_compensation = (d->*Get(DielEc{})) ? 1 : 0;
     }
     else if (m->Is<MetallicRoughnessMaterial>())
     {

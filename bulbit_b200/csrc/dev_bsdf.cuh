@@ -1,5 +1,5 @@
-// BxDFs on the device: Lambertian, Conductor, Dielectric and
-// Metallic-Roughness with the Trowbridge-Reitz distribution, restated from
+// BxDFs on the device: Lambertian, Conductor, Dielectric (each of the last
+// two with its energy-compensated form) and Metallic-Roughness with the Trowbridge-Reitz distribution, restated from
 // src/bxdf/{lambertian,conductor,dielectric,metallic_roughness}_bxdf.cpp,
 // include/bulbit/microfacet.h and include/bulbit/scattering.h with the same
 // operation order.
@@ -46,6 +46,69 @@ __device__ __forceinline__ float TableBilinear(const float* img, int w, int h, f
     float v00 = img[i0 + j0 * w], v10 = img[i1 + j0 * w];
     float v01 = img[i0 + j1 * w], v11 = img[i1 + j1 * w];
     return (1 - fu) * (1 - fv) * v00 + (1 - fu) * fv * v01 + fu * (1 - fv) * v10 + fu * fv * v11;
+}
+
+// Energy tables of the rough dielectric in the reference's layout
+// (DielectricMultiScatteringBxDF::PrepareReflectanceTexture,
+// src/bxdf/microfacet.cpp:168-237): E and E_inv 32 x 32 x 32 (x: f0 =
+// MapIORtoF0(eta), y: cos theta, z: alpha; E for eta >= 1, E_inv for the
+// inverse interface), E_avg and E_inv_avg 32 x 32 (x: f0, y: alpha). Filled on
+// the device by DielectricEnergyTablesKernel (render.cu).
+static __device__ float g_dms_e[kEnergyTableSize * kEnergyTableSize * kEnergyTableSize];
+static __device__ float g_dms_e_inv[kEnergyTableSize * kEnergyTableSize * kEnergyTableSize];
+static __device__ float g_dms_e_avg[kEnergyTableSize * kEnergyTableSize];
+static __device__ float g_dms_e_inv_avg[kEnergyTableSize * kEnergyTableSize];
+
+// ImageTexture3D<Float>::Evaluate: trilinear, texel coordinates clamped,
+// lerped along x, then y, then z (include/bulbit/textures3d.h:33-88).
+__device__ __forceinline__ float TableTrilinear(const float* img, int n, float u, float v, float w)
+{
+    float x = u * float(n) - 0.5f;
+    float y = v * float(n) - 0.5f;
+    float z = w * float(n) - 0.5f;
+    float fx = floorf(x), fy = floorf(y), fz = floorf(z);
+    int i0 = int(fx), i1 = i0 + 1;
+    int j0 = int(fy), j1 = j0 + 1;
+    int k0 = int(fz), k1 = k0 + 1;
+    i0 = min(max(i0, 0), n - 1);
+    j0 = min(max(j0, 0), n - 1);
+    k0 = min(max(k0, 0), n - 1);
+    i1 = min(max(i1, 0), n - 1);
+    j1 = min(max(j1, 0), n - 1);
+    k1 = min(max(k1, 0), n - 1);
+    float fu = x - fx;
+    float fv = y - fy;
+    float fw = z - fz;
+    auto at = [&](int i, int j, int k) { return img[(k * n + j) * n + i]; };
+    float v00 = (1 - fu) * at(i0, j0, k0) + fu * at(i1, j0, k0);
+    float v01 = (1 - fu) * at(i0, j0, k1) + fu * at(i1, j0, k1);
+    float v10 = (1 - fu) * at(i0, j1, k0) + fu * at(i1, j1, k0);
+    float v11 = (1 - fu) * at(i0, j1, k1) + fu * at(i1, j1, k1);
+    float v0 = (1 - fv) * v00 + fv * v10;
+    float v1 = (1 - fv) * v01 + fv * v11;
+    return (1 - fw) * v0 + fw * v1;
+}
+
+// MapF0toIOR / MapIORtoF0 (include/bulbit/scattering.h:189-208).
+__device__ __forceinline__ float MapF0toIOR(float f0)
+{
+    float sqrt_f0 = sqrtf(Sqr(Sqr(f0)));
+    return (1 + sqrt_f0) / (1 - sqrt_f0);
+}
+__device__ __forceinline__ float MapIORtoF0(float ior) { return sqrtf((ior - 1) / (ior + 1)); }
+
+// FresnelDielectricAverage (include/bulbit/scattering.h:154-172): the
+// polynomial / rational fits of the hemispherical average of the dielectric
+// Fresnel term from the Imageworks 2017 course notes (p. 23).
+__device__ __forceinline__ float FresnelDielectricAverage(float eta_p)
+{
+    if (eta_p < 1)
+    {
+        const float eta2 = eta_p * eta_p;
+        const float eta3 = eta_p * eta2;
+        return 0.997118f + 0.1014f * eta_p - 0.965241f * eta2 - 0.130607f * eta3;
+    }
+    return (eta_p - 1) / (4.08567f + 1.00071f * eta_p);
 }
 
 struct TrowbridgeReitz
@@ -234,7 +297,7 @@ struct BSDF
     const float* ck;
     TrowbridgeReitz mf;
     float metallic;
-    int32_t ms;      // conductor: energy compensation (multiple-scattering lobe)
+    int32_t ms;      // conductor / dielectric: energy compensation (multiple-scattering lobe)
 
     // ---- Lambertian (src/bxdf/lambertian_bxdf.cpp)
     __device__ Spec LambertF(V3 wo, V3 wi) const
@@ -425,6 +488,10 @@ struct BSDF
         float dwm_dwi = AbsDot(wi, wm) / Sqr(Dot(wi, wm) + Dot(wo, wm) / eta_p);
         return mf.PDF(wo, wm) * dwm_dwi * pt / (pr + pt);
     }
+    // kToLight: radiance transport (the integrator); false: importance
+    // transport (TransportDirection::ToCamera, the energy-table integrals),
+    // which leaves out the 1 / eta'^2 solid-angle factor.
+    template <bool kToLight = true>
     __device__ bool DielectricSample(BSDFSample* s, V3 wo, float u0, P2 u12) const
     {
         if (eta == 1 || mf.EffectivelySmooth())
@@ -445,7 +512,7 @@ struct BSDF
                 float eta_p;
                 if (!Refract(&wi, wo, V3{ 0, 0, 1 }, eta, &eta_p)) return false;
                 float ft = T / AbsCosTheta(wi);
-                ft /= Sqr(eta_p);
+                if (kToLight) ft /= Sqr(eta_p);
                 *s = BSDFSample{ r * ft, wi, pt / (pr + pt), kFlagSpecular | kFlagTransmission, eta_p };
             }
             return true;
@@ -473,9 +540,225 @@ struct BSDF
             float dwm_dwi = AbsDot(wi, wm) / denom;
             float pdf = mf.PDF(wo, wm) * dwm_dwi * pt / (pr + pt);
             float ft = T * mf.D(wm) * mf.G(wo, wi) * fabsf(Dot(wi, wm) * Dot(wo, wm) / (wi.z * wo.z * denom));
-            ft /= Sqr(eta_p);
+            if (kToLight) ft /= Sqr(eta_p);
             *s = BSDFSample{ r * ft, wi, pdf, kFlagGlossy | kFlagTransmission, eta_p };
         }
+        return true;
+    }
+
+    // ---- Energy-compensated dielectric (src/bxdf/dielectric_multi_scattering_bxdf.cpp,
+    // include/bulbit/bxdfs.h:145-240), radiance transport: the rough
+    // dielectric plus a diffuse-like multiple-scattering lobe on each side,
+    // reflection and transmission split by the energy-conserving ratio.
+    __device__ float DmsE(V3 w, float e) const
+    {
+        if (e >= 1)
+        {
+            return TableTrilinear(g_dms_e, kEnergyTableSize, MapIORtoF0(e), fabsf(w.z), mf.MeanAlpha());
+        }
+        return TableTrilinear(g_dms_e_inv, kEnergyTableSize, MapIORtoF0(1 / e), fabsf(w.z), mf.MeanAlpha());
+    }
+    __device__ float DmsEAvg(float e) const
+    {
+        if (e >= 1)
+        {
+            return TableBilinear(g_dms_e_avg, kEnergyTableSize, kEnergyTableSize, MapIORtoF0(e), mf.MeanAlpha());
+        }
+        return TableBilinear(g_dms_e_inv_avg, kEnergyTableSize, kEnergyTableSize, MapIORtoF0(1 / e),
+                             mf.MeanAlpha());
+    }
+    // ComputeScatteringRatio (include/bulbit/bxdfs.h:222-242): the share of
+    // the multiple-scattering energy leaving on wo's side.
+    __device__ float DmsRatio(float eta_o) const
+    {
+        float eta_i = eta >= 1 ? eta : 1 / eta;
+        float eta_t = 1 / eta_i;
+        float a = (1 - FresnelDielectricAverage(eta_i)) / (1 - DmsEAvg(eta_t));
+        float b = Sqr(eta_i) * (1 - FresnelDielectricAverage(eta_t)) / (1 - DmsEAvg(eta_i));
+        float x = 1 / (a / b + 1);
+        if (eta_o >= 1)
+        {
+            return 1 - x * (1 - FresnelDielectricAverage(eta_o));
+        }
+        return 1 - (1 - x) * (1 - FresnelDielectricAverage(eta_o));
+    }
+    __device__ float DmsReflectLobe(V3 wo, V3 wi, float eta_o, float ratio) const
+    {
+        return ratio * (1 - DmsE(wi, eta_o)) * (1 - DmsE(wo, eta_o)) / fmaxf(1e-4f, kPi * (1 - DmsEAvg(eta_o)));
+    }
+    __device__ float DmsTransmitLobe(V3 wo, V3 wi, float eta_o, float eta_i, float ratio) const
+    {
+        return (1 - ratio) * (1 - DmsE(wi, eta_i)) * (1 - DmsE(wo, eta_o)) /
+               fmaxf(1e-4f, kPi * (1 - DmsEAvg(eta_i)));
+    }
+    // Lerp(pdf_ms, pdf_ss, E_o) (include/bulbit/math.h:87-90).
+    __device__ static float DmsLerp(float pdf_ms, float pdf_ss, float e_o) { return pdf_ms * (1 - e_o) + pdf_ss * e_o; }
+
+    __device__ Spec DielectricMsF(V3 wo, V3 wi) const
+    {
+        if (eta == 1 || mf.EffectivelySmooth()) return spec(0);
+        float cos_theta_o = wo.z;
+        float cos_theta_i = wi.z;
+        float eta_p = 1;
+        bool reflect = cos_theta_i * cos_theta_o > 0;
+        if (!reflect) eta_p = cos_theta_o > 0 ? eta : (1 / eta);
+        float eta_o = cos_theta_o > 0 ? eta : 1 / eta;
+        float eta_i = cos_theta_o > 0 ? 1 / eta : eta;
+        V3 wm = wi * eta_p + wo;
+        if (cos_theta_i == 0 || cos_theta_o == 0 || Length2(wm) == 0) return spec(0);
+        NormalizeInPlace(wm);
+        if (DotZ(wm) < 0) wm = -wm;
+        if (Dot(wm, wi) * cos_theta_i < 0 || Dot(wm, wo) * cos_theta_o < 0) return spec(0);
+        float ratio = DmsRatio(eta_o);
+        float F = FresnelDielectric(Dot(wo, wm), eta);
+        if (reflect)
+        {
+            float fr_ss = F * mf.D(wm) * mf.G(wo, wi) / (4 * cos_theta_i * cos_theta_o);
+            return spec(fr_ss + DmsReflectLobe(wo, wi, eta_o, ratio));
+        }
+        float denom = Sqr(Dot(wi, wm) + Dot(wo, wm) / eta_p);
+        float ft_ss =
+            (1 - F) * mf.D(wm) * mf.G(wo, wi) * fabsf(Dot(wi, wm) * Dot(wo, wm) / (cos_theta_i * cos_theta_o * denom));
+        float ft_ms = DmsTransmitLobe(wo, wi, eta_o, eta_i, ratio);
+        ft_ss /= Sqr(eta_p);
+        return r * (ft_ss + ft_ms);
+    }
+    __device__ float DielectricMsPDF(V3 wo, V3 wi) const
+    {
+        if (eta == 1 || mf.EffectivelySmooth()) return 0;
+        float cos_theta_o = wo.z;
+        float cos_theta_i = wi.z;
+        float eta_p = 1;
+        bool reflect = cos_theta_i * cos_theta_o > 0;
+        if (!reflect) eta_p = cos_theta_o > 0 ? eta : (1 / eta);
+        float eta_o = cos_theta_o > 0 ? eta : 1 / eta;
+        V3 wm = wi * eta_p + wo;
+        if (cos_theta_i == 0 || cos_theta_o == 0 || Length2(wm) == 0) return 0;
+        NormalizeInPlace(wm);
+        if (DotZ(wm) < 0) wm = -wm;
+        if (Dot(wm, wi) * cos_theta_i < 0 || Dot(wm, wo) * cos_theta_o < 0) return 0;
+        float ratio = DmsRatio(eta_o);
+        float E_o = Clamp(DmsE(wo, eta_o), 1e-4f, 1 - 1e-4f);
+        float R = FresnelDielectric(Dot(wo, wm), eta);
+        float T = 1 - R;
+        float pr_ss = R, pt_ss = T;
+        float pr_ms = ratio, pt_ms = 1 - ratio;
+        if (pr_ss == 0 && pt_ss == 0 && pr_ms == 0 && pt_ms == 0) return 0;
+        float p_ss_sum = pr_ss + pt_ss;
+        float p_ms_sum = pr_ms + pt_ms;
+        pr_ss /= p_ss_sum;
+        pt_ss /= p_ss_sum;
+        pr_ms /= p_ms_sum;
+        pt_ms /= p_ms_sum;
+        if (reflect)
+        {
+            float pdf_ss = pr_ss * mf.PDF(wo, wm) / (4 * AbsDot(wo, wm));
+            float pdf_ms = pr_ms * (AbsCosTheta(wi) * kInvPi);
+            return DmsLerp(pdf_ms, pdf_ss, E_o);
+        }
+        float dwm_dwi = AbsDot(wi, wm) / Sqr(Dot(wi, wm) + Dot(wo, wm) / eta_p);
+        float pdf_ss = pt_ss * mf.PDF(wo, wm) * dwm_dwi;
+        float pdf_ms = pt_ms * (AbsCosTheta(wi) * kInvPi);
+        return DmsLerp(pdf_ms, pdf_ss, E_o);
+    }
+    __device__ bool DielectricMsSample(BSDFSample* s, V3 wo, float u0, P2 u12) const
+    {
+        if (eta == 1 || mf.EffectivelySmooth())
+        {
+            // The perfect specular branch is DielectricBxDF's.
+            return DielectricSample(s, wo, u0, u12);
+        }
+        float eta_o = wo.z > 0 ? eta : 1 / eta;
+        float eta_i = wo.z > 0 ? 1 / eta : eta;
+        float ratio = DmsRatio(eta_o);
+        float E_o = Clamp(DmsE(wo, eta_o), 1e-4f, 1 - 1e-4f);
+        if (u0 < E_o)
+        {
+            // single scattering: a visible microfacet normal, then reflect or refract
+            V3 wm = mf.SampleWm(wo, u12);
+            NormalizeInPlace(wm);
+            if (DotZ(wm) < 0) wm = -wm;
+            float R = FresnelDielectric(Dot(wo, wm), eta);
+            float T = 1 - R;
+            float pr_ss = R, pt_ss = T;
+            float pr_ms = ratio, pt_ms = 1 - ratio;
+            if (pr_ss == 0 && pt_ss == 0) return false;
+            float p_ss_sum = pr_ss + pt_ss;
+            float p_ms_sum = pr_ms + pt_ms;
+            pr_ss /= p_ss_sum;
+            pt_ss /= p_ss_sum;
+            pr_ms /= p_ms_sum;
+            pt_ms /= p_ms_sum;
+            u0 /= E_o;
+            if (u0 < pr_ss)
+            {
+                V3 wi = Reflect(wo, wm);
+                if (!SameHemisphere(wo, wi)) return false;
+                float pdf_ss = pr_ss * mf.PDF(wo, wm) / (4 * AbsDot(wo, wm));
+                float pdf_ms = pr_ms * (AbsCosTheta(wi) * kInvPi);
+                float fr_ss = R * mf.D(wm) * mf.G(wo, wi) / (4 * wi.z * wo.z);
+                float fr_ms = DmsReflectLobe(wo, wi, eta_o, ratio);
+                *s = BSDFSample{ spec(fr_ss + fr_ms), wi, DmsLerp(pdf_ms, pdf_ss, E_o), kFlagGlossy | kFlagReflection, 1 };
+                return true;
+            }
+            V3 wi{ 0, 0, 0 };
+            float unused;
+            bool tir = !Refract(&wi, wo, wm, eta, &unused);
+            if (SameHemisphere(wo, wi) || wi.z == 0 || tir) return false;
+            float eta_p = wo.z > 0 ? eta : (1 / eta);
+            float denom = Sqr(Dot(wi, wm) + Dot(wo, wm) / eta_p);
+            float dwm_dwi = AbsDot(wi, wm) / denom;
+            float pdf_ss = pt_ss * mf.PDF(wo, wm) * dwm_dwi;
+            float pdf_ms = pt_ms * (AbsCosTheta(wi) * kInvPi);
+            float ft_ss =
+                T * mf.D(wm) * mf.G(wo, wi) * fabsf(Dot(wi, wm) * Dot(wo, wm) / (wi.z * wo.z * denom));
+            float ft_ms = DmsTransmitLobe(wo, wi, eta_o, eta_i, ratio);
+            ft_ss /= Sqr(eta_p);
+            *s = BSDFSample{ r * (ft_ss + ft_ms), wi, DmsLerp(pdf_ms, pdf_ss, E_o), kFlagGlossy | kFlagTransmission,
+                             eta_p };
+            return true;
+        }
+        // multiple scattering: a cosine-distributed direction on one side
+        float pr_ms = ratio, pt_ms = 1 - ratio;
+        if (pr_ms == 0 && pt_ms == 0) return false;
+        float p_ms_sum = pr_ms + pt_ms;
+        pr_ms /= p_ms_sum;
+        pt_ms /= p_ms_sum;
+        u0 = (u0 - E_o) / (1 - E_o);
+        V3 wi = SampleCosineHemisphere(u12);
+        if (u0 < pr_ms)
+        {
+            if (wo.z < 0) wi = -wi;
+            V3 wm = Normalize(wi + wo);
+            float R = FresnelDielectric(Dot(wo, wm), eta);
+            float pr_ss = R, pt_ss = 1 - R;
+            float p_ss_sum = pr_ss + pt_ss;
+            pr_ss /= p_ss_sum;
+            pt_ss /= p_ss_sum;
+            float pdf_ss = pr_ss * mf.PDF(wo, wm) / (4 * AbsDot(wo, wm));
+            float pdf_ms = pr_ms * (AbsCosTheta(wi) * kInvPi);
+            float fr_ss = R * mf.D(wm) * mf.G(wo, wi) / (4 * wi.z * wo.z);
+            float fr_ms = DmsReflectLobe(wo, wi, eta_o, ratio);
+            *s = BSDFSample{ spec(fr_ss + fr_ms), wi, DmsLerp(pdf_ms, pdf_ss, E_o), kFlagDiffuse | kFlagReflection, 1 };
+            return true;
+        }
+        if (wo.z > 0) wi = -wi;
+        V3 wm = Normalize(wi * eta_o + wo);
+        if (DotZ(wm) < 0) wm = -wm;
+        float R = FresnelDielectric(Dot(wo, wm), eta);
+        float T = 1 - R;
+        float pr_ss = R, pt_ss = 1 - R;
+        float p_ss_sum = pr_ss + pt_ss;
+        pr_ss /= p_ss_sum;
+        pt_ss /= p_ss_sum;
+        float denom = Sqr(Dot(wi, wm) + Dot(wo, wm) / eta_o);
+        float dwm_dwi = AbsDot(wi, wm) / denom;
+        float pdf_ss = pt_ss * mf.PDF(wo, wm) * dwm_dwi;
+        float pdf_ms = pt_ms * (AbsCosTheta(wi) * kInvPi);
+        float ft_ss = T * mf.D(wm) * mf.G(wo, wi) * fabsf(Dot(wi, wm) * Dot(wo, wm) / (wi.z * wo.z * denom));
+        float ft_ms = DmsTransmitLobe(wo, wi, eta_o, eta_i, ratio);
+        ft_ss /= Sqr(eta_o);
+        *s = BSDFSample{ r * (ft_ss + ft_ms), wi, DmsLerp(pdf_ms, pdf_ss, E_o), kFlagDiffuse | kFlagTransmission, eta_o };
         return true;
     }
 
@@ -561,7 +844,7 @@ struct BSDF
         {
         case BBG_MAT_DIFFUSE: return LambertF(wo, wi);
         case BBG_MAT_CONDUCTOR: return ms ? ConductorMsF(wo, wi) : ConductorF(wo, wi);
-        case BBG_MAT_DIELECTRIC: return DielectricF(wo, wi);
+        case BBG_MAT_DIELECTRIC: return ms ? DielectricMsF(wo, wi) : DielectricF(wo, wi);
         default: return MRF(wo, wi);
         }
     }
@@ -574,7 +857,7 @@ struct BSDF
         {
         case BBG_MAT_DIFFUSE: return LambertPDF(wo, wi);
         case BBG_MAT_CONDUCTOR: return ms ? ConductorMsPDF(wo, wi) : ConductorPDF(wo, wi);
-        case BBG_MAT_DIELECTRIC: return DielectricPDF(wo, wi);
+        case BBG_MAT_DIELECTRIC: return ms ? DielectricMsPDF(wo, wi) : DielectricPDF(wo, wi);
         default: return MRPDF(wo, wi);
         }
     }
@@ -587,7 +870,7 @@ struct BSDF
         {
         case BBG_MAT_DIFFUSE: ok = LambertSample(s, wo, u12); break;
         case BBG_MAT_CONDUCTOR: ok = ms ? ConductorMsSample(s, wo, u0, u12) : ConductorSample(s, wo, u12); break;
-        case BBG_MAT_DIELECTRIC: ok = DielectricSample(s, wo, u0, u12); break;
+        case BBG_MAT_DIELECTRIC: ok = ms ? DielectricMsSample(s, wo, u0, u12) : DielectricSample(s, wo, u0, u12); break;
         default: ok = MRSample(s, wo, u0, u12); break;
         }
         if (!ok) return false;

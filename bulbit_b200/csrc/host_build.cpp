@@ -582,13 +582,12 @@ bbg_status MakeMaterial(const bbg_material& m, MaterialDev* out)
     }
     case BBG_MAT_DIELECTRIC:
     {
-        if (m.energy_compensation)
-        {
-            return Fail(BBG_ERR_UNSUPPORTED, "energy-compensated dielectric materials are not supported");
-        }
         // DielectricMaterial::GetBSDF (src/material/dielectric_material.cpp:28-52);
-        // DielectricBxDF stores Sqrt(r) (include/bulbit/bxdfs.h:85-90). The
-        // relative eta and the flags depend on the hit side and are set per hit.
+        // DielectricBxDF and DielectricMultiScatteringBxDF store Sqrt(r)
+        // (include/bulbit/bxdfs.h:85-90, 148-153). The relative eta and the
+        // flags depend on the hit side and are set per hit; the flags are the
+        // same with and without energy compensation.
+        out->ms = m.energy_compensation ? 1 : 0;
         out->eta[0] = m.eta[0];
         for (int c = 0; c < 3; ++c)
         {

@@ -1415,9 +1415,9 @@ __global__ void __launch_bounds__(kBlock) FilmKernel(Scenes sc, WaveDev w)
 constexpr int kEnergySamples = 1024; // 32 x 32 strata, PrepareReflectanceTextures(32, 1024)
 
 // The stratified samples of PrepareReflectanceTextures (src/bxdf/microfacet.cpp:239-275):
-// RNG(3); per sample a permuted 1-D stratum (u0, drawn but unused by GGX) and
-// a permuted 2-D stratum, in that draw order. One thread.
-__global__ void GgxEnergySamplesKernel(P2* u12)
+// RNG(3); per sample a permuted 1-D stratum u0 and a permuted 2-D stratum
+// u12, in that draw order. One thread.
+__global__ void EnergySamplesKernel(float* u0s, P2* u12)
 {
     uint64_t st = 0; // RNG(3): Seed(initstate = 3, initseq = 1)
     PcgNext(st);
@@ -1426,8 +1426,7 @@ __global__ void GgxEnergySamplesKernel(P2* u12)
     for (int i = 0; i < kEnergySamples; ++i)
     {
         int32_t s0 = int32_t(PermutationElement(uint32_t(i), kEnergySamples, 1));
-        float u0 = (float(s0) + Next1D(st)) / float(kEnergySamples);
-        (void)u0;
+        u0s[i] = (float(s0) + Next1D(st)) / float(kEnergySamples);
         int32_t s1 = int32_t(PermutationElement(uint32_t(i), kEnergySamples, 2));
         int32_t x = s1 % 32, y = s1 / 32;
         float a = Next1D(st);
@@ -1482,6 +1481,72 @@ __global__ void GgxEnergyAverageKernel()
         }
         g_ggx_e_avg[j] = 2 * r_sum;
     }
+}
+
+// Energy tables of the rough dielectric (src/bxdf/microfacet.cpp:168-237):
+// entry (k, i, j) of E (E_inv) is rho(wo) of DielectricBxDF(ior_k (1 / ior_k),
+// GGX(alpha_j)) under importance transport (TransportDirection::ToCamera), the
+// samples summed in order (src/bxdf/bxdf.cpp:8-20), then the Spectrum's
+// Average of the three equal channels. One thread per entry of both tables.
+__global__ void DielectricEnergyTablesKernel(const float* u0s, const P2* u12)
+{
+    constexpr int n = kEnergyTableSize;
+    constexpr int n3 = n * n * n;
+    const float d = 1.0f / n;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= 2 * n3)
+    {
+        return;
+    }
+    bool inv = e >= n3;
+    int c = inv ? e - n3 : e;
+    int k = c % n, i = (c / n) % n, j = c / (n * n);
+    float ior = MapF0toIOR(d / 2 + d * float(k));
+    float a = d / 2 + d * float(j);
+    float cos_theta = d / 2 + d * float(i);
+    float sin_theta = sqrtf(1 - Sqr(cos_theta));
+    V3 wo{ sin_theta, 0, cos_theta };
+    BSDF b;
+    b.type = BBG_MAT_DIELECTRIC;
+    b.eta = inv ? 1 / ior : ior;
+    b.mf = TrowbridgeReitz{ a, a };
+    b.r = spec(1);
+    b.ms = 0;
+    float r = 0;
+    for (int q = 0; q < kEnergySamples; ++q)
+    {
+        BSDFSample smp;
+        if (b.DielectricSample<false>(&smp, wo, u0s[q], u12[q]))
+        {
+            r += smp.f.r * AbsCosTheta(smp.wi) / smp.pdf;
+        }
+    }
+    r = r / float(kEnergySamples);
+    (inv ? g_dms_e_inv : g_dms_e)[c] = (r + r + r) / 3;
+}
+
+// E_avg(f0, alpha) = 2 sum_i E(f0, cos theta_i, alpha) cos theta_i d, both
+// interfaces. One thread per (k, j).
+__global__ void DielectricEnergyAverageKernel()
+{
+    constexpr int n = kEnergyTableSize;
+    const float d = 1.0f / n;
+    int e = blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n * n)
+    {
+        return;
+    }
+    int k = e % n, j = e / n;
+    float r_sum = 0, r_inv_sum = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        float cos_theta = d / 2 + d * float(i);
+        int c = (j * n + i) * n + k;
+        r_sum += g_dms_e[c] * cos_theta * d;
+        r_inv_sum += g_dms_e_inv[c] * cos_theta * d;
+    }
+    g_dms_e_avg[j * n + k] = 2 * r_sum;
+    g_dms_e_inv_avg[j * n + k] = 2 * r_inv_sum;
 }
 
 // ---------------------------------------------------------------- sampler probe
@@ -2109,9 +2174,10 @@ bbg_status InitWaveEngine(bbg_integrator* I)
     return BBG_OK;
 }
 
-// Fills the GGX energy tables on the current device, once per process and
-// device (they depend on nothing but the reference's fixed sample set).
-bbg_status EnsureGgxTables()
+// Fills the GGX and rough-dielectric energy tables on the current device,
+// once per process and device (they depend on nothing but the reference's
+// fixed sample set).
+bbg_status EnsureEnergyTables()
 {
     static std::mutex mutex;
     static std::vector<bool> done;
@@ -2123,10 +2189,15 @@ bbg_status EnsureGgxTables()
         return BBG_OK;
     }
     DevBuf<P2> u12;
+    DevBuf<float> u0;
     BBG_TRY(u12.alloc(kEnergySamples));
-    GgxEnergySamplesKernel<<<1, 1>>>(u12.p);
+    BBG_TRY(u0.alloc(kEnergySamples));
+    EnergySamplesKernel<<<1, 1>>>(u0.p, u12.p);
     GgxEnergyTablesKernel<<<(kEnergyTableSize * kEnergyTableSize + 127) / 128, 128>>>(u12.p);
     GgxEnergyAverageKernel<<<1, kEnergyTableSize>>>();
+    constexpr int kDmsEntries = 2 * kEnergyTableSize * kEnergyTableSize * kEnergyTableSize;
+    DielectricEnergyTablesKernel<<<(kDmsEntries + 127) / 128, 128>>>(u0.p, u12.p);
+    DielectricEnergyAverageKernel<<<(kEnergyTableSize * kEnergyTableSize + 127) / 128, 128>>>();
     BBG_CUDA(cudaGetLastError());
     BBG_CUDA(cudaDeviceSynchronize());
     if (done.size() <= size_t(dev))
@@ -2150,7 +2221,7 @@ bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim
         BBG_TRY(MakeMaterial(mats[i], &md[i]));
         if (md[i].ms)
         {
-            BBG_TRY(EnsureGgxTables());
+            BBG_TRY(EnsureEnergyTables());
         }
     }
     std::vector<int4> info(size_t(a->n_prims));
@@ -2725,9 +2796,24 @@ bbg_status bbg_ggx_energy_tables(float* e_out, float* e_avg_out)
         return Fail(BBG_ERR_INVALID_ARG, "bbg_ggx_energy_tables: bad argument");
     }
     BBG_TRY(CheckDevice());
-    BBG_TRY(EnsureGgxTables());
+    BBG_TRY(EnsureEnergyTables());
     BBG_CUDA(cudaMemcpyFromSymbol(e_out, g_ggx_e, sizeof(g_ggx_e)));
     BBG_CUDA(cudaMemcpyFromSymbol(e_avg_out, g_ggx_e_avg, sizeof(g_ggx_e_avg)));
+    return BBG_OK;
+}
+
+bbg_status bbg_dielectric_energy_tables(float* e_out, float* e_inv_out, float* e_avg_out, float* e_inv_avg_out)
+{
+    if (!e_out || !e_inv_out || !e_avg_out || !e_inv_avg_out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_dielectric_energy_tables: bad argument");
+    }
+    BBG_TRY(CheckDevice());
+    BBG_TRY(EnsureEnergyTables());
+    BBG_CUDA(cudaMemcpyFromSymbol(e_out, g_dms_e, sizeof(g_dms_e)));
+    BBG_CUDA(cudaMemcpyFromSymbol(e_inv_out, g_dms_e_inv, sizeof(g_dms_e_inv)));
+    BBG_CUDA(cudaMemcpyFromSymbol(e_avg_out, g_dms_e_avg, sizeof(g_dms_e_avg)));
+    BBG_CUDA(cudaMemcpyFromSymbol(e_inv_avg_out, g_dms_e_inv_avg, sizeof(g_dms_e_inv_avg)));
     return BBG_OK;
 }
 

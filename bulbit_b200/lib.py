@@ -405,6 +405,17 @@ def ggx_energy_tables():
     return e.reshape(32, 32), a
 
 
+def dielectric_energy_tables():
+    """bbg_dielectric_energy_tables: (E, E_inv) 32x32x32 indexed [alpha][cos][f0]
+    and (E_avg, E_inv_avg) 32x32 indexed [alpha][f0]."""
+    e = np.zeros(32 ** 3, np.float32)
+    ei = np.zeros(32 ** 3, np.float32)
+    a = np.zeros(32 * 32, np.float32)
+    ai = np.zeros(32 * 32, np.float32)
+    check(get_lib().bbg_dielectric_energy_tables(_p(e), _p(ei), _p(a), _p(ai)), "bbg_dielectric_energy_tables")
+    return e.reshape(32, 32, 32), ei.reshape(32, 32, 32), a.reshape(32, 32), ai.reshape(32, 32)
+
+
 def mixture_sample(outputs, u):
     """Sample the vMF mixtures that network output rows (n, 40) describe, with
     uniforms u (n, 3) -> (unit directions (n, 3), mixture density (n,))."""

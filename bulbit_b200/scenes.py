@@ -171,12 +171,13 @@ def conductor(eta, k, roughness, reflectance=(1.0, 1.0, 1.0), energy_compensatio
     return m
 
 
-def dielectric(ior, roughness=0.0, reflectance=(1.0, 1.0, 1.0)):
+def dielectric(ior, roughness=0.0, reflectance=(1.0, 1.0, 1.0), energy_compensation=False):
     m = abi.Material()
     m.type = abi.BBG_MAT_DIELECTRIC
     m.eta[:] = [ior, ior, ior]
     m.roughness[:] = [roughness, roughness]
     m.reflectance[:] = list(reflectance)
+    m.energy_compensation = 1 if energy_compensation else 0
     return m
 
 

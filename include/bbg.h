@@ -235,8 +235,8 @@ enum
 {
     BBG_MAT_NONE = -1,
     BBG_MAT_DIFFUSE = 0,            /* DiffuseMaterial, roughness 0: LambertianBxDF */
-    BBG_MAT_CONDUCTOR = 1,          /* ConductorMaterial, energy_compensation = false */
-    BBG_MAT_DIELECTRIC = 2,         /* DielectricMaterial, energy_compensation = false */
+    BBG_MAT_CONDUCTOR = 1,          /* ConductorMaterial */
+    BBG_MAT_DIELECTRIC = 2,         /* DielectricMaterial */
     BBG_MAT_METALLIC_ROUGHNESS = 3  /* MetallicRoughnessMaterial */
 };
 
@@ -258,9 +258,10 @@ typedef struct bbg_material
     float k[3];
     float roughness[2];
     float metallic;
-    int32_t energy_compensation; /* conductor: ConductorMaterial's energy_compensation
-                                    (multiple-scattering lobe from the GGX energy
-                                    tables); dielectrics support only 0 */
+    int32_t energy_compensation; /* CONDUCTOR / DIELECTRIC: the material's
+                                    energy_compensation (ConductorMultiScatteringBxDF /
+                                    DielectricMultiScatteringBxDF: a multiple-
+                                    scattering lobe from the energy tables) */
 } bbg_material;
 
 enum
@@ -445,6 +446,14 @@ bbg_status bbg_batch_render(bbg_batch* batch, int32_t n, bbg_integrator* const* 
  * PrepareReflectanceTextures, :239-275): e_out 32 x 32 (index cos_i + 32 *
  * alpha_j), e_avg_out 32. Computed on the device once per process. */
 bbg_status bbg_ggx_energy_tables(float* e_out, float* e_avg_out);
+
+/* The rough-dielectric energy tables the energy-compensated dielectric uses
+ * (DielectricMultiScatteringBxDF::PrepareReflectanceTexture,
+ * src/bxdf/microfacet.cpp:168-237): e_out and e_inv_out 32 x 32 x 32 (index
+ * f0_k + 32 * (cos_i + 32 * alpha_j); e for eta >= 1, e_inv for the inverse
+ * interface), e_avg_out and e_inv_avg_out 32 x 32 (index f0_k + 32 *
+ * alpha_j). Computed on the device once per process. */
+bbg_status bbg_dielectric_energy_tables(float* e_out, float* e_inv_out, float* e_avg_out, float* e_inv_avg_out);
 
 /* ------------------------------------------------------------ autotuning */
 

@@ -23,9 +23,9 @@
 //
 // Supported scene content (checked in the constructors, which throw
 // std::runtime_error otherwise): Triangle and Sphere shapes; DiffuseMaterial,
-// ConductorMaterial (energy compensation on or off), DielectricMaterial
-// (energy compensation off) and MetallicRoughnessMaterial with constant
-// textures and no normal or alpha maps;
+// ConductorMaterial and DielectricMaterial (energy compensation on or off)
+// and MetallicRoughnessMaterial with constant textures and no normal or alpha
+// maps;
 // PointLight, SpotLight, UniformInfiniteLight, DiffuseAreaLight with a
 // constant emission; PerspectiveCamera with a Box, Tent or Gaussian filter;
 // IndependentSampler or StratifiedSampler.

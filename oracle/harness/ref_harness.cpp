@@ -24,6 +24,8 @@
 #include "bulbit/materials.h"
 #include "bulbit/microfacet.h"
 #include "bulbit/textures.h"
+#include "bulbit/textures3d.h"
+#include "bulbit/bxdfs.h"
 #include "bulbit/parallel_for.h"
 #include "bulbit/samplers.h"
 #include "bulbit/scene.h"
@@ -67,6 +69,11 @@ BBREF_STEAL(CamLensRadius, &PerspectiveCamera::lens_radius)
 BBREF_STEAL(GgxE, &TrowbridgeReitzDistribution::E_texture)
 BBREF_STEAL(GgxEAvg, &TrowbridgeReitzDistribution::E_avg_texture)
 BBREF_STEAL(FloatTexImage, &ImageTexture<Float>::image)
+BBREF_STEAL(DmsE, &DielectricMultiScatteringBxDF::E_texture)
+BBREF_STEAL(DmsEInv, &DielectricMultiScatteringBxDF::E_inv_texture)
+BBREF_STEAL(DmsEAvg, &DielectricMultiScatteringBxDF::E_avg_texture)
+BBREF_STEAL(DmsEInvAvg, &DielectricMultiScatteringBxDF::E_inv_avg_texture)
+BBREF_STEAL(FloatTex3DImage, &ImageTexture3D<Float>::image)
 
 namespace
 {
@@ -176,7 +183,7 @@ Material* MakeMaterial(Scene& scene, const bbg_material& m)
     case BBG_MAT_DIELECTRIC:
         return scene.CreateMaterial<DielectricMaterial>(m.eta[0], FloatTex(scene, m.roughness[0]),
                                                         FloatTex(scene, m.roughness[1]), SpecTex(scene, m.reflectance),
-                                                        false);
+                                                        m.energy_compensation != 0);
     case BBG_MAT_METALLIC_ROUGHNESS:
         return scene.CreateMaterial<MetallicRoughnessMaterial>(SpecTex(scene, m.reflectance),
                                                                FloatTex(scene, m.metallic),
@@ -603,7 +610,7 @@ void bbref_set_sampler(int32_t kind, int32_t x_samples, int32_t jitter)
 int bbref_ggx_energy_tables(float* e_out, float* e_avg_out)
 {
     EnsurePool(0);
-    PrepareReflectanceTextures(32, 1024);
+    InScratchDir([] { PrepareReflectanceTextures(32, 1024); });
     const auto& e = *(*Get(GgxE{}));
     const auto& e_avg = *(*Get(GgxEAvg{}));
     const auto& ei = e.*Get(FloatTexImage{});
@@ -615,6 +622,30 @@ int bbref_ggx_energy_tables(float* e_out, float* e_avg_out)
     for (int32 i = 0; i < 32; ++i)
     {
         e_avg_out[i] = ai[i];
+    }
+    return 0;
+}
+
+// The reference's rough-dielectric energy tables after
+// PrepareReflectanceTextures(32, 1024): E, E_inv 32^3 and E_avg, E_inv_avg 32^2
+// in the images' own layouts.
+int bbref_dielectric_energy_tables(float* e_out, float* e_inv_out, float* e_avg_out, float* e_inv_avg_out)
+{
+    EnsurePool(0);
+    InScratchDir([] { PrepareReflectanceTextures(32, 1024); });
+    const auto& e = (*(*Get(DmsE{}))).*Get(FloatTex3DImage{});
+    const auto& ei = (*(*Get(DmsEInv{}))).*Get(FloatTex3DImage{});
+    const auto& a = (*(*Get(DmsEAvg{}))).*Get(FloatTexImage{});
+    const auto& ai = (*(*Get(DmsEInvAvg{}))).*Get(FloatTexImage{});
+    for (int32 i = 0; i < 32 * 32 * 32; ++i)
+    {
+        e_out[i] = e[i];
+        e_inv_out[i] = ei[i];
+    }
+    for (int32 i = 0; i < 32 * 32; ++i)
+    {
+        e_avg_out[i] = a[i];
+        e_inv_avg_out[i] = ai[i];
     }
     return 0;
 }

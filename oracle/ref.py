@@ -45,6 +45,7 @@ def lib():
             "bbref_light_pmf": (I32, [P, P]),
             "bbref_sampler_draws": (I32, [I32, I32, I32, I32, I32, P]),
             "bbref_ggx_energy_tables": (I32, [P, P]),
+            "bbref_dielectric_energy_tables": (I32, [P, P, P, P]),
             "bbref_set_sampler": (None, [I32, I32, I32]),
             "bbref_pcg32": (I32, [C.c_uint64, C.c_uint64, I32, P]),
             "bbref_hash_pixel_sample": (C.c_uint64, [I32, I32, I32, I32]),
@@ -186,6 +187,17 @@ def ggx_energy_tables():
     a = np.zeros(32, np.float32)
     lib().bbref_ggx_energy_tables(_p(e), _p(a))
     return e.reshape(32, 32), a
+
+
+def dielectric_energy_tables():
+    """The reference's rough-dielectric energy tables: (E, E_inv) 32x32x32
+    indexed [alpha][cos][f0], (E_avg, E_inv_avg) 32x32 indexed [alpha][f0]."""
+    e = np.zeros(32 ** 3, np.float32)
+    ei = np.zeros(32 ** 3, np.float32)
+    a = np.zeros(32 * 32, np.float32)
+    ai = np.zeros(32 * 32, np.float32)
+    lib().bbref_dielectric_energy_tables(_p(e), _p(ei), _p(a), _p(ai))
+    return e.reshape(32, 32, 32), ei.reshape(32, 32, 32), a.reshape(32, 32), ai.reshape(32, 32)
 
 
 def pcg32(initstate, initseq, n):

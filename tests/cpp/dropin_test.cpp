@@ -95,9 +95,10 @@ void MeshScene(Scene& scene)
         scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(0.161f, 0.492f, 1.426f)),
         scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(4.08769f, 2.32625f, 1.846f)),
         scene.CreateTexture<ConstantTexture, Float>(0.3f), scene.CreateTexture<ConstantTexture, Float>(0.3f));
+    // Rough glass, also with the library default (energy_compensation = true).
     auto* glass = scene.CreateMaterial<DielectricMaterial>(
-        1.5f, scene.CreateTexture<ConstantTexture, Float>(0.0f), scene.CreateTexture<ConstantTexture, Float>(0.0f),
-        scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(1.0f)), false);
+        1.5f, scene.CreateTexture<ConstantTexture, Float>(0.25f), scene.CreateTexture<ConstantTexture, Float>(0.25f),
+        scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(1.0f)));
     std::vector<Primitive*> light_prims;
     for (int32 i = 0; i < 8; ++i)
     {
