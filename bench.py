@@ -214,6 +214,8 @@ def run_pt(args, barrier, world):
     t0 = time.perf_counter()
     acc = lib.GpuAccel(scene)
     build_s = time.perf_counter() - t0
+    if args.traversal != "default":
+        acc.set_traversal(abi.BBG_TRAVERSAL_WIDE if args.traversal == "wide" else abi.BBG_TRAVERSAL_ORDERED)
     integ = lib.GpuPathIntegrator(acc, scene)
     cam = lib.camera(scene.camera)
     params = abi.RenderParams()
@@ -292,10 +294,12 @@ def run_guided(args):
     selection 1/2); its spp is chosen from a probe render so its device time
     matches the plain arm's; every sample, the training ones included, counts
     toward its image."""
-    from bulbit_b200 import lib, scenes
+    from bulbit_b200 import abi, lib, scenes
     res, wave, steps = args.guided_res, 1 << 21, 8
     scene = scenes.cornell_icosphere(levels=8, width=res, height=res, spp=64, max_bounces=16)
     acc = lib.GpuAccel(scene)
+    if args.traversal != "default":
+        acc.set_traversal(abi.BBG_TRAVERSAL_WIDE if args.traversal == "wide" else abi.BBG_TRAVERSAL_ORDERED)
     integ = lib.GpuPathIntegrator(acc, scene)
     ref_film = integ.render(spp=16384, seed=7)
     ref = ref_film.image()
@@ -309,10 +313,14 @@ def run_guided(args):
         f = integ.render(spp=spp, seed=seed, guide=g, train=True, wave_paths=wave, steps=steps, lr=1e-2)
         return f, g
 
-    probe, _ = guided(64, 3, 5)
-    spp_eq = max(1, int(64 * t_plain / probe.stats.device_ms))
+    # Per-spp cost from the faster of two probes (a one-off stall of one
+    # probe would otherwise skew the match), then one correction either way
+    # if the matched render misses the plain arm's time by more than 5 %
+    # (time is not linear in spp: whole waves).
+    t_probe = min(guided(64, 3, 5)[0].stats.device_ms, guided(64, 9, 10)[0].stats.device_ms)
+    spp_eq = max(1, int(64 * t_plain / t_probe))
     gf, g = guided(spp_eq, 4, 6)
-    if gf.stats.device_ms > 1.05 * t_plain and spp_eq > 1:  # time is not linear in spp (whole waves)
+    if abs(gf.stats.device_ms - t_plain) > 0.05 * t_plain:
         spp_eq = max(1, int(spp_eq * t_plain / gf.stats.device_ms))
         gf, g = guided(spp_eq, 4, 6)
     t_guided = gf.stats.device_ms
@@ -325,7 +333,7 @@ def run_guided(args):
         "metric": "relMSE at equal time, guided / plain", "value": (e_guided * t_guided) / (e_plain * t_plain),
         "higher_is_better": False, "raw_relmse_ratio": e_guided / e_plain,
         "plain": {"spp": 64, "device_ms": t_plain, "relMSE": e_plain},
-        "guided": {"spp": spp_eq, "device_ms": t_guided, "relMSE": e_guided,
+        "guided": {"spp": spp_eq, "device_ms": t_guided, "relMSE": e_guided, "probe_64spp_device_ms": t_probe,
                    "trained_guide_64spp_relMSE": e_same, "trained_guide_64spp_device_ms": same_spp.stats.device_ms},
         "reference": {"spp": 16384, "device_ms": ref_film.stats.device_ms},
         "config": {"workload": f"Cornell box + displaced gold icosphere (1,310,720 triangles) at {res}x{res}, "
@@ -451,6 +459,8 @@ def main():
     ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided", "batch", "guided-frame"])
     ap.add_argument("--no-autotune", action="store_true", help="path tracing: default launch configuration only")
     ap.add_argument("--guided-res", type=int, default=256)
+    ap.add_argument("--traversal", default="default", choices=["default", "ordered", "wide"],
+                    help="rays and pt workloads: node layout of the timed traversal")
     ap.add_argument("--pt-res", type=int, default=1024)
     ap.add_argument("--pt-steps", type=int, default=3)
     ap.add_argument("--pt-wave", type=int, default=1 << 24)
@@ -463,7 +473,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from bulbit_b200 import lib, scenes
+    from bulbit_b200 import abi, lib, scenes
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -524,6 +534,8 @@ def main():
     acc.intersect_any_device(dev_a, occ, sptr)
     nodes_a, prims_a = acc.last_counts()
     acc.set_counting(False)
+    if args.traversal != "default":
+        acc.set_traversal(abi.BBG_TRAVERSAL_WIDE if args.traversal == "wide" else abi.BBG_TRAVERSAL_ORDERED)
 
     def step(events=None):
         with torch.cuda.stream(stream):
@@ -587,7 +599,7 @@ def main():
                    "parallelism": f"replicas x{world}", "bvh_build_s": round(build_s, 3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
                      "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "PersistentTraceKernel<closest> (bulbit_b200/csrc/accel.cu)",
+                     "kernel": "PersistentTraceKernel<closest, 8-wide> (bulbit_b200/csrc/accel.cu)",
                      "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_closest,
                      "per_ray": {"nodes": nodes_c / n_rays, "prims": prims_c / n_rays,

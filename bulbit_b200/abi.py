@@ -35,6 +35,7 @@ BBG_MAT_METALLIC_ROUGHNESS = 3
 
 BBG_TRAVERSAL_ORDERED = 0
 BBG_TRAVERSAL_REFERENCE = 1
+BBG_TRAVERSAL_WIDE = 2
 
 BBG_FILTER_BOX = 0
 BBG_FILTER_TENT = 1

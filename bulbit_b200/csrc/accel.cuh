@@ -22,6 +22,11 @@ struct bbg_accel
     bbg::DevBuf<int2> leaves;  // (first slot, count) per leaf
     int32_t root = 0;
     bool ordered = true;
+    bbg::DevBuf<float4> wide8; // 6 float4 per node (8-wide layout; empty if not built)
+    int32_t root8 = 0;
+    int32_t n_wide8 = 0;
+    int32_t depth8 = 0;
+    bool use_wide8 = false;    // ordered queries run over the 8-wide layout
     bool device_built = false; // tree built on the device (child-box layout only)
 
     // Shading data (the reference Mesh arrays and shapes).
@@ -54,7 +59,11 @@ struct bbg_accel
     bbg::DevBuf<int32_t> work; // persistent-kernel work counter
     int64_t last_nodes = 0, last_prims = 0;
 
-    bbg::AccelView view() const { return bbg::AccelView{ nodes.p, slots.p, wide.p, leaves.p, root, ordered ? 1 : 0 }; }
+    bbg::AccelView view() const
+    {
+        return bbg::AccelView{ nodes.p, slots.p, wide.p, leaves.p, root, ordered ? 1 : 0, wide8.p, root8 };
+    }
+    bool wide8_active() const { return ordered && use_wide8 && wide8.p != nullptr; }
 };
 
 namespace bbg

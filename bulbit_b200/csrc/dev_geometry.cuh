@@ -30,6 +30,8 @@ struct AccelView
     const int2* leaves;   // (first slot, count) per leaf
     int32_t root;         // child-box layout root reference
     int32_t ordered;      // 1: nearest-first traversal over the child-box layout
+    const float4* wide8 = nullptr; // 8-wide layout: 6 per node (null: not built)
+    int32_t root8 = 0;             // 8-wide root node
 };
 
 struct RayQ
@@ -603,6 +605,287 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
             {
                 src.Store(item, res);
                 item = -1;
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------- 8-wide layout
+//
+// The reference's binary SAH tree collapsed into nodes of up to eight
+// children (the compressed wide BVH of Ylitie, Karras and Laine, "Efficient
+// Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017).
+// 96 bytes per node, six float4:
+//   [0]   origin p (the node box's lower corner), meta = biased exponents
+//         e_x | e_y << 8 | e_z << 16 of the per-axis scales s = 2^e, and
+//         << 24 the mask of interior-child slots
+//   [1-3] child boxes as bytes, child k in byte k & 3 of word k >> 2:
+//         qlo_x, qlo_y, qlo_z, qhi_x, qhi_y, qhi_z (two words each)
+//   [4-5] child references: >= 0 node, < 0 a leaf ~(first slot << 5 |
+//         count); an empty slot is a leaf of no primitives with an inverted
+//         box
+// Child k's box is [p + qlo s, p + qhi s], rounded outward when built, so it
+// contains the binary node it stands for and no ray that reaches a leaf in
+// the binary tree is culled here. Slots are assigned so that, for a ray whose
+// direction signs form the octant code o (bit a set for a negative axis),
+// visiting slots in the order k ^ o for k = 0..7 is roughly front to back.
+
+// Byte `sh` of w as a float: 2^23 + byte assembled in the mantissa, minus 2^23.
+__device__ __forceinline__ float ByteAsFloat(uint32_t w, int sh)
+{
+    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + uint32_t(sh))) - 8388608.0f;
+}
+
+// Three-input minimum / maximum (PTX min.f32 / max.f32 with three sources;
+// a NaN source is ignored as by fminf / fmaxf).
+__device__ __forceinline__ float Max3(float a, float b, float c)
+{
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float Min3(float a, float b, float c)
+{
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+
+// Moves bit k of each byte of m to bit k ^ oct (oct in 0..7).
+__device__ __forceinline__ uint32_t PermuteByOctant(uint32_t m, uint32_t oct)
+{
+    if (oct & 1u) m = ((m & 0x5555u) << 1) | ((m >> 1) & 0x5555u);
+    if (oct & 2u) m = ((m & 0x3333u) << 2) | ((m >> 2) & 0x3333u);
+    if (oct & 4u) m = ((m & 0x0f0fu) << 4) | ((m >> 4) & 0x0f0fu);
+    return m;
+}
+
+// Tests the ray against a node's eight child boxes. Bits of *inner / *leaf
+// are visit positions (slot ^ octant) of the hit interior / leaf children;
+// the node's references are returned for the caller to pick from.
+__device__ __forceinline__ void IntersectNode8(const float4* nd, const RayQ& q, uint32_t oct, float t_min, float t_max,
+                                               uint32_t* inner, uint32_t* leaf, int4* refs_lo, int4* refs_hi)
+{
+    float4 h = __ldg(nd);
+    uint4 w1 = __ldg(reinterpret_cast<const uint4*>(nd + 1));
+    uint4 w2 = __ldg(reinterpret_cast<const uint4*>(nd + 2));
+    uint4 w3 = __ldg(reinterpret_cast<const uint4*>(nd + 3));
+    *refs_lo = __ldg(reinterpret_cast<const int4*>(nd + 4));
+    *refs_hi = __ldg(reinterpret_cast<const int4*>(nd + 5));
+    uint32_t meta = __float_as_uint(h.w);
+    // Plane k of axis a sits at p_a + q s_a: t = q (s_a / d_a) + (p_a / d_a - o_a / d_a).
+    float bx = __uint_as_float((meta & 0xffu) << 23) * q.inv_dir.x;
+    float by = __uint_as_float(((meta >> 8) & 0xffu) << 23) * q.inv_dir.y;
+    float bz = __uint_as_float(((meta >> 16) & 0xffu) << 23) * q.inv_dir.z;
+    float ax = __fmaf_rn(h.x, q.inv_dir.x, -q.oinv.x);
+    float ay = __fmaf_rn(h.y, q.inv_dir.y, -q.oinv.y);
+    float az = __fmaf_rn(h.z, q.inv_dir.z, -q.oinv.z);
+    // Entry planes are the low bounds on a positive axis, the high ones on a negative axis.
+    uint32_t nx0 = q.neg[0] ? w2.z : w1.x, nx1 = q.neg[0] ? w2.w : w1.y;
+    uint32_t fx0 = q.neg[0] ? w1.x : w2.z, fx1 = q.neg[0] ? w1.y : w2.w;
+    uint32_t ny0 = q.neg[1] ? w3.x : w1.z, ny1 = q.neg[1] ? w3.y : w1.w;
+    uint32_t fy0 = q.neg[1] ? w1.z : w3.x, fy1 = q.neg[1] ? w1.w : w3.y;
+    uint32_t nz0 = q.neg[2] ? w3.z : w2.x, nz1 = q.neg[2] ? w3.w : w2.y;
+    uint32_t fz0 = q.neg[2] ? w2.x : w3.z, fz1 = q.neg[2] ? w2.y : w3.w;
+    uint32_t hits = 0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+    {
+        const int sh = k & 3;
+        const bool hi = k >= 4;
+        float tnx = __fmaf_rn(ByteAsFloat(hi ? nx1 : nx0, sh), bx, ax);
+        float tfx = __fmaf_rn(ByteAsFloat(hi ? fx1 : fx0, sh), bx, ax);
+        float tny = __fmaf_rn(ByteAsFloat(hi ? ny1 : ny0, sh), by, ay);
+        float tfy = __fmaf_rn(ByteAsFloat(hi ? fy1 : fy0, sh), by, ay);
+        float tnz = __fmaf_rn(ByteAsFloat(hi ? nz1 : nz0, sh), bz, az);
+        float tfz = __fmaf_rn(ByteAsFloat(hi ? fz1 : fz0, sh), bz, az);
+        float t0 = Max3(tnx, tny, fmaxf(tnz, t_min));
+        float t1 = Min3(tfx, tfy, fminf(tfz, t_max));
+        if (t0 <= t1)
+        {
+            hits |= 1u << k;
+        }
+    }
+    // Slot-order masks (interior slots from the header), then visit positions.
+    uint32_t imask = meta >> 24;
+    uint32_t m = PermuteByOctant((hits & imask) | ((hits & ~imask) << 8), oct);
+    *inner = m & 0xffu;
+    *leaf = m >> 8;
+}
+
+__device__ __forceinline__ int32_t ChildRef8(const float4* wide8, int32_t node, uint32_t slot)
+{
+    return __ldg(reinterpret_cast<const int32_t*>(wide8 + 6 * size_t(node) + 4) + slot);
+}
+
+// Reference of slot k (0..7) from the two int4 of a node, by selects (no
+// indexed register array, which would live in local memory).
+__device__ __forceinline__ int32_t SelectRef8(const int4& a, const int4& b, uint32_t k)
+{
+    int4 v = (k & 4u) ? b : a;
+    int32_t lo = (k & 1u) ? v.y : v.x;
+    int32_t hi = (k & 1u) ? v.w : v.z;
+    return (k & 2u) ? hi : lo;
+}
+
+// A leaf child's reference in the 8-wide layout: ~(first slot << 5 | count),
+// count 1..31.
+constexpr int kLeaf8CountBits = 5;
+
+// Persistent traversal of the 8-wide layout (same work-source protocol as
+// TracePersistent). Each iteration opens one node: its hit leaf children's
+// primitives are tested at once, and the nearest hit interior child (by the
+// octant order) becomes the next node, the rest of them pushed as a group
+// (node << 8 | visit positions left). The next node's reference comes from
+// the registers of the node just opened; only a group taken off the stack
+// reads its reference from memory. Every push is one tree level deeper than
+// the last, so the tree depth bounds the stack.
+template <bool ANY, class Src, int BLOCK = kTraversalBlock, int SHORT = kShortStack>
+__device__ __forceinline__ void TracePersistentWide(const AccelView& a, int32_t n, int32_t* next, Src& src)
+{
+    const unsigned kFull = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const int tid = threadIdx.x;
+    int32_t item = -1;
+    bool exhausted = false;
+    RayQ q;
+    float t_min = 0, t_max = 0;
+    TraceResult res{ -1, 0, 0, 0 };
+    __shared__ int32_t s_stack[(SHORT > 0 ? SHORT : 1) * BLOCK];
+    int32_t spill[kStackCapacity - SHORT];
+    int sp = 0;
+    uint32_t oct = 0;
+    int32_t pending = kNoNode; // next node to open
+    AccelView av = a;
+
+    auto push = [&](int32_t e) {
+        if (sp < SHORT)
+        {
+            s_stack[sp * BLOCK + tid] = e;
+        }
+        else
+        {
+            spill[sp - SHORT] = e;
+        }
+        ++sp;
+    };
+    auto pop = [&]() -> int32_t {
+        --sp;
+        return sp < SHORT ? s_stack[sp * BLOCK + tid] : spill[sp - SHORT];
+    };
+
+    while (true)
+    {
+        __syncwarp();
+        bool busy = item >= 0;
+        unsigned have = __ballot_sync(kFull, busy);
+        if (!exhausted && __popc(have) < kRefill)
+        {
+            unsigned need = ~have;
+            int32_t cnt = __popc(need);
+            int32_t base = 0;
+            if (lane == 0)
+            {
+                base = atomicAdd(next, cnt);
+            }
+            base = __shfl_sync(kFull, base, 0);
+            exhausted = base + cnt >= n;
+            if (!busy)
+            {
+                int32_t r = base + __popc(need & ((1u << lane) - 1u));
+                if (r < n)
+                {
+                    item = r;
+                    src.Load(r, &q, &t_min, &t_max);
+                    if constexpr (requires { src.View(r); })
+                    {
+                        av = src.View(r);
+                    }
+                    res = TraceResult{ -1, t_max, 0, 0 };
+                    sp = 0;
+                    oct = uint32_t(q.neg[0]) | (uint32_t(q.neg[1]) << 1) | (uint32_t(q.neg[2]) << 2);
+                    pending = av.root8;
+                    busy = true;
+                }
+            }
+            have = __ballot_sync(kFull, busy);
+        }
+        if (have == 0)
+        {
+            break;
+        }
+        if (busy)
+        {
+            if (pending == kNoNode)
+            {
+                // The current group is spent: continue with the group below.
+                int32_t e = pop();
+                int32_t gnode = e >> 8;
+                uint32_t gmask = uint32_t(e) & 0xffu;
+                uint32_t pos = uint32_t(__ffs(gmask) - 1);
+                gmask &= gmask - 1;
+                pending = ChildRef8(av.wide8, gnode, pos ^ oct);
+                if (gmask != 0)
+                {
+                    push((gnode << 8) | int32_t(gmask));
+                }
+            }
+            const int32_t node = pending;
+            uint32_t im, lm;
+            int4 ra, rb;
+            IntersectNode8(av.wide8 + 6 * size_t(node), q, oct, t_min, t_max, &im, &lm, &ra, &rb);
+            // The node's hit leaves.
+            while (lm != 0)
+            {
+                uint32_t pos = uint32_t(__ffs(lm) - 1);
+                lm &= lm - 1;
+                uint32_t lf = ~uint32_t(SelectRef8(ra, rb, pos ^ oct));
+                int32_t first = int32_t(lf >> kLeaf8CountBits);
+                int32_t count = int32_t(lf & ((1u << kLeaf8CountBits) - 1u));
+                bool stop = false;
+                for (int32_t i = 0; i < count; ++i)
+                {
+                    if (TestSlot(av, first + i, q, t_min, t_max, &res))
+                    {
+                        if (ANY)
+                        {
+                            stop = true;
+                            break;
+                        }
+                        t_max = res.t;
+                    }
+                    if (t_max <= t_min)
+                    {
+                        stop = true;
+                        break;
+                    }
+                }
+                if (stop)
+                {
+                    lm = 0;
+                    im = 0;
+                    sp = 0;
+                }
+            }
+            // The nearest hit interior child next; the others as a group.
+            if (im != 0)
+            {
+                uint32_t pos = uint32_t(__ffs(im) - 1);
+                im &= im - 1;
+                pending = SelectRef8(ra, rb, pos ^ oct);
+                if (im != 0)
+                {
+                    push((node << 8) | int32_t(im));
+                }
+            }
+            else
+            {
+                pending = kNoNode;
+                if (sp == 0)
+                {
+                    src.Store(item, res);
+                    item = -1;
+                }
             }
         }
     }

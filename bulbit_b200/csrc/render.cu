@@ -391,7 +391,9 @@ struct ShadowBatchSrc : ShadowSrc
 
 // Launch shapes of the traversal passes the autotuner chooses from: threads
 // per block and stack entries per thread kept in shared memory (0: the
-// whole traversal stack in local memory).
+// whole traversal stack in local memory). A trace shape passed to the launch
+// functions is a shape index, plus kNumShapes when the tree's 8-wide layout is
+// traversed.
 struct TraversalShape
 {
     int block;
@@ -400,7 +402,7 @@ struct TraversalShape
 constexpr int kNumShapes = 4;
 constexpr TraversalShape kShapes[kNumShapes] = { { 128, 16 }, { 128, 0 }, { 128, 8 }, { 256, 16 } };
 
-template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack>
+template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack, bool WIDE = false>
 __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int parity)
 {
     const int32_t n = w.counts[parity];
@@ -411,12 +413,25 @@ __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int
     const SceneDev& s = sc.Scene(0);
     if constexpr (kIsBatch<Scenes>)
     {
-        // Every scene of a batch uses the child-box layout (checked on the host).
+        // Every scene of a batch uses the ordered traversal, all over the same
+        // layout (checked on the host).
         ClosestBatchSrc src{ { w.queue[parity], w.o_pdf, w.d_eta, w.hit }, w.flags, sc.scenes };
-        TracePersistent<false, ClosestBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
+        if constexpr (WIDE)
+        {
+            TracePersistentWide<false, ClosestBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
+        }
+        else
+        {
+            TracePersistent<false, ClosestBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
+        }
         return;
     }
     ClosestSrc src{ w.queue[parity], w.o_pdf, w.d_eta, w.hit };
+    if constexpr (WIDE)
+    {
+        TracePersistentWide<false, ClosestSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
+        return;
+    }
     if (s.accel.ordered)
     {
         TracePersistent<false, ClosestSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
@@ -431,7 +446,7 @@ __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int
     }
 }
 
-template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack>
+template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack, bool WIDE = false>
 __global__ void __launch_bounds__(BLOCK) ShadowKernel(Scenes sc, WaveDev w)
 {
     const int32_t n = w.counts[2];
@@ -443,10 +458,22 @@ __global__ void __launch_bounds__(BLOCK) ShadowKernel(Scenes sc, WaveDev w)
     if constexpr (kIsBatch<Scenes>)
     {
         ShadowBatchSrc src{ { w.sh_o, w.sh_d, w.sh_c, w.L }, w.flags, sc.scenes };
-        TracePersistent<true, ShadowBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
+        if constexpr (WIDE)
+        {
+            TracePersistentWide<true, ShadowBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
+        }
+        else
+        {
+            TracePersistent<true, ShadowBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
+        }
         return;
     }
     ShadowSrc src{ w.sh_o, w.sh_d, w.sh_c, w.L };
+    if constexpr (WIDE)
+    {
+        TracePersistentWide<true, ShadowSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
+        return;
+    }
     if (s.accel.ordered)
     {
         TracePersistent<true, ShadowSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
@@ -1735,7 +1762,7 @@ namespace
 template <class Scenes>
 struct GridsT
 {
-    int raygen, closest[kNumShapes], shade, shadow[kNumShapes], film, shade_a, shade_b;
+    int raygen, closest[2 * kNumShapes], shade, shadow[2 * kNumShapes], film, shade_a, shade_b;
     GridsT()
     {
         raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel<Scenes>), kBlock);
@@ -1753,39 +1780,49 @@ struct GridsT
     {
         constexpr TraversalShape t = kShapes[K];
         closest[K] = PersistentGrid(
-            reinterpret_cast<const void*>(ClosestKernel<Scenes, t.block, t.short_stack>), t.block);
+            reinterpret_cast<const void*>(ClosestKernel<Scenes, t.block, t.short_stack, false>), t.block);
         shadow[K] = PersistentGrid(
-            reinterpret_cast<const void*>(ShadowKernel<Scenes, t.block, t.short_stack>), t.block);
+            reinterpret_cast<const void*>(ShadowKernel<Scenes, t.block, t.short_stack, false>), t.block);
+        closest[kNumShapes + K] = PersistentGrid(
+            reinterpret_cast<const void*>(ClosestKernel<Scenes, t.block, t.short_stack, true>), t.block);
+        shadow[kNumShapes + K] = PersistentGrid(
+            reinterpret_cast<const void*>(ShadowKernel<Scenes, t.block, t.short_stack, true>), t.block);
     }
 };
 using Grids = GridsT<OneScene>;
 
-template <int K, class Scenes>
+template <int K, bool WIDE, class Scenes>
 void LaunchTraceShape(const GridsT<Scenes>& gr, const Scenes& sc, const WaveDev& w, int parity, bool shadow,
                       cudaStream_t st)
 {
     constexpr TraversalShape t = kShapes[K];
+    constexpr int g = (WIDE ? kNumShapes : 0) + K;
     if (shadow)
     {
-        ShadowKernel<Scenes, t.block, t.short_stack><<<gr.shadow[K], t.block, 0, st>>>(sc, w);
+        ShadowKernel<Scenes, t.block, t.short_stack, WIDE><<<gr.shadow[g], t.block, 0, st>>>(sc, w);
     }
     else
     {
-        ClosestKernel<Scenes, t.block, t.short_stack><<<gr.closest[K], t.block, 0, st>>>(sc, w, parity);
+        ClosestKernel<Scenes, t.block, t.short_stack, WIDE><<<gr.closest[g], t.block, 0, st>>>(sc, w, parity);
     }
 }
 
-// The closest-hit (shadow = false) or shadow pass with launch shape `shape`.
+// The closest-hit (shadow = false) or shadow pass with trace shape
+// `shape` (a kShapes index, + kNumShapes over the 8-wide layout).
 template <class Scenes>
 void LaunchTrace(int shape, const GridsT<Scenes>& gr, const Scenes& sc, const WaveDev& w, int parity, bool shadow,
                  cudaStream_t st)
 {
     switch (shape)
     {
-    case 1: LaunchTraceShape<1>(gr, sc, w, parity, shadow, st); break;
-    case 2: LaunchTraceShape<2>(gr, sc, w, parity, shadow, st); break;
-    case 3: LaunchTraceShape<3>(gr, sc, w, parity, shadow, st); break;
-    default: LaunchTraceShape<0>(gr, sc, w, parity, shadow, st); break;
+    case 1: LaunchTraceShape<1, false>(gr, sc, w, parity, shadow, st); break;
+    case 2: LaunchTraceShape<2, false>(gr, sc, w, parity, shadow, st); break;
+    case 3: LaunchTraceShape<3, false>(gr, sc, w, parity, shadow, st); break;
+    case kNumShapes + 0: LaunchTraceShape<0, true>(gr, sc, w, parity, shadow, st); break;
+    case kNumShapes + 1: LaunchTraceShape<1, true>(gr, sc, w, parity, shadow, st); break;
+    case kNumShapes + 2: LaunchTraceShape<2, true>(gr, sc, w, parity, shadow, st); break;
+    case kNumShapes + 3: LaunchTraceShape<3, true>(gr, sc, w, parity, shadow, st); break;
+    default: LaunchTraceShape<0, false>(gr, sc, w, parity, shadow, st); break;
     }
 }
 
@@ -2054,11 +2091,13 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
 
     const int iterations = I->max_bounces + 1;
     const Grids gr;
+    // The tuned launch shape over the accel's layout (8-wide when selected).
+    const int trace_shape = I->shape + (I->accel->wide8_active() ? kNumShapes : 0);
     bool use_graph = p->use_graph != 0;
     if (use_graph && (!I->graph || I->graph_capacity != wave_paths || I->graph_iterations != iterations ||
                       !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f) ||
                       I->graph_guide_handle != gc.guide || !SameGuide(I->graph_guide, gc.dev) ||
-                      I->graph_guide_lr != gc.lr || I->graph_shape != I->shape))
+                      I->graph_guide_lr != gc.lr || I->graph_shape != trace_shape))
     {
         if (I->graph)
         {
@@ -2067,7 +2106,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         cudaGraph_t g;
         BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        bbg_status es = Enqueue(I, gr, s, f, gc, iterations, I->shape, st);
+        bbg_status es = Enqueue(I, gr, s, f, gc, iterations, trace_shape, st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         BBG_TRY(es);
         if (ce != cudaSuccess)
@@ -2083,7 +2122,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         I->graph_guide = gc.dev;
         I->graph_guide_handle = gc.guide;
         I->graph_guide_lr = gc.lr;
-        I->graph_shape = I->shape;
+        I->graph_shape = trace_shape;
     }
 
     // Device time of the render itself: buffer set-up and graph capture
@@ -2102,7 +2141,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         else
         {
-            BBG_TRY(Enqueue(I, gr, s, f, gc, iterations, I->shape, st));
+            BBG_TRY(Enqueue(I, gr, s, f, gc, iterations, trace_shape, st));
         }
         // Paths still queued after max_bounces + 1 levels only come from
         // material-less surfaces, which do not count a bounce
@@ -2118,7 +2157,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
             {
                 return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
             }
-            BBG_TRY(EnqueueLevel(gr, s, I->Wave(), gc, parity, I->shape, st));
+            BBG_TRY(EnqueueLevel(gr, s, I->Wave(), gc, parity, trace_shape, st));
             parity ^= 1;
             BBG_CUDA(cudaMemcpyAsync(&left, I->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             BBG_CUDA(cudaStreamSynchronize(st));
@@ -2437,9 +2476,16 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     }
     BBG_TRY(E->Reserve(wave_paths));
     const BatchGrids gr;
+    // The 8-wide layout only when every scene's accel traverses it.
+    bool all_wide = true;
+    for (int32_t i = 0; i < n; ++i)
+    {
+        all_wide = all_wide && integrators[i]->accel->wide8_active();
+    }
+    const int trace_shape = B->shape + (all_wide ? kNumShapes : 0);
     const bool use_graph = params[0].use_graph != 0;
     if (use_graph && (!E->graph || B->graph_capacity != wave_paths || B->graph_iterations != iterations ||
-                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != B->shape))
+                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != trace_shape))
     {
         if (E->graph)
         {
@@ -2448,7 +2494,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         cudaGraph_t g;
         BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        bbg_status es = EnqueueBatch(gr, table, E->Wave(), iterations, B->shape, st);
+        bbg_status es = EnqueueBatch(gr, table, E->Wave(), iterations, trace_shape, st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         BBG_TRY(es);
         if (ce != cudaSuccess)
@@ -2460,7 +2506,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         B->graph_capacity = wave_paths;
         B->graph_iterations = iterations;
         B->graph_table = table;
-        B->graph_shape = B->shape;
+        B->graph_shape = trace_shape;
     }
 
     BBG_CUDA(cudaMemsetAsync(E->stats.p, 0, 2 * sizeof(unsigned long long), st));
@@ -2481,7 +2527,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         else
         {
-            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), iterations, B->shape, st));
+            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), iterations, trace_shape, st));
         }
         // Paths still queued come from material-less surfaces (no bounce
         // counted): drain them level by level, then redo the film pass.
@@ -2496,7 +2542,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             {
                 return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
             }
-            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), parity, B->shape, st));
+            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), parity, trace_shape, st));
             parity ^= 1;
             BBG_CUDA(cudaMemcpyAsync(&left, E->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             BBG_CUDA(cudaStreamSynchronize(st));

@@ -129,7 +129,8 @@ class GpuAccel:
         return nodes, slots
 
     def set_traversal(self, mode):
-        """abi.BBG_TRAVERSAL_ORDERED (default) or abi.BBG_TRAVERSAL_REFERENCE."""
+        """abi.BBG_TRAVERSAL_WIDE (default for host-built trees), abi.BBG_TRAVERSAL_ORDERED or
+        abi.BBG_TRAVERSAL_REFERENCE."""
         check(get_lib().bbg_accel_set_traversal(self.h, mode), "bbg_accel_set_traversal")
 
     def set_counting(self, on):

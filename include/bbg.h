@@ -208,17 +208,22 @@ bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays, int64_t n
 bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
                              bbg_memory mem, void* stream);
 
-/* Traversal order. ORDERED (the default) visits the nearer child first over
- * a child-box node layout and skips subtrees beyond the closest hit so far;
- * REFERENCE visits nodes in BVH::RayCast's own order (include/bulbit/bvh.h:
- * 102-155). Both run the same primitive tests and return the same closest
- * primitive and t; they can differ only on rays whose two nearest hits have
- * exactly equal t (the reference keeps the last one it visits). Any-hit
- * results are identical. */
+/* Traversal order. WIDE (the default for trees built on the host) traverses
+ * the tree collapsed into 8-wide nodes with byte-quantised child boxes
+ * (rounded outward), children ordered by ray octant; ORDERED (the default for
+ * trees built on the device, and where the 8-wide layout cannot be built)
+ * visits the nearer child first over a binary child-box node layout and
+ * skips subtrees beyond the closest hit so far; REFERENCE visits nodes in
+ * BVH::RayCast's own order (include/bulbit/bvh.h:102-155). All run the same
+ * primitive tests and return the same closest primitive and t; they can
+ * differ only on rays whose two nearest hits have exactly equal t (the
+ * reference keeps the last one it visits). Any-hit results are identical.
+ * The choice also applies to renders with the accel. */
 enum
 {
     BBG_TRAVERSAL_ORDERED = 0,
-    BBG_TRAVERSAL_REFERENCE = 1
+    BBG_TRAVERSAL_REFERENCE = 1,
+    BBG_TRAVERSAL_WIDE = 2
 };
 bbg_status bbg_accel_set_traversal(bbg_accel* accel, int32_t mode);
 
@@ -432,7 +437,8 @@ bbg_status bbg_batch_destroy(bbg_batch* batch);
 /* Renders n scenes (1 <= n <= 2048): integrators[i] seen through cameras[i]
  * with params[i] into films[i] (host or device memory as mem says). Every
  * params[i].spp must be equal and params[i].guide NULL; every accel must use
- * the default traversal (BBG_TRAVERSAL_ORDERED). The wave size and CUDA-graph
+ * an ordered traversal (WIDE or ORDERED; the 8-wide layout is traversed when
+ * every accel selects it). The wave size and CUDA-graph
  * choice come from params[0]. stats (optional) receives the batch's totals.
  * Calls on one batch must not overlap, nor overlap renders of the same
  * integrators (their film buffers are reused for host-memory films). */

@@ -68,6 +68,6 @@ def test_batch_rejects_what_it_cannot_render(batch_scenes):
             b.render(integs, spp=4)
         assert e.value.status == abi.BBG_ERR_UNSUPPORTED
     finally:
-        acc.set_traversal(abi.BBG_TRAVERSAL_ORDERED)
+        acc.set_traversal(abi.BBG_TRAVERSAL_WIDE)
     films, _ = b.render(integs, spp=2)  # still usable after the rejections
     assert all(f.count.sum() > 0 for f in films)

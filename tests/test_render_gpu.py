@@ -24,7 +24,7 @@ def path_rel_err(a, b):
     return np.where(num == 0, 0.0, num / np.maximum(den, 1e-30))
 
 
-def render_both(oracle, scene, use_ref_tree=True, **kw):
+def render_both(oracle, scene, use_ref_tree=True, traversal=None, **kw):
     rs = oracle.RefScene(scene)
     rs.make_integrator()
     tree = rs.bvh() if use_ref_tree else None
@@ -35,6 +35,8 @@ def render_both(oracle, scene, use_ref_tree=True, **kw):
         if pos is not None:
             scene.positions, scene.normals, scene.tangents, scene.uvs = pos, nrm, tan, uv
     acc = lib.GpuAccel(scene, bvh=tree)
+    if traversal is not None:
+        acc.set_traversal(traversal)
     integ = lib.GpuPathIntegrator(acc, scene)
     film = integ.render(path_L=True, **kw)
     ref_L, _ = rs.trace_paths()
@@ -87,9 +89,10 @@ def test_readme_scene_image_and_film_state(oracle):
     assert np.isclose(my_var, var, rtol=1e-3, atol=1e-6).mean() > 0.999
 
 
-def test_cornell_paths(oracle):
+@pytest.mark.parametrize("traversal", [abi.BBG_TRAVERSAL_ORDERED, abi.BBG_TRAVERSAL_WIDE], ids=["binary", "wide8"])
+def test_cornell_paths(oracle, traversal):
     scene = scenes.cornell_icosphere(levels=4, width=48, height=48, spp=8, max_bounces=16)
-    rs, acc, integ, film, ref_L = render_both(oracle, scene)
+    rs, acc, integ, film, ref_L = render_both(oracle, scene, traversal=traversal)
     check_paths("cornell_gold", film.path_L, ref_L)
 
 

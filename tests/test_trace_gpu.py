@@ -37,11 +37,13 @@ def run_parity(oracle, scene, closest, anyq, use_ref_tree):
     ref_prim, ref_t, _ = rs.intersect(closest)
     ref_occ, _ = rs.intersect_any(anyq)
     fracs = {}
-    for mode in (abi.BBG_TRAVERSAL_REFERENCE, abi.BBG_TRAVERSAL_ORDERED):
+    names = {abi.BBG_TRAVERSAL_REFERENCE: "reference-order", abi.BBG_TRAVERSAL_ORDERED: "ordered",
+             abi.BBG_TRAVERSAL_WIDE: "8-wide"}
+    for mode in (abi.BBG_TRAVERSAL_REFERENCE, abi.BBG_TRAVERSAL_ORDERED, abi.BBG_TRAVERSAL_WIDE):
         acc.set_traversal(mode)
         prim, t, _, _ = acc.intersect(closest)
         frac, unexplained, t_bad = compare_closest(rs, closest, prim, t, ref_prim, ref_t)
-        name = "reference-order" if mode == abi.BBG_TRAVERSAL_REFERENCE else "ordered"
+        name = names[mode]
         print(f"{scene.name} [{name}]: closest mismatch fraction {frac:.2e} ({int(round(frac * len(prim)))} rays), "
               f"hit rate {(ref_prim >= 0).mean():.3f}")
         assert not unexplained, unexplained[:5]
@@ -150,14 +152,21 @@ def test_closest_and_any_agree_at_full_size():
     acc = lib.GpuAccel(scene)
     rc = torch.from_numpy(closest).cuda()
     ra = torch.from_numpy(anyq).cuda()
-    hits = torch.empty((rc.shape[0], 4), dtype=torch.float32, device="cuda")
-    occ = torch.empty(rc.shape[0], dtype=torch.uint8, device="cuda")
-    acc.intersect_device(rc, hits)
-    acc.intersect_any_device(ra, occ)
-    prim = hits[:, 0].view(torch.int32)
-    t = hits[:, 1]
-    expect = (prim >= 0) & (t <= ra[:, 7])
-    assert torch.equal(expect.to(torch.uint8), occ)
+    for mode in (abi.BBG_TRAVERSAL_ORDERED, abi.BBG_TRAVERSAL_WIDE):
+        acc.set_traversal(mode)
+        hits = torch.empty((rc.shape[0], 4), dtype=torch.float32, device="cuda")
+        occ = torch.empty(rc.shape[0], dtype=torch.uint8, device="cuda")
+        acc.intersect_device(rc, hits)
+        acc.intersect_any_device(ra, occ)
+        prim = hits[:, 0].view(torch.int32)
+        t = hits[:, 1]
+        expect = (prim >= 0) & (t <= ra[:, 7])
+        assert torch.equal(expect.to(torch.uint8), occ)
+        if mode == abi.BBG_TRAVERSAL_ORDERED:
+            ordered_prim = prim.clone()
+        else:
+            # the two layouts agree except on exact ties
+            assert (prim != ordered_prim).float().mean().item() < 1e-5
 
 
 def classify_against_brute_force(rs, rays, prim, t, ref_prim, ref_t):
