@@ -34,6 +34,11 @@ namespace bbg
 {
 
 constexpr int kBlock = 128;
+// Shading kernels are held to 128 registers (4 blocks of kBlock per SM): the
+// BSDF dispatch would otherwise take 168 with spills, at 3 blocks per SM.
+#ifndef BBG_SHADE_MIN_BLOCKS
+#define BBG_SHADE_MIN_BLOCKS 4
+#endif
 
 struct SceneDev
 {
@@ -629,7 +634,7 @@ __device__ __forceinline__ int32_t SampleLight(const SceneDev& s, float u, float
 }
 
 template <class Scenes>
-__global__ void __launch_bounds__(kBlock) ShadeKernel(Scenes sc, WaveDev w, int parity)
+__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) ShadeKernel(Scenes sc, WaveDev w, int parity)
 {
     const int32_t* q = w.queue[parity];
     int32_t* q_next = w.queue[parity ^ 1];
@@ -985,7 +990,7 @@ __device__ __forceinline__ bool DirectLight(const SceneDev& s, const BSDF& bsdf,
     return true;
 }
 
-__global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, GuideDev g, int parity)
+__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(SceneDev s, WaveDev w, GuideDev g, int parity)
 {
     const int32_t* q = w.queue[parity];
     int32_t* q_next = w.queue[parity ^ 1];
@@ -1160,7 +1165,7 @@ __global__ void __launch_bounds__(kBlock) GuidedShadeA(SceneDev s, WaveDev w, Gu
     }
 }
 
-__global__ void __launch_bounds__(kBlock) GuidedShadeB(SceneDev s, WaveDev w, GuideDev g, int parity)
+__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(SceneDev s, WaveDev w, GuideDev g, int parity)
 {
     int32_t* q_next = w.queue[parity ^ 1];
     const int32_t n = w.counts[5];
