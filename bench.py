@@ -327,6 +327,17 @@ def run_guided(args):
     e_guided = rel_mse(gf.image(), ref)
     same_spp = integ.render(spp=64, seed=8, guide=g)  # the trained guide, no more training
     e_same = rel_mse(same_spp.image(), ref)
+    # Optional: a guide trained far longer than one frame allows (args.guided_pretrain
+    # frames of 64 spp, 8 Adam steps per 2^21-path wave), then judged at equal spp.
+    pretrained = None
+    if args.guided_pretrain > 0:
+        gp = lib.GpuGuide(acc.bounds(), seed=11)
+        for k in range(args.guided_pretrain):
+            integ.render(spp=64, seed=1000 + k, guide=gp, train=True, wave_paths=wave, steps=steps, lr=1e-2)
+        pre = [rel_mse(integ.render(spp=64, seed=2000 + k, guide=gp).image(), ref) for k in range(2)]
+        pl = [rel_mse(integ.render(spp=64, seed=3000 + k).image(), ref) for k in range(2)]
+        pretrained = {"frames": args.guided_pretrain, "adam_steps": args.guided_pretrain * steps * -(-res * res * 64 // wave),
+                      "guided_64spp_relMSE": pre, "plain_64spp_relMSE": pl}
     # Monte Carlo error falls as 1/time, so relMSE x time compares the two at
     # exactly equal time; the raw ratio at the matched spp is reported too.
     out = {
@@ -336,6 +347,7 @@ def run_guided(args):
         "guided": {"spp": spp_eq, "device_ms": t_guided, "relMSE": e_guided, "probe_64spp_device_ms": t_probe,
                    "trained_guide_64spp_relMSE": e_same, "trained_guide_64spp_device_ms": same_spp.stats.device_ms},
         "reference": {"spp": 16384, "device_ms": ref_film.stats.device_ms},
+        "pretrained_guide": pretrained,
         "config": {"workload": f"Cornell box + displaced gold icosphere (1,310,720 triangles) at {res}x{res}, "
                                "16 bounces; relMSE against a 16384-spp plain render",
                    "wave_paths": wave, "guide_steps_per_wave": steps, "guide_batch": 1 << 16, "guide_lr": 1e-2,
@@ -459,6 +471,8 @@ def main():
     ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided", "batch", "guided-frame"])
     ap.add_argument("--no-autotune", action="store_true", help="path tracing: default launch configuration only")
     ap.add_argument("--guided-res", type=int, default=256)
+    ap.add_argument("--guided-pretrain", type=int, default=0,
+                    help="guided workload: also judge a guide trained for this many frames at equal spp")
     ap.add_argument("--traversal", default="default", choices=["default", "ordered", "wide"],
                     help="rays and pt workloads: node layout of the timed traversal")
     ap.add_argument("--pt-res", type=int, default=1024)
