@@ -559,7 +559,12 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     for (int s = 0; s < 2; ++s)
     {
         BBG_CUDA(cudaStreamCreateWithFlags(&a->copy_stream[s], cudaStreamNonBlocking));
-        BBG_CUDA(cudaEventCreateWithFlags(&a->stage_done[s], cudaEventDisableTiming));
+    }
+    for (int s = 0; s < bbg_accel::kHostStages; ++s)
+    {
+        BBG_CUDA(cudaEventCreateWithFlags(&a->ev_in[s], cudaEventDisableTiming));
+        BBG_CUDA(cudaEventCreateWithFlags(&a->ev_traced[s], cudaEventDisableTiming));
+        BBG_CUDA(cudaEventCreateWithFlags(&a->ev_out[s], cudaEventDisableTiming));
     }
 
     if (device_build)
@@ -656,40 +661,65 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     return BBG_OK;
 }
 
-constexpr int64_t kChunkRays = int64_t(1) << 20;
+constexpr int64_t kChunkRays = int64_t(1) << 22;
 
 // Host-memory query: chunks of rays staged through two streams so the copies
 // of one chunk overlap the traversal of the other.
 template <bool ANY>
 bbg_status TraceHost(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out)
 {
+    // Chunks cycle through the staging ring: the copy in of chunk k + 1 and
+    // the copy out of chunk k - 1 overlap the trace of chunk k. Chunk sizes
+    // grow from 256K rays to 4M and shrink again towards the end (at most
+    // half of what is left), so the first copy in and the last copy out,
+    // which nothing overlaps, are short. All traces run in order on one
+    // stream (the persistent kernel's work counter is per accel); a slot is
+    // refilled only after its trace and its copy out finished.
+    constexpr int R = bbg_accel::kHostStages;
+    constexpr int64_t kFirstChunk = int64_t(1) << 18;
     const size_t out_bytes = ANY ? 1 : sizeof(bbg_hit);
-    for (int s = 0; s < 2; ++s)
+    const int64_t chunk = std::min(n, kChunkRays);
+    for (int s = 0; s < R; ++s)
     {
-        BBG_TRY(a->stage_in[s].alloc(2 * size_t(std::min(n, kChunkRays))));
-        BBG_TRY(a->stage_out[s].alloc((size_t(std::min(n, kChunkRays)) * out_bytes + 15) / 16));
+        BBG_TRY(a->stage_in[s].alloc(2 * size_t(chunk)));
+        BBG_TRY(a->stage_out[s].alloc((size_t(chunk) * out_bytes + 15) / 16));
     }
-    for (int64_t c = 0, k = 0; c < n; c += kChunkRays, ++k)
+    cudaStream_t cin = a->copy_stream[0], cout = a->copy_stream[1], comp = a->stream;
+    for (int64_t c = 0, k = 0, m = 0; c < n; c += m, ++k)
     {
-        int s = int(k & 1);
-        int64_t m = std::min(kChunkRays, n - c);
-        cudaStream_t st = a->copy_stream[s];
-        BBG_CUDA(cudaMemcpyAsync(a->stage_in[s].p, rays + c, size_t(m) * sizeof(bbg_ray), cudaMemcpyHostToDevice, st));
+        const int s = int(k % R);
+        const int64_t left = n - c;
+        const int64_t ramp_up = kFirstChunk << std::min<int64_t>(k, 4);
+        const int64_t ramp_down = std::max(left / 2, kFirstChunk);
+        m = std::min({ chunk, ramp_up, ramp_down, left });
+        if (k >= R)
+        {
+            BBG_CUDA(cudaStreamWaitEvent(cin, a->ev_traced[s], 0));
+        }
+        BBG_CUDA(cudaMemcpyAsync(a->stage_in[s].p, rays + c, size_t(m) * sizeof(bbg_ray), cudaMemcpyHostToDevice, cin));
+        BBG_CUDA(cudaEventRecord(a->ev_in[s], cin));
+        BBG_CUDA(cudaStreamWaitEvent(comp, a->ev_in[s], 0));
+        if (k >= R)
+        {
+            BBG_CUDA(cudaStreamWaitEvent(comp, a->ev_out[s], 0));
+        }
         if (ANY)
         {
-            BBG_TRY(LaunchIntersectAny(a, a->stage_in[s].p, m, reinterpret_cast<uint8_t*>(a->stage_out[s].p), st));
+            BBG_TRY(LaunchIntersectAny(a, a->stage_in[s].p, m, reinterpret_cast<uint8_t*>(a->stage_out[s].p), comp));
         }
         else
         {
-            BBG_TRY(LaunchIntersect(a, a->stage_in[s].p, m, a->stage_out[s].p, st));
+            BBG_TRY(LaunchIntersect(a, a->stage_in[s].p, m, a->stage_out[s].p, comp));
         }
+        BBG_CUDA(cudaEventRecord(a->ev_traced[s], comp));
+        BBG_CUDA(cudaStreamWaitEvent(cout, a->ev_traced[s], 0));
         BBG_CUDA(cudaMemcpyAsync(static_cast<char*>(out) + size_t(c) * out_bytes, a->stage_out[s].p,
-                                 size_t(m) * out_bytes, cudaMemcpyDeviceToHost, st));
+                                 size_t(m) * out_bytes, cudaMemcpyDeviceToHost, cout));
+        BBG_CUDA(cudaEventRecord(a->ev_out[s], cout));
     }
-    for (int s = 0; s < 2; ++s)
-    {
-        BBG_CUDA(cudaStreamSynchronize(a->copy_stream[s]));
-    }
+    BBG_CUDA(cudaStreamSynchronize(cout));
+    BBG_CUDA(cudaStreamSynchronize(comp));
+    BBG_CUDA(cudaStreamSynchronize(cin));
     return BBG_OK;
 }
 
@@ -790,9 +820,15 @@ bbg_status bbg_accel_destroy(bbg_accel* a)
             cudaStreamSynchronize(a->copy_stream[s]);
             cudaStreamDestroy(a->copy_stream[s]);
         }
-        if (a->stage_done[s])
+    }
+    for (int s = 0; s < bbg_accel::kHostStages; ++s)
+    {
+        for (cudaEvent_t e : { a->ev_in[s], a->ev_traced[s], a->ev_out[s] })
         {
-            cudaEventDestroy(a->stage_done[s]);
+            if (e)
+            {
+                cudaEventDestroy(e);
+            }
         }
     }
     delete a;

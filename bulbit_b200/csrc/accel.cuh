@@ -47,11 +47,16 @@ struct bbg_accel
     std::vector<float> host_positions;
     std::vector<bbg_sphere> host_spheres;
 
-    // Staging for host-memory calls (two pipeline stages).
-    bbg::DevBuf<float4> stage_in[2];
-    bbg::DevBuf<float4> stage_out[2];
+    // Staging for host-memory calls: a ring of kHostStages slots; rays go in
+    // on copy_stream[0], the kernels run on `stream`, results come back on
+    // copy_stream[1], ordered by per-slot events.
+    static constexpr int kHostStages = 3;
+    bbg::DevBuf<float4> stage_in[kHostStages];
+    bbg::DevBuf<float4> stage_out[kHostStages];
     cudaStream_t copy_stream[2] = { nullptr, nullptr };
-    cudaEvent_t stage_done[2] = { nullptr, nullptr };
+    cudaEvent_t ev_in[kHostStages] = {};     // slot's rays copied in
+    cudaEvent_t ev_traced[kHostStages] = {}; // slot's rays traced (stage_in free)
+    cudaEvent_t ev_out[kHostStages] = {};    // slot's results copied out (stage_out free)
 
     // Traversal counters (nodes, prims) of the last call when enabled.
     bool counting = false;
