@@ -15,6 +15,8 @@
 #include "bbg_internal.h"
 #include "dev_math.cuh"
 
+#include <cuda_fp16.h>
+
 #ifndef BBG_SLAB_FMA
 #define BBG_SLAB_FMA 1
 #endif
@@ -630,10 +632,14 @@ __device__ __forceinline__ void TracePersistent(const AccelView& a, int32_t n, i
 // direction signs form the octant code o (bit a set for a negative axis),
 // visiting slots in the order k ^ o for k = 0..7 is roughly front to back.
 
-// Byte `sh` of w as a float: 2^23 + byte assembled in the mantissa, minus 2^23.
-__device__ __forceinline__ float ByteAsFloat(uint32_t w, int sh)
+// Bytes 2 pair and 2 pair + 1 of w as floats: one byte permute assembles the
+// half2 (1024 + b0, 1024 + b1) (bits 0x64bb), converted and less 1024, exactly.
+__device__ __forceinline__ float2 BytePairAsFloat(uint32_t w, int pair)
 {
-    return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + uint32_t(sh))) - 8388608.0f;
+    uint32_t h = __byte_perm(w, 0x64646464u, pair ? 0x4342u : 0x4140u);
+    __half2 v = *reinterpret_cast<__half2*>(&h);
+    float2 f = __half22float2(v);
+    return make_float2(f.x - 1024.0f, f.y - 1024.0f);
 }
 
 // Three-input minimum / maximum (PTX min.f32 / max.f32 with three sources;
@@ -689,21 +695,24 @@ __device__ __forceinline__ void IntersectNode8(const float4* nd, const RayQ& q, 
     uint32_t fz0 = q.neg[2] ? w2.x : w3.z, fz1 = q.neg[2] ? w2.y : w3.w;
     uint32_t hits = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k)
+    for (int j = 0; j < 4; ++j) // children 2j and 2j + 1
     {
-        const int sh = k & 3;
-        const bool hi = k >= 4;
-        float tnx = __fmaf_rn(ByteAsFloat(hi ? nx1 : nx0, sh), bx, ax);
-        float tfx = __fmaf_rn(ByteAsFloat(hi ? fx1 : fx0, sh), bx, ax);
-        float tny = __fmaf_rn(ByteAsFloat(hi ? ny1 : ny0, sh), by, ay);
-        float tfy = __fmaf_rn(ByteAsFloat(hi ? fy1 : fy0, sh), by, ay);
-        float tnz = __fmaf_rn(ByteAsFloat(hi ? nz1 : nz0, sh), bz, az);
-        float tfz = __fmaf_rn(ByteAsFloat(hi ? fz1 : fz0, sh), bz, az);
-        float t0 = Max3(tnx, tny, fmaxf(tnz, t_min));
-        float t1 = Min3(tfx, tfy, fminf(tfz, t_max));
-        if (t0 <= t1)
+        const int pair = j & 1;
+        const bool hi = j >= 2;
+        float2 qnx = BytePairAsFloat(hi ? nx1 : nx0, pair), qfx = BytePairAsFloat(hi ? fx1 : fx0, pair);
+        float2 qny = BytePairAsFloat(hi ? ny1 : ny0, pair), qfy = BytePairAsFloat(hi ? fy1 : fy0, pair);
+        float2 qnz = BytePairAsFloat(hi ? nz1 : nz0, pair), qfz = BytePairAsFloat(hi ? fz1 : fz0, pair);
+        float t0a = Max3(__fmaf_rn(qnx.x, bx, ax), __fmaf_rn(qny.x, by, ay), fmaxf(__fmaf_rn(qnz.x, bz, az), t_min));
+        float t1a = Min3(__fmaf_rn(qfx.x, bx, ax), __fmaf_rn(qfy.x, by, ay), fminf(__fmaf_rn(qfz.x, bz, az), t_max));
+        float t0b = Max3(__fmaf_rn(qnx.y, bx, ax), __fmaf_rn(qny.y, by, ay), fmaxf(__fmaf_rn(qnz.y, bz, az), t_min));
+        float t1b = Min3(__fmaf_rn(qfx.y, bx, ax), __fmaf_rn(qfy.y, by, ay), fminf(__fmaf_rn(qfz.y, bz, az), t_max));
+        if (t0a <= t1a)
         {
-            hits |= 1u << k;
+            hits |= 1u << (2 * j);
+        }
+        if (t0b <= t1b)
+        {
+            hits |= 1u << (2 * j + 1);
         }
     }
     // Slot-order masks (interior slots from the header), then visit positions.
