@@ -2,6 +2,7 @@
 // tree, and the batched closest-hit / any-hit traversal kernels.
 
 #include "accel.cuh"
+#include "wide8_build.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -249,136 +250,7 @@ bbg_status UploadShading(bbg_accel* a, const bbg_geometry* g)
     return BBG_OK;
 }
 
-// One child of a node being collapsed: its box and reference (>= 0 binary
-// interior node awaiting its own wide node, < 0 ~leaf).
-struct Child8
-{
-    float lo[3], hi[3];
-    int32_t bnode; // binary node index
-};
-
-// Assigns up to eight children to slots so that slot k holds a child whose
-// centroid lies toward corner k of the parent (bit a of k set: the + side of
-// axis a); rays with octant code o then meet the children roughly front to
-// back in the order k ^ o. Greedy on the largest remaining
-// centroid-offset . corner-direction product.
-void AssignSlots8(const std::vector<Child8>& cs, const float plo[3], const float phi[3], int32_t slot_of[8])
-{
-    const int n = int(cs.size());
-    double pc[3];
-    for (int a = 0; a < 3; ++a)
-    {
-        pc[a] = 0.5 * (double(plo[a]) + double(phi[a]));
-    }
-    double score[8][8];
-    for (int c = 0; c < n; ++c)
-    {
-        for (int k = 0; k < 8; ++k)
-        {
-            double d = 0;
-            for (int a = 0; a < 3; ++a)
-            {
-                double off = 0.5 * (double(cs[c].lo[a]) + double(cs[c].hi[a])) - pc[a];
-                d += ((k >> a) & 1) ? off : -off;
-            }
-            score[c][k] = d;
-        }
-    }
-    bool child_done[8] = {}, slot_used[8] = {};
-    for (int round = 0; round < n; ++round)
-    {
-        int bc = -1, bk = -1;
-        double best = 0;
-        for (int c = 0; c < n; ++c)
-        {
-            if (child_done[c]) continue;
-            for (int k = 0; k < 8; ++k)
-            {
-                if (slot_used[k]) continue;
-                if (bc < 0 || score[c][k] > best)
-                {
-                    best = score[c][k];
-                    bc = c;
-                    bk = k;
-                }
-            }
-        }
-        child_done[bc] = true;
-        slot_used[bk] = true;
-        slot_of[bc] = bk;
-    }
-}
-
-// Quantises child boxes to bytes on a per-axis grid p + q 2^e over the parent
-// box, rounding outward: every decoded box contains its child's box exactly
-// (checked in double precision, where p + q 2^e is exact).
-void QuantizeNode8(const std::vector<Child8>& cs, const int32_t slot_of[8], const int32_t refs[8], float4* out)
-{
-    float plo[3], phi[3];
-    for (int a = 0; a < 3; ++a)
-    {
-        plo[a] = cs[0].lo[a];
-        phi[a] = cs[0].hi[a];
-        for (const Child8& c : cs)
-        {
-            plo[a] = std::min(plo[a], c.lo[a]);
-            phi[a] = std::max(phi[a], c.hi[a]);
-        }
-    }
-    uint8_t qlo[3][8], qhi[3][8];
-    uint32_t meta = 0;
-    for (int a = 0; a < 3; ++a)
-    {
-        double p = plo[a];
-        double ext = double(phi[a]) - p;
-        int e = -126;
-        if (ext > 0)
-        {
-            e = std::max(-126, int(std::ceil(std::log2(ext / 255.0))));
-        }
-        while (e < 127 && p + 255.0 * std::ldexp(1.0, e) < double(phi[a]))
-        {
-            ++e;
-        }
-        double sc = std::ldexp(1.0, e);
-        meta |= uint32_t(e + 127) << (8 * a);
-        if (a == 0)
-        {
-            for (int k = 0; k < 8; ++k)
-            {
-                meta |= (refs[k] >= 0 ? 1u : 0u) << (24 + k);
-            }
-        }
-        for (int k = 0; k < 8; ++k)
-        {
-            qlo[a][k] = 255; // empty slot: an inverted box
-            qhi[a][k] = 0;
-        }
-        for (size_t c = 0; c < cs.size(); ++c)
-        {
-            double lo = cs[c].lo[a], hi = cs[c].hi[a];
-            double fl = std::floor((lo - p) / sc), fh = std::ceil((hi - p) / sc);
-            int ql = int(std::clamp(fl, 0.0, 255.0)), qh = int(std::clamp(fh, 0.0, 255.0));
-            while (ql > 0 && p + ql * sc > lo) --ql;
-            while (qh < 255 && p + qh * sc < hi) ++qh;
-            qlo[a][slot_of[c]] = uint8_t(ql);
-            qhi[a][slot_of[c]] = uint8_t(qh);
-        }
-    }
-    auto word = [](const uint8_t* b) {
-        return BitsToFloat(uint32_t(b[0]) | uint32_t(b[1]) << 8 | uint32_t(b[2]) << 16 | uint32_t(b[3]) << 24);
-    };
-    out[0] = make_float4(plo[0], plo[1], plo[2], BitsToFloat(meta));
-    out[1] = make_float4(word(qlo[0]), word(qlo[0] + 4), word(qlo[1]), word(qlo[1] + 4));
-    out[2] = make_float4(word(qlo[2]), word(qlo[2] + 4), word(qhi[0]), word(qhi[0] + 4));
-    out[3] = make_float4(word(qhi[1]), word(qhi[1] + 4), word(qhi[2]), word(qhi[2] + 4));
-    out[4] = make_float4(BitsToFloat(uint32_t(refs[0])), BitsToFloat(uint32_t(refs[1])), BitsToFloat(uint32_t(refs[2])),
-                         BitsToFloat(uint32_t(refs[3])));
-    out[5] = make_float4(BitsToFloat(uint32_t(refs[4])), BitsToFloat(uint32_t(refs[5])), BitsToFloat(uint32_t(refs[6])),
-                         BitsToFloat(uint32_t(refs[7])));
-}
-
-// Collapses the binary tree (reference layout, leaf references `ref`) into
+// Collapses the binary tree (reference layout) into
 // the 8-wide layout: each wide node takes its binary node's two children and
 // repeatedly opens the interior child of largest surface area until it holds
 // eight children or only leaves. Nodes are numbered breadth first, a node's
@@ -394,11 +266,6 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
         c.bnode = b;
         return c;
     };
-    auto area = [&](int32_t b) {
-        double d[3];
-        for (int a = 0; a < 3; ++a) d[a] = double(nodes[b].bmax[a]) - double(nodes[b].bmin[a]);
-        return d[0] * d[1] + d[1] * d[2] + d[2] * d[0];
-    };
     struct Pending
     {
         int32_t bnode, wnode, depth;
@@ -410,26 +277,26 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
     for (size_t qi = 0; qi < queue.size(); ++qi)
     {
         Pending pd = queue[qi];
-        std::vector<Child8> cs;
+        Child8 cs[8];
+        int n = 0;
         if (nodes[pd.bnode].count > 0)
         {
-            cs.push_back(child_of(pd.bnode)); // a single-leaf tree
+            cs[n++] = child_of(pd.bnode); // a single-leaf tree
         }
         else
         {
-            cs.push_back(child_of(pd.bnode + 1));
-            cs.push_back(child_of(nodes[pd.bnode].offset));
-            while (cs.size() < 8)
+            cs[n++] = child_of(pd.bnode + 1);
+            cs[n++] = child_of(nodes[pd.bnode].offset);
+            while (n < 8)
             {
                 int best = -1;
                 double best_area = -1;
-                for (size_t j = 0; j < cs.size(); ++j)
+                for (int j = 0; j < n; ++j)
                 {
-                    int32_t b = cs[j].bnode;
-                    if (nodes[b].count == 0 && area(b) > best_area)
+                    if (nodes[cs[j].bnode].count == 0 && Wide8Area(cs[j]) > best_area)
                     {
-                        best_area = area(b);
-                        best = int(j);
+                        best_area = Wide8Area(cs[j]);
+                        best = j;
                     }
                 }
                 if (best < 0)
@@ -438,35 +305,27 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
                 }
                 int32_t b = cs[best].bnode;
                 cs[best] = child_of(b + 1);
-                cs.push_back(child_of(nodes[b].offset));
+                cs[n++] = child_of(nodes[b].offset);
             }
         }
         float plo[3], phi[3];
-        for (int a = 0; a < 3; ++a)
-        {
-            plo[a] = cs[0].lo[a];
-            phi[a] = cs[0].hi[a];
-            for (const Child8& c : cs)
-            {
-                plo[a] = std::min(plo[a], c.lo[a]);
-                phi[a] = std::max(phi[a], c.hi[a]);
-            }
-        }
+        Wide8Union(cs, n, plo, phi);
         int32_t slot_of[8];
-        AssignSlots8(cs, plo, phi, slot_of);
+        AssignSlots8(cs, n, plo, phi, slot_of);
         int32_t refs[8];
         for (int k = 0; k < 8; ++k) refs[k] = ~0; // empty: a leaf of no primitives
-        for (size_t c = 0; c < cs.size(); ++c)
+        for (int c = 0; c < n; ++c)
         {
             int32_t b = cs[c].bnode;
             if (nodes[b].count > 0)
             {
-                // ~(first slot << 5 | count): the leaf's range without an indirection.
-                if (nodes[b].count >= (1 << kLeaf8CountBits) || nodes[b].offset >= (1 << (31 - kLeaf8CountBits)))
+                // The leaf's range in the reference, without an indirection.
+                if (nodes[b].count >= (1 << kWide8LeafCountBits) ||
+                    nodes[b].offset >= (1 << (31 - kWide8LeafCountBits)))
                 {
                     return false;
                 }
-                refs[slot_of[c]] = ~((nodes[b].offset << kLeaf8CountBits) | int32_t(nodes[b].count));
+                refs[slot_of[c]] = Wide8LeafRef(nodes[b].offset, int32_t(nodes[b].count));
             }
             else
             {
@@ -481,7 +340,7 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
             }
         }
         out->resize(6 * size_t(n_wide), make_float4(0, 0, 0, 0));
-        QuantizeNode8(cs, slot_of, refs, out->data() + 6 * size_t(pd.wnode));
+        QuantizeNode8(cs, n, slot_of, refs, out->data() + 6 * size_t(pd.wnode));
     }
     *depth_out = depth;
     return depth <= kStackCapacity;
@@ -880,9 +739,9 @@ bbg_status bbg_accel_set_traversal(bbg_accel* a, int32_t mode)
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_set_traversal: bad argument");
     }
-    if (a->device_built && mode != BBG_TRAVERSAL_ORDERED)
+    if (a->device_built && mode == BBG_TRAVERSAL_REFERENCE)
     {
-        return Fail(BBG_ERR_UNSUPPORTED, "a tree built on the device has only the child-box layout");
+        return Fail(BBG_ERR_UNSUPPORTED, "a tree built on the device has no reference node layout");
     }
     if (mode == BBG_TRAVERSAL_WIDE && !a->wide8.p && a->n_prims > 0)
     {

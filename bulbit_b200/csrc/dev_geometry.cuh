@@ -14,6 +14,7 @@
 
 #include "bbg_internal.h"
 #include "dev_math.cuh"
+#include "wide8_build.cuh"
 
 #include <cuda_fp16.h>
 
@@ -737,9 +738,6 @@ __device__ __forceinline__ int32_t SelectRef8(const int4& a, const int4& b, uint
     return (k & 2u) ? hi : lo;
 }
 
-// A leaf child's reference in the 8-wide layout: ~(first slot << 5 | count),
-// count 1..31.
-constexpr int kLeaf8CountBits = 5;
 
 // Persistent traversal of the 8-wide layout (same work-source protocol as
 // TracePersistent). Each iteration opens one node: its hit leaf children's
@@ -849,8 +847,8 @@ __device__ __forceinline__ void TracePersistentWide(const AccelView& a, int32_t 
                 uint32_t pos = uint32_t(__ffs(lm) - 1);
                 lm &= lm - 1;
                 uint32_t lf = ~uint32_t(SelectRef8(ra, rb, pos ^ oct));
-                int32_t first = int32_t(lf >> kLeaf8CountBits);
-                int32_t count = int32_t(lf & ((1u << kLeaf8CountBits) - 1u));
+                int32_t first = int32_t(lf >> kWide8LeafCountBits);
+                int32_t count = int32_t(lf & ((1u << kWide8LeafCountBits) - 1u));
                 bool stop = false;
                 for (int32_t i = 0; i < count; ++i)
                 {

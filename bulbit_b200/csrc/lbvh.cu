@@ -9,6 +9,7 @@
 // hit at exactly the same t (the primitive tests are the same).
 
 #include "accel.cuh"
+#include "wide8_build.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -286,7 +287,154 @@ __global__ void SlotsKernel(const int32_t* sorted_ids, const int2* prim_shape, c
     }
 }
 
+// One level of the collapse into the 8-wide layout, top down: wide node w
+// (w2b[w] names the radix-tree node it stands for) takes that node's two
+// children and opens the interior child of largest surface area until it
+// holds eight children or only leaves, allocates consecutive wide nodes for
+// its interior children (the next level) and writes its record. Leaf j is
+// sorted primitive j in slot j.
+__global__ void Wide8LevelKernel(const int2* children, const float4* node_box, const float4* boxes,
+                                 const int32_t* sorted_ids, int32_t* w2b, int32_t begin, int32_t end,
+                                 int32_t capacity, int32_t* counter, int32_t* overflow, float4* wide8)
+{
+    auto child_of = [&](int32_t r) {
+        Child8 c;
+        float4 lo, hi;
+        if (r < 0)
+        {
+            int32_t prim = sorted_ids[~r];
+            lo = boxes[2 * prim];
+            hi = boxes[2 * prim + 1];
+        }
+        else
+        {
+            lo = node_box[2 * r];
+            hi = node_box[2 * r + 1];
+        }
+        c.lo[0] = lo.x, c.lo[1] = lo.y, c.lo[2] = lo.z;
+        c.hi[0] = hi.x, c.hi[1] = hi.y, c.hi[2] = hi.z;
+        c.bnode = r;
+        return c;
+    };
+    for (int32_t w = begin + blockIdx.x * blockDim.x + threadIdx.x; w < end; w += gridDim.x * blockDim.x)
+    {
+        int32_t b = w2b[w];
+        Child8 cs[8];
+        int n = 0;
+        int2 c2 = children[b];
+        cs[n++] = child_of(c2.x);
+        cs[n++] = child_of(c2.y);
+        while (n < 8)
+        {
+            int best = -1;
+            double best_area = -1;
+            for (int j = 0; j < n; ++j)
+            {
+                if (cs[j].bnode >= 0 && Wide8Area(cs[j]) > best_area)
+                {
+                    best_area = Wide8Area(cs[j]);
+                    best = j;
+                }
+            }
+            if (best < 0)
+            {
+                break;
+            }
+            int2 o = children[cs[best].bnode];
+            cs[best] = child_of(o.x);
+            cs[n++] = child_of(o.y);
+        }
+        float plo[3], phi[3];
+        Wide8Union(cs, n, plo, phi);
+        int32_t slot_of[8];
+        AssignSlots8(cs, n, plo, phi, slot_of);
+        int32_t inner = 0;
+        for (int c = 0; c < n; ++c)
+        {
+            inner += cs[c].bnode >= 0 ? 1 : 0;
+        }
+        int32_t base = inner > 0 ? atomicAdd(counter, inner) : 0;
+        if (base + inner > capacity)
+        {
+            atomicExch(overflow, 1);
+            continue;
+        }
+        int32_t refs[8];
+        for (int k = 0; k < 8; ++k)
+        {
+            refs[k] = ~0; // empty: a leaf of no primitives
+        }
+        for (int c = 0, i = 0; c < n; ++c)
+        {
+            if (cs[c].bnode >= 0)
+            {
+                refs[slot_of[c]] = base + i;
+                w2b[base + i] = cs[c].bnode;
+                ++i;
+            }
+            else
+            {
+                refs[slot_of[c]] = Wide8LeafRef(~cs[c].bnode, 1);
+            }
+        }
+        QuantizeNode8(cs, n, slot_of, refs, wide8 + 6 * size_t(w));
+    }
+}
+
 } // namespace
+
+// Collapses the radix tree into the 8-wide layout on the device, one kernel
+// per level (the host reads the level sizes back). Leaves it unbuilt (the
+// binary layout remains the default) if the tree exceeds the layout's
+// encodings; every wide node stands for a distinct interior radix-tree node,
+// so n - 1 nodes always suffice.
+static bbg_status BuildWide8OnDevice(bbg_accel* a, int32_t n, const DevBuf<int2>& children,
+                                     const DevBuf<float4>& node_box, const DevBuf<float4>& boxes,
+                                     const DevBuf<int32_t>& sorted_ids, int grid)
+{
+    const int32_t capacity = n - 1;
+    if (n < 2 || capacity >= (1 << 23) - 1 || n >= (1 << (31 - kWide8LeafCountBits)))
+    {
+        return BBG_OK;
+    }
+    cudaStream_t st = a->stream;
+    DevBuf<int32_t> w2b, counter;
+    BBG_TRY(w2b.alloc(size_t(capacity)));
+    BBG_TRY(counter.alloc(2)); // [0] nodes allocated, [1] overflow flag
+    BBG_TRY(a->wide8.alloc(6 * size_t(capacity)));
+    const int32_t init[2] = { 1, 0 };
+    const int32_t root = 0;
+    BBG_CUDA(cudaMemcpyAsync(counter.p, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    BBG_CUDA(cudaMemcpyAsync(w2b.p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    int32_t begin = 0, end = 1, depth = 0, state[2] = { 1, 0 };
+    while (begin < end)
+    {
+        ++depth;
+        if (depth > kStackCapacity)
+        {
+            a->wide8.reset();
+            return BBG_OK;
+        }
+        int g = std::max(1, std::min((end - begin + kLbvhBlock - 1) / kLbvhBlock, grid));
+        Wide8LevelKernel<<<g, kLbvhBlock, 0, st>>>(children.p, node_box.p, boxes.p, sorted_ids.p, w2b.p, begin, end,
+                                                   capacity, counter.p, counter.p + 1, a->wide8.p);
+        BBG_CUDA(cudaMemcpyAsync(state, counter.p, sizeof(state), cudaMemcpyDeviceToHost, st));
+        BBG_CUDA(cudaStreamSynchronize(st));
+        BBG_CUDA(cudaGetLastError());
+        if (state[1] != 0)
+        {
+            a->wide8.reset();
+            return BBG_OK;
+        }
+        begin = end;
+        end = state[0];
+    }
+    a->n_wide8 = end;
+    a->root8 = 0;
+    a->depth8 = depth;
+    a->use_wide8 = true;
+    return BBG_OK;
+}
 
 bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g)
 {
@@ -360,6 +508,10 @@ bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g)
         a->root = 0;
         bounds[0] = rb[0].x, bounds[1] = rb[0].y, bounds[2] = rb[0].z;
         bounds[3] = rb[1].x, bounds[4] = rb[1].y, bounds[5] = rb[1].z;
+        if (max_depth + 1 <= kStackCapacity)
+        {
+            BBG_TRY(BuildWide8OnDevice(a, n, children, node_box, boxes, ids_sorted, grid));
+        }
     }
     BBG_CUDA(cudaGetLastError());
     if (max_depth + 1 > kStackCapacity)

@@ -171,8 +171,9 @@ bbg_status bbg_accel_create(const bbg_geometry* geometry, const bbg_bvh* bvh, bb
  * where the SAH build (reference BVH::BVH, src/accel/bvh.cpp:8) takes seconds
  * on millions of primitives. The tree differs from the reference's, so closest
  * hits agree with BVH::Intersect except between primitives hit at exactly the
- * same t; traversal is the ordered mode only (no reference node order, no
- * counting, no export). */
+ * same t; the binary radix tree is also collapsed into the 8-wide layout on
+ * the device (traversal WIDE by default, ORDERED selectable; no reference
+ * node order, no counting, no export). */
 bbg_status bbg_accel_create_device_build(const bbg_geometry* geometry, bbg_accel** out);
 bbg_status bbg_accel_destroy(bbg_accel* accel);
 
@@ -208,13 +209,13 @@ bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays, int64_t n
 bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
                              bbg_memory mem, void* stream);
 
-/* Traversal order. WIDE (the default for trees built on the host) traverses
- * the tree collapsed into 8-wide nodes with byte-quantised child boxes
- * (rounded outward), children ordered by ray octant; ORDERED (the default for
- * trees built on the device, and where the 8-wide layout cannot be built)
- * visits the nearer child first over a binary child-box node layout and
- * skips subtrees beyond the closest hit so far; REFERENCE visits nodes in
- * BVH::RayCast's own order (include/bulbit/bvh.h:102-155). All run the same
+/* Traversal order. WIDE (the default) traverses the tree collapsed into
+ * 8-wide nodes with byte-quantised child boxes (rounded outward), children
+ * ordered by ray octant; ORDERED (the default where the 8-wide layout cannot
+ * be built) visits the nearer child first over a binary child-box node
+ * layout and skips subtrees beyond the closest hit so far; REFERENCE visits
+ * nodes in BVH::RayCast's own order (include/bulbit/bvh.h:102-155; not for
+ * trees built on the device). All run the same
  * primitive tests and return the same closest primitive and t; they can
  * differ only on rays whose two nearest hits have exactly equal t (the
  * reference keeps the last one it visits). Any-hit results are identical.

@@ -210,17 +210,22 @@ def test_device_built_tree_parity(oracle):
         rs = oracle.RefScene(scene)
         acc = lib.GpuAccel(scene, device_build=True)
         ref_prim, ref_t, _ = rs.intersect(rays)
-        prim, t, _, _ = acc.intersect(rays)
-        ties, leaks_ref, leaks_dev, unexplained = classify_against_brute_force(rs, rays, prim, t, ref_prim, ref_t)
-        print(f"device-built tree, {scene.name}: {len(rays)} rays, mismatches: {ties} near-ties, "
-              f"{leaks_ref} through the reference tree, {leaks_dev} through the device tree")
-        assert not unexplained, unexplained[:5]
-        assert leaks_ref + leaks_dev <= 1e-3 * len(rays)
-        same = (prim == ref_prim) & (ref_prim >= 0)
-        assert np.array_equal(t[same].view(np.uint32), ref_t[same].view(np.uint32))
-        if anyq is not None:
-            ref_occ, _ = rs.intersect_any(anyq)
-            assert np.array_equal(acc.intersect_any(anyq), ref_occ)
+        # the 8-wide layout collapsed on the device (the default), then the binary one
+        for mode in (abi.BBG_TRAVERSAL_WIDE, abi.BBG_TRAVERSAL_ORDERED):
+            acc.set_traversal(mode)
+            prim, t, _, _ = acc.intersect(rays)
+            ties, leaks_ref, leaks_dev, unexplained = classify_against_brute_force(rs, rays, prim, t, ref_prim,
+                                                                                   ref_t)
+            print(f"device-built tree ({'8-wide' if mode == abi.BBG_TRAVERSAL_WIDE else 'binary'}), {scene.name}: "
+                  f"{len(rays)} rays, mismatches: {ties} near-ties, {leaks_ref} through the reference tree, "
+                  f"{leaks_dev} through the device tree")
+            assert not unexplained, unexplained[:5]
+            assert leaks_ref + leaks_dev <= 1e-3 * len(rays)
+            same = (prim == ref_prim) & (ref_prim >= 0)
+            assert np.array_equal(t[same].view(np.uint32), ref_t[same].view(np.uint32))
+            if anyq is not None:
+                ref_occ, _ = rs.intersect_any(anyq)
+                assert np.array_equal(acc.intersect_any(anyq), ref_occ)
     for call in (lambda: acc.set_traversal(abi.BBG_TRAVERSAL_REFERENCE), lambda: acc.set_counting(True),
                  lambda: acc.export()):
         with pytest.raises(lib.BbgError) as e:
