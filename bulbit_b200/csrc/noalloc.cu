@@ -52,11 +52,19 @@ struct StaticSrc
     }
 };
 
+template <bool WIDE>
 __global__ void __launch_bounds__(kBlock) StaticTraceKernel(AccelView a, const float4* rays, int32_t n, float4* hits,
                                                             int32_t* next)
 {
     StaticSrc src{ rays, hits };
-    TracePersistent<false>(a, n, next, src);
+    if constexpr (WIDE)
+    {
+        TracePersistentWide<false>(a, n, next, src);
+    }
+    else
+    {
+        TracePersistent<false>(a, n, next, src);
+    }
 }
 
 __global__ void __launch_bounds__(kBlock) StaticTraceReferenceKernel(AccelView a, const float4* rays, int32_t n,
@@ -140,9 +148,10 @@ extern "C" bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays
     {
         // The array keeps the previous call's contents: the counter must start at 0.
         BBG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));
-        int grid = PersistentGrid(reinterpret_cast<const void*>(StaticTraceKernel), kBlock);
+        auto k = accel->wide8_active() ? StaticTraceKernel<true> : StaticTraceKernel<false>;
+        int grid = PersistentGrid(reinterpret_cast<const void*>(k), kBlock);
         grid = int(std::min<int64_t>(grid, (n + kBlock - 1) / kBlock));
-        StaticTraceKernel<<<grid, kBlock, 0, st>>>(accel->view(), d_rays, m, d_hits, counter);
+        k<<<grid, kBlock, 0, st>>>(accel->view(), d_rays, m, d_hits, counter);
     }
     else
     {

@@ -34,7 +34,9 @@ def test_static_entry_point_matches_intersect_on_two_calls():
     acc = lib.GpuAccel(scene)
     first, _ = scenes.soup_rays(MAX_RAYS, seed=2)
     second, _ = scenes.soup_rays(50_000, seed=7)
-    for rays in (first, second):
+    # the 8-wide layout (default) on the first call, the binary one on the second
+    for rays, mode in ((first, abi.BBG_TRAVERSAL_WIDE), (second, abi.BBG_TRAVERSAL_ORDERED)):
+        acc.set_traversal(mode)
         st, hits = static_intersect(acc, rays)
         assert st == abi.BBG_OK, lib.get_lib().bbg_last_error()
         prim, t, u, v = acc.intersect(rays)
