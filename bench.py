@@ -212,7 +212,7 @@ def run_pt(args, barrier, world):
     res = args.pt_res
     scene = scenes.cornell_icosphere(levels=8, width=res, height=res, spp=64, max_bounces=16)
     t0 = time.perf_counter()
-    acc = lib.GpuAccel(scene)
+    acc = lib.GpuAccel(scene, split=args.pt_split)
     build_s = time.perf_counter() - t0
     if args.traversal != "default":
         acc.set_traversal(abi.BBG_TRAVERSAL_WIDE if args.traversal == "wide" else abi.BBG_TRAVERSAL_ORDERED)
@@ -276,6 +276,22 @@ def run_pt(args, barrier, world):
     }
     integ.close()
     acc.close()
+    # The same frame over a tree built on split references (a different tree
+    # from the reference's SAH tree: hits agree except exact ties), default
+    # launch configuration; its host build time beside the plain SAH build's.
+    if args.pt_split is None and args.pt_split_report > 0:
+        t0 = time.perf_counter()
+        acc = lib.GpuAccel(scene, split=args.pt_split_report)
+        split_build_s = time.perf_counter() - t0
+        integ = lib.GpuPathIntegrator(acc, scene)
+        params.wave_paths = args.pt_wave
+        split_ms, split_rays = timed()
+        out["split_reference_tree"] = {
+            "budget": args.pt_split_report, "value": world * paths * steps / (split_ms / 1e3), "unit": "paths/s",
+            "mrays_per_s": world * split_rays / (split_ms / 1e3) / 1e6, "ms_per_frame": split_ms / steps,
+            "bvh_build_s": round(split_build_s, 3)}
+        integ.close()
+        acc.close()
     return out, scene
 
 
@@ -476,6 +492,10 @@ def main():
     ap.add_argument("--traversal", default="default", choices=["default", "ordered", "wide"],
                     help="rays and pt workloads: node layout of the timed traversal")
     ap.add_argument("--pt-res", type=int, default=1024)
+    ap.add_argument("--pt-split", type=float, default=None,
+                    help="path tracing: build the tree over split references with this budget per primitive")
+    ap.add_argument("--pt-split-report", type=float, default=3.0,
+                    help="path tracing: also time the frame over a split-reference tree of this budget (0: skip)")
     ap.add_argument("--pt-steps", type=int, default=3)
     ap.add_argument("--pt-wave", type=int, default=1 << 24)
     args = ap.parse_args()

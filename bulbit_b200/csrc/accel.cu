@@ -193,39 +193,6 @@ float BitsToFloat(uint32_t bits)
     return f;
 }
 
-bbg_status CheckGeometry(const bbg_geometry* g)
-{
-    if (!g || g->n_prims < 0 || g->n_vertices < 0 || g->n_triangles < 0 || g->n_spheres < 0)
-    {
-        return Fail(BBG_ERR_INVALID_ARG, "geometry: null or negative count");
-    }
-    if (g->n_prims > 0 && (!g->prim_kind || !g->prim_index))
-    {
-        return Fail(BBG_ERR_INVALID_ARG, "geometry: prim_kind / prim_index missing");
-    }
-    if (g->n_triangles > 0 && (!g->tri_indices || !g->positions))
-    {
-        return Fail(BBG_ERR_INVALID_ARG, "geometry: triangles without indices or positions");
-    }
-    for (int32_t t = 0; t < 3 * g->n_triangles; ++t)
-    {
-        if (g->tri_indices[t] < 0 || g->tri_indices[t] >= g->n_vertices)
-        {
-            return Fail(BBG_ERR_INVALID_ARG, "geometry: triangle vertex %d out of range", g->tri_indices[t]);
-        }
-    }
-    for (int32_t i = 0; i < g->n_prims; ++i)
-    {
-        int32_t k = g->prim_kind[i], idx = g->prim_index[i];
-        bool ok = (k == BBG_PRIM_TRIANGLE && idx >= 0 && idx < g->n_triangles) ||
-                  (k == BBG_PRIM_SPHERE && idx >= 0 && idx < g->n_spheres && g->spheres);
-        if (!ok)
-        {
-            return Fail(BBG_ERR_INVALID_ARG, "geometry: primitive %d has kind %d index %d", i, k, idx);
-        }
-    }
-    return BBG_OK;
-}
 
 // Shading data (the reference Mesh arrays and shapes).
 bbg_status UploadShading(bbg_accel* a, const bbg_geometry* g)
@@ -379,7 +346,8 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     }
     else if (bvh)
     {
-        if (!bvh->nodes || !bvh->slot_prims || bvh->n_nodes <= 0 || bvh->n_slots != g->n_prims)
+        // A primitive may fill several slots (trees over split references).
+        if (!bvh->nodes || !bvh->slot_prims || bvh->n_nodes <= 0 || bvh->n_slots < g->n_prims)
         {
             return Fail(BBG_ERR_INVALID_ARG, "bvh: %d slots for %d primitives", bvh->n_slots, g->n_prims);
         }
@@ -641,6 +609,34 @@ bbg_status bbg_accel_create_device_build(const bbg_geometry* geometry, bbg_accel
     }
     *out = a;
     return BBG_OK;
+}
+
+bbg_status bbg_accel_create_split(const bbg_geometry* geometry, float budget, bbg_accel** out)
+{
+    if (!out || !(budget >= 0.0f) || budget > 64.0f)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_create_split: bad argument (budget in [0, 64])");
+    }
+    *out = nullptr;
+    BBG_TRY(CheckGeometry(geometry));
+    if (geometry->n_prims == 0)
+    {
+        return bbg_accel_create(geometry, nullptr, out);
+    }
+    std::vector<float> aabbs;
+    std::vector<int32_t> ref_prims;
+    BBG_TRY(SplitReferences(*geometry, budget, &aabbs, &ref_prims));
+    const int32_t n_refs = int32_t(ref_prims.size());
+    std::vector<bbg_bvh_node> nodes(2 * size_t(n_refs) - 1);
+    std::vector<int32_t> slots(static_cast<size_t>(n_refs));
+    int32_t n_nodes = 0;
+    BBG_TRY(BuildBvh(aabbs.data(), n_refs, nodes.data(), slots.data(), &n_nodes));
+    for (int32_t& s : slots)
+    {
+        s = ref_prims[size_t(s)];
+    }
+    const bbg_bvh tree{ n_nodes, nodes.data(), n_refs, slots.data() };
+    return bbg_accel_create(geometry, &tree, out);
 }
 
 bbg_status bbg_accel_create(const bbg_geometry* geometry, const bbg_bvh* bvh, bbg_accel** out)

@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <string>
+#include <vector>
 
 #ifdef __CUDACC__
 #define BBG_HD __host__ __device__ __forceinline__
@@ -103,6 +104,14 @@ bbg_status Fail(bbg_status s, const char* fmt, ...);
 // Reference-exact host computations.
 void PrimAabbs(const bbg_geometry& g, float* aabbs);
 bbg_status BuildBvh(const float* aabbs, int32_t n, bbg_bvh_node* nodes, int32_t* slots, int32_t* n_nodes);
+// Index and pointer checks of a geometry record (counts, vertex and
+// primitive references in range).
+bbg_status CheckGeometry(const bbg_geometry* g);
+// Reference splitting before the SAH build (see host_build.cpp): references
+// (box, primitive) for every primitive, with poorly filled triangle boxes
+// split up to `budget` extra references per primitive.
+bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<float>* ref_aabbs,
+                           std::vector<int32_t>* ref_prims);
 bbg_status ValidateBvh(const bbg_bvh_node* nodes, int32_t n_nodes, int32_t n_slots, int32_t n_prims,
                        const int32_t* slot_prims, int32_t* max_depth);
 void CameraFromSpec(const bbg_camera_spec& s, bbg_camera* out);

@@ -157,6 +157,274 @@ void PrimAabbs(const bbg_geometry& g, float* aabbs)
     }
 }
 
+bbg_status CheckGeometry(const bbg_geometry* g)
+{
+    if (!g || g->n_prims < 0 || g->n_vertices < 0 || g->n_triangles < 0 || g->n_spheres < 0)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "geometry: null or negative count");
+    }
+    if (g->n_prims > 0 && (!g->prim_kind || !g->prim_index))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "geometry: prim_kind / prim_index missing");
+    }
+    if (g->n_triangles > 0 && (!g->tri_indices || !g->positions))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "geometry: triangles without indices or positions");
+    }
+    for (int32_t t = 0; t < 3 * g->n_triangles; ++t)
+    {
+        if (g->tri_indices[t] < 0 || g->tri_indices[t] >= g->n_vertices)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "geometry: triangle vertex %d out of range", g->tri_indices[t]);
+        }
+    }
+    for (int32_t i = 0; i < g->n_prims; ++i)
+    {
+        int32_t k = g->prim_kind[i], idx = g->prim_index[i];
+        bool ok = (k == BBG_PRIM_TRIANGLE && idx >= 0 && idx < g->n_triangles) ||
+                  (k == BBG_PRIM_SPHERE && idx >= 0 && idx < g->n_spheres && g->spheres);
+        if (!ok)
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "geometry: primitive %d has kind %d index %d", i, k, idx);
+        }
+    }
+    return BBG_OK;
+}
+
+// ---------------------------------------------------------------- reference splitting
+// Early split clipping (Ernst & Greiner, "Early Split Clipping for Bounding
+// Volume Hierarchies", IEEE RT 2007): a triangle whose box it fills poorly
+// (long thin or diagonal triangles, the displaced spheres' slivers) makes the
+// tree's boxes overlap. Before the build, the reference whose box wastes the
+// most surface area (box area less twice the area of the triangle part it
+// holds) is split at the midpoint of its box's longest axis, each half
+// keeping the box of the triangle clipped to it, until the budget of extra
+// references is spent. Boxes are computed in double precision, rounded
+// outward to float and padded by 10 epsilon as Triangle::GetAABB pads
+// (src/geometry/triangle.cpp:40-51), so every part of a triangle lies inside
+// one of its references' boxes; a ray's closest hit is therefore found, and
+// a triangle split across leaves may be tested more than once (same result).
+
+namespace
+{
+
+struct SplitRef
+{
+    double lo[3], hi[3];
+    int32_t prim;
+};
+
+// Sutherland-Hodgman against one axis-aligned half-space.
+int ClipAxis(const double (*in)[3], int n, int axis, double m, bool keep_below, double (*out)[3])
+{
+    int k = 0;
+    for (int i = 0; i < n; ++i)
+    {
+        const double* a = in[i];
+        const double* b = in[(i + 1) % n];
+        bool ia = keep_below ? a[axis] <= m : a[axis] >= m;
+        bool ib = keep_below ? b[axis] <= m : b[axis] >= m;
+        if (ia)
+        {
+            std::memcpy(out[k++], a, sizeof(double) * 3);
+        }
+        if (ia != ib)
+        {
+            double t = (m - a[axis]) / (b[axis] - a[axis]);
+            for (int c = 0; c < 3; ++c)
+            {
+                out[k][c] = a[c] + t * (b[c] - a[c]);
+            }
+            out[k][axis] = m;
+            ++k;
+        }
+    }
+    return k;
+}
+
+double PolygonArea(const double (*p)[3], int n)
+{
+    double c[3] = { 0, 0, 0 };
+    for (int i = 1; i + 1 < n; ++i)
+    {
+        double u[3], v[3];
+        for (int k = 0; k < 3; ++k)
+        {
+            u[k] = p[i][k] - p[0][k];
+            v[k] = p[i + 1][k] - p[0][k];
+        }
+        c[0] += u[1] * v[2] - u[2] * v[1];
+        c[1] += u[2] * v[0] - u[0] * v[2];
+        c[2] += u[0] * v[1] - u[1] * v[0];
+    }
+    return 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
+}
+
+// Box (and area) of the triangle clipped to [lo, hi]; false if nothing is left.
+bool ClippedBox(const double tri[3][3], const double lo[3], const double hi[3], double out_lo[3], double out_hi[3],
+                double* area)
+{
+    double a[12][3], b[12][3];
+    int n = 3;
+    std::memcpy(a, tri, sizeof(double) * 9);
+    for (int axis = 0; axis < 3 && n > 0; ++axis)
+    {
+        n = ClipAxis(a, n, axis, lo[axis], false, b);
+        n = ClipAxis(b, n, axis, hi[axis], true, a);
+    }
+    if (n == 0)
+    {
+        return false;
+    }
+    *area = PolygonArea(a, n);
+    for (int c = 0; c < 3; ++c)
+    {
+        out_lo[c] = out_hi[c] = a[0][c];
+    }
+    for (int i = 1; i < n; ++i)
+    {
+        for (int c = 0; c < 3; ++c)
+        {
+            out_lo[c] = std::min(out_lo[c], a[i][c]);
+            out_hi[c] = std::max(out_hi[c], a[i][c]);
+        }
+    }
+    // The clipped polygon lies inside the box it was clipped to.
+    for (int c = 0; c < 3; ++c)
+    {
+        out_lo[c] = std::max(out_lo[c], lo[c]);
+        out_hi[c] = std::min(out_hi[c], hi[c]);
+    }
+    return true;
+}
+
+double BoxArea(const double lo[3], const double hi[3])
+{
+    double d0 = hi[0] - lo[0], d1 = hi[1] - lo[1], d2 = hi[2] - lo[2];
+    return 2 * (d0 * d1 + d1 * d2 + d2 * d0);
+}
+
+float RoundDown(double v)
+{
+    float f = float(v);
+    return double(f) > v ? std::nextafter(f, -std::numeric_limits<float>::infinity()) : f;
+}
+
+float RoundUp(double v)
+{
+    float f = float(v);
+    return double(f) < v ? std::nextafter(f, std::numeric_limits<float>::infinity()) : f;
+}
+
+} // namespace
+
+bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<float>* ref_aabbs,
+                           std::vector<int32_t>* ref_prims)
+{
+    const int32_t n = g.n_prims;
+    std::vector<float> prim_aabbs(6 * size_t(n));
+    PrimAabbs(g, prim_aabbs.data());
+    const int64_t max_refs = std::min<int64_t>(int64_t(n) + int64_t(double(budget) * n), (int64_t(1) << 31) - 1);
+    std::vector<SplitRef> refs;
+    refs.reserve(size_t(max_refs));
+    // Max-heap on wasted box area over the splittable (triangle) references.
+    std::vector<std::pair<double, int32_t>> heap;
+    for (int32_t i = 0; i < n; ++i)
+    {
+        SplitRef r;
+        r.prim = i;
+        if (g.prim_kind[i] == BBG_PRIM_TRIANGLE)
+        {
+            const int32_t* v = g.tri_indices + 3 * size_t(g.prim_index[i]);
+            double tri[3][3];
+            for (int c = 0; c < 3; ++c)
+            {
+                for (int k = 0; k < 3; ++k)
+                {
+                    tri[k][c] = g.positions[3 * size_t(v[k]) + c];
+                }
+                r.lo[c] = std::min(std::min(tri[0][c], tri[1][c]), tri[2][c]);
+                r.hi[c] = std::max(std::max(tri[0][c], tri[1][c]), tri[2][c]);
+            }
+            heap.emplace_back(BoxArea(r.lo, r.hi) - 2 * PolygonArea(tri, 3), int32_t(refs.size()));
+        }
+        refs.push_back(r);
+    }
+    std::make_heap(heap.begin(), heap.end());
+    while (!heap.empty() && int64_t(refs.size()) < max_refs)
+    {
+        std::pop_heap(heap.begin(), heap.end());
+        int32_t ri = heap.back().second;
+        heap.pop_back();
+        SplitRef r = refs[size_t(ri)];
+        int axis = 0;
+        for (int c = 1; c < 3; ++c)
+        {
+            if (r.hi[c] - r.lo[c] > r.hi[axis] - r.lo[axis])
+            {
+                axis = c;
+            }
+        }
+        const double m = 0.5 * (r.lo[axis] + r.hi[axis]);
+        if (!(m > r.lo[axis] && m < r.hi[axis]))
+        {
+            continue; // too small to split
+        }
+        const int32_t* v = g.tri_indices + 3 * size_t(g.prim_index[r.prim]);
+        double tri[3][3];
+        for (int k = 0; k < 3; ++k)
+        {
+            for (int c = 0; c < 3; ++c)
+            {
+                tri[k][c] = g.positions[3 * size_t(v[k]) + c];
+            }
+        }
+        double llo[3], lhi[3], rlo[3], rhi[3];
+        std::memcpy(llo, r.lo, sizeof(llo));
+        std::memcpy(lhi, r.hi, sizeof(lhi));
+        std::memcpy(rlo, r.lo, sizeof(rlo));
+        std::memcpy(rhi, r.hi, sizeof(rhi));
+        lhi[axis] = m;
+        rlo[axis] = m;
+        SplitRef left{}, right{};
+        left.prim = right.prim = r.prim;
+        double al = 0, ar = 0;
+        bool hl = ClippedBox(tri, llo, lhi, left.lo, left.hi, &al);
+        bool hr = ClippedBox(tri, rlo, rhi, right.lo, right.hi, &ar);
+        if (!hl || !hr)
+        {
+            continue; // the box was not tight on this axis: keep the reference whole
+        }
+        refs[size_t(ri)] = left;
+        heap.emplace_back(BoxArea(left.lo, left.hi) - 2 * al, ri);
+        std::push_heap(heap.begin(), heap.end());
+        heap.emplace_back(BoxArea(right.lo, right.hi) - 2 * ar, int32_t(refs.size()));
+        std::push_heap(heap.begin(), heap.end());
+        refs.push_back(right);
+    }
+    // Boxes: unsplit references keep the primitive's own box bit for bit.
+    const float pad = kEps * 10;
+    ref_aabbs->resize(6 * refs.size());
+    ref_prims->resize(refs.size());
+    for (size_t i = 0; i < refs.size(); ++i)
+    {
+        const SplitRef& r = refs[i];
+        (*ref_prims)[i] = r.prim;
+        float* box = ref_aabbs->data() + 6 * i;
+        if (g.prim_kind[r.prim] != BBG_PRIM_TRIANGLE)
+        {
+            std::memcpy(box, prim_aabbs.data() + 6 * size_t(r.prim), 6 * sizeof(float));
+            continue;
+        }
+        for (int c = 0; c < 3; ++c)
+        {
+            box[c] = RoundDown(r.lo[c]) - pad;
+            box[3 + c] = RoundUp(r.hi[c]) + pad;
+        }
+    }
+    return BBG_OK;
+}
+
 // ---------------------------------------------------------------- SAH build
 // BVH::BuildRecursive (src/accel/bvh.cpp:56-271) and FlattenBVH (:273-297).
 // The same std::partition / std::nth_element calls run on the same element
@@ -837,6 +1105,36 @@ bbg_status bbg_bvh_build(const float* prim_aabbs, int32_t n_prims, bbg_bvh_node*
         return bbg::Fail(BBG_ERR_INVALID_ARG, "bbg_bvh_build: null buffer or n_prims <= 0");
     }
     return bbg::BuildBvh(prim_aabbs, n_prims, nodes_out, slot_prims_out, n_nodes_out);
+}
+
+bbg_status bbg_split_references(const bbg_geometry* g, float budget, int32_t capacity, float* aabbs_out,
+                                int32_t* prims_out, int32_t* n_out)
+{
+    if (!g || !aabbs_out || !prims_out || !n_out || !(budget >= 0.0f) || budget > 64.0f || capacity < 0)
+    {
+        return bbg::Fail(BBG_ERR_INVALID_ARG, "bbg_split_references: bad argument");
+    }
+    bbg_status st = bbg::CheckGeometry(g);
+    if (st != BBG_OK)
+    {
+        return st;
+    }
+    std::vector<float> aabbs;
+    std::vector<int32_t> prims;
+    st = bbg::SplitReferences(*g, budget, &aabbs, &prims);
+    if (st != BBG_OK)
+    {
+        return st;
+    }
+    if (int64_t(prims.size()) > capacity)
+    {
+        return bbg::Fail(BBG_ERR_INVALID_ARG, "bbg_split_references: %zu references exceed the capacity %d",
+                         prims.size(), capacity);
+    }
+    std::memcpy(aabbs_out, aabbs.data(), aabbs.size() * sizeof(float));
+    std::memcpy(prims_out, prims.data(), prims.size() * sizeof(int32_t));
+    *n_out = int32_t(prims.size());
+    return BBG_OK;
 }
 
 bbg_status bbg_prim_aabbs(const bbg_geometry* g, float* aabbs_out)

@@ -69,6 +69,18 @@ def prim_aabbs(scene):
     return out
 
 
+def split_references(scene, budget):
+    """bbg_split_references: (reference boxes (m, 6), their primitives (m,))."""
+    g = scene.geometry()
+    cap = int(scene.n_prims * (1 + budget)) + 1
+    boxes = np.zeros((cap, 6), np.float32)
+    prims = np.zeros(cap, np.int32)
+    n = C.c_int32()
+    check(get_lib().bbg_split_references(C.byref(g), float(budget), cap, _p(boxes), _p(prims), C.byref(n)),
+          "bbg_split_references")
+    return boxes[:n.value].copy(), prims[:n.value].copy()
+
+
 def camera(spec):
     out = abi.Camera()
     check(get_lib().bbg_camera_perspective(C.byref(spec), C.byref(out)), "bbg_camera_perspective")
@@ -82,13 +94,20 @@ NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("offset", "<i4")
 class GpuAccel:
     """The GPU accel beside the reference BVH (bbg_accel_*)."""
 
-    def __init__(self, scene, bvh=None, device_build=False):
+    def __init__(self, scene, bvh=None, device_build=False, split=None):
+        """bvh: the reference's tree (nodes, slots); device_build: the linear BVH
+        built on the device; split: extra references per primitive for the
+        split-reference SAH build (bbg_accel_create_split)."""
         self.scene = scene
         self._g = scene.geometry()
         self.h = C.c_void_p()
         if device_build:
             check(get_lib().bbg_accel_create_device_build(C.byref(self._g), C.byref(self.h)),
                   "bbg_accel_create_device_build")
+            return
+        if split is not None:
+            check(get_lib().bbg_accel_create_split(C.byref(self._g), float(split), C.byref(self.h)),
+                  "bbg_accel_create_split")
             return
         bvh_arg = None
         if bvh is not None:

@@ -162,8 +162,25 @@ bbg_status bbg_prim_aabbs(const bbg_geometry* geometry, float* aabbs_out);
 
 /* Uploads geometry and a tree to device 0. bvh == NULL builds the tree with
  * bbg_bvh_build. The tree is validated (child and slot ranges, no cycles)
- * before upload. */
+ * before upload; it has at least one slot per primitive (the reference's
+ * tree exactly one; a primitive may fill several). */
 bbg_status bbg_accel_create(const bbg_geometry* geometry, const bbg_bvh* bvh, bbg_accel** out);
+
+/* Uploads geometry with a tree built over split references (early split
+ * clipping): triangles whose boxes they fill poorly are split along the
+ * longest axis of their box, each part keeping the box of the triangle
+ * clipped to it (rounded outward, padded like Triangle::GetAABB), up to
+ * budget extra references per primitive (budget in [0, 64]; 0 builds the
+ * reference's own tree), then bbg_bvh_build runs over the references. A
+ * triangle may sit in several leaves; closest hits agree with BVH::Intersect
+ * except between primitives hit at exactly the same t. */
+bbg_status bbg_accel_create_split(const bbg_geometry* geometry, float budget, bbg_accel** out);
+
+/* The references bbg_accel_create_split builds over (host only): their boxes
+ * (6 floats each) and primitives, at most n_prims * (1 + budget) of them;
+ * capacity is the room in the output arrays. */
+bbg_status bbg_split_references(const bbg_geometry* geometry, float budget, int32_t capacity, float* aabbs_out,
+                                int32_t* prims_out, int32_t* n_out);
 
 /* Uploads geometry and builds the tree on the device: a linear BVH (Morton
  * codes of the primitive boxes' centres, radix sort, the binary radix tree

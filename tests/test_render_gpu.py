@@ -215,6 +215,19 @@ def test_point_and_sphere_area_lights_and_passthrough(oracle):
     check_paths("lights_passthrough", film.path_L, ref_L)
 
 
+def test_split_reference_tree_paths(oracle):
+    """Per-path parity of renders over the split-reference tree."""
+    scene = scenes.cornell_icosphere(levels=4, width=48, height=48, spp=8, max_bounces=16)
+    rs = oracle.RefScene(scene)
+    rs.make_integrator()
+    scene.positions, scene.normals, scene.tangents, scene.uvs = rs.mesh_arrays()
+    acc = lib.GpuAccel(scene, split=1.0)
+    integ = lib.GpuPathIntegrator(acc, scene)
+    film = integ.render(path_L=True)
+    ref_L, _ = rs.trace_paths()
+    check_paths("cornell, split-reference tree", film.path_L, ref_L)
+
+
 def test_device_built_tree_paths(oracle):
     """Path tracing over the device-built linear BVH (over the reference's
     mesh arrays, as the drop-in uploads them): the per-path radiance bar holds,

@@ -190,6 +190,40 @@ def classify_against_brute_force(rs, rays, prim, t, ref_prim, ref_t):
     return ties, leaks_ref, leaks_dev, unexplained
 
 
+def test_split_reference_tree_parity(oracle):
+    """The SAH tree over split references (bbg_accel_create_split): closest hits
+    agree with the reference BVH except near-ties, any-hit agrees, in both
+    layouts."""
+    cornell = scenes.cornell_icosphere(levels=6, width=8, height=8)
+    rng = np.random.default_rng(9)
+    n = 200_000
+    rays = np.zeros((n, 8), np.float32)
+    rays[:, :3] = rng.uniform(-0.95, 0.95, (n, 3))
+    d = rng.normal(size=(n, 3))
+    rays[:, 3:6] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    rays[:, 6], rays[:, 7] = 1e-4, np.inf
+    anyq = rays.copy()
+    anyq[:, 7] = rng.uniform(0.05, 2.0, n).astype(np.float32)
+    soup = scenes.triangle_soup(100_000, seed=5)
+    srays, sany = scenes.soup_rays(1 << 18, seed=6)
+    for scene, cl, an in ((cornell, rays, anyq), (soup, srays, sany)):
+        rs = oracle.RefScene(scene)
+        acc = lib.GpuAccel(scene, split=1.0)
+        ref_prim, ref_t, _ = rs.intersect(cl)
+        ref_occ, _ = rs.intersect_any(an)
+        for mode in (abi.BBG_TRAVERSAL_WIDE, abi.BBG_TRAVERSAL_ORDERED):
+            acc.set_traversal(mode)
+            prim, t, _, _ = acc.intersect(cl)
+            ties, leaks_ref, leaks_dev, unexplained = classify_against_brute_force(rs, cl, prim, t, ref_prim, ref_t)
+            print(f"split-reference tree, {scene.name}: {ties} near-ties, {leaks_ref} + {leaks_dev} leaks")
+            assert not unexplained, unexplained[:5]
+            assert leaks_ref + leaks_dev <= 1e-3 * len(cl)
+            same = (prim == ref_prim) & (ref_prim >= 0)
+            assert np.array_equal(t[same].view(np.uint32), ref_t[same].view(np.uint32))
+            assert np.array_equal(acc.intersect_any(an), ref_occ)
+        acc.close()
+
+
 def test_device_built_tree_parity(oracle):
     """The linear BVH built on the device: closest hits agree with the
     reference BVH except near-ties (or rays that one tree's boxes would let
