@@ -220,6 +220,7 @@ def run_pt(args, barrier, world):
     cam = lib.camera(scene.camera)
     params = abi.RenderParams()
     params.spp, params.seed, params.wave_paths, params.use_graph = 64, 0, args.pt_wave, 1
+    params.shade_order = abi.BBG_SHADE_QUEUE if args.shade_order == "queue" else abi.BBG_SHADE_SORTED
     n_pix = res * res
     rgb = torch.empty((n_pix, 3), dtype=torch.float32, device="cuda")
     cnt = torch.empty(n_pix, dtype=torch.int32, device="cuda")
@@ -494,6 +495,8 @@ def main():
     ap.add_argument("--pt-res", type=int, default=1024)
     ap.add_argument("--pt-split", type=float, default=None,
                     help="path tracing: build the tree over split references with this budget per primitive")
+    ap.add_argument("--shade-order", default="sorted", choices=["sorted", "queue"],
+                    help="path tracing: shade each level grouped by material kind, or in queue order")
     ap.add_argument("--pt-split-report", type=float, default=3.0,
                     help="path tracing: also time the frame over a split-reference tree of this budget (0: skip)")
     ap.add_argument("--pt-steps", type=int, default=3)

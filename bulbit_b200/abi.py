@@ -36,6 +36,8 @@ BBG_MAT_METALLIC_ROUGHNESS = 3
 BBG_TRAVERSAL_ORDERED = 0
 BBG_TRAVERSAL_REFERENCE = 1
 BBG_TRAVERSAL_WIDE = 2
+BBG_SHADE_SORTED = 0
+BBG_SHADE_QUEUE = 1
 
 BBG_FILTER_BOX = 0
 BBG_FILTER_TENT = 1
@@ -113,7 +115,8 @@ class RenderParams(C.Structure):
                 ("use_graph", C.c_int32), ("light_alias", C.c_int32), ("guide", C.c_void_p),
                 ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float),
                 ("guide_select", C.c_float), ("guide_steps", C.c_int32),
-                ("sampler", C.c_int32), ("x_samples", C.c_int32), ("jitter", C.c_int32)]
+                ("sampler", C.c_int32), ("x_samples", C.c_int32), ("jitter", C.c_int32),
+                ("shade_order", C.c_int32)]
 
 
 class Tuning(C.Structure):

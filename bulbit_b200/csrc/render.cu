@@ -90,7 +90,16 @@ struct WaveDev
     unsigned long long* stats; // closest rays, shadow rays
     const int64_t* wave;       // [0] first path, [1] paths in wave
     int32_t* dim;              // stratified sampler: next dimension per slot
+    // Shading order (null sorted: queue order): each level's queue sorted by
+    // shading kind into `sorted` through per-position keys and kind counts.
+    int32_t* sorted;
+    uint8_t* keys;
+    int32_t* sort_counts; // [0, kShadeKinds) totals, [kShadeKinds, 2 kShadeKinds) cursors
 };
+
+// Shading kinds a level's paths are grouped by: escaped, no material, then
+// each material type with and without energy compensation.
+constexpr int kShadeKinds = 2 + 2 * 4;
 
 constexpr int32_t kSpecularBit = 1 << 16;
 constexpr int32_t kAnyNonSpecularBit = 1 << 17;
@@ -636,7 +645,7 @@ __device__ __forceinline__ int32_t SampleLight(const SceneDev& s, float u, float
 template <class Scenes>
 __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) ShadeKernel(Scenes sc, WaveDev w, int parity)
 {
-    const int32_t* q = w.queue[parity];
+    const int32_t* q = w.sorted ? w.sorted : w.queue[parity];
     int32_t* q_next = w.queue[parity ^ 1];
     const int32_t n = w.counts[parity];
 
@@ -1390,6 +1399,112 @@ __global__ void ResetKernel(WaveDev w, int parity)
     w.counts[3] = 0;
     w.counts[4] = 0;
     w.counts[5] = 0;
+    if (w.sorted)
+    {
+        for (int k = 0; k < 2 * kShadeKinds; ++k)
+        {
+            w.sort_counts[k] = 0;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- shading order
+
+template <class Scenes>
+__device__ __forceinline__ int32_t ShadeKind(const Scenes& sc, const WaveDev& w, int32_t slot)
+{
+    int32_t prim = __float_as_int(w.hit[slot].x);
+    if (prim < 0)
+    {
+        return 0;
+    }
+    const SceneDev& s = sc.Scene(w.flags[slot] >> kSceneShift);
+    int32_t m = s.prim_info[prim].z;
+    if (m < 0)
+    {
+        return 1;
+    }
+    const MaterialDev& md = s.materials[m];
+    return 2 + 2 * min(max(md.type, 0), 3) + (md.ms ? 1 : 0);
+}
+
+// Counting sort of a level's queue by shading kind, pass 1: the kind of every
+// queued path (read from its hit) and the kinds' totals (block-aggregated).
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock) ShadeKindsKernel(Scenes sc, WaveDev w, int parity)
+{
+    __shared__ int32_t bc[kShadeKinds];
+    const int32_t* q = w.queue[parity];
+    const int32_t n = w.counts[parity];
+    for (int32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock)
+    {
+        if (threadIdx.x < kShadeKinds)
+        {
+            bc[threadIdx.x] = 0;
+        }
+        __syncthreads();
+        const int32_t j = base + int32_t(threadIdx.x);
+        if (j < n)
+        {
+            int32_t k = ShadeKind(sc, w, q[j]);
+            w.keys[j] = uint8_t(k);
+            atomicAdd(&bc[k], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < kShadeKinds && bc[threadIdx.x] > 0)
+        {
+            atomicAdd(&w.sort_counts[threadIdx.x], bc[threadIdx.x]);
+        }
+        __syncthreads();
+    }
+}
+
+// Pass 2: every block reserves, per kind, a range after the kinds before it
+// (the totals' prefix) and writes its paths' slots there; the order inside a
+// kind is arbitrary (paths do not depend on one another).
+__global__ void __launch_bounds__(kBlock) ShadeScatterKernel(WaveDev w, int parity)
+{
+    __shared__ int32_t bc[kShadeKinds], boff[kShadeKinds], start[kShadeKinds];
+    const int32_t* q = w.queue[parity];
+    const int32_t n = w.counts[parity];
+    if (threadIdx.x == 0)
+    {
+        int32_t acc = 0;
+        for (int k = 0; k < kShadeKinds; ++k)
+        {
+            start[k] = acc;
+            acc += w.sort_counts[k];
+        }
+    }
+    for (int32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock)
+    {
+        if (threadIdx.x < kShadeKinds)
+        {
+            bc[threadIdx.x] = 0;
+        }
+        __syncthreads();
+        const int32_t j = base + int32_t(threadIdx.x);
+        int32_t k = 0, local = 0;
+        if (j < n)
+        {
+            k = w.keys[j];
+            local = atomicAdd(&bc[k], 1);
+        }
+        __syncthreads();
+        if (threadIdx.x < kShadeKinds)
+        {
+            boff[threadIdx.x] =
+                bc[threadIdx.x] > 0 ? start[threadIdx.x] + atomicAdd(&w.sort_counts[kShadeKinds + threadIdx.x],
+                                                                     bc[threadIdx.x])
+                                    : 0;
+        }
+        __syncthreads();
+        if (j < n)
+        {
+            w.sorted[boff[k] + local] = q[j];
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------- film
@@ -1646,6 +1761,11 @@ struct bbg_integrator
     bbg_guide* graph_guide_handle = nullptr;
     float graph_guide_lr = 0;
     int graph_shape = -1;
+    bool graph_shade_sort = false;
+    // Shading order of the current render (params.shade_order).
+    bool shade_sort = true;
+    DevBuf<int32_t> sorted, sort_counts;
+    DevBuf<uint8_t> keys;
     // Launch shape of the traversal passes (index into kShapes) and wave size
     // for renders that do not name one (0: 2^22 paths); set by the autotuner.
     int32_t shape = 0;
@@ -1736,6 +1856,9 @@ struct bbg_integrator
         w.stats = stats.p;
         w.wave = wave.p;
         w.dim = dim.p;
+        w.sorted = shade_sort ? sorted.p : nullptr;
+        w.keys = keys.p;
+        w.sort_counts = sort_counts.p;
         return w;
     }
 
@@ -1750,11 +1873,14 @@ struct bbg_integrator
         }
         rng.reset();
         BBG_TRY(rng.alloc(m));
-        for (auto* b : { &flags, &queue0, &queue1, &dim })
+        for (auto* b : { &flags, &queue0, &queue1, &dim, &sorted })
         {
             b->reset();
             BBG_TRY(b->alloc(m));
         }
+        keys.reset();
+        BBG_TRY(keys.alloc(m));
+        BBG_TRY(sort_counts.alloc(2 * kShadeKinds));
         capacity = n;
         return BBG_OK;
     }
@@ -1767,7 +1893,7 @@ namespace
 template <class Scenes>
 struct GridsT
 {
-    int raygen, closest[2 * kNumShapes], shade, shadow[2 * kNumShapes], film, shade_a, shade_b;
+    int raygen, closest[2 * kNumShapes], shade, shadow[2 * kNumShapes], film, shade_a, shade_b, kinds, scatter;
     GridsT()
     {
         raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel<Scenes>), kBlock);
@@ -1779,6 +1905,8 @@ struct GridsT
         film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel<Scenes>), kBlock);
         shade_a = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeA), kBlock);
         shade_b = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeB), kBlock);
+        kinds = PersistentGrid(reinterpret_cast<const void*>(ShadeKindsKernel<Scenes>), kBlock);
+        scatter = PersistentGrid(reinterpret_cast<const void*>(ShadeScatterKernel), kBlock);
     }
     template <int K>
     void Shape()
@@ -1880,6 +2008,11 @@ bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, co
     }
     else
     {
+        if (w.sorted)
+        {
+            ShadeKindsKernel<<<gr.kinds, kBlock, 0, st>>>(one, w, parity);
+            ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
+        }
         ShadeKernel<<<gr.shade, kBlock, 0, st>>>(one, w, parity);
     }
     LaunchTrace(shape, gr, one, w, parity, true, st);
@@ -1942,6 +2075,11 @@ bool SameFilm(const FilmDev& a, const FilmDev& b)
 // filter's table (once per sigma and extent) for MakeSceneDev.
 bbg_status PrepareSamplerAndFilter(bbg_integrator* I, const bbg_camera* cam, const bbg_render_params* p)
 {
+    if (p->shade_order != BBG_SHADE_SORTED && p->shade_order != BBG_SHADE_QUEUE)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "shade_order %d", p->shade_order);
+    }
+    I->shade_sort = p->shade_order == BBG_SHADE_SORTED;
     if (p->sampler != BBG_SAMPLER_INDEPENDENT &&
         (p->sampler != BBG_SAMPLER_STRATIFIED || p->x_samples <= 0 || p->spp % p->x_samples != 0))
     {
@@ -2102,7 +2240,8 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     if (use_graph && (!I->graph || I->graph_capacity != wave_paths || I->graph_iterations != iterations ||
                       !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f) ||
                       I->graph_guide_handle != gc.guide || !SameGuide(I->graph_guide, gc.dev) ||
-                      I->graph_guide_lr != gc.lr || I->graph_shape != trace_shape))
+                      I->graph_guide_lr != gc.lr || I->graph_shape != trace_shape ||
+                      I->graph_shade_sort != I->shade_sort))
     {
         if (I->graph)
         {
@@ -2128,6 +2267,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         I->graph_guide_handle = gc.guide;
         I->graph_guide_lr = gc.lr;
         I->graph_shape = trace_shape;
+        I->graph_shade_sort = I->shade_sort;
     }
 
     // Device time of the render itself: buffer set-up and graph capture
@@ -2361,6 +2501,11 @@ bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const Wa
 {
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
     LaunchTrace(shape, gr, t, w, parity, false, st);
+    if (w.sorted)
+    {
+        ShadeKindsKernel<<<gr.kinds, kBlock, 0, st>>>(t, w, parity);
+        ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
+    }
     ShadeKernel<<<gr.shade, kBlock, 0, st>>>(t, w, parity);
     LaunchTrace(shape, gr, t, w, parity, true, st);
     return BBG_OK;
@@ -2396,6 +2541,7 @@ struct bbg_batch
     int graph_iterations = -1;
     bbg::SceneTable graph_table{};
     int graph_shape = -1;
+    bool graph_shade_sort = false;
     int32_t shape = 0;      // as bbg_integrator::shape, for the batch
     int64_t tuned_wave = 0; // as bbg_integrator::tuned_wave
 };
@@ -2465,6 +2611,11 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
 
     bbg_integrator* E = &B->engine;
     cudaStream_t st = E->stream;
+    if (params[0].shade_order != BBG_SHADE_SORTED && params[0].shade_order != BBG_SHADE_QUEUE)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: shade_order %d", params[0].shade_order);
+    }
+    E->shade_sort = params[0].shade_order == BBG_SHADE_SORTED;
     BBG_TRY(B->scenes.upload(B->host_scenes.data(), B->host_scenes.size(), st));
     BBG_TRY(B->films.upload(B->host_films.data(), B->host_films.size(), st));
     BBG_TRY(B->pixel_start.upload(B->host_pixel_start.data(), B->host_pixel_start.size(), st));
@@ -2490,7 +2641,8 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     const int trace_shape = B->shape + (all_wide ? kNumShapes : 0);
     const bool use_graph = params[0].use_graph != 0;
     if (use_graph && (!E->graph || B->graph_capacity != wave_paths || B->graph_iterations != iterations ||
-                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != trace_shape))
+                      std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != trace_shape ||
+                      B->graph_shade_sort != E->shade_sort))
     {
         if (E->graph)
         {
@@ -2512,6 +2664,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         B->graph_iterations = iterations;
         B->graph_table = table;
         B->graph_shape = trace_shape;
+        B->graph_shade_sort = E->shade_sort;
     }
 
     BBG_CUDA(cudaMemsetAsync(E->stats.p, 0, 2 * sizeof(unsigned long long), st));

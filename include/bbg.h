@@ -404,12 +404,23 @@ typedef struct bbg_render_params
                              seed), src/sampler/stratified_sampler.cpp */
     int32_t x_samples;    /* stratified: strata along x (spp must be a multiple) */
     int32_t jitter;       /* stratified: jitter within strata */
+    int32_t shade_order;  /* BBG_SHADE_SORTED (0): each bounce level's paths are
+                             shaded grouped by material kind (a counting sort
+                             of the level's queue); BBG_SHADE_QUEUE: in queue
+                             order. Results are identical; guided renders shade
+                             in queue order. */
 } bbg_render_params;
 
 enum
 {
     BBG_SAMPLER_INDEPENDENT = 0,
     BBG_SAMPLER_STRATIFIED = 1
+};
+
+enum
+{
+    BBG_SHADE_SORTED = 0,
+    BBG_SHADE_QUEUE = 1
 };
 
 /* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields

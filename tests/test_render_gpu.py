@@ -260,7 +260,10 @@ def test_graph_and_wave_size_do_not_change_results():
     a = integ.render(path_L=True, use_graph=True)
     b = integ.render(path_L=True, use_graph=False, wave_paths=1000)
     c = integ.render(path_L=True, use_graph=True, wave_paths=4 * 7)
+    # shading in queue order instead of grouped by material kind
+    d = integ.render(path_L=True, use_graph=True, shade_order=abi.BBG_SHADE_QUEUE)
     assert np.array_equal(a.path_L, b.path_L) and np.array_equal(a.path_L, c.path_L)
+    assert np.array_equal(a.path_L, d.path_L) and np.array_equal(a.rgb_sum, d.rgb_sum)
     assert np.array_equal(a.rgb_sum, c.rgb_sum) and np.array_equal(a.count, b.count)
     assert a.stats.closest_rays > 40 * 30 * 4 and a.stats.shadow_rays > 0
 
