@@ -24,7 +24,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-prec-div=true", "-prec-sqrt=true",
                      "-std=c++20", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC]
-CXX_FLAGS = ["-O2", "-std=c++20", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
+CXX_FLAGS = ["-O2", "-std=c++20", "-fPIC", "-pthread", "-I" + INCLUDE, "-I" + CSRC,
              "-I" + os.path.join(CUDA_HOME, "include")]
 
 CU_SOURCES = ["accel.cu", "render.cu", "noalloc.cu", "guide.cu", "lbvh.cu"]
@@ -70,7 +70,7 @@ def build(verbose=False, ptxas_info=False):
             out.append(text)
     if jobs or not os.path.exists(LIB):
         tmp = LIB + ".tmp"
-        _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs)
+        _run([NVCC] + ARCH + ["-shared", "-o", tmp] + objs + ["-lpthread"])
         shutil.move(tmp, LIB)
     if verbose:
         print("\n".join(o for o in out if o.strip()))

@@ -15,6 +15,7 @@
 #include <cstring>
 #include <limits>
 #include <span>
+#include <thread>
 #include <vector>
 
 namespace bbg
@@ -432,7 +433,11 @@ bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<floa
 // identical; leaves take their slots in depth-first order (the reference's
 // single-threaded order; above 64Ki primitives it builds the two halves of a
 // node concurrently, which permutes whole leaves inside the slot array but not
-// the tree).
+// the tree). Here too the halves of nodes above 64Ki primitives are built on
+// separate threads (a few levels deep): a node's partition touches only its
+// own span, and its right half's leaves start at a slot known in advance (the
+// node's first slot + the left half's size), so the tree and the depth-first
+// slot order are the same as single-threaded.
 
 namespace
 {
@@ -450,18 +455,18 @@ struct BuildNode
     int32_t child1 = -1, child2 = -1;
 };
 
+constexpr size_t kParallelBuildSpan = size_t(1) << 16;
+
 struct Builder
 {
     std::vector<BuildNode> nodes;
-    std::vector<int32_t> ordered;
-    int32_t ordered_offset = 0;
+    int32_t* ordered = nullptr; // slot -> primitive, shared by the threads (disjoint ranges)
+    int parallel_levels = 0;    // levels of the recursion that may still fork a thread
     bool too_many_in_leaf = false;
 
-    int32_t MakeLeaf(std::span<BuildPrim> span, const Box& bounds)
+    int32_t MakeLeaf(std::span<BuildPrim> span, const Box& bounds, int32_t offset)
     {
         int32_t count = int32_t(span.size());
-        int32_t offset = ordered_offset;
-        ordered_offset += count;
         for (int32_t i = 0; i < count; ++i)
         {
             ordered[offset + i] = int32_t(span[i].index);
@@ -478,7 +483,8 @@ struct Builder
         return int32_t(nodes.size() - 1);
     }
 
-    int32_t Build(std::span<BuildPrim> span)
+    // Builds the subtree over span; its leaves fill slots from slot_base on.
+    int32_t Build(std::span<BuildPrim> span, int32_t slot_base, int depth = 0)
     {
         int32_t primitive_count = int32_t(span.size());
 
@@ -490,7 +496,7 @@ struct Builder
 
         if (span_bounds.SurfaceArea() == 0 || primitive_count == 1)
         {
-            return MakeLeaf(span, span_bounds);
+            return MakeLeaf(span, span_bounds, slot_base);
         }
 
         Box centroid_bounds;
@@ -513,7 +519,7 @@ struct Builder
 
         if (extent == 0)
         {
-            return MakeLeaf(span, span_bounds);
+            return MakeLeaf(span, span_bounds, slot_base);
         }
 
         int32_t mid;
@@ -593,14 +599,41 @@ struct Builder
             }
             else
             {
-                return MakeLeaf(span, span_bounds);
+                return MakeLeaf(span, span_bounds, slot_base);
             }
         }
 
         int32_t self = int32_t(nodes.size());
         nodes.push_back(BuildNode{});
-        int32_t c1 = Build(span.subspan(0, mid));
-        int32_t c2 = Build(span.subspan(mid));
+        int32_t c1, c2;
+        if (depth < parallel_levels && span.size() > kParallelBuildSpan)
+        {
+            Builder right;
+            right.ordered = ordered;
+            right.parallel_levels = parallel_levels;
+            int32_t right_root = -1;
+            std::thread t([&] { right_root = right.Build(span.subspan(size_t(mid)), slot_base + mid, depth + 1); });
+            c1 = Build(span.subspan(0, size_t(mid)), slot_base, depth + 1);
+            t.join();
+            // Splice the right subtree's nodes after this builder's.
+            const int32_t off = int32_t(nodes.size());
+            for (BuildNode bn : right.nodes)
+            {
+                if (bn.count == 0)
+                {
+                    bn.child1 += off;
+                    bn.child2 += off;
+                }
+                nodes.push_back(bn);
+            }
+            c2 = right_root + off;
+            too_many_in_leaf = too_many_in_leaf || right.too_many_in_leaf;
+        }
+        else
+        {
+            c1 = Build(span.subspan(0, size_t(mid)), slot_base, depth + 1);
+            c2 = Build(span.subspan(size_t(mid)), slot_base + mid, depth + 1);
+        }
         BuildNode& n = nodes[self];
         n.axis = axis;
         n.child1 = c1;
@@ -646,17 +679,23 @@ bbg_status BuildBvh(const float* aabbs, int32_t n, bbg_bvh_node* nodes_out, int3
         prims[i].aabb.min = Load3(aabbs + 6 * size_t(i));
         prims[i].aabb.max = Load3(aabbs + 6 * size_t(i) + 3);
     }
+    std::vector<int32_t> ordered(static_cast<size_t>(n));
     Builder b;
-    b.ordered.resize(size_t(n));
+    b.ordered = ordered.data();
+    unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    while ((1u << b.parallel_levels) < hw && b.parallel_levels < 6)
+    {
+        ++b.parallel_levels;
+    }
     b.nodes.reserve(size_t(2) * size_t(std::max(n, 1)));
-    int32_t root = b.Build(std::span<BuildPrim>(prims));
+    int32_t root = b.Build(std::span<BuildPrim>(prims), 0);
     if (b.too_many_in_leaf)
     {
         return Fail(BBG_ERR_BAD_BVH, "a leaf holds more than 65535 primitives (uint16 primitive_count)");
     }
     int32_t offset = 0;
     b.Flatten(root, nodes_out, &offset);
-    std::memcpy(slots_out, b.ordered.data(), sizeof(int32_t) * size_t(n));
+    std::memcpy(slots_out, ordered.data(), sizeof(int32_t) * size_t(n));
     *n_nodes_out = offset;
     return BBG_OK;
 }

@@ -30,14 +30,20 @@ def assert_same_tree(mine, ref):
     # where the reference built subtrees concurrently).
     assert leaf_sets(mn, ms) == leaf_sets(rn, rs)
     assert sorted(ms.tolist()) == list(range(ms.shape[0]))
+    # This builder's leaves take consecutive slots in depth-first node order
+    # (also where it built subtrees on separate threads).
+    leaves = mn[mn["count"] > 0]
+    starts = np.concatenate([[0], np.cumsum(leaves["count"].astype(np.int64))[:-1]])
+    assert np.array_equal(leaves["offset"], starts)
 
 
 @pytest.mark.parametrize("make", [
     lambda: scenes.triangle_soup(2000, seed=1),
     lambda: scenes.triangle_soup(100_000, seed=5),
+    lambda: scenes.triangle_soup(400_000, seed=6),
     lambda: scenes.cornell_icosphere(levels=4, width=16, height=16),
     lambda: scenes.readme_sphere(),
-], ids=["soup2k", "soup100k_parallel_ref_build", "cornell_ico4", "readme_sphere"])
+], ids=["soup2k", "soup100k_parallel_ref_build", "soup400k_parallel_builds", "cornell_ico4", "readme_sphere"])
 def test_builder_matches_reference(oracle, make):
     scene = make()
     rs = oracle.RefScene(scene)
