@@ -680,20 +680,23 @@ __device__ __forceinline__ void IntersectNode8(const float4* nd, const RayQ& q, 
     *refs_lo = __ldg(reinterpret_cast<const int4*>(nd + 4));
     *refs_hi = __ldg(reinterpret_cast<const int4*>(nd + 5));
     uint32_t meta = __float_as_uint(h.w);
-    // Plane k of axis a sits at p_a + q s_a: t = q (s_a / d_a) + (p_a / d_a - o_a / d_a).
+    // Plane k of axis a sits at p_a + q s_a: t = q (s_a / d_a) + (p_a - o_a) / d_a.
     float bx = __uint_as_float((meta & 0xffu) << 23) * q.inv_dir.x;
     float by = __uint_as_float(((meta >> 8) & 0xffu) << 23) * q.inv_dir.y;
     float bz = __uint_as_float(((meta >> 16) & 0xffu) << 23) * q.inv_dir.z;
-    float ax = __fmaf_rn(h.x, q.inv_dir.x, -q.oinv.x);
-    float ay = __fmaf_rn(h.y, q.inv_dir.y, -q.oinv.y);
-    float az = __fmaf_rn(h.z, q.inv_dir.z, -q.oinv.z);
+    // (p - o) / d in the reference's slab form; the ray's signs from 1/d
+    // (kept in predicates rather than per-ray registers).
+    float ax = (h.x - q.o.x) * q.inv_dir.x;
+    float ay = (h.y - q.o.y) * q.inv_dir.y;
+    float az = (h.z - q.o.z) * q.inv_dir.z;
+    const bool negx = q.inv_dir.x < 0, negy = q.inv_dir.y < 0, negz = q.inv_dir.z < 0;
     // Entry planes are the low bounds on a positive axis, the high ones on a negative axis.
-    uint32_t nx0 = q.neg[0] ? w2.z : w1.x, nx1 = q.neg[0] ? w2.w : w1.y;
-    uint32_t fx0 = q.neg[0] ? w1.x : w2.z, fx1 = q.neg[0] ? w1.y : w2.w;
-    uint32_t ny0 = q.neg[1] ? w3.x : w1.z, ny1 = q.neg[1] ? w3.y : w1.w;
-    uint32_t fy0 = q.neg[1] ? w1.z : w3.x, fy1 = q.neg[1] ? w1.w : w3.y;
-    uint32_t nz0 = q.neg[2] ? w3.z : w2.x, nz1 = q.neg[2] ? w3.w : w2.y;
-    uint32_t fz0 = q.neg[2] ? w2.x : w3.z, fz1 = q.neg[2] ? w2.y : w3.w;
+    uint32_t nx0 = negx ? w2.z : w1.x, nx1 = negx ? w2.w : w1.y;
+    uint32_t fx0 = negx ? w1.x : w2.z, fx1 = negx ? w1.y : w2.w;
+    uint32_t ny0 = negy ? w3.x : w1.z, ny1 = negy ? w3.y : w1.w;
+    uint32_t fy0 = negy ? w1.z : w3.x, fy1 = negy ? w1.w : w3.y;
+    uint32_t nz0 = negz ? w3.z : w2.x, nz1 = negz ? w3.w : w2.y;
+    uint32_t fz0 = negz ? w2.x : w3.z, fz1 = negz ? w2.y : w3.w;
     uint32_t hits = 0;
 #pragma unroll
     for (int j = 0; j < 4; ++j) // children 2j and 2j + 1
@@ -810,7 +813,7 @@ __device__ __forceinline__ void TracePersistentWide(const AccelView& a, int32_t 
                     }
                     res = TraceResult{ -1, t_max, 0, 0 };
                     sp = 0;
-                    oct = uint32_t(q.neg[0]) | (uint32_t(q.neg[1]) << 1) | (uint32_t(q.neg[2]) << 2);
+                    oct = uint32_t(q.inv_dir.x < 0) | (uint32_t(q.inv_dir.y < 0) << 1) | (uint32_t(q.inv_dir.z < 0) << 2);
                     pending = av.root8;
                     busy = true;
                 }
