@@ -413,8 +413,10 @@ __device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const Ra
 // Per ray the node and primitive tests are exactly those of TraceOrdered.
 // Src supplies Load(item, RayQ*, t_min*, t_max*) and Store(item, result).
 constexpr int32_t kNoNode = int32_t(0x80000000);
+// 28 of 32 measured best for both layouts (16: -9 %, 24: -2.5 %, 32: -9 % on
+// the 1M-triangle soup's closest + any-hit rays; path tracing unchanged).
 #ifndef BBG_REFILL
-#define BBG_REFILL 24
+#define BBG_REFILL 28
 #endif
 #ifndef BBG_SHORT_STACK
 #define BBG_SHORT_STACK 16
