@@ -27,7 +27,7 @@ struct bbg_accel
     int32_t n_wide8 = 0;
     int32_t depth8 = 0;
     bool use_wide8 = false;    // ordered queries run over the 8-wide layout
-    bool device_built = false; // tree built on the device (child-box layout only)
+    bool device_built = false; // tree built on the device (no reference node layout)
 
     // Shading data (the reference Mesh arrays and shapes).
     bbg::DevBuf<int2> prim_shape;     // (kind, index) per primitive

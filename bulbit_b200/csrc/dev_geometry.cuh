@@ -321,85 +321,6 @@ __device__ __forceinline__ bool SlabTest(float lx, float ly, float lz, float hx,
     return t0 <= t1;
 }
 
-// Nearest-child-first traversal over the child-box layout: each interior
-// node holds both children's boxes, so one 64-byte fetch tests two boxes; the
-// nearer hit child is visited first, the farther is pushed with its entry
-// distance and skipped on pop once a closer hit is known. The same primitive
-// tests run in a different order than RayCast, so the closest hit is the
-// same primitive and t except where two hits have exactly equal t.
-template <bool ANY>
-__device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const RayQ& q, float t_min, float t_max)
-{
-    TraceResult res{ -1, t_max, 0, 0 };
-    int2 stack[kStackCapacity];
-    int sp = 0;
-    int32_t ref = a.root;
-
-    while (true)
-    {
-        if (ref >= 0)
-        {
-            const float4* n = a.wide + 4 * size_t(ref);
-            float4 f0 = __ldg(n);
-            float4 f1 = __ldg(n + 1);
-            float4 f2 = __ldg(n + 2);
-            int4 f3 = __ldg(reinterpret_cast<const int4*>(n + 3));
-            float e0, e1;
-            bool h0 = SlabTest(f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, q, t_min, t_max, &e0);
-            bool h1 = SlabTest(f1.z, f1.w, f2.x, f2.y, f2.z, f2.w, q, t_min, t_max, &e1);
-            if (h0 && h1)
-            {
-                bool swap = e1 < e0;
-                int32_t near = swap ? f3.y : f3.x;
-                int32_t far = swap ? f3.x : f3.y;
-                float far_entry = swap ? e0 : e1;
-                stack[sp++] = make_int2(far, __float_as_int(far_entry));
-                ref = near;
-                continue;
-            }
-            if (h0 || h1)
-            {
-                ref = h0 ? f3.x : f3.y;
-                continue;
-            }
-        }
-        else
-        {
-            int2 leaf = __ldg(a.leaves + (~ref));
-            for (int32_t i = 0; i < leaf.y; ++i)
-            {
-                if (TestSlot(a, leaf.x + i, q, t_min, t_max, &res))
-                {
-                    if (ANY)
-                    {
-                        return res;
-                    }
-                    t_max = res.t;
-                }
-                if (t_max <= t_min)
-                {
-                    return res;
-                }
-            }
-        }
-        // Pop the next entry that can still hold a closer hit.
-        ref = 0x7fffffff;
-        while (sp > 0)
-        {
-            int2 e = stack[--sp];
-            if (__int_as_float(e.y) <= t_max)
-            {
-                ref = e.x;
-                break;
-            }
-        }
-        if (ref == 0x7fffffff)
-        {
-            break;
-        }
-    }
-    return res;
-}
 
 // Persistent warp-cooperative traversal over the child-box layout (the
 // while-while scheme of Aila & Laine, "Understanding the efficiency of ray
@@ -410,7 +331,11 @@ __device__ __forceinline__ TraceResult TraceOrdered(const AccelView& a, const Ra
 //   * each round first walks interior nodes until every busy lane has found a
 //     leaf (a lane that reaches a leaf postpones it and keeps walking), then
 //     tests leaves together, so node and leaf work do not serialise the warp.
-// Per ray the node and primitive tests are exactly those of TraceOrdered.
+// Per ray: nearest child first over the child-box layout (each interior node
+// holds both children's boxes, so one 64-byte fetch tests two), the farther
+// child pushed with its entry distance and skipped on pop once a closer hit
+// is known; the same primitive tests as BVH::RayCast in a different order, so
+// the closest hit is the same except between hits at exactly equal t.
 // Src supplies Load(item, RayQ*, t_min*, t_max*) and Store(item, result).
 constexpr int32_t kNoNode = int32_t(0x80000000);
 // 28 of 32 measured best for both layouts (16: -9 %, 24: -2.5 %, 32: -9 % on
@@ -903,14 +828,5 @@ __device__ __forceinline__ void TracePersistentWide(const AccelView& a, int32_t 
     }
 }
 
-template <bool ANY>
-__device__ __forceinline__ TraceResult Trace(const AccelView& a, const RayQ& q, float t_min, float t_max)
-{
-    if (a.ordered)
-    {
-        return TraceOrdered<ANY>(a, q, t_min, t_max);
-    }
-    return TraceReference<ANY, false>(a, q, t_min, t_max);
-}
 
 } // namespace bbg
