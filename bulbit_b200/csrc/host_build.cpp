@@ -325,7 +325,12 @@ bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<floa
     const int32_t n = g.n_prims;
     std::vector<float> prim_aabbs(6 * size_t(n));
     PrimAabbs(g, prim_aabbs.data());
-    const int64_t max_refs = std::min<int64_t>(int64_t(n) + int64_t(double(budget) * n), (int64_t(1) << 31) - 1);
+    // At most 2^30 references, so a tree over them (2 m - 1 nodes) fits int32.
+    const int64_t max_refs = std::min<int64_t>(int64_t(n) + int64_t(double(budget) * n), int64_t(1) << 30);
+    if (n > (int32_t(1) << 30))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "split references: %d primitives exceed 2^30", n);
+    }
     std::vector<SplitRef> refs;
     refs.reserve(size_t(max_refs));
     // Max-heap on wasted box area over the splittable (triangle) references.
