@@ -47,3 +47,18 @@ def test_split_references_cover_their_triangles():
         d = bx[:, 3:] - bx[:, :3]
         return 2 * (d[:, 0] * d[:, 1] + d[:, 1] * d[:, 2] + d[:, 2] * d[:, 0])
     assert area(boxes).sum() < area(own).sum()
+
+
+def test_spheres_are_never_split():
+    scene = scenes.readme_sphere()
+    boxes, prims = lib.split_references(scene, 4.0)
+    assert np.array_equal(prims, np.arange(scene.n_prims))
+    assert np.array_equal(boxes, lib.prim_aabbs(scene))
+
+
+def test_budget_bounds_the_reference_count():
+    scene = scenes.triangle_soup(5000, seed=3)
+    for budget in (0.25, 0.5, 2.0):
+        _, prims = lib.split_references(scene, budget)
+        assert len(prims) <= scene.n_prims * (1 + budget) + 1
+        assert np.array_equal(np.unique(prims), np.arange(scene.n_prims))
