@@ -332,10 +332,10 @@ GpuBVH::GpuBVH(const BVH& bvh)
     Upload(&tree);
 }
 
-GpuBVH::GpuBVH(const std::vector<Primitive*>& primitives)
+GpuBVH::GpuBVH(const std::vector<Primitive*>& primitives, GpuTree tree, float split_budget)
     : prims_(primitives.begin(), primitives.end())
 {
-    Upload(nullptr);
+    Upload(nullptr, tree, split_budget);
 }
 
 GpuBVH::~GpuBVH()
@@ -346,7 +346,7 @@ GpuBVH::~GpuBVH()
     }
 }
 
-void GpuBVH::Upload(const bbg_bvh* tree)
+void GpuBVH::Upload(const bbg_bvh* tree, GpuTree kind, float split_budget)
 {
     std::vector<float> positions, normals, tangents, uvs;
     std::vector<int32_t> tri_indices, prim_kind, prim_index;
@@ -427,7 +427,18 @@ void GpuBVH::Upload(const bbg_bvh* tree)
     g.n_prims = int32_t(prims_.size());
     g.prim_kind = prim_kind.data();
     g.prim_index = prim_index.data();
-    Check(bbg_accel_create(&g, tree, &accel_), "bbg_accel_create");
+    if (tree || kind == GpuTree::Reference || prims_.empty())
+    {
+        Check(bbg_accel_create(&g, tree, &accel_), "bbg_accel_create");
+    }
+    else if (kind == GpuTree::DeviceLinear)
+    {
+        Check(bbg_accel_create_device_build(&g, &accel_), "bbg_accel_create_device_build");
+    }
+    else
+    {
+        Check(bbg_accel_create_split(&g, split_budget, &accel_), "bbg_accel_create_split");
+    }
     float b[6];
     Check(bbg_accel_bounds(accel_, b), "bbg_accel_bounds");
     bounds_ = AABB(Point3(b[0], b[1], b[2]), Point3(b[3], b[4], b[5]));

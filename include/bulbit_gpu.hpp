@@ -56,14 +56,30 @@
 namespace bulbit_gpu
 {
 
+// The tree a GpuBVH built from a primitive list uses. Reference: the same
+// SAH tree as BVH::BVH (hits identical to the reference's). DeviceLinear: a
+// linear BVH built on the GPU in milliseconds. SplitReferences: the SAH
+// build over split triangle references (faster traversal of long or
+// diagonal triangles, a longer build). The last two change only which of
+// two hits at exactly the same t is returned.
+enum class GpuTree
+{
+    Reference,
+    DeviceLinear,
+    SplitReferences
+};
+
 class GpuBVH : public bulbit::Intersectable
 {
 public:
     // The reference's own tree (BVH::nodes, BVH::primitives), node for node.
     explicit GpuBVH(const bulbit::BVH& bvh);
-    // The same SAH tree built by the library (bbg_bvh_build) from the
-    // primitives, in the order given (primitive index = position).
-    explicit GpuBVH(const std::vector<bulbit::Primitive*>& primitives);
+    // A tree built by the library from the primitives, in the order given
+    // (primitive index = position): by default the same SAH tree as
+    // BVH::BVH (bbg_bvh_build); split_budget = extra references per
+    // primitive for GpuTree::SplitReferences.
+    explicit GpuBVH(const std::vector<bulbit::Primitive*>& primitives, GpuTree tree = GpuTree::Reference,
+                    float split_budget = 3.0f);
     ~GpuBVH() override;
 
     GpuBVH(const GpuBVH&) = delete;
@@ -89,7 +105,7 @@ public:
     bbg_accel* Handle() const { return accel_; }
 
 private:
-    void Upload(const bbg_bvh* tree);
+    void Upload(const bbg_bvh* tree, GpuTree kind = GpuTree::Reference, float split_budget = 0.0f);
 
     std::vector<const bulbit::Primitive*> prims_;
     std::unordered_map<const bulbit::Primitive*, int32_t> index_;

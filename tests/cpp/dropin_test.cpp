@@ -268,8 +268,13 @@ int main()
             BVH bvh(scene.GetPrimitives());
             bulbit_gpu::GpuBVH gpu(bvh);
             bulbit_gpu::GpuBVH gpu_own(scene.GetPrimitives()); // the library's own build of the same tree
+            // Other trees over the same primitives (hits equal except exact ties).
+            bulbit_gpu::GpuBVH gpu_split(scene.GetPrimitives(), bulbit_gpu::GpuTree::SplitReferences, 2.0f);
+            bulbit_gpu::GpuBVH gpu_dev(scene.GetPrimitives(), bulbit_gpu::GpuTree::DeviceLinear);
             CompareQueries(bvh, gpu, Point3(0, 1.2f, 0), 2.5f, &r, "mesh");
             CompareQueries(bvh, gpu_own, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_own_tree");
+            CompareQueries(bvh, gpu_split, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_split_tree");
+            CompareQueries(bvh, gpu_dev, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_device_tree");
             // The camera's default filter (GaussianFilter) and a stratified sampler.
             GaussianFilter filter;
             Point3 eye(0.0f, 1.5f, 5.0f), at(0.0f, 1.2f, 0.0f);
