@@ -265,3 +265,25 @@ def test_device_built_tree_parity(oracle):
         with pytest.raises(lib.BbgError) as e:
             call()
         assert e.value.status == abi.BBG_ERR_UNSUPPORTED
+
+
+def test_oversized_leaf_falls_back_to_the_binary_layout(oracle):
+    """64 coincident triangles make one leaf of 64 primitives, more than the
+    8-wide layout encodes: the accel keeps the binary layout (WIDE is
+    refused), and hits still match the reference."""
+    scene = scenes.triangle_soup(2000, seed=9)
+    pos = scene.positions.copy()
+    pos[: 3 * 64] = np.tile(pos[:3], (64, 1))
+    scene.positions = pos
+    rs = oracle.RefScene(scene)
+    acc = lib.GpuAccel(scene, bvh=rs.bvh())
+    with pytest.raises(lib.BbgError) as e:
+        acc.set_traversal(abi.BBG_TRAVERSAL_WIDE)
+    assert e.value.status == abi.BBG_ERR_UNSUPPORTED
+    closest, anyq = scenes.soup_rays(50_000, seed=3)
+    ref_prim, ref_t, _ = rs.intersect(closest)
+    prim, t, _, _ = acc.intersect(closest)
+    frac, unexplained, t_bad = compare_closest(rs, closest, prim, t, ref_prim, ref_t)
+    assert not unexplained and t_bad.size == 0
+    ref_occ, _ = rs.intersect_any(anyq)
+    assert np.array_equal(acc.intersect_any(anyq), ref_occ)
