@@ -488,6 +488,83 @@ int bbref_intersect_all(void* handle, const bbg_ray* r, int32_t max_out, int32_t
     return count;
 }
 
+// Traversal work of BVH::RayCast (include/bulbit/bvh.h:102-155) for each
+// query: its loop replayed with the reference's own nodes, AABB::TestRay and
+// Primitive::Intersect / IntersectAny, counting nodes popped (each is
+// slab-tested) and primitive tests, for closest-hit (any = 0, the
+// BVH::Intersect callback) or any-hit (the BVH::IntersectAny callback)
+// queries. Returns the totals over the n rays.
+int bbref_count_traversal(void* handle, const bbg_ray* rays, int64_t n, int32_t any, int64_t* nodes_out,
+                          int64_t* prims_out)
+{
+    auto* rs = static_cast<RefScene*>(handle);
+    const auto* nodes = rs->bvh.get()->*Get(BVHNodes{});
+    const auto& prims = rs->bvh.get()->*Get(BVHPrims{});
+    int64_t total_nodes = 0, total_prims = 0;
+    for (int64_t k = 0; k < n; ++k)
+    {
+        const bbg_ray& br = rays[k];
+        Ray r(Point3(br.o[0], br.o[1], br.o[2]), Vec3(br.d[0], br.d[1], br.d[2]));
+        Float t_min = br.t_min, t_max = br.t_max;
+        const Vec3 inv_dir(1 / r.d.x, 1 / r.d.y, 1 / r.d.z);
+        const int32 is_dir_neg[3] = { int32(inv_dir.x < 0), int32(inv_dir.y < 0), int32(inv_dir.z < 0) };
+        std::vector<int32> stack{ 0 };
+        bool done = false;
+        while (!stack.empty() && !done)
+        {
+            int32 index = stack.back();
+            stack.pop_back();
+            ++total_nodes;
+            if (!nodes[index].aabb.TestRay(r.o, t_min, t_max, inv_dir, is_dir_neg))
+            {
+                continue;
+            }
+            if (nodes[index].primitive_count > 0)
+            {
+                for (int32 i = 0; i < nodes[index].primitive_count; ++i)
+                {
+                    ++total_prims;
+                    const Primitive* p = prims[nodes[index].primitives_offset + i];
+                    Float t;
+                    if (any)
+                    {
+                        t = p->IntersectAny(r, t_min, t_max) ? t_min : t_max;
+                    }
+                    else
+                    {
+                        Intersection isect;
+                        t = p->Intersect(&isect, r, t_min, t_max) ? isect.t : t_max;
+                    }
+                    if (t <= t_min)
+                    {
+                        done = true;
+                        break;
+                    }
+                    t_max = t;
+                }
+            }
+            else
+            {
+                int32 child1 = index + 1;
+                int32 child2 = nodes[index].child2_offset;
+                if (is_dir_neg[nodes[index].axis])
+                {
+                    stack.push_back(child1);
+                    stack.push_back(child2);
+                }
+                else
+                {
+                    stack.push_back(child2);
+                    stack.push_back(child1);
+                }
+            }
+        }
+    }
+    *nodes_out = total_nodes;
+    *prims_out = total_prims;
+    return 0;
+}
+
 // The derived state of the reference PerspectiveCamera for a spec.
 int bbref_camera(const bbg_camera_spec* spec, bbg_camera* out)
 {

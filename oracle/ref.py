@@ -46,6 +46,7 @@ def lib():
             "bbref_sampler_draws": (I32, [I32, I32, I32, I32, I32, P]),
             "bbref_ggx_energy_tables": (I32, [P, P]),
             "bbref_dielectric_energy_tables": (I32, [P, P, P, P]),
+            "bbref_count_traversal": (I32, [P, P, C.c_int64, I32, P, P]),
             "bbref_set_sampler": (None, [I32, I32, I32]),
             "bbref_pcg32": (I32, [C.c_uint64, C.c_uint64, I32, P]),
             "bbref_hash_pixel_sample": (C.c_uint64, [I32, I32, I32, I32]),
@@ -126,6 +127,14 @@ class RefScene:
         occ = np.zeros(rays.shape[0], np.uint8)
         secs = lib().bbref_intersect_any(self.h, _p(rays), rays.shape[0], _p(occ))
         return occ, secs
+
+    def count_traversal(self, rays, any_hit=False):
+        """Nodes popped and primitive tests of BVH::RayCast over the rays (totals)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        nodes, prims = C.c_int64(), C.c_int64()
+        lib().bbref_count_traversal(self.h, _p(rays), rays.shape[0], 1 if any_hit else 0, C.byref(nodes),
+                                    C.byref(prims))
+        return nodes.value, prims.value
 
     def intersect_all(self, ray, max_out=64):
         ray = np.ascontiguousarray(ray, np.float32)

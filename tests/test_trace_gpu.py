@@ -287,3 +287,37 @@ def test_oversized_leaf_falls_back_to_the_binary_layout(oracle):
     assert not unexplained and t_bad.size == 0
     ref_occ, _ = rs.intersect_any(anyq)
     assert np.array_equal(acc.intersect_any(anyq), ref_occ)
+
+
+def test_traversal_counts_match_a_replay_of_the_reference():
+    """The counting run behind the roofline's algorithmic bytes (nodes popped
+    and primitive tests in BVH::RayCast's order) equals the oracle's replay of
+    RayCast with the reference's own TestRay and primitive tests, for
+    closest-hit and any-hit queries (64K rays each)."""
+    from oracle import ref
+    soup = scenes.triangle_soup(1 << 20, seed=1)
+    closest, anyq = scenes.soup_rays(1 << 16, seed=2)
+    cornell = scenes.cornell_icosphere(levels=6, width=8, height=8)
+    rng = np.random.default_rng(12)
+    n = 1 << 16
+    crays = np.zeros((n, 8), np.float32)
+    crays[:, :3] = rng.uniform(-0.95, 0.95, (n, 3))
+    d = rng.normal(size=(n, 3))
+    crays[:, 3:6] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    crays[:, 6], crays[:, 7] = 1e-4, np.inf
+    cany = crays.copy()
+    cany[:, 7] = rng.uniform(0.05, 2.0, n).astype(np.float32)
+    for scene, cl, an in ((soup, closest, anyq), (cornell, crays, cany)):
+        rs = ref.RefScene(scene)
+        acc = lib.GpuAccel(scene, bvh=rs.bvh())
+        acc.set_counting(True)
+        acc.intersect(cl)
+        gpu_closest = acc.last_counts()
+        acc.intersect_any(an)
+        gpu_any = acc.last_counts()
+        cpu_closest = rs.count_traversal(cl)
+        cpu_any = rs.count_traversal(an, any_hit=True)
+        print(f"{scene.name}: closest {gpu_closest} vs {cpu_closest}, any {gpu_any} vs {cpu_any}")
+        assert tuple(gpu_closest) == cpu_closest
+        assert tuple(gpu_any) == cpu_any
+        acc.close()
