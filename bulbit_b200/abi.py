@@ -157,6 +157,7 @@ EXPORTS = [
     ("bbg_integrator_light_pmf", I32, [P, P]),
     ("bbg_render", I32, [P, P, P, P, I32, P]),
     ("bbg_sampler_draws", I32, [I32, I32, I32, I32, I32, P]),
+    ("bbg_bsdf_probe", I32, [P, I32, I32, P, P, P, P]),
     ("bbg_ggx_energy_tables", I32, [P, P]),
     ("bbg_dielectric_energy_tables", I32, [P, P, P, P]),
     ("bbg_accel_create_split", I32, [P, C.c_float, P]),

@@ -1696,6 +1696,31 @@ __global__ void DielectricEnergyAverageKernel()
     g_dms_e_inv_avg[j * n + k] = 2 * r_inv_sum;
 }
 
+// ---------------------------------------------------------------- BSDF probe
+
+// Material::GetBSDF at a surface with shading normal +z and tangent +x (so
+// local and world directions coincide), then BSDF::f, PDF and Sample_f per
+// query; out: f (3), pdf, and the sample's f (3), wi (3), pdf, flags (-1 if
+// Sample_f fails) — 12 floats per query.
+__global__ void BsdfProbeKernel(MaterialDev m, int32_t front_face, int32_t n, const float* wo, const float* wi,
+                                const float* u, float* out)
+{
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        BSDF b = MakeBSDF(m, V3{ 0, 0, 1 }, V3{ 1, 0, 0 }, front_face != 0);
+        V3 o = load3(wo + 3 * size_t(i)), w = load3(wi + 3 * size_t(i));
+        Spec f = b.F(o, w);
+        float pdf = b.PDF(o, w);
+        BSDFSample s{};
+        bool ok = b.Sample(&s, o, u[3 * size_t(i)], P2{ u[3 * size_t(i) + 1], u[3 * size_t(i) + 2] });
+        float* r = out + 12 * size_t(i);
+        r[0] = f.r, r[1] = f.g, r[2] = f.b, r[3] = pdf;
+        r[4] = ok ? s.f.r : 0, r[5] = ok ? s.f.g : 0, r[6] = ok ? s.f.b : 0;
+        r[7] = ok ? s.wi.x : 0, r[8] = ok ? s.wi.y : 0, r[9] = ok ? s.wi.z : 0;
+        r[10] = ok ? s.pdf : 0, r[11] = ok ? float(s.flags) : -1.0f;
+    }
+}
+
 // ---------------------------------------------------------------- sampler probe
 
 __global__ void SamplerDrawsKernel(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out)
@@ -3018,6 +3043,35 @@ bbg_status bbg_dielectric_energy_tables(float* e_out, float* e_inv_out, float* e
     BBG_CUDA(cudaMemcpyFromSymbol(e_inv_out, g_dms_e_inv, sizeof(g_dms_e_inv)));
     BBG_CUDA(cudaMemcpyFromSymbol(e_avg_out, g_dms_e_avg, sizeof(g_dms_e_avg)));
     BBG_CUDA(cudaMemcpyFromSymbol(e_inv_avg_out, g_dms_e_inv_avg, sizeof(g_dms_e_inv_avg)));
+    return BBG_OK;
+}
+
+bbg_status bbg_bsdf_probe(const bbg_material* material, int32_t front_face, int32_t n, const float* wo,
+                          const float* wi, const float* u, float* out)
+{
+    if (!material || n < 0 || (n > 0 && (!wo || !wi || !u || !out)))
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_bsdf_probe: bad argument");
+    }
+    BBG_TRY(CheckDevice());
+    MaterialDev md{};
+    BBG_TRY(MakeMaterial(*material, &md));
+    if (md.ms)
+    {
+        BBG_TRY(EnsureEnergyTables());
+    }
+    if (n == 0)
+    {
+        return BBG_OK;
+    }
+    DevBuf<float> d_wo, d_wi, d_u, d_out;
+    BBG_TRY(d_wo.upload(wo, 3 * size_t(n)));
+    BBG_TRY(d_wi.upload(wi, 3 * size_t(n)));
+    BBG_TRY(d_u.upload(u, 3 * size_t(n)));
+    BBG_TRY(d_out.alloc(12 * size_t(n)));
+    BsdfProbeKernel<<<std::min((n + 127) / 128, 1024), 128>>>(md, front_face, n, d_wo.p, d_wi.p, d_u.p, d_out.p);
+    BBG_CUDA(cudaGetLastError());
+    BBG_CUDA(cudaMemcpy(out, d_out.p, 12 * size_t(n) * sizeof(float), cudaMemcpyDeviceToHost));
     return BBG_OK;
 }
 

@@ -418,6 +418,17 @@ class GpuBatch:
         return films, stats
 
 
+def bsdf_probe(material, wo, wi, u, front_face=True):
+    """bbg_bsdf_probe: (n, 12) per query — f rgb, pdf, sample f rgb, wi, pdf, flags (-1: no sample)."""
+    wo = np.ascontiguousarray(wo, np.float32)
+    wi = np.ascontiguousarray(wi, np.float32)
+    u = np.ascontiguousarray(u, np.float32)
+    out = np.zeros((wo.shape[0], 12), np.float32)
+    check(get_lib().bbg_bsdf_probe(C.byref(material), 1 if front_face else 0, wo.shape[0], _p(wo), _p(wi), _p(u),
+                                   _p(out)), "bbg_bsdf_probe")
+    return out
+
+
 def ggx_energy_tables():
     """bbg_ggx_energy_tables: (E 32x32 indexed [alpha][cos], E_avg 32)."""
     e = np.zeros(32 * 32, np.float32)

@@ -526,6 +526,15 @@ bbg_status bbg_batch_autotune(bbg_batch* batch, int32_t n, bbg_integrator* const
  * StartPixelSample(pixel, sample) with the given seed, computed on the device. */
 bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out);
 
+/* Material::GetBSDF (src/material/*.cpp) at a surface with shading normal +z
+ * and tangent +x (local = world directions; front_face selects the
+ * dielectric's relative eta), then BSDF::f, PDF and Sample_f
+ * (include/bulbit/bsdf.h:73-125) for n queries (wo, wi, u: 3 floats each).
+ * out: 12 floats per query — f (rgb), pdf, the sample's f (rgb), wi, pdf and
+ * flags (-1 where Sample_f fails). */
+bbg_status bbg_bsdf_probe(const bbg_material* material, int32_t front_face, int32_t n, const float* wo,
+                          const float* wi, const float* u, float* out);
+
 /* --------------------------------------------------------- path guiding */
 
 /* Neural path guiding (no counterpart in the reference: an added learned

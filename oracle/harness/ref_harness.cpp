@@ -565,6 +565,49 @@ int bbref_count_traversal(void* handle, const bbg_ray* rays, int64_t n, int32_t 
     return 0;
 }
 
+// Material::GetBSDF at a surface with shading normal +z and tangent +x, then
+// BSDF::f, PDF and Sample_f per query, in bbg_bsdf_probe's output layout.
+int bbref_bsdf_probe(const bbg_material* m, int32_t front_face, int32_t n, const float* wo, const float* wi,
+                     const float* u, float* out)
+{
+    EnsurePool(0);
+    static bool tables = false;
+    if (!tables)
+    {
+        InScratchDir([] { PrepareReflectanceTextures(32, 1024); });
+        tables = true;
+    }
+    Scene scene;
+    const Material* mat = MakeMaterial(scene, *m);
+    Intersection isect{};
+    isect.front_face = front_face != 0;
+    isect.normal = Vec3(0, 0, 1);
+    isect.shading.normal = Vec3(0, 0, 1);
+    isect.shading.tangent = Vec3(1, 0, 0);
+    isect.uv = Point2(0.5f, 0.5f);
+    Allocator alloc;
+    BSDF bsdf;
+    if (!mat || !mat->GetBSDF(&bsdf, isect, alloc))
+    {
+        return -1;
+    }
+    for (int32_t i = 0; i < n; ++i)
+    {
+        Vec3 o(wo[3 * i], wo[3 * i + 1], wo[3 * i + 2]);
+        Vec3 w(wi[3 * i], wi[3 * i + 1], wi[3 * i + 2]);
+        Spectrum f = bsdf.f(o, w);
+        Float pdf = bsdf.PDF(o, w);
+        BSDFSample s;
+        bool ok = bsdf.Sample_f(&s, o, u[3 * i], Point2(u[3 * i + 1], u[3 * i + 2]));
+        float* r = out + 12 * size_t(i);
+        r[0] = f.r, r[1] = f.g, r[2] = f.b, r[3] = pdf;
+        r[4] = ok ? s.f.r : 0, r[5] = ok ? s.f.g : 0, r[6] = ok ? s.f.b : 0;
+        r[7] = ok ? s.wi.x : 0, r[8] = ok ? s.wi.y : 0, r[9] = ok ? s.wi.z : 0;
+        r[10] = ok ? s.pdf : 0, r[11] = ok ? float(int32(s.flags)) : -1.0f;
+    }
+    return 0;
+}
+
 // The derived state of the reference PerspectiveCamera for a spec.
 int bbref_camera(const bbg_camera_spec* spec, bbg_camera* out)
 {

@@ -47,6 +47,7 @@ def lib():
             "bbref_ggx_energy_tables": (I32, [P, P]),
             "bbref_dielectric_energy_tables": (I32, [P, P, P, P]),
             "bbref_count_traversal": (I32, [P, P, C.c_int64, I32, P, P]),
+            "bbref_bsdf_probe": (I32, [P, I32, I32, P, P, P, P]),
             "bbref_set_sampler": (None, [I32, I32, I32]),
             "bbref_pcg32": (I32, [C.c_uint64, C.c_uint64, I32, P]),
             "bbref_hash_pixel_sample": (C.c_uint64, [I32, I32, I32, I32]),
@@ -207,6 +208,18 @@ def dielectric_energy_tables():
     ai = np.zeros(32 * 32, np.float32)
     lib().bbref_dielectric_energy_tables(_p(e), _p(ei), _p(a), _p(ai))
     return e.reshape(32, 32, 32), ei.reshape(32, 32, 32), a.reshape(32, 32), ai.reshape(32, 32)
+
+
+def bsdf_probe(material, wo, wi, u, front_face=True):
+    """The reference's Material::GetBSDF then f / PDF / Sample_f (bbg_bsdf_probe's layout)."""
+    wo = np.ascontiguousarray(wo, np.float32)
+    wi = np.ascontiguousarray(wi, np.float32)
+    u = np.ascontiguousarray(u, np.float32)
+    out = np.zeros((wo.shape[0], 12), np.float32)
+    rc = lib().bbref_bsdf_probe(C.byref(material), 1 if front_face else 0, wo.shape[0], _p(wo), _p(wi), _p(u),
+                                _p(out))
+    assert rc == 0
+    return out
 
 
 def pcg32(initstate, initseq, n):
