@@ -345,7 +345,7 @@ def run_guided(args):
     same_spp = integ.render(spp=64, seed=8, guide=g)  # the trained guide, no more training
     e_same = rel_mse(same_spp.image(), ref)
     # Optional: a guide trained far longer than one frame allows (args.guided_pretrain
-    # frames of 64 spp, 8 Adam steps per 2^21-path wave), then judged at equal spp.
+    # frames of 64 spp, 8 Adam steps per 2^21-path wave), then compared at equal spp.
     pretrained = None
     if args.guided_pretrain > 0:
         gp = lib.GpuGuide(acc.bounds(), seed=11)
@@ -489,7 +489,7 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="path tracing: default launch configuration only")
     ap.add_argument("--guided-res", type=int, default=256)
     ap.add_argument("--guided-pretrain", type=int, default=0,
-                    help="guided workload: also judge a guide trained for this many frames at equal spp")
+                    help="guided workload: also evaluate a guide trained for this many frames at equal spp")
     ap.add_argument("--traversal", default="default", choices=["default", "ordered", "wide"],
                     help="rays and pt workloads: node layout of the timed traversal")
     ap.add_argument("--pt-res", type=int, default=1024)

@@ -1,7 +1,7 @@
 // Neural path guiding: a small MLP that maps a shading point to an 8-lobe
 // von Mises-Fisher mixture over directions, sampled in one-sample MIS with the
 // BSDF. No counterpart in the reference renderer; the plain path tracer is
-// its fallback and the judge of its error.
+// its fallback and the yardstick of its error.
 //
 // Network: 80 inputs -> 64 -> 64 -> 64 (ReLU) -> 40 outputs, BF16 weights and
 // activations, FP32 accumulation (mma.sync m16n8k16), FP32 biases and master

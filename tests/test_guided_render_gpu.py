@@ -1,5 +1,5 @@
 """Guided path tracing on the GPU: one-sample MIS between the neural vMF
-guide and the BSDF. The plain path tracer is the judge:
+guide and the BSDF, measured against the plain path tracer:
 
 * unbiased: the guided image mean agrees with the plain one within their Monte
   Carlo standard errors (4 sigma), with an untrained and a trained guide, and

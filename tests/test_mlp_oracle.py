@@ -1,5 +1,5 @@
-"""Pins the path-guiding MLP's CPU oracle (oracle/mlp_ref.py) before it
-judges the GPU kernels: its analytic parameter gradient of the vMF-mixture
+"""Pins the path-guiding MLP's CPU oracle (oracle/mlp_ref.py) before the GPU
+kernels are checked against it: its analytic parameter gradient of the vMF-mixture
 negative log-likelihood agrees with central finite differences, its mixture
 density integrates to 1 over the sphere, and Adam reduces to the published
 update (Kingma & Ba, 2015)."""
