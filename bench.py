@@ -120,6 +120,25 @@ def profile_traffic(name):
 
 # ------------------------------------------------------------------ reference arm
 
+def max_over_ranks(values, device="cpu"):
+    """Element-wise maximum of each rank's values (timings) over all ranks;
+    every rank calls it, in the same order. Without a process group, the
+    values themselves."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized() or dist.get_world_size() == 1:
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.tolist()]
+
+
+def whole_job_rate(units_per_rank, world, max_ms):
+    """Units per second of the whole job: every rank's units over the slowest
+    rank's time."""
+    return world * units_per_rank / (max_ms / 1e3)
+
+
 def run_reference(args, rank):
     """The reference's own CPU BVH (oracle/_ref, compiled from its sources)
     on the same workload: each step traces a bounded sample of the rays on all
@@ -244,7 +263,9 @@ def run_pt(args, barrier, world):
 
     # Default launch configuration, then the autotuned one (which the
     # reported value uses; params.wave_paths = 0 lets the tuned wave apply).
+    # Device times are the maximum over ranks.
     default_ms, default_rays = timed()
+    default_ms = max_over_ranks([default_ms], device="cuda")[0]
     if args.no_autotune:
         tuning = abi.Tuning(128, 16, args.pt_wave, 0.0, 0)
         tune_s = 0.0
@@ -255,13 +276,14 @@ def run_pt(args, barrier, world):
         tune_s = time.perf_counter() - t0
         params.wave_paths = 0
         dev_ms, rays = timed()
+        dev_ms = max_over_ranks([dev_ms], device="cuda")[0]
     # End to end through the C ABI with a host film (copied back in the call).
     t0 = time.perf_counter()
     film = integ.render(spp=64)
-    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks([time.perf_counter() - t0], device="cuda")[0]
     paths = stats.paths
     out = {
-        "value": world * paths * steps / (dev_ms / 1e3), "unit": "paths/s",
+        "value": whole_job_rate(paths * steps, world, dev_ms), "unit": "paths/s",
         "mrays_per_s": world * rays / (dev_ms / 1e3) / 1e6, "ms_per_frame": dev_ms / steps,
         "steps": steps, "closest_rays_per_frame": stats.closest_rays, "shadow_rays_per_frame": stats.shadow_rays,
         "default_config_ms_per_frame": default_ms / steps,
@@ -271,7 +293,7 @@ def run_pt(args, barrier, world):
                              "wave_paths": tuning.wave_paths, "autotune_s": round(tune_s, 2)},
                    "cuda_graph": True},
         "image_mean": float(np.nanmean(film.image())),
-        "e2e": {"value": world * paths / e2e_s, "unit": "paths/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": whole_job_rate(paths, world, e2e_s * 1e3), "unit": "paths/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": n_pix * (12 + 4 + 8)},
         "gpu_launches_per_frame": -(-paths // (tuning.wave_paths - tuning.wave_paths % 64)) * (2 + 4 * 17),
     }
@@ -287,8 +309,9 @@ def run_pt(args, barrier, world):
         integ = lib.GpuPathIntegrator(acc, scene)
         params.wave_paths = args.pt_wave
         split_ms, split_rays = timed()
+        split_ms = max_over_ranks([split_ms], device="cuda")[0]
         out["split_reference_tree"] = {
-            "budget": args.pt_split_report, "value": world * paths * steps / (split_ms / 1e3), "unit": "paths/s",
+            "budget": args.pt_split_report, "value": whole_job_rate(paths * steps, world, split_ms), "unit": "paths/s",
             "mrays_per_s": world * split_rays / (split_ms / 1e3) / 1e6, "ms_per_frame": split_ms / steps,
             "bvh_build_s": round(split_build_s, 3)}
         integ.close()
@@ -611,14 +634,11 @@ def main():
     e2e_steps, e2e_s = 0, float("nan")
     if not args.no_e2e:
         e2e_steps, e2e_s = run_e2e(args, acc, closest, anyq, barrier)
-    if world > 1:
-        tt = torch.tensor([ms, e2e_s], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms, e2e_s = float(tt[0]), float(tt[1])
+    ms, e2e_s = max_over_ranks([ms, e2e_s], device="cuda")
 
     rays_per_step = 2 * n_rays
-    value = world * rays_per_step * args.steps / (ms / 1e3) / 1e6
-    e2e_value = world * rays_per_step * e2e_steps / e2e_s / 1e6 if e2e_steps else None
+    value = whole_job_rate(rays_per_step * args.steps, world, ms) / 1e6
+    e2e_value = whole_job_rate(rays_per_step * e2e_steps, world, e2e_s * 1e3) / 1e6 if e2e_steps else None
 
     peaks, peak_kind = load_peaks()
     avg_closest_ms = statistics.mean(closest_ms)
