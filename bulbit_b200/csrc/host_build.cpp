@@ -461,6 +461,30 @@ struct BuildNode
 };
 
 constexpr size_t kParallelBuildSpan = size_t(1) << 16;
+// Spans at least this long compute their bounds and SAH buckets on several
+// threads (min / max and counts: the same values in any order).
+constexpr size_t kParallelReduceSpan = size_t(1) << 18;
+
+// Runs fn(begin, end, chunk) over `threads` contiguous chunks of [0, n).
+template <class F>
+void ForChunks(size_t n, int threads, F&& fn)
+{
+    const size_t chunk = (n + size_t(threads) - 1) / size_t(threads);
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; ++t)
+    {
+        const size_t b = size_t(t) * chunk, e = std::min(n, b + chunk);
+        if (b < e)
+        {
+            pool.emplace_back([&fn, b, e, t] { fn(b, e, t); });
+        }
+    }
+    fn(0, std::min(n, chunk), 0);
+    for (std::thread& th : pool)
+    {
+        th.join();
+    }
+}
 
 struct Builder
 {
@@ -492,11 +516,34 @@ struct Builder
     int32_t Build(std::span<BuildPrim> span, int32_t slot_base, int depth = 0)
     {
         int32_t primitive_count = int32_t(span.size());
+        // Threads for this node's reductions: the machine's, shared among the
+        // nodes of this depth that build concurrently.
+        const int reduce_threads =
+            span.size() >= kParallelReduceSpan ? std::max(1, int(std::thread::hardware_concurrency()) >> depth) : 1;
 
         Box span_bounds;
-        for (const BuildPrim& p : span)
+        if (reduce_threads > 1)
         {
-            span_bounds = Box::Union(span_bounds, p.aabb);
+            std::vector<Box> part(static_cast<size_t>(reduce_threads));
+            ForChunks(span.size(), reduce_threads, [&](size_t b, size_t e, int t) {
+                Box acc;
+                for (size_t i = b; i < e; ++i)
+                {
+                    acc = Box::Union(acc, span[i].aabb);
+                }
+                part[size_t(t)] = acc;
+            });
+            for (const Box& bx : part)
+            {
+                span_bounds = Box::Union(span_bounds, bx);
+            }
+        }
+        else
+        {
+            for (const BuildPrim& p : span)
+            {
+                span_bounds = Box::Union(span_bounds, p.aabb);
+            }
         }
 
         if (span_bounds.SurfaceArea() == 0 || primitive_count == 1)
@@ -505,9 +552,28 @@ struct Builder
         }
 
         Box centroid_bounds;
-        for (const BuildPrim& p : span)
+        if (reduce_threads > 1)
         {
-            centroid_bounds = Box::Union(centroid_bounds, p.aabb.Center());
+            std::vector<Box> part(static_cast<size_t>(reduce_threads));
+            ForChunks(span.size(), reduce_threads, [&](size_t b, size_t e, int t) {
+                Box acc;
+                for (size_t i = b; i < e; ++i)
+                {
+                    acc = Box::Union(acc, span[i].aabb.Center());
+                }
+                part[size_t(t)] = acc;
+            });
+            for (const Box& bx : part)
+            {
+                centroid_bounds = Box::Union(centroid_bounds, bx);
+            }
+        }
+        else
+        {
+            for (const BuildPrim& p : span)
+            {
+                centroid_bounds = Box::Union(centroid_bounds, p.aabb.Center());
+            }
         }
 
         int32_t axis = 0;
@@ -546,15 +612,37 @@ struct Builder
                 Box bounds;
             } buckets[bucket_size];
 
-            for (const BuildPrim& p : span)
-            {
-                int32_t b = int32_t(bucket_size * (p.aabb.Center() - centroid_bounds.min)[axis] / extent);
-                if (b == bucket_size)
+            auto fill = [&](size_t b0, size_t e0, Bucket* out) {
+                for (size_t i = b0; i < e0; ++i)
                 {
-                    b = b - 1;
+                    const BuildPrim& p = span[i];
+                    int32_t b = int32_t(bucket_size * (p.aabb.Center() - centroid_bounds.min)[axis] / extent);
+                    if (b == bucket_size)
+                    {
+                        b = b - 1;
+                    }
+                    out[b].count++;
+                    out[b].bounds = Box::Union(out[b].bounds, p.aabb);
                 }
-                buckets[b].count++;
-                buckets[b].bounds = Box::Union(buckets[b].bounds, p.aabb);
+            };
+            if (reduce_threads > 1)
+            {
+                std::vector<Bucket> part(size_t(reduce_threads) * bucket_size);
+                ForChunks(span.size(), reduce_threads,
+                          [&](size_t b0, size_t e0, int t) { fill(b0, e0, part.data() + size_t(t) * bucket_size); });
+                for (int t = 0; t < reduce_threads; ++t)
+                {
+                    for (int32_t b = 0; b < bucket_size; ++b)
+                    {
+                        const Bucket& pb = part[size_t(t) * bucket_size + size_t(b)];
+                        buckets[b].count += pb.count;
+                        buckets[b].bounds = Box::Union(buckets[b].bounds, pb.bounds);
+                    }
+                }
+            }
+            else
+            {
+                fill(0, span.size(), buckets);
             }
 
             Box left_bound, right_bound;
