@@ -57,50 +57,111 @@ def dist_env():
 # ------------------------------------------------------------------ clocks
 
 class ClockSampler:
-    """nvidia-smi clock / throttle samples while the timed region runs."""
+    """SM clock and clock-event (throttle) reason samples while a timed
+    region runs: an NVML thread every 10 ms, or nvidia-smi where NVML cannot
+    be loaded. The GPU is found by its PCI bus id, so a remapping
+    CUDA_VISIBLE_DEVICES cannot point the samples at another GPU. start()
+    returns once the first sample is in, so even a short region is covered."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, gpu_index):
-        self.gpu = gpu_index
-        self.proc = None
-        self.path = None
+    def __init__(self, cuda_index, period_s=0.01):
+        self.period = period_s
+        self.bus_id = None
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(cuda_index)
+            self.bus_id = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+        except Exception:  # no CUDA device visible: sample by index
+            pass
+        self.cuda_index = cuda_index
+        self.thread = self.proc = self.path = None
+        self.samples = []  # (sm_mhz, sm_max_mhz, set of active reason names)
 
-    def start(self):
+    def _start_nvml(self):
+        import threading
+        import pynvml as nv
+        nv.nvmlInit()
+        h = (nv.nvmlDeviceGetHandleByPciBusId(self.bus_id) if self.bus_id
+             else nv.nvmlDeviceGetHandleByIndex(self.cuda_index))
+        max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        self.done, first = threading.Event(), threading.Event()
+
+        def run():
+            try:
+                while True:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((float(sm), float(max_mhz), {n for n, b in bits.items() if r & b}))
+                    first.set()
+                    if self.done.wait(self.period):
+                        break
+            finally:
+                first.set()
+                nv.nvmlShutdown()
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        first.wait(5.0)
+
+    def _start_smi(self):
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
+        target = self.bus_id if self.bus_id else str(self.cuda_index)
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", target, f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+             "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        t0 = time.perf_counter()
+        while time.perf_counter() - t0 < 5.0 and self.proc.poll() is None and os.path.getsize(self.path) == 0:
+            time.sleep(0.01)
+
+    def start(self):
+        self.samples = []
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+            self._start_nvml()
+            return
+        except Exception:  # no NVML library or no such device: fall back
+            self.thread = None
+        try:
+            self._start_smi()
         except OSError:
             self.proc = None
 
     def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        with open(self.path) as f:
-            for line in f:
-                parts = [p.strip() for p in line.split(",")]
-                if len(parts) < 9:
-                    continue
-                try:
-                    sm.append(float(parts[1]))
-                    mx.append(float(parts[2]))
-                except ValueError:
-                    continue
-                for name, val in zip(names, parts[5:9]):
-                    if val.lower().startswith("active"):
-                        reasons.add(name)
-        os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        if self.thread is not None:
+            self.done.set()
+            self.thread.join(5.0)
+            source = "nvml"
+        elif self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait()
+            with open(self.path) as f:
+                for line in f:
+                    parts = [p.strip() for p in line.split(",")]
+                    if len(parts) < 9:
+                        continue
+                    try:
+                        sm, mx = float(parts[1]), float(parts[2])
+                    except ValueError:
+                        continue
+                    self.samples.append((sm, mx, {n for n, v in zip(self.NAMES, parts[5:9])
+                                                  if v.lower().startswith("active")}))
+            os.unlink(self.path)
+            source = "nvidia-smi"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"], "samples": 0}
+        sm = [s[0] for s in self.samples]
+        reasons = set().union(*(s[2] for s in self.samples)) if self.samples else set()
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(s[1] for s in self.samples) if sm else None,
+                "reasons": sorted(reasons), "samples": len(sm), "source": source}
 
 
 # ------------------------------------------------------------------ profiles
@@ -249,17 +310,24 @@ def run_pt(args, barrier, world):
     stats = abi.RenderStats()
     steps = max(1, args.pt_steps)
 
-    def timed():
+    def timed(clocks=None):
         for _ in range(max(1, args.warmup)):
             integ.render_device(cam, params, fs, stats)
         barrier()
+        if clocks is not None:
+            clocks.start()
         ms, r = 0.0, 0
         for _ in range(steps):
             integ.render_device(cam, params, fs, stats)
             ms += stats.device_ms
             r += stats.closest_rays + stats.shadow_rays
+        if clocks is not None:
+            clocks.info = clocks.stop()
         barrier()
         return ms, r
+
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.info = None
 
     # Default launch configuration, then the autotuned one (which the
     # reported value uses; params.wave_paths = 0 lets the tuned wave apply).
@@ -269,13 +337,14 @@ def run_pt(args, barrier, world):
     if args.no_autotune:
         tuning = abi.Tuning(128, 16, args.pt_wave, 0.0, 0)
         tune_s = 0.0
-        dev_ms, rays = default_ms, default_rays
+        dev_ms, rays = timed(clocks)
+        dev_ms = max_over_ranks([dev_ms], device="cuda")[0]
     else:
         t0 = time.perf_counter()
         tuning = integ.autotune(spp=64, seed=0)
         tune_s = time.perf_counter() - t0
         params.wave_paths = 0
-        dev_ms, rays = timed()
+        dev_ms, rays = timed(clocks)
         dev_ms = max_over_ranks([dev_ms], device="cuda")[0]
     # End to end through the C ABI with a host film (copied back in the call).
     t0 = time.perf_counter()
@@ -292,6 +361,7 @@ def run_pt(args, barrier, world):
                    "tuned": {"block": tuning.block, "short_stack": tuning.short_stack,
                              "wave_paths": tuning.wave_paths, "autotune_s": round(tune_s, 2)},
                    "cuda_graph": True},
+        "clocks": clocks.info,
         "image_mean": float(np.nanmean(film.image())),
         "e2e": {"value": whole_job_rate(paths, world, e2e_s * 1e3), "unit": "paths/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": n_pix * (12 + 4 + 8)},
