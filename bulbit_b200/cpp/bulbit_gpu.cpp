@@ -138,6 +138,20 @@ Float ConstScalar(const FloatTexture* t, const char* what)
     return c->*Get(ConstFloat{});
 }
 
+// True when the alpha test never discards a hit: no alpha texture, or a
+// constant one that is not below 1 (include/bulbit/primitive.h:60-66 tests
+// only alpha < 1), which is what the CLI's material builders attach
+// (cli/material_builder.cpp, alpha = 1 by default).
+bool OpaqueAlpha(const FloatTexture* alpha)
+{
+    if (!alpha)
+    {
+        return true;
+    }
+    auto* c = dynamic_cast<const ConstantTexture<Float>*>(alpha);
+    return c && !(c->*Get(ConstFloat{}) < 1);
+}
+
 // The material of one primitive as the device describes it
 // (src/material/*_material.cpp GetBSDF, constant textures only).
 bbg_material TranslateMaterial(const Material* m)
@@ -146,9 +160,15 @@ bbg_material TranslateMaterial(const Material* m)
     if (m->Is<DiffuseMaterial>())
     {
         const DiffuseMaterial* d = m->Cast<DiffuseMaterial>();
-        if (d->roughness || d->normal || d->alpha)
+        if (d->normal || !OpaqueAlpha(d->alpha))
         {
-            Unsupported("DiffuseMaterial with roughness, normal or alpha textures");
+            Unsupported("DiffuseMaterial with a normal texture or alpha below 1");
+        }
+        // GetBSDF takes LambertianBxDF unless the roughness is > 0
+        // (src/material/diffuse_material.cpp:22-33).
+        if (d->roughness && ConstScalar(d->roughness, "DiffuseMaterial roughness") > 0)
+        {
+            Unsupported("DiffuseMaterial with roughness > 0 (EONBxDF)");
         }
         out.type = BBG_MAT_DIFFUSE;
         PutSpec(out.reflectance, ConstSpectrum(d->reflectance, "DiffuseMaterial reflectance"));
@@ -156,9 +176,9 @@ bbg_material TranslateMaterial(const Material* m)
     else if (m->Is<ConductorMaterial>())
     {
         const ConductorMaterial* c = m->Cast<ConductorMaterial>();
-        if (c->*Get(CondNormal{}) || c->*Get(CondAlpha{}))
+        if (c->*Get(CondNormal{}) || !OpaqueAlpha(c->*Get(CondAlpha{})))
         {
-            Unsupported("ConductorMaterial with normal or alpha textures");
+            Unsupported("ConductorMaterial with a normal texture or alpha below 1");
         }
         out.type = BBG_MAT_CONDUCTOR;
         const SpectrumTexture* eta = c->*Get(CondEta{});
@@ -193,9 +213,9 @@ bbg_material TranslateMaterial(const Material* m)
     else if (m->Is<MetallicRoughnessMaterial>())
     {
         const MetallicRoughnessMaterial* r = m->Cast<MetallicRoughnessMaterial>();
-        if (r->*Get(MrNormal{}) || r->*Get(MrAlpha{}))
+        if (r->*Get(MrNormal{}) || !OpaqueAlpha(r->*Get(MrAlpha{})))
         {
-            Unsupported("MetallicRoughnessMaterial with normal or alpha textures");
+            Unsupported("MetallicRoughnessMaterial with a normal texture or alpha below 1");
         }
         out.type = BBG_MAT_METALLIC_ROUGHNESS;
         PutSpec(out.reflectance, ConstSpectrum(r->*Get(MrBase{}), "MetallicRoughnessMaterial basecolor"));
@@ -408,9 +428,9 @@ void GpuBVH::Upload(const bbg_bvh* tree, GpuTree kind, float split_budget)
         }
         if (const Material* m = p->GetMaterial())
         {
-            if (m->GetAlphaTexture())
+            if (!OpaqueAlpha(m->GetAlphaTexture()))
             {
-                Unsupported("materials with alpha textures");
+                Unsupported("materials with alpha below 1 (cut-outs)");
             }
         }
     }
@@ -653,6 +673,17 @@ Rendering* GpuPathIntegrator::Render(Allocator& alloc, const Camera* camera)
       }
     }));
     return progress;
+}
+
+Integrator* CreateGpuIntegrator(Allocator& alloc, const IntegratorInfo& info, const GpuBVH* accel,
+                                const std::vector<Light*>& lights, const Sampler* sampler)
+{
+    if (info.type != IntegratorType::path)
+    {
+        return nullptr;
+    }
+    return alloc.new_object<GpuPathIntegrator>(accel, lights, sampler, info.max_bounces, info.rr_min_bounces,
+                                               info.regularize_bsdf);
 }
 
 } // namespace bulbit_gpu

@@ -24,8 +24,9 @@
 // Supported scene content (checked in the constructors, which throw
 // std::runtime_error otherwise): Triangle and Sphere shapes; DiffuseMaterial,
 // ConductorMaterial and DielectricMaterial (energy compensation on or off)
-// and MetallicRoughnessMaterial with constant textures and no normal or alpha
-// maps;
+// and MetallicRoughnessMaterial with constant textures and no normal maps
+// (alpha only as a constant not below 1, which the alpha test never cuts;
+// DiffuseMaterial roughness only as a constant not above 0, Lambertian);
 // PointLight, SpotLight, UniformInfiniteLight, DiffuseAreaLight with a
 // constant emission; PerspectiveCamera with a Box, Tent or Gaussian filter;
 // IndependentSampler or StratifiedSampler.
@@ -44,6 +45,7 @@
 #include "bulbit/lights.h"
 #include "bulbit/materials.h"
 #include "bulbit/progress.h"
+#include "bulbit/renderer_info.h"
 #include "bulbit/samplers.h"
 #include "bulbit/shapes.h"
 
@@ -137,5 +139,14 @@ private:
     bbg_integrator* integrator_ = nullptr;
     bbg_render_stats stats_{};
 };
+
+// Integrator::Create (src/integrator/integrator.cpp:16-31) with the GPU
+// accel: IntegratorType::path gives a GpuPathIntegrator with the info's
+// max_bounces, rr_min_bounces and regularize_bsdf, allocated from alloc
+// (released with alloc.delete_object, as the reference's callers do). The
+// other integrator types have no GPU implementation here: nullptr, which is
+// what Integrator::Create returns for a type it cannot make.
+bulbit::Integrator* CreateGpuIntegrator(::Allocator& alloc, const bulbit::IntegratorInfo& info, const GpuBVH* accel,
+                                        const std::vector<bulbit::Light*>& lights, const bulbit::Sampler* sampler);
 
 } // namespace bulbit_gpu

@@ -241,6 +241,38 @@ void CompareRender(Scene& scene, const BVH& bvh, const bulbit_gpu::GpuBVH& gpu, 
     alloc.delete_object(b);
 }
 
+// Which constant textures the drop-in accepts: a roughness of 0 (Lambertian,
+// src/material/diffuse_material.cpp:22-33) and an alpha of 1 (never cut,
+// include/bulbit/primitive.h:60-66) are accepted, as the reference CLI's
+// material builders attach them; a roughness above 0 (EONBxDF) and an alpha
+// below 1 (cut-outs) are refused with an exception.
+void CheckMaterialAcceptance(Result* r)
+{
+    auto attempt = [](Float roughness, Float alpha) {
+        Scene scene;
+        auto* mat = scene.CreateMaterial<DiffuseMaterial>(
+            scene.CreateTexture<ConstantTexture, Spectrum>(Spectrum(0.5f)),
+            scene.CreateTexture<ConstantTexture, Float>(roughness), nullptr,
+            scene.CreateTexture<ConstantTexture, Float>(alpha));
+        scene.CreatePrimitive(scene.CreateShape<Sphere>(Point3(0, 0, 0), 1.0f), mat, MediumInterface{});
+        scene.CreateLight<UniformInfiniteLight>(Spectrum(1.0f));
+        IndependentSampler sampler(1);
+        try
+        {
+            bulbit_gpu::GpuBVH gpu(scene.GetPrimitives());
+            bulbit_gpu::GpuPathIntegrator integrator(&gpu, scene.GetLights(), &sampler, 2);
+        }
+        catch (const std::runtime_error&)
+        {
+            return false;
+        }
+        return true;
+    };
+    r->Expect(attempt(0.0f, 1.0f), "material_opaque_lambertian_accepted_ok");
+    r->Expect(!attempt(0.3f, 1.0f), "material_eon_refused_ok");
+    r->Expect(!attempt(0.0f, 0.5f), "material_cutout_refused_ok");
+}
+
 } // namespace
 
 int main()
@@ -283,6 +315,7 @@ int main()
             StratifiedSampler sampler(8, 4, true, 3);
             CompareRender(scene, bvh, gpu, camera, sampler, 12, &r, "mesh");
         }
+        CheckMaterialAcceptance(&r);
     }
     catch (const std::exception& e)
     {
