@@ -53,6 +53,9 @@ BULBIT_GPU_STEAL(CamVertical, &PerspectiveCamera::vertical)
 BULBIT_GPU_STEAL(CamU, &PerspectiveCamera::u)
 BULBIT_GPU_STEAL(CamV, &PerspectiveCamera::v)
 BULBIT_GPU_STEAL(CamLensRadius, &PerspectiveCamera::lens_radius)
+BULBIT_GPU_STEAL(FilmSamples, &Film::samples)
+BULBIT_GPU_STEAL(FilmCounts, &Film::sample_counts)
+BULBIT_GPU_STEAL(FilmMoments, &Film::moments)
 BULBIT_GPU_STEAL(SamplerSeed, &IndependentSampler::seed)
 BULBIT_GPU_STEAL(StratSeed, &StratifiedSampler::seed)
 BULBIT_GPU_STEAL(StratX, &StratifiedSampler::x_samples)
@@ -635,29 +638,25 @@ Rendering* GpuPathIntegrator::Render(Allocator& alloc, const Camera* camera)
       try
       {
         const int64_t pixels = int64_t(cam.width) * cam.height;
-        const int32_t spp = params.spp;
         std::vector<float> rgb(3 * static_cast<size_t>(pixels)), moments(2 * static_cast<size_t>(pixels));
         std::vector<int32_t> count(static_cast<size_t>(pixels));
-        std::vector<float> path_L(3 * static_cast<size_t>(pixels) * static_cast<size_t>(spp));
-        bbg_film film{ rgb.data(), count.data(), moments.data(), path_L.data() };
+        bbg_film film{ rgb.data(), count.data(), moments.data(), nullptr };
         Check(bbg_render(handle, &cam, &params, &film, BBG_MEM_HOST, stats), "bbg_render");
-        // Film::AddSample for every sample, in each pixel in sample order as
-        // UniDirectionalRayIntegrator::Render does (src/integrator/integrator.cpp:183-197;
-        // BoxFilter weight 1); pixels are independent, so rows run in parallel.
+        // The device film is Film::AddSample (src/reconstruction/film.cpp:26-38)
+        // applied to every non-nullish sample of a pixel in sample order, as
+        // UniDirectionalRayIntegrator::Render calls it (src/integrator/integrator.cpp:183-197),
+        // starting from the zeroed film the constructor leaves: its sums, counts
+        // and luminance moments are the Film's state, stored as they are.
         Film& f = progress->MutableFilm();
+        Spectrum* samples = (f.*Get(FilmSamples{})).get();
+        int32* counts = (f.*Get(FilmCounts{})).get();
+        Point2* mom = (f.*Get(FilmMoments{})).get();
         ParallelFor(0, cam.height, [&](int32 y) {
-            for (int32 x = 0; x < cam.width; ++x)
+            for (int64_t p = int64_t(y) * cam.width; p < int64_t(y + 1) * cam.width; ++p)
             {
-                const size_t base = (size_t(y) * size_t(cam.width) + size_t(x)) * size_t(spp);
-                for (int32 s = 0; s < spp; ++s)
-                {
-                    const float* l = &path_L[3 * (base + size_t(s))];
-                    Spectrum L(l[0], l[1], l[2]);
-                    if (!L.IsNullish())
-                    {
-                        f.AddSample(Point2i(x, y), L);
-                    }
-                }
+                samples[p] = Spectrum(rgb[3 * p], rgb[3 * p + 1], rgb[3 * p + 2]);
+                counts[p] = count[p];
+                mom[p] = Point2(moments[2 * p], moments[2 * p + 1]);
             }
         });
         progress->done.store(true, std::memory_order_release);

@@ -16,10 +16,11 @@
 // OccludedBatch. GpuPathIntegrator is an Integrator with PathIntegrator's
 // constructor (include/bulbit/integrators.h:92-114): the base constructor
 // preprocesses the lights exactly as the reference does, and Render()
-// returns at once a Rendering whose job renders on the GPU and fills its Film
-// through Film::AddSample, sample by sample in the reference's order, so the
-// Film state (sums, counts, luminance moments) is the one the reference's
-// Render() would leave, up to the per-path tolerance of the GPU arithmetic.
+// returns at once a Rendering whose job renders on the GPU and leaves its Film
+// in the state Film::AddSample leaves after the reference's samples in the
+// reference's order (sums, counts and luminance moments, accumulated on the
+// device per pixel in sample order), the state the reference's Render() would
+// leave, up to the per-path tolerance of the GPU arithmetic.
 //
 // Supported scene content (checked in the constructors, which throw
 // std::runtime_error otherwise): Triangle and Sphere shapes; DiffuseMaterial,
