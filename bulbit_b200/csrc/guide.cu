@@ -33,7 +33,7 @@ __device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_
         int row = lane >> 1, half = lane & 1;
         int64_t item = tile * 16 + row;
         float raw[kGuideRaw];
-        bool valid = item < n;
+        bool valid = item < n && src.Valid(item);
         if (valid)
         {
             src.Raw(item, raw);
@@ -67,7 +67,7 @@ __device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_
     for (int half = 0; half < 2; ++half)
     {
         int64_t item = tile * 16 + g + 8 * half;
-        if (item < n)
+        if (item < n && src.Valid(item))
         {
             float* o = src.Out(item);
 #pragma unroll
@@ -107,6 +107,7 @@ struct ArraySrc
     const int32_t* index; // optional indirection (query i -> record index[i])
 
     __device__ __forceinline__ int64_t Id(int64_t i) const { return index ? int64_t(index[i]) : i; }
+    __device__ __forceinline__ bool Valid(int64_t i) const { return !index || index[i] >= 0; }
     __device__ __forceinline__ void Raw(int64_t i, float* r) const
     {
         const float* p = raw + kGuideRaw * Id(i);
@@ -140,6 +141,53 @@ __global__ void __launch_bounds__(32 * kFwdWarps) GuideForwardKernel(const float
 }
 
 constexpr size_t kFwdSmem = size_t(kBfFwd) * 2 + size_t(kCBias) * 4 + size_t(kFwdWarps) * 16 * kXLd * 2;
+
+static_assert(kGuideGroupChunk == 16 * kFwdWarps, "a chunk is one block's set of warp tiles");
+
+// Grouped forward: each block takes a contiguous run of chunks and stages a
+// group's weights whenever the run enters a new group (a chunk never spans
+// two groups), then each warp runs its tile of the chunk with them.
+__global__ void __launch_bounds__(32 * kFwdWarps) GuideGroupedForwardKernel(const float* raw, const int32_t* index,
+                                                                             const int32_t* chunk_start,
+                                                                             int32_t n_groups, const GuideGroup* groups,
+                                                                             float* out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smem);
+    float* bs = reinterpret_cast<float*>(smem + kBfFwd * 2);
+    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem + kBfFwd * 2 + kCBias * 4);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    __nv_bfloat16* x = xs + warp * 16 * kXLd;
+    const int64_t chunks = chunk_start[n_groups];
+    const int64_t c0 = chunks * blockIdx.x / gridDim.x, c1 = chunks * (blockIdx.x + 1) / gridDim.x;
+    const int64_t n = chunks * kGuideGroupChunk;
+    ArraySrc src{ raw, out, index };
+    int32_t staged = -1;
+    for (int64_t c = c0; c < c1; ++c)
+    {
+        // The group whose chunk range holds c (block-uniform).
+        int32_t lo = 0, hi = n_groups - 1;
+        while (lo < hi)
+        {
+            int32_t mid = (lo + hi + 1) >> 1;
+            if (chunk_start[mid] <= c)
+            {
+                lo = mid;
+            }
+            else
+            {
+                hi = mid - 1;
+            }
+        }
+        if (lo != staged)
+        {
+            __syncthreads(); // every warp is done with the previous group's weights
+            StageWeights(groups[lo].wg, groups[lo].pg, ws, bs, kBfFwd);
+            staged = lo;
+        }
+        ForwardTile(src, c * kFwdWarps + warp, n, groups[lo].bounds, ws, bs, x, lane);
+    }
+}
 
 // ---------------------------------------------------------------- training
 
@@ -657,6 +705,31 @@ bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index
     BBG_TRY(GuidePrepare(G, &grid));
     GuideForwardKernel<<<grid, 32 * kFwdWarps, kFwdSmem, st>>>(raw_dev, index_dev, n_dev, n_host, G->bounds,
                                                                  G->bf16.p, G->params.p, out_dev);
+    BBG_CUDA(cudaGetLastError());
+    return BBG_OK;
+}
+
+bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, const int32_t* chunk_start_dev,
+                               int32_t n_groups, const GuideGroup* groups_dev, float* out_dev, cudaStream_t st)
+{
+    static bool smem_set = false;
+    static int grid = 0;
+    if (!smem_set)
+    {
+        BBG_CUDA(cudaFuncSetAttribute(GuideGroupedForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kFwdSmem)));
+        int sms = 148, per = 1;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideGroupedForwardKernel, 32 * kFwdWarps, kFwdSmem);
+        grid = sms * std::max(per, 1);
+        smem_set = true;
+    }
+    if (n_groups <= 0)
+    {
+        return BBG_OK;
+    }
+    GuideGroupedForwardKernel<<<grid, 32 * kFwdWarps, kFwdSmem, st>>>(raw_dev, index_dev, chunk_start_dev, n_groups,
+                                                                        groups_dev, out_dev);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
 }

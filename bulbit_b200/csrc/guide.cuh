@@ -31,12 +31,32 @@ struct bbg_guide
 
 namespace bbg
 {
+// Queries per chunk of the grouped forward (its warps' 16-query tiles): each
+// group's queries start on a chunk boundary, so a chunk reads one group's
+// weights.
+constexpr int kGuideGroupChunk = 128;
+
+// One group's guide as the grouped forward reads it (the device addresses
+// of its BF16 weight image and FP32 parameters, and its scene bounds).
+struct GuideGroup
+{
+    const __nv_bfloat16* wg;
+    const float* pg;
+    GuideBounds bounds;
+};
+
 // Sets the kernels' shared-memory limits (once) and returns the forward grid.
 bbg_status GuidePrepare(bbg_guide* G, int* grid);
 // Forward over n queries (raw records of kGuideRaw floats); index (optional)
 // maps query i to record index[i] for both raw and out. n from n_dev if set.
 bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index_dev, const int32_t* n_dev,
                         int64_t n_host, float* out_dev, cudaStream_t st);
+// Forward over queries bucketed by group (grouped BF16 GEMMs in one launch):
+// index_dev lists record indices, group g's from chunk chunk_start_dev[g] to
+// chunk_start_dev[g + 1] (kGuideGroupChunk entries each, -1 for padding);
+// groups_dev[g] holds group g's guide. Output per record, as GuideForward.
+bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, const int32_t* chunk_start_dev,
+                               int32_t n_groups, const GuideGroup* groups_dev, float* out_dev, cudaStream_t st);
 // Adds the gradient of sum_i -w_i log q_i(dir_i) to the guide's accumulator;
 // capacity bounds n (n from n_dev if set) and sizes the training scratch.
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,

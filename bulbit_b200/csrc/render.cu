@@ -107,6 +107,8 @@ constexpr int32_t kAnyNonSpecularBit = 1 << 17;
 constexpr int32_t kSceneShift = 20;
 constexpr int32_t kSceneMask = 0x7ff << kSceneShift;
 constexpr int32_t kMaxBatchScenes = 0x800;
+// Largest batch rendered with guides (one guide per scene).
+constexpr int32_t kMaxGuidedScenes = 64;
 
 struct FilmDev
 {
@@ -897,8 +899,16 @@ struct GuideDev
     float* t_raw;      // training batch: raw queries, directions, weights
     float* t_dir;
     float* t_w;
-    float* wsum;
-    int32_t rec_cap;
+    float* wsum;       // per scene: sum of the training weights
+    int32_t* rec_count; // per scene: records appended this wave
+    int32_t* rec_n;     // per scene: records kept (at most rec_cap)
+    // Batches: the guide queries bucketed by scene for the grouped forward.
+    int32_t* bucket;      // per scene: queries this level
+    int32_t* cursor;      // per scene: next free bucketed position
+    int32_t* chunk_start; // per scene + 1: first chunk of the scene's queries
+    int32_t* sorted;      // bucketed queue (-1 pads each scene to whole chunks)
+    int32_t rec_cap;   // records per scene (scene k's records start at k rec_cap)
+    int32_t n_scenes;
     int32_t stride;    // paths with index % stride == 0 record training samples
     int32_t train;
     float select;      // probability of sampling the guide rather than the BSDF
@@ -999,7 +1009,8 @@ __device__ __forceinline__ bool DirectLight(const SceneDev& s, const BSDF& bsdf,
     return true;
 }
 
-__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(SceneDev s, WaveDev w, GuideDev g, int parity)
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(Scenes sc, WaveDev w, GuideDev g, int parity)
 {
     const int32_t* q = w.queue[parity];
     int32_t* q_next = w.queue[parity ^ 1];
@@ -1012,8 +1023,10 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(Sce
         V3 ro{ o4.x, o4.y, o4.z }, rd{ d4.x, d4.y, d4.z };
         float prev_pdf = o4.w, eta_scale = d4.w;
         Spec beta{ b4.x, b4.y, b4.z }, L{ L4.x, L4.y, L4.z };
-        PathSampler rng = LoadSampler(s, w, slot);
         int32_t fl = w.flags[slot];
+        const int32_t scene_bits = fl & kSceneMask;
+        const SceneDev& s = sc.Scene(fl >> kSceneShift);
+        PathSampler rng = LoadSampler(s, w, slot);
         int32_t bounce = fl & 0xffff;
         bool specular_bounce = (fl & kSpecularBit) != 0;
         bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
@@ -1152,7 +1165,8 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(Sce
             w.d_eta[slot] = make_float4(rd.x, rd.y, rd.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
             StoreSampler(w, slot, rng);
-            w.flags[slot] = bounce | (specular_bounce ? kSpecularBit : 0) | (any_non_specular ? kAnyNonSpecularBit : 0);
+            w.flags[slot] =
+                scene_bits | bounce | (specular_bounce ? kSpecularBit : 0) | (any_non_specular ? kAnyNonSpecularBit : 0);
         }
         int32_t qi = Append(&w.counts[parity ^ 1], cont);
         if (cont)
@@ -1174,7 +1188,8 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(Sce
     }
 }
 
-__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(SceneDev s, WaveDev w, GuideDev g, int parity)
+template <class Scenes>
+__global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(Scenes sc, WaveDev w, GuideDev g, int parity)
 {
     int32_t* q_next = w.queue[parity ^ 1];
     const int32_t n = w.counts[5];
@@ -1185,8 +1200,10 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(Sce
         float4 d4 = w.d_eta[slot], b4 = w.beta[slot];
         float eta_scale = d4.w;
         Spec beta{ b4.x, b4.y, b4.z };
-        PathSampler rng = LoadSampler(s, w, slot);
         int32_t fl = w.flags[slot];
+        const int32_t scene = kIsBatch<Scenes> ? (fl >> kSceneShift) : 0;
+        const SceneDev& s = sc.Scene(scene);
+        PathSampler rng = LoadSampler(s, w, slot);
         int32_t bounce = fl & 0xffff;
         bool any_non_specular = (fl & kAnyNonSpecularBit) != 0;
         const float4* v = g.vtx + 4 * size_t(slot);
@@ -1282,9 +1299,10 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(Sce
         }
         if (g.train && pdf > 0 && !spec_sample && (wave_base + slot) % g.stride == 0)
         {
-            int32_t r = atomicAdd(&w.counts[6], 1);
+            int32_t r = atomicAdd(&g.rec_count[scene], 1);
             if (r < g.rec_cap)
             {
+                r += scene * g.rec_cap;
                 float* rr = g.rec + size_t(r) * kRecFloats;
                 const float* raw = g.raw + size_t(slot) * kGuideRaw;
                 for (int k = 0; k < kGuideRaw; ++k)
@@ -1310,7 +1328,7 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(Sce
             w.o_pdf[slot] = make_float4(point.x, point.y, point.z, pdf_b);
             w.d_eta[slot] = make_float4(wi.x, wi.y, wi.z, eta_scale);
             w.beta[slot] = make_float4(beta.r, beta.g, beta.b, 0.0f);
-            w.flags[slot] = bounce | (spec_sample ? kSpecularBit : 0) |
+            w.flags[slot] = (fl & kSceneMask) | bounce | (spec_sample ? kSpecularBit : 0) |
                             ((any_non_specular || !spec_sample) ? kAnyNonSpecularBit : 0);
         }
         StoreSampler(w, slot, rng);
@@ -1337,17 +1355,20 @@ __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeB(Sce
 // hit's emission enters with its MIS weight, so on diffuse surfaces, where
 // NEE takes nearly all of it, the guide mostly learns indirect light, and on
 // glossy ones it learns the reflected light too. Weights are then
-// normalised to mean 1 (GuideNormalizeKernel).
+// normalised to mean 1 per scene (GuideNormalizeKernel). Grid row y covers
+// scene y's records.
 __global__ void GuideFinalizeKernel(WaveDev w, GuideDev g)
 {
-    int32_t n = min(w.counts[6], g.rec_cap);
+    const int32_t scene = blockIdx.y;
+    const int32_t n = min(g.rec_count[scene], g.rec_cap);
     if (blockIdx.x == 0 && threadIdx.x == 0)
     {
-        w.counts[7] = n;
+        g.rec_n[scene] = n;
     }
     float local = 0;
-    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
+        const int32_t r = scene * g.rec_cap + i;
         const float* rr = g.rec + size_t(r) * kRecFloats;
         float4 Lf = w.L[g.rec_slot[r]];
         bool started = !isnan(rr[17]);
@@ -1375,18 +1396,19 @@ __global__ void GuideFinalizeKernel(WaveDev w, GuideDev g)
     }
     if ((threadIdx.x & 31) == 0 && local != 0.0f)
     {
-        atomicAdd(g.wsum, local);
+        atomicAdd(&g.wsum[scene], local);
     }
 }
 
-__global__ void GuideNormalizeKernel(WaveDev w, GuideDev g)
+__global__ void GuideNormalizeKernel(GuideDev g)
 {
-    int32_t n = w.counts[7];
-    float sum = *g.wsum;
+    const int32_t scene = blockIdx.y;
+    const int32_t n = g.rec_n[scene];
+    float sum = g.wsum[scene];
     float scale = sum > 0 ? float(n) / sum : 0.0f;
-    for (int32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x)
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     {
-        g.t_w[r] *= scale;
+        g.t_w[size_t(scene) * g.rec_cap + i] *= scale;
     }
 }
 
@@ -1771,10 +1793,12 @@ struct bbg_integrator
 
     // Guided rendering: per-slot query / output / vertex state, training records.
     int64_t g_capacity = 0;
-    int32_t g_rec_cap = 0;
+    int64_t g_rec_cap = 0;
     DevBuf<float> g_raw, g_out, g_rec, g_traw, g_tdir, g_tw, g_wsum;
     DevBuf<float4> g_vtx;
     DevBuf<int32_t> g_queue, g_recid, g_recslot, g_slice;
+    // Per scene (a batch has several): record counters, bucketed queries.
+    DevBuf<int32_t> g_reccount, g_recn, g_bucket, g_cursor, g_chunk, g_sorted;
 
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -1796,7 +1820,9 @@ struct bbg_integrator
     int32_t shape = 0;
     int64_t tuned_wave = 0;
 
-    bbg_status ReserveGuide(int64_t n, int32_t rec_cap, int32_t steps)
+    // Guide buffers for waves of n paths over n_scenes scenes, rec_cap
+    // training records per scene and steps Adam steps per wave.
+    bbg_status ReserveGuide(int64_t n, int32_t rec_cap, int32_t steps, int32_t n_scenes = 1)
     {
         if (n > g_capacity)
         {
@@ -1815,9 +1841,10 @@ struct bbg_integrator
             BBG_TRY(g_recid.alloc(m));
             g_capacity = n;
         }
-        if (rec_cap > g_rec_cap)
+        const int64_t rec_total = int64_t(rec_cap) * n_scenes;
+        if (rec_total > g_rec_cap)
         {
-            size_t r = size_t(rec_cap);
+            size_t r = size_t(rec_total);
             for (auto* b : { &g_rec, &g_traw, &g_tdir, &g_tw })
             {
                 b->reset();
@@ -1828,10 +1855,18 @@ struct bbg_integrator
             BBG_TRY(g_tdir.alloc(r * 3));
             BBG_TRY(g_tw.alloc(r));
             BBG_TRY(g_recslot.alloc(r));
-            g_rec_cap = rec_cap;
+            g_rec_cap = rec_total;
         }
-        BBG_TRY(g_wsum.alloc(1));
-        BBG_TRY(g_slice.alloc(size_t(std::max(1, steps))));
+        const size_t ns = size_t(n_scenes);
+        BBG_TRY(g_wsum.alloc(ns));
+        BBG_TRY(g_slice.alloc(size_t(std::max(1, steps)) * ns));
+        BBG_TRY(g_reccount.alloc(ns));
+        BBG_TRY(g_recn.alloc(ns));
+        BBG_TRY(g_bucket.alloc(ns));
+        BBG_TRY(g_cursor.alloc(ns));
+        BBG_TRY(g_chunk.alloc(ns + 1));
+        BBG_TRY(g_sorted.alloc(size_t(n) + ns * kGuideGroupChunk));
+        BBG_CUDA(cudaMemsetAsync(g_bucket.p, 0, ns * sizeof(int32_t), stream));
         return BBG_OK;
     }
 
@@ -1849,7 +1884,14 @@ struct bbg_integrator
         g.t_dir = g_tdir.p;
         g.t_w = g_tw.p;
         g.wsum = g_wsum.p;
-        g.rec_cap = g_rec_cap;
+        g.rec_count = g_reccount.p;
+        g.rec_n = g_recn.p;
+        g.bucket = g_bucket.p;
+        g.cursor = g_cursor.p;
+        g.chunk_start = g_chunk.p;
+        g.sorted = g_sorted.p;
+        g.rec_cap = int32_t(g_rec_cap);
+        g.n_scenes = 1;
         g.stride = stride;
         g.train = train;
         return g;
@@ -1928,8 +1970,8 @@ struct GridsT
         Shape<3>();
         shade = PersistentGrid(reinterpret_cast<const void*>(ShadeKernel<Scenes>), kBlock);
         film = PersistentGrid(reinterpret_cast<const void*>(FilmKernel<Scenes>), kBlock);
-        shade_a = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeA), kBlock);
-        shade_b = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeB), kBlock);
+        shade_a = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeA<Scenes>), kBlock);
+        shade_b = PersistentGrid(reinterpret_cast<const void*>(GuidedShadeB<Scenes>), kBlock);
         kinds = PersistentGrid(reinterpret_cast<const void*>(ShadeKindsKernel<Scenes>), kBlock);
         scatter = PersistentGrid(reinterpret_cast<const void*>(ShadeScatterKernel), kBlock);
     }
@@ -1995,13 +2037,14 @@ struct GuideCtx
     int32_t* slice = nullptr; // per step: its number of samples (device)
 };
 
-// Splits the wave's training samples into gc.steps batches of gc.batch.
-__global__ void GuideSliceKernel(WaveDev w, int32_t* slice, int32_t batch, int32_t steps)
+// Splits each scene's training samples of the wave into gc.steps batches of
+// gc.batch: slice[scene * steps + k].
+__global__ void GuideSliceKernel(GuideDev g, int32_t* slice, int32_t batch, int32_t steps)
 {
-    int32_t n = w.counts[7];
-    for (int32_t k = threadIdx.x; k < steps; k += blockDim.x)
+    for (int32_t i = threadIdx.x; i < g.n_scenes * steps; i += blockDim.x)
     {
-        slice[k] = max(0, min(batch, n - k * batch));
+        int32_t scene = i / steps, k = i % steps;
+        slice[i] = max(0, min(batch, g.rec_n[scene] - k * batch));
     }
 }
 
@@ -2012,10 +2055,76 @@ __global__ void GuideWaveStartKernel(WaveDev w, GuideDev g)
     {
         g.rec_id[i] = -1;
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0)
+    if (blockIdx.x == 0)
     {
-        w.counts[6] = 0;
-        *g.wsum = 0;
+        for (int32_t k = threadIdx.x; k < g.n_scenes; k += blockDim.x)
+        {
+            g.rec_count[k] = 0;
+            g.wsum[k] = 0;
+        }
+    }
+}
+
+// Bucketing of a level's guide queries by scene for the grouped forward:
+// counts, chunk-aligned offsets (with the padding marked -1), scatter.
+__global__ void GuideBucketCountKernel(WaveDev w, GuideDev g)
+{
+    extern __shared__ int32_t hist[];
+    for (int32_t k = threadIdx.x; k < g.n_scenes; k += blockDim.x)
+    {
+        hist[k] = 0;
+    }
+    __syncthreads();
+    const int32_t n = w.counts[5];
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        atomicAdd(&hist[w.flags[g.queue[j]] >> kSceneShift], 1);
+    }
+    __syncthreads();
+    for (int32_t k = threadIdx.x; k < g.n_scenes; k += blockDim.x)
+    {
+        if (hist[k])
+        {
+            atomicAdd(&g.bucket[k], hist[k]);
+        }
+    }
+}
+
+__global__ void GuideBucketOffsetKernel(GuideDev g)
+{
+    __shared__ int32_t start[kMaxGuidedScenes + 1], count[kMaxGuidedScenes];
+    if (threadIdx.x == 0)
+    {
+        int32_t at = 0;
+        for (int32_t k = 0; k < g.n_scenes; ++k)
+        {
+            count[k] = g.bucket[k];
+            start[k] = at;
+            g.chunk_start[k] = at / kGuideGroupChunk;
+            g.cursor[k] = at;
+            g.bucket[k] = 0; // ready for the next level
+            at += (count[k] + kGuideGroupChunk - 1) / kGuideGroupChunk * kGuideGroupChunk;
+        }
+        start[g.n_scenes] = at;
+        g.chunk_start[g.n_scenes] = at / kGuideGroupChunk;
+    }
+    __syncthreads();
+    for (int32_t k = 0; k < g.n_scenes; ++k)
+    {
+        for (int32_t i = start[k] + count[k] + threadIdx.x; i < start[k + 1]; i += blockDim.x)
+        {
+            g.sorted[i] = -1;
+        }
+    }
+}
+
+__global__ void GuideBucketScatterKernel(WaveDev w, GuideDev g)
+{
+    const int32_t n = w.counts[5];
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        int32_t slot = g.queue[j];
+        g.sorted[atomicAdd(&g.cursor[w.flags[slot] >> kSceneShift], 1)] = slot;
     }
 }
 
@@ -2027,9 +2136,9 @@ bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, co
     LaunchTrace(shape, gr, one, w, parity, false, st);
     if (gc.guide)
     {
-        GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(s, w, gc.dev, parity);
+        GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(one, w, gc.dev, parity);
         BBG_TRY(GuideForward(gc.guide, gc.dev.raw, gc.dev.queue, w.counts + 5, 0, gc.dev.out, st));
-        GuidedShadeB<<<gr.shade_b, kBlock, 0, st>>>(s, w, gc.dev, parity);
+        GuidedShadeB<<<gr.shade_b, kBlock, 0, st>>>(one, w, gc.dev, parity);
     }
     else
     {
@@ -2063,19 +2172,27 @@ bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const 
     return BBG_OK;
 }
 
-// One online training step on the wave's records (after all its levels).
-bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, cudaStream_t st)
+// The online training steps on the wave's records (after all its levels):
+// gc.steps Adam steps of each scene's guide on that scene's records (guides[k]
+// for scene k; one scene outside batches).
+bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, bbg_guide* const* guides, cudaStream_t st)
 {
     WaveDev w = I->Wave();
-    GuideFinalizeKernel<<<256, 256, 0, st>>>(w, gc.dev);
-    GuideNormalizeKernel<<<256, 256, 0, st>>>(w, gc.dev);
-    GuideSliceKernel<<<1, 32, 0, st>>>(w, gc.slice, gc.batch, gc.steps);
-    for (int32_t k = 0; k < gc.steps; ++k)
+    const int32_t ns = gc.dev.n_scenes;
+    const dim3 grid(unsigned(std::max(1, 256 / ns)), unsigned(ns));
+    GuideFinalizeKernel<<<grid, 256, 0, st>>>(w, gc.dev);
+    GuideNormalizeKernel<<<grid, 256, 0, st>>>(gc.dev);
+    GuideSliceKernel<<<1, 256, 0, st>>>(gc.dev, gc.slice, gc.batch, gc.steps);
+    for (int32_t scene = 0; scene < ns; ++scene)
     {
-        size_t off = size_t(k) * size_t(gc.batch);
-        BBG_TRY(GuideAccumulate(gc.guide, gc.dev.t_raw + off * kGuideRaw, gc.dev.t_dir + off * 3, gc.dev.t_w + off,
-                                gc.slice + k, 0, gc.batch, st));
-        BBG_TRY(GuideApply(gc.guide, gc.lr, gc.slice + k, 0, st));
+        for (int32_t k = 0; k < gc.steps; ++k)
+        {
+            size_t off = size_t(scene) * size_t(gc.dev.rec_cap) + size_t(k) * size_t(gc.batch);
+            const int32_t* n = gc.slice + size_t(scene) * gc.steps + k;
+            BBG_TRY(GuideAccumulate(guides[scene], gc.dev.t_raw + off * kGuideRaw, gc.dev.t_dir + off * 3,
+                                    gc.dev.t_w + off, n, 0, gc.batch, st));
+            BBG_TRY(GuideApply(guides[scene], gc.lr, n, 0, st));
+        }
     }
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
@@ -2339,7 +2456,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         }
         if (gc.guide && gc.dev.train)
         {
-            BBG_TRY(EnqueueTraining(I, gc, st));
+            BBG_TRY(EnqueueTraining(I, gc, &gc.guide, st));
         }
     }
     BBG_CUDA(cudaEventRecord(e1, st));
@@ -2521,28 +2638,48 @@ bbg_status CreateIntegrator(bbg_integrator* I, bbg_accel* a, const int32_t* prim
 
 using BatchGrids = GridsT<SceneTable>;
 
-bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int parity, int shape,
-                             cudaStream_t st)
+// One bounce level of a batch. With guides (gc.guide set; groups[k] is
+// scene k's guide), the level's guide queries are bucketed by scene and the
+// scenes' MLPs run as one grouped forward between the two guided passes.
+bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, const GuideCtx& gc,
+                             const GuideGroup* groups, int parity, int shape, cudaStream_t st)
 {
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
     LaunchTrace(shape, gr, t, w, parity, false, st);
-    if (w.sorted)
+    if (gc.guide)
     {
-        ShadeKindsKernel<<<gr.kinds, kBlock, 0, st>>>(t, w, parity);
-        ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
+        GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(t, w, gc.dev, parity);
+        GuideBucketCountKernel<<<gr.scatter, kBlock, size_t(gc.dev.n_scenes) * sizeof(int32_t), st>>>(w, gc.dev);
+        GuideBucketOffsetKernel<<<1, 256, 0, st>>>(gc.dev);
+        GuideBucketScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, gc.dev);
+        BBG_TRY(GuideForwardGrouped(gc.dev.raw, gc.dev.sorted, gc.dev.chunk_start, gc.dev.n_scenes, groups,
+                                    gc.dev.out, st));
+        GuidedShadeB<<<gr.shade_b, kBlock, 0, st>>>(t, w, gc.dev, parity);
     }
-    ShadeKernel<<<gr.shade, kBlock, 0, st>>>(t, w, parity);
+    else
+    {
+        if (w.sorted)
+        {
+            ShadeKindsKernel<<<gr.kinds, kBlock, 0, st>>>(t, w, parity);
+            ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
+        }
+        ShadeKernel<<<gr.shade, kBlock, 0, st>>>(t, w, parity);
+    }
     LaunchTrace(shape, gr, t, w, parity, true, st);
     return BBG_OK;
 }
 
-bbg_status EnqueueBatch(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, int iterations, int shape,
-                        cudaStream_t st)
+bbg_status EnqueueBatch(const BatchGrids& gr, const SceneTable& t, const WaveDev& w, const GuideCtx& gc,
+                        const GuideGroup* groups, int iterations, int shape, cudaStream_t st)
 {
     RaygenKernel<<<gr.raygen, kBlock, 0, st>>>(t, w);
+    if (gc.guide && gc.dev.train)
+    {
+        GuideWaveStartKernel<<<gr.raygen, kBlock, 0, st>>>(w, gc.dev);
+    }
     for (int k = 0; k < iterations; ++k)
     {
-        BBG_TRY(EnqueueBatchLevel(gr, t, w, k & 1, shape, st));
+        BBG_TRY(EnqueueBatchLevel(gr, t, w, gc, groups, k & 1, shape, st));
     }
     FilmKernel<<<gr.film, kBlock, 0, st>>>(t, w);
     BBG_CUDA(cudaGetLastError());
@@ -2567,8 +2704,14 @@ struct bbg_batch
     bbg::SceneTable graph_table{};
     int graph_shape = -1;
     bool graph_shade_sort = false;
+    bbg::GuideDev graph_guide{};
+    const bbg::GuideGroup* graph_groups = nullptr;
     int32_t shape = 0;      // as bbg_integrator::shape, for the batch
     int64_t tuned_wave = 0; // as bbg_integrator::tuned_wave
+    // Guided batches: each scene's guide, as the grouped forward reads them.
+    bbg::DevBuf<bbg::GuideGroup> groups;
+    std::vector<bbg::GuideGroup> host_groups;
+    std::vector<bbg_guide*> guides;
 };
 
 namespace
@@ -2592,11 +2735,19 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         bbg_integrator* I = integrators[i];
         const bbg_camera* cam = &cams[i];
         const bbg_film* film = &films[i];
-        if (!I || params[i].spp != spp || spp <= 0 || params[i].guide || cam->width <= 0 || cam->height <= 0 ||
-            !film->rgb_sum || !film->count || !film->moments)
+        if (!I || params[i].spp != spp || spp <= 0 || (params[i].guide != nullptr) != (params[0].guide != nullptr) ||
+            cam->width <= 0 || cam->height <= 0 || !film->rgb_sum || !film->count || !film->moments)
         {
-            return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: scene %d: bad argument (spp must match, no guide)",
+            return Fail(BBG_ERR_INVALID_ARG,
+                        "bbg_batch_render: scene %d: bad argument (spp must match; a guide for every scene or none)",
                         int(i));
+        }
+        for (int32_t j = 0; j < i && params[i].guide; ++j)
+        {
+            if (params[j].guide == params[i].guide)
+            {
+                return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: scenes %d and %d share a guide", int(j), int(i));
+            }
         }
         if (!I->accel->ordered)
         {
@@ -2657,6 +2808,48 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     }
     BBG_TRY(E->Reserve(wave_paths));
     const BatchGrids gr;
+
+    // Guides: one per scene, trained on that scene's records; the training
+    // settings are the first scene's.
+    GuideCtx gc;
+    const bbg_render_params* p0 = &params[0];
+    if (p0->guide)
+    {
+        if (n > kMaxGuidedScenes)
+        {
+            return Fail(BBG_ERR_UNSUPPORTED, "bbg_batch_render: at most %d scenes with guides", int(kMaxGuidedScenes));
+        }
+        gc.guide = p0->guide;
+        gc.lr = p0->guide_lr > 0 ? p0->guide_lr : 1e-2f;
+        const int32_t batch = p0->guide_batch > 0 ? p0->guide_batch : (1 << 16);
+        const int32_t steps = p0->guide_steps > 0 ? p0->guide_steps : 1;
+        const int64_t samples = int64_t(batch) * steps;
+        if (p0->guide_train && samples * n > (int64_t(1) << 28))
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "guide_batch x guide_steps x scenes exceeds 2^28 training samples");
+        }
+        const int32_t stride = int32_t(std::max<int64_t>(1, (2 * wave_paths + samples - 1) / samples));
+        BBG_TRY(E->ReserveGuide(wave_paths, p0->guide_train ? int32_t(samples) : 0, steps, n));
+        gc.batch = batch;
+        gc.steps = steps;
+        gc.dev = E->Guide(p0->guide_train ? 1 : 0, stride);
+        gc.dev.rec_cap = p0->guide_train ? int32_t(samples) : 0;
+        gc.dev.n_scenes = n;
+        gc.slice = E->g_slice.p;
+        gc.dev.select = (p0->guide_select > 0 && p0->guide_select <= 1) ? p0->guide_select : 0.5f;
+        B->guides.assign(size_t(n), nullptr);
+        B->host_groups.resize(size_t(n));
+        for (int32_t i = 0; i < n; ++i)
+        {
+            bbg_guide* G = params[i].guide;
+            int dummy;
+            BBG_TRY(GuidePrepare(G, &dummy));
+            B->guides[i] = G;
+            B->host_groups[i] = GuideGroup{ G->bf16.p, G->params.p, G->bounds };
+        }
+        BBG_TRY(B->groups.upload(B->host_groups.data(), B->host_groups.size(), st));
+    }
+    const GuideGroup* groups = p0->guide ? B->groups.p : nullptr;
     // The 8-wide layout only when every scene's accel traverses it.
     bool all_wide = true;
     for (int32_t i = 0; i < n; ++i)
@@ -2667,7 +2860,8 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     const bool use_graph = params[0].use_graph != 0;
     if (use_graph && (!E->graph || B->graph_capacity != wave_paths || B->graph_iterations != iterations ||
                       std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != trace_shape ||
-                      B->graph_shade_sort != E->shade_sort))
+                      B->graph_shade_sort != E->shade_sort || !SameGuide(B->graph_guide, gc.dev) ||
+                      B->graph_groups != groups))
     {
         if (E->graph)
         {
@@ -2676,7 +2870,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         cudaGraph_t g;
         BBG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        bbg_status es = EnqueueBatch(gr, table, E->Wave(), iterations, trace_shape, st);
+        bbg_status es = EnqueueBatch(gr, table, E->Wave(), gc, groups, iterations, trace_shape, st);
         cudaError_t ce = cudaStreamEndCapture(st, &g);
         BBG_TRY(es);
         if (ce != cudaSuccess)
@@ -2690,6 +2884,8 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         B->graph_table = table;
         B->graph_shape = trace_shape;
         B->graph_shade_sort = E->shade_sort;
+        B->graph_guide = gc.dev;
+        B->graph_groups = groups;
     }
 
     BBG_CUDA(cudaMemsetAsync(E->stats.p, 0, 2 * sizeof(unsigned long long), st));
@@ -2710,7 +2906,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         else
         {
-            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), iterations, trace_shape, st));
+            BBG_TRY(EnqueueBatch(gr, table, E->Wave(), gc, groups, iterations, trace_shape, st));
         }
         // Paths still queued come from material-less surfaces (no bounce
         // counted): drain them level by level, then redo the film pass.
@@ -2725,7 +2921,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             {
                 return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
             }
-            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), parity, trace_shape, st));
+            BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), gc, groups, parity, trace_shape, st));
             parity ^= 1;
             BBG_CUDA(cudaMemcpyAsync(&left, E->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
             BBG_CUDA(cudaStreamSynchronize(st));
@@ -2733,6 +2929,10 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         if (extra > 0)
         {
             FilmKernel<<<gr.film, kBlock, 0, st>>>(table, E->Wave());
+        }
+        if (gc.guide && gc.dev.train)
+        {
+            BBG_TRY(EnqueueTraining(E, gc, B->guides.data(), st));
         }
     }
     BBG_CUDA(cudaEventRecord(e1, st));

@@ -394,9 +394,11 @@ class GpuBatch:
         check(get_lib().bbg_batch_autotune(self.h, n, ints, cams, params, C.byref(out)), "bbg_batch_autotune")
         return out
 
-    def render(self, integrators, spp, seeds=None, wave_paths=0, use_graph=True, path_L=False):
+    def render(self, integrators, spp, seeds=None, wave_paths=0, use_graph=True, path_L=False, guides=None,
+               train=False, batch=0, lr=0.0, select=0.0, steps=0):
         """Render each GpuPathIntegrator's scene (its own camera) at spp ->
-        (list of Film, batch RenderStats)."""
+        (list of Film, batch RenderStats). guides: one GpuGuide per scene
+        (grouped forward in the batch; trained online with train=True)."""
         n = len(integrators)
         seeds = [it.scene.seed for it in integrators] if seeds is None else seeds
         ints = (C.c_void_p * n)(*[it.h.value for it in integrators])
@@ -409,6 +411,13 @@ class GpuBatch:
             params[i].seed = seeds[i]
             params[i].wave_paths = wave_paths
             params[i].use_graph = 1 if use_graph else 0
+            if guides is not None:
+                params[i].guide = guides[i].h
+                params[i].guide_train = 1 if train else 0
+                params[i].guide_batch = batch
+                params[i].guide_lr = lr
+                params[i].guide_select = select
+                params[i].guide_steps = steps
             film = Film(cams[i].width, cams[i].height, spps[i], path_L=path_L)
             films.append(film)
             fstructs[i] = film.struct()

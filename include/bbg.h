@@ -465,10 +465,16 @@ bbg_status bbg_batch_create(bbg_batch** out);
 bbg_status bbg_batch_destroy(bbg_batch* batch);
 /* Renders n scenes (1 <= n <= 2048): integrators[i] seen through cameras[i]
  * with params[i] into films[i] (host or device memory as mem says). Every
- * params[i].spp must be equal and params[i].guide NULL; every accel must use
- * an ordered traversal (WIDE or ORDERED; the 8-wide layout is traversed when
- * every accel selects it). The wave size and CUDA-graph
- * choice come from params[0]. stats (optional) receives the batch's totals.
+ * params[i].spp must be equal; every accel must use an ordered traversal
+ * (WIDE or ORDERED; the 8-wide layout is traversed when every accel selects
+ * it). The wave size and CUDA-graph choice come from params[0].
+ * Guided batches: either every params[i].guide is set (a distinct guide per
+ * scene, n <= 64) or none is. Each bounce level then buckets the guide
+ * queries by scene and runs all scenes' MLPs in one grouped forward launch
+ * (each 128-query chunk with its scene's weights); with guide_train, each
+ * scene's guide is trained on that scene's records of the wave. The guide
+ * settings (train, batch, steps, lr, select) come from params[0].
+ * stats (optional) receives the batch's totals.
  * Calls on one batch must not overlap, nor overlap renders of the same
  * integrators (their film buffers are reused for host-memory films). */
 bbg_status bbg_batch_render(bbg_batch* batch, int32_t n, bbg_integrator* const* integrators,
