@@ -2174,8 +2174,10 @@ bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const 
 
 // The online training steps on the wave's records (after all its levels):
 // gc.steps Adam steps of each scene's guide on that scene's records (guides[k]
-// for scene k; one scene outside batches).
-bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, bbg_guide* const* guides, cudaStream_t st)
+// for scene k; one scene outside batches). Only scenes first..last can have
+// records (the scenes the wave's paths belong to).
+bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, bbg_guide* const* guides, cudaStream_t st,
+                           int32_t first = 0, int32_t last = 0)
 {
     WaveDev w = I->Wave();
     const int32_t ns = gc.dev.n_scenes;
@@ -2183,7 +2185,7 @@ bbg_status EnqueueTraining(bbg_integrator* I, const GuideCtx& gc, bbg_guide* con
     GuideFinalizeKernel<<<grid, 256, 0, st>>>(w, gc.dev);
     GuideNormalizeKernel<<<grid, 256, 0, st>>>(gc.dev);
     GuideSliceKernel<<<1, 256, 0, st>>>(gc.dev, gc.slice, gc.batch, gc.steps);
-    for (int32_t scene = 0; scene < ns; ++scene)
+    for (int32_t scene = first; scene <= last && scene < ns; ++scene)
     {
         for (int32_t k = 0; k < gc.steps; ++k)
         {
@@ -2932,7 +2934,12 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         }
         if (gc.guide && gc.dev.train)
         {
-            BBG_TRY(EnqueueTraining(E, gc, B->guides.data(), st));
+            // The scenes whose pixels the wave's paths cover.
+            const auto& ps = B->host_pixel_start;
+            const int64_t px_lo = base / spp, px_hi = (base + count - 1) / spp;
+            const int32_t first = int32_t(std::upper_bound(ps.begin(), ps.end(), px_lo) - ps.begin()) - 1;
+            const int32_t last = int32_t(std::upper_bound(ps.begin(), ps.end(), px_hi) - ps.begin()) - 1;
+            BBG_TRY(EnqueueTraining(E, gc, B->guides.data(), st, first, last));
         }
     }
     BBG_CUDA(cudaEventRecord(e1, st));
