@@ -524,7 +524,7 @@ def run_batch(args):
     b.render(integs, spp=32, seeds=[1] * 16)  # capture
     pfilms, pst = b.render(integs, spp=32, seeds=[2] * 16)
     guides = [lib.GpuGuide(a.bounds(), seed=5) for a in accs]
-    gfilms, gst = b.render(integs, spp=32, seeds=[3] * 16, guides=guides, train=True, wave_paths=1 << 18, steps=1)
+    gfilms, gst = b.render(integs, spp=32, seeds=[3] * 16, guides=guides, train=True, wave_paths=1 << 22, steps=4)
     time_ratio = gst.device_ms / pst.device_ms
     ratios = []
     for row, ref, pf, gf in zip(per_scene, refs, pfilms, gfilms):
@@ -536,9 +536,9 @@ def run_batch(args):
     guided_batch = {"plain_batch_ms": pst.device_ms, "guided_batch_ms": gst.device_ms, "time_ratio": time_ratio,
                     "relMSE_ratio_geomean": float(np.exp(np.mean(np.log(ratios)))),
                     "equal_time_ratio_geomean": float(np.exp(np.mean(np.log(ratios)))) * time_ratio,
-                    "config": "16 scenes at 96x96, 32 spp, one guide per scene trained online (each 262,144-path "
-                              "wave: every ninth path records its guided vertices, one Adam step of up to 65,536 "
-                              "records per scene), relMSE against 4096-spp plain renders"}
+                    "config": "16 scenes at 96x96, 32 spp, one guide per scene trained online (after each "
+                              "4,194,304-path wave, 4 Adam steps of up to 65,536 records per scene the wave covers), "
+                              "relMSE against 4096-spp plain renders"}
     for g in guides:
         g.close()
     out = {

@@ -734,18 +734,26 @@ bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, c
     return BBG_OK;
 }
 
+bbg_status GuideReserveTraining(bbg_guide* G, int64_t capacity)
+{
+    const int64_t ld = std::max<int64_t>(16, (capacity + 15) / 16 * 16);
+    BBG_TRY(G->scratch.alloc(size_t(kScratchRows) * size_t(ld)));
+    const int64_t chunks = (ld + kGradChunk - 1) / kGradChunk;
+    BBG_TRY(G->partial.alloc(size_t(chunks) * kGuideParams));
+    return BBG_OK;
+}
+
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
                            const int32_t* n_dev, int64_t n_host, int64_t capacity, cudaStream_t st)
 {
     const int64_t ld = std::max<int64_t>(16, (capacity + 15) / 16 * 16);
-    BBG_TRY(G->scratch.alloc(size_t(kScratchRows) * size_t(ld)));
+    BBG_TRY(GuideReserveTraining(G, capacity));
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
     GuideTrainKernel<<<sms, 32 * kTrainWarps, kTrainSmem, st>>>(raw_dev, dirs_dev, weights_dev, n_dev, n_host,
                                                                 G->bounds, G->bf16.p, G->params.p, G->scratch.p, ld,
                                                                 G->grad.p, G->loss.p);
     const int64_t chunks = (ld + kGradChunk - 1) / kGradChunk;
-    BBG_TRY(G->partial.alloc(size_t(chunks) * kGuideParams));
     const int64_t items = chunks * kGradTiles;
     const int grid = int(std::max<int64_t>(1, std::min<int64_t>((items + kGradWarps - 1) / kGradWarps, 8 * sms)));
     GuideWeightGradKernel<<<grid, 32 * kGradWarps, 0, st>>>(G->scratch.p, ld, n_dev, n_host, G->partial.p);

@@ -57,6 +57,9 @@ bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index
 // groups_dev[g] holds group g's guide. Output per record, as GuideForward.
 bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, const int32_t* chunk_start_dev,
                                int32_t n_groups, const GuideGroup* groups_dev, float* out_dev, cudaStream_t st);
+// Allocates the training scratch for batches of up to capacity samples (so
+// that no allocation falls inside a timed or captured render).
+bbg_status GuideReserveTraining(bbg_guide* G, int64_t capacity);
 // Adds the gradient of sum_i -w_i log q_i(dir_i) to the guide's accumulator;
 // capacity bounds n (n from n_dev if set) and sizes the training scratch.
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,

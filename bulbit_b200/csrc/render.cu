@@ -2374,6 +2374,10 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         gc.dev.select = (p->guide_select > 0 && p->guide_select <= 1) ? p->guide_select : 0.5f;
         int dummy;
         BBG_TRY(GuidePrepare(gc.guide, &dummy));
+        if (p->guide_train)
+        {
+            BBG_TRY(GuideReserveTraining(gc.guide, batch));
+        }
     }
 
     const int iterations = I->max_bounces + 1;
@@ -2846,6 +2850,10 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             bbg_guide* G = params[i].guide;
             int dummy;
             BBG_TRY(GuidePrepare(G, &dummy));
+            if (p0->guide_train)
+            {
+                BBG_TRY(GuideReserveTraining(G, batch));
+            }
             B->guides[i] = G;
             B->host_groups[i] = GuideGroup{ G->bf16.p, G->params.p, G->bounds };
         }
