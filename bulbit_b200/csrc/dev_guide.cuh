@@ -75,22 +75,59 @@ struct GuideBounds
     float inv_extent[3];
 };
 
-// Feature f of a raw query (p, n, wo, roughness).
-__device__ __forceinline__ float GuideFeature(int f, const float* raw, const GuideBounds& b)
+// sin/cos(2^k pi x) for octaves k = k0 .. k0 + count - 1, handed to
+// put(j0 + 2 i, sin, cos): sincospif at every fourth octave, the octaves
+// between by the double-angle identities sin 2y = 2 sin y cos y,
+// cos 2y = 1 - 2 sin^2 y (each doubling at most doubles the absolute error,
+// so three steps keep it within a few float ulps of 1, far below the
+// features' BF16 rounding). An octave's value depends only on x and k, not
+// on where a run starts.
+template <class Put>
+__device__ __forceinline__ void GuideOctaves(float x, int k0, int count, int j0, Put&& put)
 {
-    if (f < 72)
+    float s = 0, c = 1;
+#pragma unroll
+    for (int i = 0; i < count; ++i)
     {
-        int axis = f / 24;
-        int k = (f % 24) >> 1;
-        float pn = (raw[axis] - b.lo[axis]) * b.inv_extent[axis];
-        float x = pn * float(1 << k);
-        return (f & 1) ? cospif(x) : sinpif(x);
+        const int k = k0 + i;
+        if (i == 0 || (k & 3) == 0)
+        {
+            sincospif(x * float(1 << k), &s, &c);
+        }
+        else
+        {
+            const float s2 = 2.0f * s * c;
+            c = 1.0f - 2.0f * s * s;
+            s = s2;
+        }
+        put(j0 + 2 * i, s, c);
     }
-    if (f < 78)
+}
+
+// Features 40 half .. 40 half + 39 of a raw query (p, n, wo, roughness),
+// handed in pairs to put(j, value j, value j + 1) for j = 0, 2, .., 38.
+// The 80 features: f < 72 is sin (f even) or cos (f odd) of 2^k pi p_a, with
+// axis a = f / 24, octave k = (f % 24) / 2 and p_a the position normalised to
+// the scene bounds; then n (3), wo (3), the roughness and a constant 1. Half
+// 0 holds axis 0's octaves and axis 1's octaves 0-7, half 1 axis 1's
+// octaves 8-11, axis 2's and the rest.
+template <class Put>
+__device__ __forceinline__ void GuideFeatures40(const float* raw, const GuideBounds& b, int half, Put&& put)
+{
+    if (half == 0)
     {
-        return raw[f - 72 + 3];
+        GuideOctaves((raw[0] - b.lo[0]) * b.inv_extent[0], 0, 12, 0, put);
+        GuideOctaves((raw[1] - b.lo[1]) * b.inv_extent[1], 0, 8, 24, put);
     }
-    return f == 78 ? raw[9] : 1.0f;
+    else
+    {
+        GuideOctaves((raw[1] - b.lo[1]) * b.inv_extent[1], 8, 4, 0, put);
+        GuideOctaves((raw[2] - b.lo[2]) * b.inv_extent[2], 0, 12, 8, put);
+        put(32, raw[3], raw[4]);
+        put(34, raw[5], raw[6]);
+        put(36, raw[7], raw[8]);
+        put(38, raw[9], 1.0f);
+    }
 }
 
 __device__ __forceinline__ uint32_t PackBf16(float lo, float hi)

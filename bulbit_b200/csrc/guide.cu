@@ -32,17 +32,22 @@ __device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_
     {
         int row = lane >> 1, half = lane & 1;
         int64_t item = tile * 16 + row;
-        float raw[kGuideRaw];
-        bool valid = item < n && src.Valid(item);
-        if (valid)
+        __nv_bfloat16* xr = x + row * kXLd + half * 40;
+        if (item < n && src.Valid(item))
         {
+            float raw[kGuideRaw];
             src.Raw(item, raw);
+            GuideFeatures40(raw, bounds, half, [&](int j, float v0, float v1) {
+                *reinterpret_cast<uint32_t*>(xr + j) = PackBf16(v0, v1);
+            });
         }
-        for (int f = half * 40; f < half * 40 + 40; f += 2)
+        else
         {
-            float v0 = valid ? GuideFeature(f, raw, bounds) : 0.0f;
-            float v1 = valid ? GuideFeature(f + 1, raw, bounds) : 0.0f;
-            *reinterpret_cast<uint32_t*>(x + row * kXLd + f) = PackBf16(v0, v1);
+#pragma unroll
+            for (int j = 0; j < 40; j += 2)
+            {
+                *reinterpret_cast<uint32_t*>(xr + j) = 0u;
+            }
         }
     }
     __syncwarp();
@@ -119,7 +124,7 @@ struct ArraySrc
     __device__ __forceinline__ float* Out(int64_t i) const { return out + kGuideOut * Id(i); }
 };
 
-__global__ void __launch_bounds__(32 * kFwdWarps) GuideForwardKernel(const float* raw, const int32_t* index,
+__global__ void __launch_bounds__(32 * kFwdWarps, 4) GuideForwardKernel(const float* raw, const int32_t* index,
                                                                       const int32_t* n_dev, int64_t n_host,
                                                                       GuideBounds bounds, const __nv_bfloat16* wg,
                                                                       const float* pg, float* out)
@@ -147,7 +152,7 @@ static_assert(kGuideGroupChunk == 16 * kFwdWarps, "a chunk is one block's set of
 // Grouped forward: each block takes a contiguous run of chunks and stages a
 // group's weights whenever the run enters a new group (a chunk never spans
 // two groups), then each warp runs its tile of the chunk with them.
-__global__ void __launch_bounds__(32 * kFwdWarps) GuideGroupedForwardKernel(const float* raw, const int32_t* index,
+__global__ void __launch_bounds__(32 * kFwdWarps, 4) GuideGroupedForwardKernel(const float* raw, const int32_t* index,
                                                                              const int32_t* chunk_start,
                                                                              int32_t n_groups, const GuideGroup* groups,
                                                                              float* out)
@@ -388,19 +393,30 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
             int row = lane >> 1, half = lane & 1;
             int64_t item = tile * 16 + row;
             bool valid = item < n;
-            float r[kGuideRaw];
+            auto put = [&](int j, float v0, float v1) {
+                const int f = half * 40 + j;
+                const __nv_bfloat16 a = __float2bfloat16_rn(v0), b = __float2bfloat16_rn(v1);
+                W.x[row * kXLd + f] = a;
+                W.x[row * kXLd + f + 1] = b;
+                W.xt[f * 16 + row] = a;
+                W.xt[(f + 1) * 16 + row] = b;
+            };
             if (valid)
             {
+                float r[kGuideRaw];
                 for (int k = 0; k < kGuideRaw; ++k)
                 {
                     r[k] = raw[kGuideRaw * item + k];
                 }
+                GuideFeatures40(r, bounds, half, put);
             }
-            for (int f = half * 40; f < half * 40 + 40; ++f)
+            else
             {
-                __nv_bfloat16 v = __float2bfloat16_rn(valid ? GuideFeature(f, r, bounds) : 0.0f);
-                W.x[row * kXLd + f] = v;
-                W.xt[f * 16 + row] = v;
+#pragma unroll
+                for (int j = 0; j < 40; j += 2)
+                {
+                    put(j, 0.0f, 0.0f);
+                }
             }
         }
         __syncwarp();
