@@ -1821,8 +1821,9 @@ struct bbg_integrator
     int64_t tuned_wave = 0;
 
     // Guide buffers for waves of n paths over n_scenes scenes, rec_cap
-    // training records per scene and steps Adam steps per wave.
-    bbg_status ReserveGuide(int64_t n, int32_t rec_cap, int32_t steps, int32_t n_scenes = 1)
+    // training records per scene and steps Adam steps per wave; grouped: the
+    // bucketed queries of the grouped forward (batches).
+    bbg_status ReserveGuide(int64_t n, int32_t rec_cap, int32_t steps, int32_t n_scenes = 1, bool grouped = false)
     {
         if (n > g_capacity)
         {
@@ -1862,11 +1863,14 @@ struct bbg_integrator
         BBG_TRY(g_slice.alloc(size_t(std::max(1, steps)) * ns));
         BBG_TRY(g_reccount.alloc(ns));
         BBG_TRY(g_recn.alloc(ns));
-        BBG_TRY(g_bucket.alloc(ns));
-        BBG_TRY(g_cursor.alloc(ns));
-        BBG_TRY(g_chunk.alloc(ns + 1));
-        BBG_TRY(g_sorted.alloc(size_t(n) + ns * kGuideGroupChunk));
-        BBG_CUDA(cudaMemsetAsync(g_bucket.p, 0, ns * sizeof(int32_t), stream));
+        if (grouped)
+        {
+            BBG_TRY(g_bucket.alloc(ns));
+            BBG_TRY(g_cursor.alloc(ns));
+            BBG_TRY(g_chunk.alloc(ns + 1));
+            BBG_TRY(g_sorted.alloc(size_t(n) + ns * kGuideGroupChunk));
+            BBG_CUDA(cudaMemsetAsync(g_bucket.p, 0, ns * sizeof(int32_t), stream));
+        }
         return BBG_OK;
     }
 
@@ -2835,7 +2839,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             return Fail(BBG_ERR_INVALID_ARG, "guide_batch x guide_steps x scenes exceeds 2^28 training samples");
         }
         const int32_t stride = int32_t(std::max<int64_t>(1, (2 * wave_paths + samples - 1) / samples));
-        BBG_TRY(E->ReserveGuide(wave_paths, p0->guide_train ? int32_t(samples) : 0, steps, n));
+        BBG_TRY(E->ReserveGuide(wave_paths, p0->guide_train ? int32_t(samples) : 0, steps, n, true));
         gc.batch = batch;
         gc.steps = steps;
         gc.dev = E->Guide(p0->guide_train ? 1 : 0, stride);

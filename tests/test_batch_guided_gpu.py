@@ -61,6 +61,9 @@ def test_guided_batch_equals_individual_guided_renders(guided_batch):
     check_equal(films, guided_batch, 4)
     films, _ = b.render(integs, spp=4, path_L=True, guides=guides, use_graph=False, wave_paths=1000)
     check_equal(films, guided_batch, 4)
+    # A batch of one scene.
+    films, _ = lib.GpuBatch().render(integs[:1], spp=4, path_L=True, guides=guides[:1])
+    check_equal(films, guided_batch[:1], 4)
     # A plain render of the same batch after the guided ones.
     films, _ = b.render(integs, spp=4, path_L=True)
     for film, integ in zip(films, integs):
