@@ -2122,13 +2122,32 @@ __global__ void GuideBucketOffsetKernel(GuideDev g)
     }
 }
 
+// Scatter with one atomic per scene per warp: the lanes of a warp that hold
+// the same scene (__match_any_sync) take consecutive positions from a range
+// their lowest lane reserves (a wave's queries mostly belong to one or two
+// scenes, so per-query atomics would all hit one cursor).
 __global__ void GuideBucketScatterKernel(WaveDev w, GuideDev g)
 {
     const int32_t n = w.counts[5];
-    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    const int lane = threadIdx.x & 31;
+    for (int32_t j0 = blockIdx.x * blockDim.x; j0 < n; j0 += gridDim.x * blockDim.x) // warp-uniform
     {
-        int32_t slot = g.queue[j];
-        g.sorted[atomicAdd(&g.cursor[w.flags[slot] >> kSceneShift], 1)] = slot;
+        const int32_t j = j0 + int32_t(threadIdx.x);
+        const bool active = j < n;
+        const int32_t slot = active ? g.queue[j] : 0;
+        const int32_t scene = active ? (w.flags[slot] >> kSceneShift) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, scene);
+        const int leader = __ffs(peers) - 1;
+        int32_t base = 0;
+        if (active && lane == leader)
+        {
+            base = atomicAdd(&g.cursor[scene], __popc(peers));
+        }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (active)
+        {
+            g.sorted[base + __popc(peers & ((1u << lane) - 1u))] = slot;
+        }
     }
 }
 
