@@ -1012,7 +1012,7 @@ __device__ __forceinline__ bool DirectLight(const SceneDev& s, const BSDF& bsdf,
 template <class Scenes>
 __global__ void __launch_bounds__(kBlock, BBG_SHADE_MIN_BLOCKS) GuidedShadeA(Scenes sc, WaveDev w, GuideDev g, int parity)
 {
-    const int32_t* q = w.queue[parity];
+    const int32_t* q = w.sorted ? w.sorted : w.queue[parity];
     int32_t* q_next = w.queue[parity ^ 1];
     const int32_t n = w.counts[parity];
     for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
@@ -2159,6 +2159,11 @@ bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, co
     LaunchTrace(shape, gr, one, w, parity, false, st);
     if (gc.guide)
     {
+        if (w.sorted)
+        {
+            ShadeKindsKernel<<<gr.kinds, kBlock, 0, st>>>(one, w, parity);
+            ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
+        }
         GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(one, w, gc.dev, parity);
         BBG_TRY(GuideForward(gc.guide, gc.dev.raw, gc.dev.queue, w.counts + 5, 0, gc.dev.out, st));
         GuidedShadeB<<<gr.shade_b, kBlock, 0, st>>>(one, w, gc.dev, parity);
@@ -2677,6 +2682,11 @@ bbg_status EnqueueBatchLevel(const BatchGrids& gr, const SceneTable& t, const Wa
     LaunchTrace(shape, gr, t, w, parity, false, st);
     if (gc.guide)
     {
+        if (w.sorted)
+        {
+            ShadeKindsKernel<<<gr.kinds, kBlock, 0, st>>>(t, w, parity);
+            ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
+        }
         GuidedShadeA<<<gr.shade_a, kBlock, 0, st>>>(t, w, gc.dev, parity);
         GuideBucketCountKernel<<<gr.scatter, kBlock, size_t(gc.dev.n_scenes) * sizeof(int32_t), st>>>(w, gc.dev);
         GuideBucketOffsetKernel<<<1, 256, 0, st>>>(gc.dev);
