@@ -116,7 +116,7 @@ class RenderParams(C.Structure):
                 ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float),
                 ("guide_select", C.c_float), ("guide_steps", C.c_int32),
                 ("sampler", C.c_int32), ("x_samples", C.c_int32), ("jitter", C.c_int32),
-                ("shade_order", C.c_int32)]
+                ("shade_order", C.c_int32), ("pass_through_levels", C.c_int32)]
 
 
 class Tuning(C.Structure):

@@ -21,22 +21,33 @@ bbg_status CheckDevice()
     {
         return Fail(BBG_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
     }
-    cudaDeviceProp prop;
-    BBG_CUDA(cudaGetDeviceProperties(&prop, 0));
-    if (prop.major != 10)
+    int dev = 0;
+    BBG_CUDA(cudaGetDevice(&dev));
+    int major = 0, minor = 0;
+    BBG_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    BBG_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+    if (major != 10)
     {
-        return Fail(BBG_ERR_NO_DEVICE, "device 0 is sm_%d%d; this library is built for sm_100a", prop.major,
-                    prop.minor);
+        return Fail(BBG_ERR_NO_DEVICE, "device %d is sm_%d%d; this library is built for sm_100a", dev, major, minor);
     }
     return BBG_OK;
 }
 
+int CurrentSmCount()
+{
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+    {
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return sms;
+}
+
 int PersistentGrid(const void* kernel, int block, size_t smem)
 {
-    int sms = 148, per_sm = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    int per_sm = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem);
-    return sms * std::max(per_sm, 1);
+    return CurrentSmCount() * std::max(per_sm, 1);
 }
 
 // Reference-order traversal (and the counting run): one thread per ray,
@@ -333,6 +344,7 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     if (g->n_prims == 0)
     {
         BBG_TRY(CheckDevice());
+        BBG_CUDA(cudaGetDevice(&a->device));
         BBG_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
         return BBG_OK;
     }
@@ -380,8 +392,13 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
         std::memcpy(a->bounds + 3, root.bmax, 3 * sizeof(float));
     }
 
+    // The handle lives on the caller's current device; every later call on it
+    // runs there (DeviceScope), whatever device is current then.
     BBG_TRY(CheckDevice());
-    BBG_CUDA(cudaSetDevice(0));
+    BBG_CUDA(cudaGetDevice(&a->device));
+    // The allocation-free query's fixed array is reserved now, at set-up
+    // (its module loads lazily), not inside that query's first call.
+    BBG_TRY(ReserveStaticScratch());
     BBG_CUDA(cudaStreamCreateWithFlags(&a->stream, cudaStreamNonBlocking));
     for (int s = 0; s < 2; ++s)
     {
@@ -663,6 +680,7 @@ bbg_status bbg_accel_destroy(bbg_accel* a)
     {
         return BBG_OK;
     }
+    DeviceScope ds(a->device);
     if (a->stream)
     {
         cudaStreamSynchronize(a->stream);
@@ -720,12 +738,22 @@ bbg_status bbg_accel_export(const bbg_accel* a, bbg_bvh_node* nodes_out, int32_t
 
 bbg_status bbg_intersect(bbg_accel* a, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem, void* stream)
 {
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "intersect: null accel");
+    }
+    DeviceScope ds(a->device);
     return Query<false>(a, rays, n, hits, mem, stream);
 }
 
 bbg_status bbg_intersect_any(bbg_accel* a, const bbg_ray* rays, int64_t n, uint8_t* occluded, bbg_memory mem,
                              void* stream)
 {
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "intersect: null accel");
+    }
+    DeviceScope ds(a->device);
     return Query<true>(a, rays, n, occluded, mem, stream);
 }
 

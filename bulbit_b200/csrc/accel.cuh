@@ -8,6 +8,7 @@
 
 struct bbg_accel
 {
+    int device = 0; // the device that was current at creation; every call runs there
     cudaStream_t stream = nullptr;
     int32_t n_prims = 0;
     int32_t n_nodes = 0;
@@ -79,4 +80,8 @@ bbg_status LaunchIntersectAny(bbg_accel* a, const float4* rays, int64_t n, uint8
 // Builds a linear BVH on the device (lbvh.cu) over the uploaded geometry:
 // fills slots, the child-box layout, leaves, root, bounds and depth.
 bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g);
+// Looks up (once per device, the current one) the device address of the
+// allocation-free query's fixed array, which also makes the array exist on
+// that device from this point until the process exits (noalloc.cu).
+bbg_status ReserveStaticScratch();
 } // namespace bbg

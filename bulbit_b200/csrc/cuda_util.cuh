@@ -83,10 +83,47 @@ struct DevBuf
     }
 };
 
-// Device 0 must be a compute-capability 10.x part (the kernels are sm_100a).
+// The current device must be a compute-capability 10.x part (the kernels are
+// sm_100a).
 bbg_status CheckDevice();
 
-// Grid size for a grid-stride kernel: resident blocks per SM x SM count.
+// Grid size for a grid-stride kernel on the current device: resident blocks
+// per SM x SM count.
 int PersistentGrid(const void* kernel, int block, size_t smem = 0);
+
+// SM count of the current device.
+int CurrentSmCount();
+
+// Makes `device` current for the scope of a call on a handle and restores the
+// caller's current device on exit. Handles remember the device that was
+// current when they were created; every later call on them runs there, so
+// one process can hold handles on several GPUs.
+class DeviceScope
+{
+public:
+    explicit DeviceScope(int device)
+    {
+        if (cudaGetDevice(&prev_) == cudaSuccess && prev_ != device)
+        {
+            ok_ = cudaSetDevice(device) == cudaSuccess;
+            switched_ = ok_;
+        }
+    }
+    ~DeviceScope()
+    {
+        if (switched_)
+        {
+            cudaSetDevice(prev_);
+        }
+    }
+    DeviceScope(const DeviceScope&) = delete;
+    DeviceScope& operator=(const DeviceScope&) = delete;
+    bool ok() const { return ok_; }
+
+private:
+    int prev_ = -1;
+    bool switched_ = false;
+    bool ok_ = true;
+};
 
 } // namespace bbg

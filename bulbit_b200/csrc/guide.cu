@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <random>
 #include <vector>
 
@@ -728,17 +729,28 @@ bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index
 bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, const int32_t* chunk_start_dev,
                                int32_t n_groups, const GuideGroup* groups_dev, float* out_dev, cudaStream_t st)
 {
-    static bool smem_set = false;
-    static int grid = 0;
-    if (!smem_set)
+    // Kernel attributes are per device: set once on each device that runs it.
+    constexpr int kMaxDevices = 64;
+    static std::mutex mutex;
+    static int grid_of[kMaxDevices] = {};
+    int dev = 0;
+    BBG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
     {
-        BBG_CUDA(cudaFuncSetAttribute(GuideGroupedForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      int(kFwdSmem)));
-        int sms = 148, per = 1;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideGroupedForwardKernel, 32 * kFwdWarps, kFwdSmem);
-        grid = sms * std::max(per, 1);
-        smem_set = true;
+        return Fail(BBG_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    }
+    int grid = 0;
+    {
+        std::lock_guard<std::mutex> lock(mutex);
+        if (!grid_of[dev])
+        {
+            BBG_CUDA(cudaFuncSetAttribute(GuideGroupedForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(kFwdSmem)));
+            int per = 1;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideGroupedForwardKernel, 32 * kFwdWarps, kFwdSmem);
+            grid_of[dev] = CurrentSmCount() * std::max(per, 1);
+        }
+        grid = grid_of[dev];
     }
     if (n_groups <= 0)
     {
@@ -764,8 +776,7 @@ bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs
 {
     const int64_t ld = std::max<int64_t>(16, (capacity + 15) / 16 * 16);
     BBG_TRY(GuideReserveTraining(G, capacity));
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    const int sms = CurrentSmCount();
     GuideTrainKernel<<<sms, 32 * kTrainWarps, kTrainSmem, st>>>(raw_dev, dirs_dev, weights_dev, n_dev, n_host,
                                                                 G->bounds, G->bf16.p, G->params.p, G->scratch.p, ld,
                                                                 G->grad.p, G->loss.p);
@@ -796,10 +807,9 @@ bbg_status GuidePrepare(bbg_guide* G, int* grid)
         BBG_CUDA(cudaFuncSetAttribute(GuideTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)));
         G->smem_set = true;
     }
-    int sms = 148, per = 1;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    int per = 1;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideForwardKernel, 32 * kFwdWarps, kFwdSmem);
-    *grid = sms * std::max(per, 1);
+    *grid = CurrentSmCount() * std::max(per, 1);
     return BBG_OK;
 }
 
@@ -846,6 +856,7 @@ namespace
 bbg_status Create(const float* aabb, uint64_t seed, bbg_guide* G)
 {
     BBG_TRY(CheckDevice());
+    BBG_CUDA(cudaGetDevice(&G->device));
     BBG_CUDA(cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking));
     for (int a = 0; a < 3; ++a)
     {
@@ -999,6 +1010,11 @@ bbg_status bbg_guide_create(const float* scene_aabb, uint64_t seed, bbg_guide** 
 
 bbg_status bbg_guide_destroy(bbg_guide* G)
 {
+    if (!G)
+    {
+        return BBG_OK;
+    }
+    DeviceScope ds(G->device);
     delete G;
     return BBG_OK;
 }
@@ -1009,6 +1025,7 @@ bbg_status bbg_guide_get_params(bbg_guide* G, float* out)
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_get_params: bad argument");
     }
+    DeviceScope ds(G->device);
     BBG_CUDA(cudaStreamSynchronize(G->stream));
     BBG_CUDA(cudaMemcpy(out, G->params.p, sizeof(float) * kGuideParams, cudaMemcpyDeviceToHost));
     return BBG_OK;
@@ -1020,6 +1037,7 @@ bbg_status bbg_guide_set_params(bbg_guide* G, const float* in)
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_set_params: bad argument");
     }
+    DeviceScope ds(G->device);
     BBG_CUDA(cudaMemcpy(G->params.p, in, sizeof(float) * kGuideParams, cudaMemcpyHostToDevice));
     GuideConvertKernel<<<64, 256, 0, G->stream>>>(G->params.p, G->bf16.p);
     BBG_CUDA(cudaStreamSynchronize(G->stream));
@@ -1032,6 +1050,7 @@ bbg_status bbg_guide_forward(bbg_guide* G, const float* raw, int64_t n, float* o
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_forward: bad argument");
     }
+    DeviceScope ds(G->device);
     if (n == 0)
     {
         return BBG_OK;
@@ -1052,6 +1071,7 @@ bbg_status bbg_guide_gradient(bbg_guide* G, const float* raw, const float* dirs,
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_gradient: bad argument");
     }
+    DeviceScope ds(G->device);
     int dummy;
     BBG_TRY(GuidePrepare(G, &dummy));
     BBG_TRY(Stage(G, raw, dirs, weights, n));
@@ -1077,6 +1097,7 @@ bbg_status bbg_guide_train_step(bbg_guide* G, const float* raw, const float* dir
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_guide_train_step: bad argument");
     }
+    DeviceScope ds(G->device);
     int dummy;
     BBG_TRY(GuidePrepare(G, &dummy));
     BBG_TRY(Stage(G, raw, dirs, weights, n));

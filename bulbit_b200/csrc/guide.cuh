@@ -6,6 +6,7 @@
 
 struct bbg_guide
 {
+    int device = 0; // the device that was current at creation; every call runs there
     cudaStream_t stream = nullptr;
     bbg::GuideBounds bounds{};
     bbg::DevBuf<float> params;  // FP32 master parameters (kGuideParams)

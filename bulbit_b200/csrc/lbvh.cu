@@ -440,8 +440,7 @@ bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g)
 {
     const int32_t n = g->n_prims;
     cudaStream_t st = a->stream;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, 0);
+    const int sms = CurrentSmCount();
     const int grid = std::max(1, std::min((n + kLbvhBlock - 1) / kLbvhBlock, 8 * sms));
 
     DevBuf<float4> boxes;

@@ -80,13 +80,64 @@ __global__ void __launch_bounds__(kBlock) StaticTraceReferenceKernel(AccelView a
     }
 }
 
-// Device address of g_static_scratch per device ordinal, looked up once per
-// device with that device current (the host-side name of a __device__ array
-// is not a device address).
+// Device address of g_static_scratch per device ordinal. The host-side name
+// of a __device__ array is not a device address: it is looked up with
+// cudaGetSymbolAddress, with that device current, once per device at set-up
+// (ReserveStaticScratch, called when an accel is created), and cached. The
+// library does not support cudaDeviceReset while any of its handles exist:
+// their device memory, and this cached address, do not survive it.
 constexpr int kMaxDevices = 64;
 std::mutex g_setup_mutex;
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
+} // namespace
+
+bbg_status ReserveStaticScratch()
+{
+    int dev = 0;
+    BBG_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices)
+    {
+        return Fail(BBG_ERR_UNSUPPORTED, "device ordinal %d out of range", dev);
+    }
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    if (g_scratch_ptr[dev])
+    {
+        return BBG_OK;
+    }
+    // Kernel modules load lazily: looking the symbol up loads this file's
+    // module on the current device and so creates the array now.
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+    if (e != cudaSuccess || !p)
+    {
+        return Fail(BBG_ERR_CUDA, "bbg_intersect_static set-up: cudaGetSymbolAddress failed: %s",
+                    cudaGetErrorString(e));
+    }
+    unsigned char* base = static_cast<unsigned char*>(p);
+    // Load the query's kernels too, and launch each once over zero rays, so
+    // that the device's code and per-thread local-memory reservations for
+    // them are made here rather than in the query's first call.
+    cudaFuncAttributes attr;
+    BBG_CUDA(cudaFuncGetAttributes(&attr, StaticTraceKernel<true>));
+    BBG_CUDA(cudaFuncGetAttributes(&attr, StaticTraceKernel<false>));
+    BBG_CUDA(cudaFuncGetAttributes(&attr, StaticTraceReferenceKernel));
+    int32_t* counter = reinterpret_cast<int32_t*>(base);
+    const AccelView none{};
+    StaticTraceKernel<true><<<1, kBlock>>>(none, nullptr, 0, nullptr, counter);
+    StaticTraceKernel<false><<<1, kBlock>>>(none, nullptr, 0, nullptr, counter);
+    StaticTraceReferenceKernel<<<1, kBlock>>>(none, nullptr, 0, nullptr);
+    BBG_CUDA(cudaGetLastError());
+    BBG_CUDA(cudaDeviceSynchronize());
+    g_scratch_ptr[dev] = base;
+    return BBG_OK;
+}
+
+namespace
+{
+
+// The cached address for the current device; set-up on a device that has
+// none yet (an accel created there always has made it).
 bbg_status ScratchAddress(unsigned char** out)
 {
     int dev = 0;
@@ -95,17 +146,16 @@ bbg_status ScratchAddress(unsigned char** out)
     {
         return Fail(BBG_ERR_UNSUPPORTED, "bbg_intersect_static: device ordinal %d out of range", dev);
     }
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch_ptr[dev])
     {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
-        if (e != cudaSuccess || !p)
+        std::lock_guard<std::mutex> lock(g_setup_mutex);
+        if (g_scratch_ptr[dev])
         {
-            return Fail(BBG_ERR_CUDA, "bbg_intersect_static: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            *out = g_scratch_ptr[dev];
+            return BBG_OK;
         }
-        g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
     }
+    BBG_TRY(ReserveStaticScratch());
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
     *out = g_scratch_ptr[dev];
     return BBG_OK;
 }
@@ -134,7 +184,9 @@ extern "C" bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays
     {
         return Fail(BBG_ERR_UNSUPPORTED, "closest-hit query on an accel with no primitives");
     }
-    BBG_CUDA(cudaSetDevice(0));
+    // The accel's device, whatever device the caller has current (restored
+    // on return).
+    DeviceScope ds(accel->device);
     unsigned char* base = nullptr;
     BBG_TRY(ScratchAddress(&base));
     int32_t* counter = reinterpret_cast<int32_t*>(base);
@@ -144,7 +196,10 @@ extern "C" bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays
     cudaStream_t st = accel->stream;
     BBG_CUDA(cudaMemcpyAsync(d_rays, rays, size_t(n) * sizeof(bbg_ray), cudaMemcpyHostToDevice, st));
     const int32_t m = int32_t(n);
-    if (accel->ordered)
+    // A counting accel traverses in the reference's node order in
+    // bbg_intersect; so does this query (so results agree on exact ties too),
+    // but it records no counts.
+    if (accel->ordered && !accel->counting)
     {
         // The array keeps the previous call's contents: the counter must start at 0.
         BBG_CUDA(cudaMemsetAsync(counter, 0, sizeof(int32_t), st));

@@ -109,6 +109,9 @@ constexpr int32_t kSceneMask = 0x7ff << kSceneShift;
 constexpr int32_t kMaxBatchScenes = 0x800;
 // Largest batch rendered with guides (one guide per scene).
 constexpr int32_t kMaxGuidedScenes = 64;
+// Extra levels after max_bounces + 1 for paths crossing material-less
+// surfaces, unless bbg_render_params.pass_through_levels sets another cap.
+constexpr int kMaxPassThroughLevels = 4096;
 
 struct FilmDev
 {
@@ -1762,6 +1765,7 @@ using namespace bbg;
 
 struct bbg_integrator
 {
+    int device = 0; // the accel's device; every call runs there
     bbg_accel* accel = nullptr;
     int32_t n_lights = 0;
     std::vector<float> pmf;
@@ -2332,6 +2336,11 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_render: bad argument");
     }
+    if (p->guide && p->guide->device != I->device)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_render: the guide lives on device %d, the integrator on device %d",
+                    p->guide->device, I->device);
+    }
     const int64_t n_pixels = int64_t(cam->width) * cam->height;
     const int64_t n_paths = n_pixels * p->spp;
 
@@ -2472,11 +2481,12 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         BBG_CUDA(cudaMemcpyAsync(&left, I->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         BBG_CUDA(cudaStreamSynchronize(st));
         int extra = 0;
+        const int max_extra = p->pass_through_levels > 0 ? p->pass_through_levels : kMaxPassThroughLevels;
         while (left > 0)
         {
-            if (++extra > 4096)
+            if (++extra > max_extra)
             {
-                return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
+                return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", max_extra);
             }
             BBG_TRY(EnqueueLevel(gr, s, I->Wave(), gc, parity, trace_shape, st));
             parity ^= 1;
@@ -2729,6 +2739,7 @@ bbg_status EnqueueBatch(const BatchGrids& gr, const SceneTable& t, const WaveDev
 
 struct bbg_batch
 {
+    int device = 0;        // the device that was current at creation; every call runs there
     bbg_integrator engine; // wave buffers, stream and graph of the batch
     bbg::DevBuf<bbg::SceneDev> scenes;
     bbg::DevBuf<bbg::FilmDev> films;
@@ -2780,6 +2791,11 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
             return Fail(BBG_ERR_INVALID_ARG,
                         "bbg_batch_render: scene %d: bad argument (spp must match; a guide for every scene or none)",
                         int(i));
+        }
+        if (I->device != B->device || (params[i].guide && params[i].guide->device != B->device))
+        {
+            return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: scene %d lives on another device than the batch (%d)",
+                        int(i), B->device);
         }
         for (int32_t j = 0; j < i && params[i].guide; ++j)
         {
@@ -2958,11 +2974,12 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
         BBG_CUDA(cudaMemcpyAsync(&left, E->counts.p + parity, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         BBG_CUDA(cudaStreamSynchronize(st));
         int extra = 0;
+        const int max_extra = p0->pass_through_levels > 0 ? p0->pass_through_levels : kMaxPassThroughLevels;
         while (left > 0)
         {
-            if (++extra > 4096)
+            if (++extra > max_extra)
             {
-                return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", extra);
+                return Fail(BBG_ERR_TIMEOUT, "paths still alive after %d pass-through levels", max_extra);
             }
             BBG_TRY(EnqueueBatchLevel(gr, table, E->Wave(), gc, groups, parity, trace_shape, st));
             parity ^= 1;
@@ -3221,7 +3238,9 @@ bbg_status bbg_integrator_create(bbg_accel* accel, const int32_t* prim_material,
     {
         return Fail(BBG_ERR_UNSUPPORTED, "integrator over an empty scene");
     }
+    DeviceScope ds(accel->device);
     auto* I = new bbg_integrator;
+    I->device = accel->device;
     I->accel = accel;
     I->max_bounces = max_bounces;
     I->rr_min_bounces = rr_min_bounces;
@@ -3240,6 +3259,7 @@ bbg_status bbg_integrator_destroy(bbg_integrator* I)
 {
     if (I)
     {
+        DeviceScope ds(I->device);
         if (I->stream) cudaStreamSynchronize(I->stream);
         delete I;
     }
@@ -3263,6 +3283,7 @@ bbg_status bbg_render(bbg_integrator* I, const bbg_camera* camera, const bbg_ren
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_render: null integrator");
     }
+    DeviceScope ds(I->device);
     return Render(I, camera, params, film, mem, stats);
 }
 
@@ -3347,6 +3368,8 @@ bbg_status bbg_batch_create(bbg_batch** out)
     *out = nullptr;
     BBG_TRY(CheckDevice());
     auto* B = new bbg_batch;
+    cudaGetDevice(&B->device);
+    B->engine.device = B->device;
     cudaError_t e = cudaStreamCreateWithFlags(&B->engine.stream, cudaStreamNonBlocking);
     bbg_status s = e == cudaSuccess ? InitWaveEngine(&B->engine)
                                     : Fail(BBG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
@@ -3363,6 +3386,7 @@ bbg_status bbg_batch_destroy(bbg_batch* B)
 {
     if (B)
     {
+        DeviceScope ds(B->device);
         if (B->engine.stream) cudaStreamSynchronize(B->engine.stream);
         delete B;
     }
@@ -3376,6 +3400,7 @@ bbg_status bbg_batch_render(bbg_batch* B, int32_t n, bbg_integrator* const* inte
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_render: null batch");
     }
+    DeviceScope ds(B->device);
     return RenderBatch(B, n, integrators, cameras, params, films, mem, stats);
 }
 
@@ -3386,6 +3411,7 @@ bbg_status bbg_integrator_autotune(bbg_integrator* I, const bbg_camera* camera, 
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_integrator_autotune: null integrator");
     }
+    DeviceScope ds(I->device);
     return AutotuneIntegrator(I, camera, params, out);
 }
 
@@ -3407,6 +3433,7 @@ bbg_status bbg_batch_autotune(bbg_batch* B, int32_t n, bbg_integrator* const* in
     {
         return Fail(BBG_ERR_INVALID_ARG, "bbg_batch_autotune: null batch");
     }
+    DeviceScope ds(B->device);
     return AutotuneBatch(B, n, integrators, cameras, params, out);
 }
 

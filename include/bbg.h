@@ -160,7 +160,11 @@ bbg_status bbg_bvh_build(const float* prim_aabbs, int32_t n_prims, bbg_bvh_node*
  * and Sphere::GetAABB (src/geometry/sphere.cpp:30) compute them. */
 bbg_status bbg_prim_aabbs(const bbg_geometry* geometry, float* aabbs_out);
 
-/* Uploads geometry and a tree to device 0. bvh == NULL builds the tree with
+/* Uploads geometry and a tree to the current device (every later call on the
+ * handle runs on that device, whichever is current then, and restores the
+ * caller's current device on return; integrators, guides and batches
+ * likewise live on the device current at their creation, an integrator on
+ * its accel's). bvh == NULL builds the tree with
  * bbg_bvh_build. The tree is validated (child and slot ranges, no cycles)
  * before upload; it has at least one slot per primitive (the reference's
  * tree exactly one; a primitive may fill several). */
@@ -213,12 +217,16 @@ bbg_status bbg_intersect(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_h
  * it exists only for such callers. rays and hits are host buffers; at most
  * 262,144 rays per call (larger n returns BBG_ERR_INVALID_ARG). The rays and
  * hits are staged through one fixed device array of about 12 MiB that every
- * device loading this library holds until the process exits; the call itself
- * allocates nothing. The first call on a device looks that array's address up
- * (once per device), so make it before any stream capture. All calls share the
- * array: calls that overlap on the GPU (from several threads or handles at
- * once) race and must be serialised by the caller. Results equal
- * bbg_intersect's for the same accel and traversal mode. */
+ * device holds, from the first accel created on it until the process exits;
+ * the call itself allocates nothing. Set-up happens when an accel is created:
+ * the array's address is looked up on that device (this loads the array) and
+ * the query's kernels are loaded, so calls do no set-up of their own. All
+ * calls share the array: calls that overlap on the GPU (from several threads
+ * or handles at once) race and must be serialised by the caller. Results
+ * equal bbg_intersect's for the same accel and traversal mode (a counting
+ * accel traverses in the reference's order, as bbg_intersect does, but this
+ * query records no counts). The library does not support cudaDeviceReset
+ * while any of its handles exist. */
 bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_hit* hits);
 
 /* Batched BVH::IntersectAny: occluded[i] = 1 if ray i hits anything in
@@ -409,6 +417,12 @@ typedef struct bbg_render_params
                              of the level's queue); BBG_SHADE_QUEUE: in queue
                              order. Results are identical; guided renders shade
                              in queue order. */
+    int32_t pass_through_levels; /* paths that cross material-less surfaces
+                             (which count no bounce) may outlive the
+                             max_bounces + 1 levels of a wave; they are traced
+                             on, level by level, for at most this many extra
+                             levels (0: 4096) before the render gives up with
+                             BBG_ERR_TIMEOUT */
 } bbg_render_params;
 
 enum

@@ -18,8 +18,9 @@ def _ensure_built():
     build.build()
     # Where the reference sources are present, bring the oracle (and the
     # drop-in test program, which links the product library) up to date.
-    if os.path.isdir("/root/reference/src"):
-        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8"], check=True,
+    ref = os.environ.get("BULBIT_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "src")):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "-j8", f"REF={ref}"], check=True,
                        stdout=subprocess.DEVNULL)
 
 

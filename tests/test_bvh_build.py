@@ -116,3 +116,16 @@ def test_oversized_leaf_is_rejected():
     with pytest.raises(lib.BbgError) as e:
         lib.bvh_build(lib.prim_aabbs(s))
     assert "65535" in str(e.value)
+
+
+@pytest.mark.parametrize("make", [
+    lambda: scenes.triangle_soup(1 << 20, seed=1),
+    lambda: scenes.cornell_icosphere(levels=8, width=16, height=16),
+], ids=["microbenchmark_soup_1048576", "cornell_1310734"])
+def test_builder_matches_reference_at_full_size(oracle, make):
+    """The trees the benchmark workloads use, node for node: the 1,048,576-
+    triangle soup and the Cornell box with the 8-level displaced icosphere."""
+    scene = make()
+    rs = oracle.RefScene(scene)
+    mine = lib.bvh_build(lib.prim_aabbs(scene))
+    assert_same_tree(mine, rs.bvh())

@@ -7,10 +7,12 @@ Checked through the C ABI against bbg_intersect on the same accel: identical
 primitive ids and bit-identical t (the tolerance these tests use for
 traversal), on two calls in a row, the second with different rays, so the
 shared array's left-over contents (its work counter in particular) cannot leak
-into the next call. This file is collected last so that a run stopping at the
-first failure has already run every other test; it also passes on its own in a
-fresh process."""
-import ctypes
+into the next call. The device's free memory (cudaMemGetInfo) is the same
+before and after each of the two calls: the array and the query's kernels are
+set up when the accel is created, so even the first call allocates nothing.
+This file is collected last so that a run stopping at the first failure has
+already run every other test; it also passes on its own in a fresh process."""
+import gc
 
 import numpy as np
 import pytest
@@ -29,16 +31,37 @@ def static_intersect(acc, rays):
     return st, hits
 
 
+def free_device_memory():
+    import torch
+    torch.cuda.synchronize()
+    return torch.cuda.mem_get_info()[0]
+
+
 def test_static_entry_point_matches_intersect_on_two_calls():
+    free_device_memory()  # the CUDA context exists before anything is measured
     scene = scenes.triangle_soup(100_000, seed=1)
     acc = lib.GpuAccel(scene)
     first, _ = scenes.soup_rays(MAX_RAYS, seed=2)
     second, _ = scenes.soup_rays(50_000, seed=7)
-    # the 8-wide layout (default) on the first call, the binary one on the second
-    for rays, mode in ((first, abi.BBG_TRAVERSAL_WIDE), (second, abi.BBG_TRAVERSAL_ORDERED)):
+    # The 8-wide layout (default) on the first call, the binary one on the
+    # second; no other library call in between, and no collection of earlier
+    # tests' handles (which would free device memory) while measuring.
+    gc.collect()
+    gc.disable()
+    try:
+        results, free = [], [free_device_memory()]
+        for rays, mode in ((first, abi.BBG_TRAVERSAL_WIDE), (second, abi.BBG_TRAVERSAL_ORDERED)):
+            acc.set_traversal(mode)
+            st, hits = static_intersect(acc, rays)
+            assert st == abi.BBG_OK, lib.get_lib().bbg_last_error()
+            results.append(hits)
+            free.append(free_device_memory())
+    finally:
+        gc.enable()
+    assert free[0] == free[1] == free[2], f"free device memory changed across the calls: {free}"
+    for rays, mode, hits in ((first, abi.BBG_TRAVERSAL_WIDE, results[0]),
+                             (second, abi.BBG_TRAVERSAL_ORDERED, results[1])):
         acc.set_traversal(mode)
-        st, hits = static_intersect(acc, rays)
-        assert st == abi.BBG_OK, lib.get_lib().bbg_last_error()
         prim, t, u, v = acc.intersect(rays)
         assert np.array_equal(hits[:, 0].view(np.int32), prim)
         assert np.array_equal(hits[:, 1].view(np.uint32), t.view(np.uint32))
@@ -46,7 +69,7 @@ def test_static_entry_point_matches_intersect_on_two_calls():
         assert (prim >= 0).mean() > 0.5
 
 
-def test_static_entry_point_reference_order_and_limit():
+def test_static_entry_point_reference_order_counting_and_limit():
     scene = scenes.triangle_soup(20_000, seed=3)
     acc = lib.GpuAccel(scene)
     acc.set_traversal(abi.BBG_TRAVERSAL_REFERENCE)
@@ -55,6 +78,15 @@ def test_static_entry_point_reference_order_and_limit():
     assert st == abi.BBG_OK
     prim, t, _, _ = acc.intersect(rays)
     assert np.array_equal(hits[:, 0].view(np.int32), prim)
+    # A counting accel: both queries traverse in the reference's order.
+    acc.set_traversal(abi.BBG_TRAVERSAL_WIDE)
+    acc.set_counting(True)
+    st, hits = static_intersect(acc, rays)
+    assert st == abi.BBG_OK
+    prim, t, _, _ = acc.intersect(rays)
+    assert np.array_equal(hits[:, 0].view(np.int32), prim)
+    assert np.array_equal(hits[:, 1].view(np.uint32), t.view(np.uint32))
+    acc.set_counting(False)
     # Beyond the fixed array: a clear error, nothing traced.
     big = np.zeros((MAX_RAYS + 1, 8), np.float32)
     st, _ = static_intersect(acc, big)
