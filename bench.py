@@ -394,6 +394,29 @@ def run_pt(args, barrier, world):
                 "d2h_bytes_per_step": n_pix * (12 + 4 + 8)},
         "gpu_launches_per_frame": -(-paths // (tuning.wave_paths - tuning.wave_paths % 64)) * (2 + 4 * 17),
     }
+    # The same SAH tree built on the device (bbg_accel_create_device_sah): its
+    # build time (geometry upload included, as in bvh_build_s), whether it is
+    # byte for byte the host build's tree, and a frame over it.
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lib.GpuAccel(scene, device_sah=True).close()  # the first build in a process also loads its kernels
+    first_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    dacc = lib.GpuAccel(scene, device_sah=True)
+    dev_build_s = time.perf_counter() - t0
+    hn, hs = acc.export()
+    dn, ds = dacc.export()
+    same_tree = bool(hn.shape == dn.shape and np.array_equal(hn.view(np.uint8), dn.view(np.uint8))
+                     and np.array_equal(hs, ds))
+    dinteg = lib.GpuPathIntegrator(dacc, scene)
+    dinteg.set_tuning(tuning.block, tuning.short_stack, tuning.wave_paths)
+    dinteg.render_device(cam, params, fs, stats)  # graph capture
+    dinteg.render_device(cam, params, fs, stats)
+    out["device_sah_tree"] = {"build_s": round(dev_build_s, 4), "first_build_in_process_s": round(first_s, 4),
+                              "host_build_s": round(build_s, 3), "identical_to_host_tree": same_tree,
+                              "ms_per_frame": stats.device_ms, "paths_per_s": stats.paths / (stats.device_ms / 1e3)}
+    dinteg.close()
+    dacc.close()
     integ.close()
     acc.close()
     # The same frame over a tree built on split references (a different tree
@@ -815,6 +838,17 @@ def main():
         step(ev_d[k])
     torch.cuda.synchronize()
     dev_ms = sum(e[0].elapsed_time(e[2]) for e in ev_d)
+    # The reference's SAH tree built on the device: build time beside the
+    # host build (a second build; the first in a process loads the kernels).
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    lib.GpuAccel(scene, device_sah=True).close()
+    first_sah_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    lib.GpuAccel(scene, device_sah=True).close()
+    line["device_sah_tree"] = {"build_ms": (time.perf_counter() - t0) * 1e3,
+                               "first_build_in_process_ms": first_sah_s * 1e3, "host_sah_build_ms": build_s * 1e3,
+                               "tree": "the host SAH build's tree, node for node (tests/test_device_sah_gpu.py)"}
     line["device_built_tree"] = {
         "build_ms": device_build_s * 1e3, "first_build_in_process_ms": first_device_build_s * 1e3,
         "host_sah_build_ms": build_s * 1e3,

@@ -142,6 +142,7 @@ EXPORTS = [
     ("bbg_prim_aabbs", I32, [P, P]),
     ("bbg_accel_create", I32, [P, P, P]),
     ("bbg_accel_create_device_build", I32, [P, P]),
+    ("bbg_accel_create_device_sah", I32, [P, P]),
     ("bbg_accel_destroy", I32, [P]),
     ("bbg_accel_bounds", I32, [P, P]),
     ("bbg_accel_export", I32, [P, P, P, P, P]),

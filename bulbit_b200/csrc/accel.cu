@@ -324,8 +324,16 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
     return depth <= kStackCapacity;
 }
 
-bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, bool device_build = false)
+enum class DeviceTree
 {
+    None,   // the tree is given or built on the host
+    Linear, // linear BVH built on the device (lbvh.cu)
+    Sah     // the reference's SAH tree built on the device (sah_build.cu)
+};
+
+bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, DeviceTree device_tree = DeviceTree::None)
+{
+    const bool device_build = device_tree != DeviceTree::None;
     // Host-side checks and the tree come first: a malformed scene or tree is
     // rejected before any device work.
     BBG_TRY(CheckGeometry(g));
@@ -353,7 +361,8 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     // (device_build) built on the device after the geometry is uploaded.
     if (device_build)
     {
-        a->device_built = true;
+        a->device_built = device_tree == DeviceTree::Linear;
+        a->device_sah = device_tree == DeviceTree::Sah;
         a->ordered = true;
     }
     else if (bvh)
@@ -414,7 +423,7 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     if (device_build)
     {
         BBG_TRY(UploadShading(a, g));
-        BBG_TRY(BuildLbvh(a, g));
+        BBG_TRY(device_tree == DeviceTree::Sah ? BuildSahOnDevice(a, g) : BuildLbvh(a, g));
         BBG_TRY(a->counters.alloc(2));
         BBG_TRY(a->work.alloc(1));
         BBG_CUDA(cudaStreamSynchronize(a->stream));
@@ -618,7 +627,25 @@ bbg_status bbg_accel_create_device_build(const bbg_geometry* geometry, bbg_accel
     }
     *out = nullptr;
     auto* a = new bbg_accel;
-    bbg_status s = CreateAccel(geometry, nullptr, a, true);
+    bbg_status s = CreateAccel(geometry, nullptr, a, DeviceTree::Linear);
+    if (s != BBG_OK)
+    {
+        bbg_accel_destroy(a);
+        return s;
+    }
+    *out = a;
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_create_device_sah(const bbg_geometry* geometry, bbg_accel** out)
+{
+    if (!out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_create_device_sah: out is NULL");
+    }
+    *out = nullptr;
+    auto* a = new bbg_accel;
+    bbg_status s = CreateAccel(geometry, nullptr, a, DeviceTree::Sah);
     if (s != BBG_OK)
     {
         bbg_accel_destroy(a);
@@ -731,6 +758,21 @@ bbg_status bbg_accel_export(const bbg_accel* a, bbg_bvh_node* nodes_out, int32_t
     }
     if (n_nodes_out) *n_nodes_out = a->n_nodes;
     if (n_slots_out) *n_slots_out = a->n_slots;
+    if (a->device_sah)
+    {
+        // The tree lives on the device only.
+        DeviceScope ds(a->device);
+        if (nodes_out)
+        {
+            BBG_CUDA(cudaMemcpy(nodes_out, a->nodes.p, size_t(a->n_nodes) * sizeof(bbg_bvh_node), cudaMemcpyDeviceToHost));
+        }
+        if (slot_prims_out)
+        {
+            BBG_CUDA(cudaMemcpy(slot_prims_out, a->slot_prims.p, size_t(a->n_slots) * sizeof(int32_t),
+                                cudaMemcpyDeviceToHost));
+        }
+        return BBG_OK;
+    }
     if (nodes_out) std::memcpy(nodes_out, a->host_nodes.data(), a->host_nodes.size() * sizeof(bbg_bvh_node));
     if (slot_prims_out) std::memcpy(slot_prims_out, a->host_slots.data(), a->host_slots.size() * sizeof(int32_t));
     return BBG_OK;

@@ -28,7 +28,9 @@ struct bbg_accel
     int32_t n_wide8 = 0;
     int32_t depth8 = 0;
     bool use_wide8 = false;    // ordered queries run over the 8-wide layout
-    bool device_built = false; // tree built on the device (no reference node layout)
+    bool device_built = false; // linear BVH built on the device (no reference node layout)
+    bool device_sah = false;   // the reference's SAH tree built on the device (tree arrays device-only)
+    bbg::DevBuf<int32_t> slot_prims; // device_sah: slot -> primitive (for export)
 
     // Shading data (the reference Mesh arrays and shapes).
     bbg::DevBuf<int2> prim_shape;     // (kind, index) per primitive
@@ -80,6 +82,11 @@ bbg_status LaunchIntersectAny(bbg_accel* a, const float4* rays, int64_t n, uint8
 // Builds a linear BVH on the device (lbvh.cu) over the uploaded geometry:
 // fills slots, the child-box layout, leaves, root, bounds and depth.
 bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g);
+// Builds the reference's binned SAH tree on the device (sah_build.cu) over the
+// uploaded geometry, node for node as BuildBvh does on the host: fills the
+// reference nodes, slots, the child-box layout, leaves, root, the 8-wide
+// layout, bounds, depth and the slot order.
+bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g);
 // Looks up (once per device, the current one) the device address of the
 // allocation-free query's fixed array, which also makes the array exist on
 // that device from this point until the process exits (noalloc.cu).

@@ -94,13 +94,18 @@ NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("offset", "<i4")
 class GpuAccel:
     """The GPU accel beside the reference BVH (bbg_accel_*)."""
 
-    def __init__(self, scene, bvh=None, device_build=False, split=None):
+    def __init__(self, scene, bvh=None, device_build=False, split=None, device_sah=False):
         """bvh: the reference's tree (nodes, slots); device_build: the linear BVH
-        built on the device; split: extra references per primitive for the
-        split-reference SAH build (bbg_accel_create_split)."""
+        built on the device; device_sah: the reference's SAH tree built on the
+        device (bbg_accel_create_device_sah); split: extra references per
+        primitive for the split-reference SAH build (bbg_accel_create_split)."""
         self.scene = scene
         self._g = scene.geometry()
         self.h = C.c_void_p()
+        if device_sah:
+            check(get_lib().bbg_accel_create_device_sah(C.byref(self._g), C.byref(self.h)),
+                  "bbg_accel_create_device_sah")
+            return
         if device_build:
             check(get_lib().bbg_accel_create_device_build(C.byref(self._g), C.byref(self.h)),
                   "bbg_accel_create_device_build")

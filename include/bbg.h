@@ -196,6 +196,19 @@ bbg_status bbg_split_references(const bbg_geometry* geometry, float budget, int3
  * the device (traversal WIDE by default, ORDERED selectable; no reference
  * node order, no counting, no export). */
 bbg_status bbg_accel_create_device_build(const bbg_geometry* geometry, bbg_accel** out);
+
+/* Uploads geometry and builds, on the device, the tree bbg_bvh_build builds
+ * on the host: the reference's 12-bucket binned SAH tree
+ * (BVH::BuildRecursive / FlattenBVH, src/accel/bvh.cpp:56-297) node for node
+ * (same boxes, axes, child offsets and leaf primitives in the same order,
+ * leaves in depth-first slot order), in milliseconds instead of the host
+ * build's seconds on millions of primitives. One launch per tree level: a
+ * block per node of more than 32 primitives, a warp per smaller one; the
+ * bucket and cost arithmetic is the reference's, and std::partition's swap
+ * order is reproduced by prefix sums. Every traversal mode, counting and
+ * bbg_accel_export work as for a host-built tree (export copies the tree
+ * from the device). */
+bbg_status bbg_accel_create_device_sah(const bbg_geometry* geometry, bbg_accel** out);
 bbg_status bbg_accel_destroy(bbg_accel* accel);
 
 /* Root AABB (6 floats), as BVH::GetAABB (src/accel/bvh.cpp:363). */
