@@ -500,8 +500,13 @@ def run_guided(args):
                       "guided_64spp_relMSE": pre, "plain_64spp_relMSE": pl}
     # Monte Carlo error falls as 1/time, so relMSE x time compares the two at
     # exactly equal time; the raw ratio at the matched spp is reported too.
+    mlp = profile_values("guide_mlp_cornell128.md")
     out = {
         "metric": "relMSE at equal time, guided / plain", "value": (e_guided * t_guided) / (e_plain * t_plain),
+        "mlp": {"kernels": "GuideForwardKernel, GuideWeightGradKernel (bulbit_b200/csrc/guide.cu; mma.sync BF16)",
+                "forward_tensor_pipe_active": mlp.get("forward_tensor_pipe_active"),
+                "wgrad_tensor_pipe_active": mlp.get("wgrad_tensor_pipe_active"),
+                "profile": "profiles/guide_mlp_cornell128.md"},
         "higher_is_better": False, "raw_relmse_ratio": e_guided / e_plain,
         "plain": {"spp": 64, "device_ms": t_plain, "relMSE": e_plain},
         "guided": {"spp": spp_eq, "device_ms": t_guided, "relMSE": e_guided, "probe_64spp_device_ms": t_probe,
