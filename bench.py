@@ -523,6 +523,49 @@ def run_guided(args):
     return out
 
 
+def run_guided_sweep(args):
+    """Where the guided estimator bottoms out on the path-tracing scene (the
+    Cornell box with the displaced gold icosphere at args.guided_res): guided
+    against plain relMSE, at equal spp and at equal device time, over the
+    guide/BSDF selection probability, the training budget (frames of online
+    training before the measured renders, which keep training), and at one
+    point the learning rate and the Adam steps per wave. Each row: three
+    64-spp renders; relMSE against a 16384-spp plain render."""
+    from bulbit_b200 import lib, scenes
+    res, wave = args.guided_res, 1 << 21
+    scene = scenes.cornell_icosphere(levels=8, width=res, height=res, spp=64, max_bounces=16)
+    acc = lib.GpuAccel(scene)
+    integ = lib.GpuPathIntegrator(acc, scene)
+    ref = integ.render(spp=16384, seed=7).image()
+    integ.render(spp=64, seed=1)  # graph capture
+    plain = [integ.render(spp=64, seed=2 + k) for k in range(3)]
+    e_plain = float(np.mean([rel_mse(f.image(), ref) for f in plain]))
+    t_plain = float(np.mean([f.stats.device_ms for f in plain]))
+    rows = []
+    grid = [(sel, pre, 1e-2, 8) for sel in (0.1, 0.25, 0.5) for pre in (0, 10, 40)]
+    grid += [(0.25, 10, 3e-3, 8), (0.25, 10, 1e-2, 32)]
+    for sel, pre, lr, steps in grid:
+        g = lib.GpuGuide(acc.bounds(), seed=11)
+        kw = dict(guide=g, train=True, wave_paths=wave, steps=steps, lr=lr, select=sel)
+        for k in range(pre):
+            integ.render(spp=64, seed=1000 + k, **kw)
+        films = [integ.render(spp=64, seed=2000 + k, **kw) for k in range(3)]
+        e = float(np.mean([rel_mse(f.image(), ref) for f in films]))
+        t = float(np.mean([f.stats.device_ms for f in films]))
+        rows.append({"select": sel, "pretrain_frames": pre, "lr": lr, "adam_steps_per_wave": steps, "relMSE": e,
+                     "device_ms": t, "relMSE_ratio": e / e_plain, "time_ratio": t / t_plain,
+                     "equal_time_ratio": e * t / (e_plain * t_plain)})
+        g.close()
+    integ.close()
+    acc.close()
+    best = min(rows, key=lambda r: r["equal_time_ratio"])
+    return {"metric": "relMSE at equal time, guided / plain (sweep)", "best": best, "rows": rows,
+            "plain": {"spp": 64, "relMSE": e_plain, "device_ms": t_plain},
+            "config": {"workload": f"Cornell box + displaced gold icosphere (1,310,720 triangles) at {res}x{res}, "
+                                   "16 bounces, 64 spp per render, relMSE against a 16384-spp plain render",
+                       "wave_paths": wave, "guide_batch": 1 << 16}}
+
+
 def run_batch(args):
     """The batched uneven multi-scene workload: 16 Cornell-box variants
     (seeds 0-15: displaced geodesic sphere of 10^4-2x10^6 triangles drawn
@@ -652,7 +695,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=N_RAYS, help="rays per query set (smaller cases for profiling)")
-    ap.add_argument("--workload", default="all", choices=["all", "rays", "pt", "guided", "batch", "guided-frame"])
+    ap.add_argument("--workload", default="all",
+                    choices=["all", "rays", "pt", "guided", "batch", "guided-frame", "guided-sweep"])
     ap.add_argument("--no-autotune", action="store_true", help="path tracing: default launch configuration only")
     ap.add_argument("--no-batch", action="store_true", help="default workload: leave out the 16-scene batch")
     ap.add_argument("--guided-res", type=int, default=256)
@@ -712,6 +756,10 @@ def main():
             print(json.dumps({"guided_frame": {"device_ms": f.stats.device_ms, "paths": f.stats.paths,
                                                "closest_rays": f.stats.closest_rays,
                                                "shadow_rays": f.stats.shadow_rays}}))
+        return
+    if args.workload == "guided-sweep":
+        if rank == 0:
+            print(json.dumps({"guided_sweep": run_guided_sweep(args)}))
         return
     if args.workload == "batch":
         if rank == 0:

@@ -458,6 +458,10 @@ void GpuBVH::Upload(const bbg_bvh* tree, GpuTree kind, float split_budget)
     {
         Check(bbg_accel_create_device_build(&g, &accel_), "bbg_accel_create_device_build");
     }
+    else if (kind == GpuTree::DeviceSah)
+    {
+        Check(bbg_accel_create_device_sah(&g, &accel_), "bbg_accel_create_device_sah");
+    }
     else
     {
         Check(bbg_accel_create_split(&g, split_budget, &accel_), "bbg_accel_create_split");

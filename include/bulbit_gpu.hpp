@@ -60,16 +60,18 @@ namespace bulbit_gpu
 {
 
 // The tree a GpuBVH built from a primitive list uses. Reference: the same
-// SAH tree as BVH::BVH (hits identical to the reference's). DeviceLinear: a
-// linear BVH built on the GPU in milliseconds. SplitReferences: the SAH
-// build over split triangle references (faster traversal of long or
-// diagonal triangles, a longer build). The last two change only which of
-// two hits at exactly the same t is returned.
+// SAH tree as BVH::BVH (hits identical to the reference's), built on the
+// host. DeviceSah: that same tree, node for node, built on the GPU in
+// milliseconds. DeviceLinear: a linear BVH built on the GPU. SplitReferences:
+// the SAH build over split triangle references (faster traversal of long or
+// diagonal triangles, a longer build). The last two change only which of two
+// hits at exactly the same t is returned.
 enum class GpuTree
 {
     Reference,
     DeviceLinear,
-    SplitReferences
+    SplitReferences,
+    DeviceSah
 };
 
 class GpuBVH : public bulbit::Intersectable
