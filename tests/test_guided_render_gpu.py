@@ -150,22 +150,3 @@ def test_guide_only_selection_is_unbiased():
     guide = lib.GpuGuide(acc.bounds(), seed=3)
     check_unbiased(plain, integ.render(spp=1024, seed=2, guide=guide, select=0.9999), "select 0.9999")
 
-
-def test_guiding_beats_plain_on_the_glass_sphere():
-    """Where the integrand is hard for the BSDF, the trained guide wins: the
-    batch's variant 14 (a displaced glass sphere of 816,094 triangles in the
-    Cornell box; much of the light reaching the floor and walls has passed
-    through the glass), at 96x96, 32 spp. After ten 32-spp frames of online
-    training, the guided relMSE against a 4096-spp plain render is below 0.6x
-    the plain tracer's at the same spp (mean of three seeds each)."""
-    scene = scenes.cornell_batch_variant(14, spp=32, resolution=96)
-    acc = lib.GpuAccel(scene)
-    integ = lib.GpuPathIntegrator(acc, scene)
-    ref = integ.render(spp=4096, seed=7).image()
-    guide = lib.GpuGuide(acc.bounds(), seed=5)
-    for i in range(10):
-        integ.render(spp=32, seed=100 + i, guide=guide, train=True, wave_paths=1 << 18, steps=4)
-    e_plain = np.mean([rel_mse(integ.render(spp=32, seed=20 + k).image(), ref) for k in range(3)])
-    e_guided = np.mean([rel_mse(integ.render(spp=32, seed=30 + k, guide=guide).image(), ref) for k in range(3)])
-    print(f"glass variant, 32 spp: plain relMSE {e_plain:.4e}, guided {e_guided:.4e}, ratio {e_guided / e_plain:.3f}")
-    assert e_guided < 0.6 * e_plain
