@@ -120,7 +120,7 @@ struct BatchSrc
 
 // Ordered traversal: persistent warps pulling rays from a work counter, over
 // the child-box layout or (WIDE) the 8-wide layout.
-template <bool ANY, bool WIDE>
+template <bool ANY, bool WIDE, bool SPHERES = true>
 __global__ void __launch_bounds__(kTraceBlock) PersistentTraceKernel(AccelView a, const float4* __restrict__ rays,
                                                                      int32_t n, float4* __restrict__ hits,
                                                                      uint8_t* __restrict__ occluded, int32_t* next)
@@ -128,7 +128,7 @@ __global__ void __launch_bounds__(kTraceBlock) PersistentTraceKernel(AccelView a
     BatchSrc<ANY> src{ rays, hits, occluded };
     if constexpr (WIDE)
     {
-        TracePersistentWide<ANY>(a, n, next, src);
+        TracePersistentWide<ANY, BatchSrc<ANY>, kTraversalBlock, kShortStack, SPHERES>(a, n, next, src);
     }
     else
     {
@@ -164,7 +164,9 @@ static bbg_status LaunchTrace(bbg_accel* a, const float4* rays, int64_t n, float
     }
     else
     {
-        auto k = a->wide8_active() ? PersistentTraceKernel<ANY, true> : PersistentTraceKernel<ANY, false>;
+        auto k = !a->wide8_active() ? PersistentTraceKernel<ANY, false>
+                 : a->has_spheres   ? PersistentTraceKernel<ANY, true>
+                                    : PersistentTraceKernel<ANY, true, false>;
         int grid = PersistentGrid(reinterpret_cast<const void*>(k), kTraceBlock);
         grid = int(std::min<int64_t>(grid, (n + kTraceBlock - 1) / kTraceBlock));
         const int64_t chunk = int64_t(1) << 30;
@@ -344,6 +346,7 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     for (int32_t i = 0; i < g->n_prims; ++i)
     {
         a->host_prim_shape[i] = make_int2(g->prim_kind[i], g->prim_index[i]);
+        a->has_spheres = a->has_spheres || g->prim_kind[i] == BBG_PRIM_SPHERE;
     }
     a->host_tri_indices.assign(g->tri_indices, g->tri_indices + 3 * size_t(g->n_triangles));
     a->host_positions.assign(g->positions, g->positions + 3 * size_t(g->n_vertices));

@@ -41,6 +41,7 @@ struct bbg_accel
     bbg::DevBuf<float> uvs;           // 2 per vertex
     bbg::DevBuf<bbg_sphere> spheres;
     bool has_shading = false;
+    bool has_spheres = false; // any sphere primitive (else the triangle-only traversal kernels run)
 
     // Host copies of the tree (export, light set-up).
     std::vector<bbg_bvh_node> host_nodes;

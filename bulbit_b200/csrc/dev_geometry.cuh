@@ -192,6 +192,9 @@ struct TraceResult
 };
 
 // One leaf slot: the primitive's test with the current [t_min, t_max].
+// SPHERES = false: the tree holds triangles only (no sphere test compiled in,
+// which keeps the traversal kernels' register count down).
+template <bool SPHERES = true>
 __device__ __forceinline__ bool TestSlot(const AccelView& a, int32_t slot, const RayQ& q, float t_min, float t_max,
                                          TraceResult* res)
 {
@@ -202,7 +205,7 @@ __device__ __forceinline__ bool TestSlot(const AccelView& a, int32_t slot, const
     uint32_t tag = __float_as_uint(s0.w);
     float t, u = 0, v = 0;
     bool hit;
-    if (tag & kSphereBit)
+    if (SPHERES && (tag & kSphereBit))
     {
         hit = IntersectSphere(V3{ s0.x, s0.y, s0.z }, s1, V3{ s2.x, s2.y, s2.z }, s2.w, q.o, q.d, t_min, t_max, &t);
     }
@@ -677,7 +680,7 @@ __device__ __forceinline__ int32_t SelectRef8(const int4& a, const int4& b, uint
 // the registers of the node just opened; only a group taken off the stack
 // reads its reference from memory. Every push is one tree level deeper than
 // the last, so the tree depth bounds the stack.
-template <bool ANY, class Src, int BLOCK = kTraversalBlock, int SHORT = kShortStack>
+template <bool ANY, class Src, int BLOCK = kTraversalBlock, int SHORT = kShortStack, bool SPHERES = true>
 __device__ __forceinline__ void TracePersistentWide(const AccelView& a, int32_t n, int32_t* next, Src& src)
 {
     const unsigned kFull = 0xffffffffu;
@@ -782,7 +785,7 @@ __device__ __forceinline__ void TracePersistentWide(const AccelView& a, int32_t 
                 bool stop = false;
                 for (int32_t i = 0; i < count; ++i)
                 {
-                    if (TestSlot(av, first + i, q, t_min, t_max, &res))
+                    if (TestSlot<SPHERES>(av, first + i, q, t_min, t_max, &res))
                     {
                         if (ANY)
                         {

@@ -412,7 +412,8 @@ struct ShadowBatchSrc : ShadowSrc
 // per block and stack entries per thread kept in shared memory (0: the
 // whole traversal stack in local memory). A trace shape passed to the launch
 // functions is a shape index, plus kNumShapes when the tree's 8-wide layout is
-// traversed.
+// traversed (2 kNumShapes when that tree holds triangles only: kernels without
+// the sphere test, fewer registers per thread).
 struct TraversalShape
 {
     int block;
@@ -421,7 +422,7 @@ struct TraversalShape
 constexpr int kNumShapes = 4;
 constexpr TraversalShape kShapes[kNumShapes] = { { 128, 16 }, { 128, 0 }, { 128, 8 }, { 256, 16 } };
 
-template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack, bool WIDE = false>
+template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack, bool WIDE = false, bool SPHERES = true>
 __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int parity)
 {
     const int32_t n = w.counts[parity];
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int
         ClosestBatchSrc src{ { w.queue[parity], w.o_pdf, w.d_eta, w.hit }, w.flags, sc.scenes };
         if constexpr (WIDE)
         {
-            TracePersistentWide<false, ClosestBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
+            TracePersistentWide<false, ClosestBatchSrc, BLOCK, SHORT, SPHERES>(s.accel, n, w.counts + 3, src);
         }
         else
         {
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int
     ClosestSrc src{ w.queue[parity], w.o_pdf, w.d_eta, w.hit };
     if constexpr (WIDE)
     {
-        TracePersistentWide<false, ClosestSrc, BLOCK, SHORT>(s.accel, n, w.counts + 3, src);
+        TracePersistentWide<false, ClosestSrc, BLOCK, SHORT, SPHERES>(s.accel, n, w.counts + 3, src);
         return;
     }
     if (s.accel.ordered)
@@ -465,7 +466,7 @@ __global__ void __launch_bounds__(BLOCK) ClosestKernel(Scenes sc, WaveDev w, int
     }
 }
 
-template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack, bool WIDE = false>
+template <class Scenes, int BLOCK = kBlock, int SHORT = kShortStack, bool WIDE = false, bool SPHERES = true>
 __global__ void __launch_bounds__(BLOCK) ShadowKernel(Scenes sc, WaveDev w)
 {
     const int32_t n = w.counts[2];
@@ -479,7 +480,7 @@ __global__ void __launch_bounds__(BLOCK) ShadowKernel(Scenes sc, WaveDev w)
         ShadowBatchSrc src{ { w.sh_o, w.sh_d, w.sh_c, w.L }, w.flags, sc.scenes };
         if constexpr (WIDE)
         {
-            TracePersistentWide<true, ShadowBatchSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
+            TracePersistentWide<true, ShadowBatchSrc, BLOCK, SHORT, SPHERES>(s.accel, n, w.counts + 4, src);
         }
         else
         {
@@ -490,7 +491,7 @@ __global__ void __launch_bounds__(BLOCK) ShadowKernel(Scenes sc, WaveDev w)
     ShadowSrc src{ w.sh_o, w.sh_d, w.sh_c, w.L };
     if constexpr (WIDE)
     {
-        TracePersistentWide<true, ShadowSrc, BLOCK, SHORT>(s.accel, n, w.counts + 4, src);
+        TracePersistentWide<true, ShadowSrc, BLOCK, SHORT, SPHERES>(s.accel, n, w.counts + 4, src);
         return;
     }
     if (s.accel.ordered)
@@ -1968,7 +1969,7 @@ namespace
 template <class Scenes>
 struct GridsT
 {
-    int raygen, closest[2 * kNumShapes], shade, shadow[2 * kNumShapes], film, shade_a, shade_b, kinds, scatter;
+    int raygen, closest[3 * kNumShapes], shade, shadow[3 * kNumShapes], film, shade_a, shade_b, kinds, scatter;
     GridsT()
     {
         raygen = PersistentGrid(reinterpret_cast<const void*>(RaygenKernel<Scenes>), kBlock);
@@ -1995,28 +1996,34 @@ struct GridsT
             reinterpret_cast<const void*>(ClosestKernel<Scenes, t.block, t.short_stack, true>), t.block);
         shadow[kNumShapes + K] = PersistentGrid(
             reinterpret_cast<const void*>(ShadowKernel<Scenes, t.block, t.short_stack, true>), t.block);
+        closest[2 * kNumShapes + K] = PersistentGrid(
+            reinterpret_cast<const void*>(ClosestKernel<Scenes, t.block, t.short_stack, true, false>), t.block);
+        shadow[2 * kNumShapes + K] = PersistentGrid(
+            reinterpret_cast<const void*>(ShadowKernel<Scenes, t.block, t.short_stack, true, false>), t.block);
     }
 };
 using Grids = GridsT<OneScene>;
 
-template <int K, bool WIDE, class Scenes>
+template <int K, bool WIDE, class Scenes, bool SPHERES = true>
 void LaunchTraceShape(const GridsT<Scenes>& gr, const Scenes& sc, const WaveDev& w, int parity, bool shadow,
                       cudaStream_t st)
 {
     constexpr TraversalShape t = kShapes[K];
-    constexpr int g = (WIDE ? kNumShapes : 0) + K;
+    constexpr int g = (WIDE ? (SPHERES ? kNumShapes : 2 * kNumShapes) : 0) + K;
     if (shadow)
     {
-        ShadowKernel<Scenes, t.block, t.short_stack, WIDE><<<gr.shadow[g], t.block, 0, st>>>(sc, w);
+        ShadowKernel<Scenes, t.block, t.short_stack, WIDE, SPHERES><<<gr.shadow[g], t.block, 0, st>>>(sc, w);
     }
     else
     {
-        ClosestKernel<Scenes, t.block, t.short_stack, WIDE><<<gr.closest[g], t.block, 0, st>>>(sc, w, parity);
+        ClosestKernel<Scenes, t.block, t.short_stack, WIDE, SPHERES>
+            <<<gr.closest[g], t.block, 0, st>>>(sc, w, parity);
     }
 }
 
 // The closest-hit (shadow = false) or shadow pass with trace shape
-// `shape` (a kShapes index, + kNumShapes over the 8-wide layout).
+// `shape`: a kShapes index, + kNumShapes over the 8-wide layout, + 2 kNumShapes
+// over the 8-wide layout of a tree of triangles only (TraceShapeOf).
 template <class Scenes>
 void LaunchTrace(int shape, const GridsT<Scenes>& gr, const Scenes& sc, const WaveDev& w, int parity, bool shadow,
                  cudaStream_t st)
@@ -2030,6 +2037,10 @@ void LaunchTrace(int shape, const GridsT<Scenes>& gr, const Scenes& sc, const Wa
     case kNumShapes + 1: LaunchTraceShape<1, true>(gr, sc, w, parity, shadow, st); break;
     case kNumShapes + 2: LaunchTraceShape<2, true>(gr, sc, w, parity, shadow, st); break;
     case kNumShapes + 3: LaunchTraceShape<3, true>(gr, sc, w, parity, shadow, st); break;
+    case 2 * kNumShapes + 0: LaunchTraceShape<0, true, Scenes, false>(gr, sc, w, parity, shadow, st); break;
+    case 2 * kNumShapes + 1: LaunchTraceShape<1, true, Scenes, false>(gr, sc, w, parity, shadow, st); break;
+    case 2 * kNumShapes + 2: LaunchTraceShape<2, true, Scenes, false>(gr, sc, w, parity, shadow, st); break;
+    case 2 * kNumShapes + 3: LaunchTraceShape<3, true, Scenes, false>(gr, sc, w, parity, shadow, st); break;
     default: LaunchTraceShape<0, false>(gr, sc, w, parity, shadow, st); break;
     }
 }
@@ -2420,7 +2431,8 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     const int iterations = I->max_bounces + 1;
     const Grids gr;
     // The tuned launch shape over the accel's layout (8-wide when selected).
-    const int trace_shape = I->shape + (I->accel->wide8_active() ? kNumShapes : 0);
+    const int trace_shape =
+        I->shape + (!I->accel->wide8_active() ? 0 : I->accel->has_spheres ? kNumShapes : 2 * kNumShapes);
     bool use_graph = p->use_graph != 0;
     if (use_graph && (!I->graph || I->graph_capacity != wave_paths || I->graph_iterations != iterations ||
                       !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f) ||
@@ -2910,12 +2922,13 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     }
     const GuideGroup* groups = p0->guide ? B->groups.p : nullptr;
     // The 8-wide layout only when every scene's accel traverses it.
-    bool all_wide = true;
+    bool all_wide = true, any_spheres = false;
     for (int32_t i = 0; i < n; ++i)
     {
         all_wide = all_wide && integrators[i]->accel->wide8_active();
+        any_spheres = any_spheres || integrators[i]->accel->has_spheres;
     }
-    const int trace_shape = B->shape + (all_wide ? kNumShapes : 0);
+    const int trace_shape = B->shape + (!all_wide ? 0 : any_spheres ? kNumShapes : 2 * kNumShapes);
     const bool use_graph = params[0].use_graph != 0;
     if (use_graph && (!E->graph || B->graph_capacity != wave_paths || B->graph_iterations != iterations ||
                       std::memcmp(&B->graph_table, &table, sizeof(table)) != 0 || B->graph_shape != trace_shape ||
