@@ -110,20 +110,9 @@ __device__ __forceinline__ bool IntersectTriangle(V3 p0, V3 e1, V3 e2, const Ray
     {
         return false;
     }
+    float invDet = 1 / det;
     V3 tvec = q.o - p0;
     const float du = Dot(tvec, pvec);
-    // Rejections that need no reciprocal, taken only where the reference's
-    // u = du * (1 / det) is certainly outside [0, 1]: du and det of opposite
-    // signs with no underflow possible (u < 0), or |du| above |det| by more
-    // than the two roundings of u can close (u > 1).
-    const float adet = fabsf(det);
-    const bool opposite = (du < 0) != (det < 0);
-    if ((opposite && adet <= 1e8f && fabsf(du) >= 1e-28f) || (!opposite && fabsf(du) > adet * 1.000001f))
-    {
-        return false;
-    }
-    // The correctly rounded reciprocal: the same float as the reference's 1 / det.
-    float invDet = __frcp_rn(det);
     float u = du * invDet;
     if (u < 0 || u > 1)
     {
