@@ -637,6 +637,181 @@ __global__ void __launch_bounds__(32 * kGradWarps) GuideWeightGradKernel(const _
     }
 }
 
+// Weight gradients on the fifth-generation tensor cores (tcgen05, sm_100a):
+// one CTA per (chunk of kGradChunk samples, layer) computes the chunk's
+// partial dW_L = dZ_L^T A_L with the accumulator in tensor memory. The
+// chunk's dZ rows (M, zero-padded to 128) and layer-input rows (N = 80 or 64)
+// are staged from the training scratch into shared memory in the canonical
+// K-major layout without swizzling: 8-row x 16-byte core matrices, 8-row
+// groups kTcSbo bytes apart and 8-sample column groups kTcLbo* bytes apart.
+// One thread issues the 16 MMAs of shape 128 x N x 16 (BF16 in, FP32
+// accumulate), a commit arrives on an mbarrier, and each warp reads its 32
+// accumulator rows back from tensor memory into the chunk's partial sums
+// (GuideGradReduceKernel then adds the chunks in a fixed order).
+constexpr int kTcRows = 128;                                  // MMA M: dZ rows, zero-padded
+constexpr int kTcMaxN = 80;                                   // widest layer input
+constexpr int kTcGroups = kGradChunk / 8;                     // 8-sample core-matrix columns
+constexpr uint32_t kTcSbo = 128;                              // bytes between 8-row groups
+constexpr uint32_t kTcLboA = (kTcRows / 8) * 128;             // bytes between column groups of A
+constexpr uint32_t kTcLboB = (kTcMaxN / 8) * 128;             // of B
+constexpr size_t kTcSmemA = size_t(kTcGroups) * kTcLboA;      // 64 KB
+constexpr size_t kTcSmemB = size_t(kTcGroups) * kTcLboB;      // 40 KB
+constexpr size_t kTcSmem = kTcSmemA + kTcSmemB + 16;          // + mbarrier and tensor-memory address
+constexpr uint32_t kTcCols = 128;                             // tensor-memory columns (N <= 80)
+constexpr int kTcThreads = 128;                               // 4 warps: one per 32 accumulator rows
+constexpr uint32_t kTcMaxPolls = 1u << 22;                    // bound on the wait for the MMAs
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start address, leading (K direction) and
+// stride (M/N direction) byte offsets, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t TcDesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return uint64_t((addr >> 4) & 0x3fffu) | (uint64_t((lbo >> 4) & 0x3fffu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3fffu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 and M >> 4.
+__device__ __forceinline__ uint32_t TcInstr(int m, int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+__global__ void __launch_bounds__(kTcThreads) GuideWeightGradTcKernel(const __nv_bfloat16* scratch, int64_t ld,
+                                                                        const int32_t* n_dev, int64_t n_host,
+                                                                        float* partial, int32_t* status)
+{
+    extern __shared__ __align__(128) uint8_t tc_smem[];
+    uint8_t* sa = tc_smem;
+    uint8_t* sb = tc_smem + kTcSmemA;
+    uint64_t* bar = reinterpret_cast<uint64_t*>(tc_smem + kTcSmemA + kTcSmemB);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + kTcSmemA + kTcSmemB + 8);
+
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    const int64_t n_pad = (n + 15) / 16 * 16;
+    const int64_t chunk = blockIdx.x;
+    if (chunk * kGradChunk >= n_pad)
+    {
+        return; // the whole block, before any tensor-memory use
+    }
+    const GradLayer L = kGradLayers[blockIdx.y];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t k0 = chunk * kGradChunk;
+    const int kvalid = int(min(int64_t(kGradChunk), n_pad - k0)); // a multiple of 16
+
+    // Stage the chunk: A = dZ rows (rows >= m zero), B = layer-input rows
+    // (rows >= n zero); samples past the batch are zero-filled.
+    for (int i = tid; i < kTcRows * kTcGroups; i += kTcThreads)
+    {
+        const int r = i / kTcGroups, g = i % kTcGroups;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (r < L.m && g * 8 < kvalid)
+        {
+            v = *reinterpret_cast<const uint4*>(scratch + (int64_t(L.dz_row) + r) * ld + k0 + g * 8);
+        }
+        *reinterpret_cast<uint4*>(sa + g * kTcLboA + (r >> 3) * kTcSbo + (r & 7) * 16) = v;
+    }
+    for (int i = tid; i < kTcMaxN * kTcGroups; i += kTcThreads)
+    {
+        const int r = i / kTcGroups, g = i % kTcGroups;
+        uint4 v = make_uint4(0, 0, 0, 0);
+        if (r < L.n && g * 8 < kvalid)
+        {
+            v = *reinterpret_cast<const uint4*>(scratch + (int64_t(L.a_row) + r) * ld + k0 + g * 8);
+        }
+        *reinterpret_cast<uint4*>(sb + g * kTcLboB + (r >> 3) * kTcSbo + (r & 7) * 16) = v;
+    }
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(tmem_slot)),
+                     "r"(kTcCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(1) : "memory");
+    }
+    // The tile stores (generic proxy) become visible to the tensor cores
+    // (async proxy); the allocated address becomes visible to every thread.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (tid == 0)
+    {
+        const uint32_t idesc = TcInstr(kTcRows, L.n);
+        const uint32_t a0 = SmemAddr(sa), b0 = SmemAddr(sb);
+        for (int ks = 0; ks < kvalid / 16; ++ks)
+        {
+            const uint64_t da = TcDesc(a0 + 2 * ks * kTcLboA, kTcLboA, kTcSbo);
+            const uint64_t db = TcDesc(b0 + 2 * ks * kTcLboB, kTcLboB, kTcSbo);
+            const uint32_t accumulate = ks > 0 ? 1u : 0u;
+            asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                         "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(SmemAddr(bar))
+                     : "memory");
+    }
+    // Bounded wait for the MMAs' completion (phase 0 of the barrier).
+    uint32_t done = 0;
+    for (uint32_t poll = 0; poll < kTcMaxPolls && !done; ++poll)
+    {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(SmemAddr(bar)), "r"(0u)
+                     : "memory");
+        if (!done)
+        {
+            __nanosleep(64);
+        }
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    // Every warp takes the same branch: all of them waited on the same barrier.
+    if (__all_sync(0xffffffffu, done))
+    {
+        const int r = warp * 32 + lane;
+        float* dst = partial + chunk * kGuideParams + L.w_off + r * L.n;
+        for (int c = 0; c < L.n; c += 16)
+        {
+            uint32_t v[16];
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                         "%12, %13, %14, %15}, [%16];"
+                         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+                           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+                           "=r"(v[14]), "=r"(v[15])
+                         : "r"(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (r < L.m)
+            {
+                for (int q = 0; q < 16; q += 4)
+                {
+                    *reinterpret_cast<float4*>(dst + c + q) =
+                        make_float4(__uint_as_float(v[q]), __uint_as_float(v[q + 1]), __uint_as_float(v[q + 2]),
+                                    __uint_as_float(v[q + 3]));
+                }
+            }
+        }
+    }
+    else if (lane == 0)
+    {
+        atomicExch(status, 1); // the MMAs did not complete within the bound
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0)
+    {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcCols));
+    }
+}
+
 // Counts an Adam step when the batch is not empty. The step number and the
 // batch size live in device memory so a captured graph replays correctly.
 __global__ void GuideStepKernel(int32_t* step, const int32_t* n_dev, int64_t n_host)
@@ -781,9 +956,9 @@ bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs
                                                                 G->bounds, G->bf16.p, G->params.p, G->scratch.p, ld,
                                                                 G->grad.p, G->loss.p);
     const int64_t chunks = (ld + kGradChunk - 1) / kGradChunk;
-    const int64_t items = chunks * kGradTiles;
-    const int grid = int(std::max<int64_t>(1, std::min<int64_t>((items + kGradWarps - 1) / kGradWarps, 8 * sms)));
-    GuideWeightGradKernel<<<grid, 32 * kGradWarps, 0, st>>>(G->scratch.p, ld, n_dev, n_host, G->partial.p);
+    // One CTA per (chunk, layer); chunks past the batch exit at once.
+    GuideWeightGradTcKernel<<<dim3(unsigned(chunks), 4), kTcThreads, kTcSmem, st>>>(G->scratch.p, ld, n_dev, n_host,
+                                                                                     G->partial.p, G->tc_status.p);
     GuideGradReduceKernel<<<(kGuideParams + 255) / 256, 256, 0, st>>>(G->partial.p, n_dev, n_host, G->grad.p);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
@@ -799,12 +974,25 @@ bbg_status GuideApply(bbg_guide* G, float lr, const int32_t* n_dev, int64_t n_ho
     return BBG_OK;
 }
 
+bbg_status GuideCheckStatus(bbg_guide* G)
+{
+    int32_t st = 0;
+    BBG_CUDA(cudaMemcpy(&st, G->tc_status.p, sizeof(st), cudaMemcpyDeviceToHost));
+    if (st != 0)
+    {
+        return Fail(BBG_ERR_TIMEOUT, "guide training: the tensor-core weight-gradient pass did not complete in time");
+    }
+    return BBG_OK;
+}
+
 bbg_status GuidePrepare(bbg_guide* G, int* grid)
 {
     if (!G->smem_set)
     {
         BBG_CUDA(cudaFuncSetAttribute(GuideForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFwdSmem)));
         BBG_CUDA(cudaFuncSetAttribute(GuideTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)));
+        BBG_CUDA(cudaFuncSetAttribute(GuideWeightGradTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      int(kTcSmem)));
         G->smem_set = true;
     }
     int per = 1;
@@ -875,6 +1063,8 @@ bbg_status Create(const float* aabb, uint64_t seed, bbg_guide* G)
     BBG_TRY(G->bf16.alloc(kBfAll));
     BBG_TRY(G->step_dev.alloc(1));
     BBG_CUDA(cudaMemsetAsync(G->step_dev.p, 0, sizeof(int32_t), G->stream));
+    BBG_TRY(G->tc_status.alloc(1));
+    BBG_CUDA(cudaMemsetAsync(G->tc_status.p, 0, sizeof(int32_t), G->stream));
     GuideConvertKernel<<<64, 256, 0, G->stream>>>(G->params.p, G->bf16.p);
     BBG_CUDA(cudaGetLastError());
     BBG_CUDA(cudaStreamSynchronize(G->stream));
@@ -1083,6 +1273,7 @@ bbg_status bbg_guide_gradient(bbg_guide* G, const float* raw, const float* dirs,
     BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));
     BBG_CUDA(cudaMemsetAsync(G->grad.p, 0, sizeof(float) * kGuideParams, G->stream));
     BBG_CUDA(cudaStreamSynchronize(G->stream));
+    BBG_TRY(GuideCheckStatus(G));
     if (loss_out)
     {
         *loss_out = loss;
@@ -1107,6 +1298,7 @@ bbg_status bbg_guide_train_step(bbg_guide* G, const float* raw, const float* dir
     float loss = 0;
     BBG_CUDA(cudaMemcpyAsync(&loss, G->loss.p, sizeof(float), cudaMemcpyDeviceToHost, G->stream));
     BBG_CUDA(cudaStreamSynchronize(G->stream));
+    BBG_TRY(GuideCheckStatus(G));
     if (loss_out)
     {
         *loss_out = loss / float(n);

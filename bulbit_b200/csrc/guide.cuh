@@ -15,6 +15,7 @@ struct bbg_guide
     bbg::DevBuf<int32_t> step_dev; // Adam step counter
     bbg::DevBuf<__nv_bfloat16> scratch; // training: transposed activations and gradients
     bbg::DevBuf<float> partial;         // training: per-chunk weight-gradient partial sums
+    bbg::DevBuf<int32_t> tc_status;     // nonzero: a tensor-core weight-gradient pass timed out
     float beta1 = 0.9f, beta2 = 0.99f;
     bool smem_set = false;
     // Staging for host-buffer calls.
@@ -65,6 +66,9 @@ bbg_status GuideReserveTraining(bbg_guide* G, int64_t capacity);
 // capacity bounds n (n from n_dev if set) and sizes the training scratch.
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
                            const int32_t* n_dev, int64_t n_host, int64_t capacity, cudaStream_t st);
+// BBG_ERR_TIMEOUT if a weight-gradient pass of this guide has given up
+// waiting for its tensor-core MMAs (synchronises with the device).
+bbg_status GuideCheckStatus(bbg_guide* G);
 // One Adam step with gradient = accumulator / n (n from n_dev if set); an
 // empty batch is skipped.
 bbg_status GuideApply(bbg_guide* G, float lr, const int32_t* n_dev, int64_t n_host, cudaStream_t st);

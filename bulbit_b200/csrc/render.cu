@@ -2522,6 +2522,10 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (gc.guide && gc.dev.train)
+    {
+        BBG_TRY(GuideCheckStatus(gc.guide));
+    }
 
     if (mem == BBG_MEM_HOST)
     {
