@@ -489,7 +489,7 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
         // Layer 3: dW3 += dY^T H3, dZ2 = (dY W3) * relu'(H3).
         // The layer inputs and output gradients, transposed, go to the
         // scratch columns of these 16 samples; the weight gradients are the
-        // GEMMs dW = dZ^T A over the whole batch (GuideWeightGradKernel).
+        // GEMMs dW = dZ^T A over the whole batch (GuideWeightGradTcKernel).
         const int64_t col0 = tile * 16;
         StoreColumns(W.xt, kGuideIn, scratch, ld, kRowX, col0, lane);
         StoreColumns(W.ht[0], kGuideHidden, scratch, ld, kRowH0, col0, lane);
@@ -529,14 +529,11 @@ __global__ void __launch_bounds__(32 * kTrainWarps) GuideTrainKernel(const float
 }
 
 // Weight gradients dW_L[m][n] = sum over the batch of dZ_L[s][m] A_L[s][n]
-// (A_L: the layer's input), from the training scratch. Work items: (layer,
-// 16-row tile of dW, chunk of kGradChunk samples); each warp runs the chunk's
-// MMAs with FP32 accumulators in registers and stores its 16 x n block as the
-// chunk's partial sum; GuideGradReduceKernel adds the chunks' partial sums to
-// the gradient (no atomics, a fixed summation order). Samples past the batch
-// are zero in the dZ rows.
+// (A_L: the layer's input), from the training scratch, per chunk of
+// kGradChunk samples (GuideWeightGradTcKernel below); GuideGradReduceKernel
+// adds the chunks' partial sums to the gradient (no atomics, a fixed
+// summation order). Samples past the batch are zero in the dZ rows.
 constexpr int kGradChunk = 256;
-constexpr int kGradWarps = 8;
 
 struct GradLayer
 {
@@ -546,7 +543,6 @@ __constant__ GradLayer kGradLayers[4] = { { kRowDZ0, kRowX, kGuideHidden, kGuide
                                           { kRowDZ1, kRowH0, kGuideHidden, kGuideHidden, kW1 },
                                           { kRowDZ2, kRowH1, kGuideHidden, kGuideHidden, kW2 },
                                           { kRowDY, kRowH2, kGuideOut, kGuideHidden, kW3 } };
-constexpr int kGradTiles = 4 + 4 + 4 + 3; // 16-row tiles over the four layers
 
 // grad[w] += sum over chunks of partial[chunk][w], for the weight entries.
 __global__ void GuideGradReduceKernel(const float* partial, const int32_t* n_dev, int64_t n_host, float* grad)
@@ -567,73 +563,6 @@ __global__ void GuideGradReduceKernel(const float* partial, const int32_t* n_dev
             s += partial[c * kGuideParams + w];
         }
         grad[w] += s;
-    }
-}
-
-__global__ void __launch_bounds__(32 * kGradWarps) GuideWeightGradKernel(const __nv_bfloat16* scratch, int64_t ld,
-                                                                           const int32_t* n_dev, int64_t n_host,
-                                                                           float* partial)
-{
-    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
-    const int64_t n_pad = (n + 15) / 16 * 16;
-    const int64_t chunks = (n_pad + kGradChunk - 1) / kGradChunk;
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const int64_t items = chunks * kGradTiles;
-    for (int64_t item = int64_t(blockIdx.x) * kGradWarps + (threadIdx.x >> 5); item < items;
-         item += int64_t(gridDim.x) * kGradWarps)
-    {
-        int tile = int(item % kGradTiles);
-        int64_t chunk = item / kGradTiles;
-        int layer = tile < 4 ? 0 : tile < 8 ? 1 : tile < 12 ? 2 : 3;
-        int mt = tile - 4 * layer;
-        const GradLayer L = kGradLayers[layer];
-        const int n_tiles = L.n / 8;
-        float acc[10][4];
-#pragma unroll
-        for (int j = 0; j < 10; ++j)
-        {
-            acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0;
-        }
-        const int64_t k_end = min(n_pad, (chunk + 1) * kGradChunk);
-#pragma unroll 4
-        for (int64_t k = chunk * kGradChunk; k < k_end; k += 16)
-        {
-            uint32_t a[4];
-            const __nv_bfloat16* ar = scratch + (int64_t(L.dz_row) + mt * 16) * ld + k;
-            a[0] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g) * ld + 2 * t);
-            a[1] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g + 8) * ld + 2 * t);
-            a[2] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g) * ld + 2 * t + 8);
-            a[3] = *reinterpret_cast<const uint32_t*>(ar + int64_t(g + 8) * ld + 2 * t + 8);
-#pragma unroll
-            for (int j = 0; j < 10; ++j)
-            {
-                if (j < n_tiles)
-                {
-                    const __nv_bfloat16* br = scratch + (int64_t(L.a_row) + j * 8 + g) * ld + k + 2 * t;
-                    uint32_t b0 = *reinterpret_cast<const uint32_t*>(br);
-                    uint32_t b1 = *reinterpret_cast<const uint32_t*>(br + 8);
-                    Mma16816(acc[j], a, b0, b1);
-                }
-            }
-        }
-#pragma unroll
-        for (int j = 0; j < 10; ++j)
-        {
-            if (j < n_tiles)
-            {
-#pragma unroll
-                for (int half = 0; half < 2; ++half)
-                {
-                    int row = mt * 16 + g + 8 * half;
-                    int col = j * 8 + 2 * t;
-                    if (row < L.m)
-                    {
-                        *reinterpret_cast<float2*>(partial + chunk * kGuideParams + L.w_off + row * L.n + col) =
-                            make_float2(acc[j][2 * half], acc[j][2 * half + 1]);
-                    }
-                }
-            }
-        }
     }
 }
 
@@ -658,7 +587,7 @@ constexpr size_t kTcSmemA = size_t(kTcGroups) * kTcLboA;      // 64 KB
 constexpr size_t kTcSmemB = size_t(kTcGroups) * kTcLboB;      // 40 KB
 constexpr size_t kTcSmem = kTcSmemA + kTcSmemB + 16;          // + mbarrier and tensor-memory address
 constexpr uint32_t kTcCols = 128;                             // tensor-memory columns (N <= 80)
-constexpr int kTcThreads = 128;                               // 4 warps: one per 32 accumulator rows
+constexpr int kTcThreads = 256;                               // 8 warps stage; warps 0-3 read 32 rows each
 constexpr uint32_t kTcMaxPolls = 1u << 22;                    // bound on the wait for the MMAs
 
 __device__ __forceinline__ uint32_t SmemAddr(const void* p)
@@ -703,28 +632,32 @@ __global__ void __launch_bounds__(kTcThreads) GuideWeightGradTcKernel(const __nv
     const int64_t k0 = chunk * kGradChunk;
     const int kvalid = int(min(int64_t(kGradChunk), n_pad - k0)); // a multiple of 16
 
-    // Stage the chunk: A = dZ rows (rows >= m zero), B = layer-input rows
-    // (rows >= n zero); samples past the batch are zero-filled.
+    // Stage the chunk with asynchronous 16-byte copies (all of a thread's
+    // copies in flight at once): A = dZ rows (rows >= m zero-filled), B =
+    // layer-input rows (rows >= n zero-filled); samples past the batch are
+    // zero-filled too (a source size of 0 reads nothing).
     for (int i = tid; i < kTcRows * kTcGroups; i += kTcThreads)
     {
         const int r = i / kTcGroups, g = i % kTcGroups;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (r < L.m && g * 8 < kvalid)
-        {
-            v = *reinterpret_cast<const uint4*>(scratch + (int64_t(L.dz_row) + r) * ld + k0 + g * 8);
-        }
-        *reinterpret_cast<uint4*>(sa + g * kTcLboA + (r >> 3) * kTcSbo + (r & 7) * 16) = v;
+        const bool in = r < L.m && g * 8 < kvalid;
+        const __nv_bfloat16* src = in ? scratch + (int64_t(L.dz_row) + r) * ld + k0 + g * 8 : scratch;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                         SmemAddr(sa + g * kTcLboA + (r >> 3) * kTcSbo + (r & 7) * 16)),
+                     "l"(src), "r"(in ? 16 : 0)
+                     : "memory");
     }
     for (int i = tid; i < kTcMaxN * kTcGroups; i += kTcThreads)
     {
         const int r = i / kTcGroups, g = i % kTcGroups;
-        uint4 v = make_uint4(0, 0, 0, 0);
-        if (r < L.n && g * 8 < kvalid)
-        {
-            v = *reinterpret_cast<const uint4*>(scratch + (int64_t(L.a_row) + r) * ld + k0 + g * 8);
-        }
-        *reinterpret_cast<uint4*>(sb + g * kTcLboB + (r >> 3) * kTcSbo + (r & 7) * 16) = v;
+        const bool in = r < L.n && g * 8 < kvalid;
+        const __nv_bfloat16* src = in ? scratch + (int64_t(L.a_row) + r) * ld + k0 + g * 8 : scratch;
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(
+                         SmemAddr(sb + g * kTcLboB + (r >> 3) * kTcSbo + (r & 7) * 16)),
+                     "l"(src), "r"(in ? 16 : 0)
+                     : "memory");
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
     if (warp == 0)
     {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(tmem_slot)),
@@ -774,8 +707,9 @@ __global__ void __launch_bounds__(kTcThreads) GuideWeightGradTcKernel(const __nv
         }
     }
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    // Every warp takes the same branch: all of them waited on the same barrier.
-    if (__all_sync(0xffffffffu, done))
+    // Warps 0-3 read the accumulator rows (warp w may access tensor-memory
+    // lanes 32w..32w+31); every warp of them takes the same branch.
+    if (warp < kTcRows / 32 && __all_sync(0xffffffffu, done))
     {
         const int r = warp * 32 + lane;
         float* dst = partial + chunk * kGuideParams + L.w_off + r * L.n;
@@ -800,7 +734,7 @@ __global__ void __launch_bounds__(kTcThreads) GuideWeightGradTcKernel(const __nv
             }
         }
     }
-    else if (lane == 0)
+    else if (!done)
     {
         atomicExch(status, 1); // the MMAs did not complete within the bound
     }
