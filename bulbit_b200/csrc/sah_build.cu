@@ -969,46 +969,73 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
         return Fail(BBG_ERR_INVALID_ARG, "device SAH build: %d primitives exceed the node index range", n);
     }
 
-    DevBuf<float4> box, cen, bounds;
-    DevBuf<int32_t> idx, scr_l, scr_r, counters, lists[4], ref;
-    DevBuf<uint32_t> leaf_at, leaves_before, root_keys;
-    DevBuf<int4> info;
-    DevBuf<int2> path;
-    BBG_TRY(box.alloc(2 * size_t(n)));
-    BBG_TRY(cen.alloc(size_t(n)));
-    BBG_TRY(idx.alloc(size_t(n)));
-    BBG_TRY(scr_l.alloc(size_t(n)));
-    BBG_TRY(scr_r.alloc(size_t(n)));
-    BBG_TRY(leaf_at.alloc(size_t(n) + 1));
-    BBG_TRY(leaves_before.alloc(size_t(n) + 1));
-    BBG_TRY(bounds.alloc(4 * size_t(max_nodes)));
-    BBG_TRY(info.alloc(size_t(max_nodes)));
-    BBG_TRY(path.alloc(size_t(max_nodes)));
-    BBG_TRY(counters.alloc(4));
-    BBG_TRY(root_keys.alloc(kKeys));
-    for (auto& l : lists)
+    // Every temporary array of the build in one allocation (carved in
+    // 256-byte-aligned pieces), so a build costs one cudaMalloc, not a dozen.
+    struct Piece
     {
-        BBG_TRY(l.alloc(size_t(n)));
+        void** ptr;
+        size_t bytes;
+    };
+    float4 *box = nullptr, *cen = nullptr, *bounds = nullptr;
+    int32_t *idx = nullptr, *scr_l = nullptr, *scr_r = nullptr, *counters = nullptr, *ref = nullptr;
+    int32_t* lists[4] = {};
+    uint32_t *leaf_at = nullptr, *leaves_before = nullptr, *root_keys = nullptr;
+    int4* info = nullptr;
+    int2* path = nullptr;
+    const size_t un = size_t(n), un1 = size_t(n) + 1, nodes = size_t(max_nodes);
+    const Piece pieces[] = {
+        { reinterpret_cast<void**>(&box), 2 * un * sizeof(float4) },
+        { reinterpret_cast<void**>(&cen), un * sizeof(float4) },
+        { reinterpret_cast<void**>(&idx), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&scr_l), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&scr_r), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&leaf_at), un1 * sizeof(uint32_t) },
+        { reinterpret_cast<void**>(&leaves_before), un1 * sizeof(uint32_t) },
+        { reinterpret_cast<void**>(&bounds), 4 * nodes * sizeof(float4) },
+        { reinterpret_cast<void**>(&info), nodes * sizeof(int4) },
+        { reinterpret_cast<void**>(&path), nodes * sizeof(int2) },
+        { reinterpret_cast<void**>(&ref), nodes * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&counters), 4 * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&root_keys), kKeys * sizeof(uint32_t) },
+        { reinterpret_cast<void**>(&lists[0]), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&lists[1]), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&lists[2]), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&lists[3]), un * sizeof(int32_t) },
+    };
+    size_t total = 0;
+    for (const Piece& pc : pieces)
+    {
+        total += (pc.bytes + 255) / 256 * 256;
     }
-    BBG_CUDA(cudaMemsetAsync(leaf_at.p, 0, sizeof(uint32_t) * (size_t(n) + 1), st));
+    DevBuf<uint8_t> arena;
+    BBG_TRY(arena.alloc(total));
+    {
+        size_t at = 0;
+        for (const Piece& pc : pieces)
+        {
+            *pc.ptr = arena.p + at;
+            at += (pc.bytes + 255) / 256 * 256;
+        }
+    }
+    BBG_CUDA(cudaMemsetAsync(leaf_at, 0, sizeof(uint32_t) * (size_t(n) + 1), st));
     uint32_t init_keys[kKeys];
     for (int q = 0; q < kKeys; ++q)
     {
         init_keys[q] = (q % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
     }
-    BBG_CUDA(cudaMemcpyAsync(root_keys.p, init_keys, sizeof(init_keys), cudaMemcpyHostToDevice, st));
+    BBG_CUDA(cudaMemcpyAsync(root_keys, init_keys, sizeof(init_keys), cudaMemcpyHostToDevice, st));
     SahPrimsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(a->prim_shape.p, a->tri_indices.p, a->positions.p,
-                                                         a->spheres.p, n, box.p, cen.p, idx.p, root_keys.p);
-    SahDev S{ box.p, cen.p, idx.p, scr_l.p, scr_r.p, leaf_at.p, bounds.p, info.p, path.p, counters.p };
-    SahRootKernel<<<1, 1, 0, st>>>(S, root_keys.p, n);
+                                                         a->spheres.p, n, box, cen, idx, root_keys);
+    SahDev S{ box, cen, idx, scr_l, scr_r, leaf_at, bounds, info, path, counters };
+    SahRootKernel<<<1, 1, 0, st>>>(S, root_keys, n);
     const int32_t init_counters[4] = { 1, 0, 0, 0 };
-    BBG_CUDA(cudaMemcpyAsync(counters.p, init_counters, sizeof(init_counters), cudaMemcpyHostToDevice, st));
+    BBG_CUDA(cudaMemcpyAsync(counters, init_counters, sizeof(init_counters), cudaMemcpyHostToDevice, st));
     const int32_t root = 0;
     // lists[0] / lists[1]: nodes of more than 32 primitives of this level and
     // the next; lists[2] / lists[3]: the smaller ones.
     int cur = 0;
     int32_t n_big = n > kSahWarpTask ? 1 : 0, n_small = 1 - n_big;
-    BBG_CUDA(cudaMemcpyAsync(n_big ? lists[0].p : lists[2].p, &root, sizeof(root), cudaMemcpyHostToDevice, st));
+    BBG_CUDA(cudaMemcpyAsync(n_big ? lists[0] : lists[2], &root, sizeof(root), cudaMemcpyHostToDevice, st));
     int depth = 0;
     int32_t state[4] = { 1, 0, 0, 0 };
     while (n_big + n_small > 0)
@@ -1017,11 +1044,11 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
         {
             return Fail(BBG_ERR_STACK_OVERFLOW, "tree depth exceeds the traversal stack (%d)", kStackCapacity);
         }
-        int32_t* big_cur = lists[cur].p;
-        int32_t* big_next = lists[1 - cur].p;
-        int32_t* small_cur = lists[2 + cur].p;
-        int32_t* small_next = lists[3 - cur].p;
-        BBG_CUDA(cudaMemsetAsync(counters.p + 1, 0, 2 * sizeof(int32_t), st));
+        int32_t* big_cur = lists[cur];
+        int32_t* big_next = lists[1 - cur];
+        int32_t* small_cur = lists[2 + cur];
+        int32_t* small_next = lists[3 - cur];
+        BBG_CUDA(cudaMemsetAsync(counters + 1, 0, 2 * sizeof(int32_t), st));
         if (n_big > 0)
         {
             SahBlockKernel<<<std::min(n_big, 8 * sms), kSahBlock, 0, st>>>(S, big_cur, n_big, big_next, small_next);
@@ -1031,7 +1058,7 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
             SahWarpKernel<<<GridFor(int64_t(n_small) * 32, kSahWarpBlock, sms), kSahWarpBlock, 0, st>>>(
                 S, small_cur, n_small, big_next, small_next);
         }
-        BBG_CUDA(cudaMemcpyAsync(state, counters.p, sizeof(state), cudaMemcpyDeviceToHost, st));
+        BBG_CUDA(cudaMemcpyAsync(state, counters, sizeof(state), cudaMemcpyDeviceToHost, st));
         BBG_CUDA(cudaStreamSynchronize(st));
         BBG_CUDA(cudaGetLastError());
         n_big = state[1];
@@ -1047,20 +1074,19 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
 
     // Leaves left of each position, then every node at its depth-first index.
     size_t scan_bytes = 0;
-    BBG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, leaf_at.p, leaves_before.p, n + 1, st));
+    BBG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, leaf_at, leaves_before, n + 1, st));
     DevBuf<uint8_t> scan_tmp;
     BBG_TRY(scan_tmp.alloc(std::max<size_t>(scan_bytes, 1)));
-    BBG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.p, scan_bytes, leaf_at.p, leaves_before.p, n + 1, st));
+    BBG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.p, scan_bytes, leaf_at, leaves_before, n + 1, st));
     uint32_t n_leaves = 0;
-    BBG_CUDA(cudaMemcpyAsync(&n_leaves, leaves_before.p + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    BBG_CUDA(cudaMemcpyAsync(&n_leaves, leaves_before + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     BBG_TRY(a->nodes.alloc(2 * size_t(n_nodes)));
-    BBG_TRY(ref.alloc(size_t(n_nodes)));
     BBG_CUDA(cudaStreamSynchronize(st));
     BBG_TRY(a->leaves.alloc(std::max<size_t>(n_leaves, 1)));
     bbg_bvh_node* nd = reinterpret_cast<bbg_bvh_node*>(a->nodes.p);
-    int32_t* bad = counters.p + 3; // zero: no leaf was too large
-    SahFlattenKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(S, leaves_before.p, n_nodes, int32_t(n_leaves), nd,
-                                                                  ref.p, a->leaves.p, bad);
+    int32_t* bad = counters + 3; // zero: no leaf was too large
+    SahFlattenKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(S, leaves_before, n_nodes, int32_t(n_leaves), nd,
+                                                                  ref, a->leaves.p, bad);
     int32_t flat_bad = 0;
     BBG_CUDA(cudaMemcpyAsync(&flat_bad, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     BBG_CUDA(cudaStreamSynchronize(st));
@@ -1069,19 +1095,19 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
         return Fail(BBG_ERR_BAD_BVH, "device SAH build: inconsistent tree (%d nodes, %u leaves)", n_nodes, n_leaves);
     }
     BBG_TRY(a->slots.alloc(3 * size_t(n)));
-    SahSlotsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(idx.p, a->prim_shape.p, a->tri_indices.p, a->positions.p,
+    SahSlotsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(idx, a->prim_shape.p, a->tri_indices.p, a->positions.p,
                                                          a->spheres.p, n, a->slots.p);
     const int32_t n_interior = n_nodes - int32_t(n_leaves);
     BBG_TRY(a->wide.alloc(4 * size_t(std::max(n_interior, 1))));
-    SahChildBoxKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(nd, ref.p, n_nodes, a->wide.p);
+    SahChildBoxKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(nd, ref, n_nodes, a->wide.p);
     BBG_CUDA(cudaGetLastError());
     int32_t root_ref = 0;
-    BBG_CUDA(cudaMemcpyAsync(&root_ref, ref.p, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    BBG_CUDA(cudaMemcpyAsync(&root_ref, ref, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     bbg_bvh_node root_node;
     BBG_CUDA(cudaMemcpyAsync(&root_node, nd, sizeof(root_node), cudaMemcpyDeviceToHost, st));
     // The slot order stays on the device for export.
     BBG_TRY(a->slot_prims.alloc(size_t(n)));
-    BBG_CUDA(cudaMemcpyAsync(a->slot_prims.p, idx.p, sizeof(int32_t) * size_t(n), cudaMemcpyDeviceToDevice, st));
+    BBG_CUDA(cudaMemcpyAsync(a->slot_prims.p, idx, sizeof(int32_t) * size_t(n), cudaMemcpyDeviceToDevice, st));
     BBG_CUDA(cudaStreamSynchronize(st));
     a->root = root_ref;
     a->n_nodes = n_nodes;
