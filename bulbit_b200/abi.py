@@ -38,8 +38,6 @@ BBG_TRAVERSAL_REFERENCE = 1
 BBG_TRAVERSAL_WIDE = 2
 BBG_SHADE_SORTED = 0
 BBG_SHADE_QUEUE = 1
-BBG_TRACE_QUEUE = 0
-BBG_TRACE_OCTANT = 1
 
 BBG_FILTER_BOX = 0
 BBG_FILTER_TENT = 1
@@ -118,8 +116,7 @@ class RenderParams(C.Structure):
                 ("guide_train", C.c_int32), ("guide_batch", C.c_int32), ("guide_lr", C.c_float),
                 ("guide_select", C.c_float), ("guide_steps", C.c_int32),
                 ("sampler", C.c_int32), ("x_samples", C.c_int32), ("jitter", C.c_int32),
-                ("shade_order", C.c_int32), ("pass_through_levels", C.c_int32),
-                ("trace_order", C.c_int32)]
+                ("shade_order", C.c_int32), ("pass_through_levels", C.c_int32)]
 
 
 class Tuning(C.Structure):

@@ -1816,11 +1816,8 @@ struct bbg_integrator
     float graph_guide_lr = 0;
     int graph_shape = -1;
     bool graph_shade_sort = false;
-    bool graph_trace_octant = false;
     // Shading order of the current render (params.shade_order).
     bool shade_sort = true;
-    // Closest-hit order of the current render (params.trace_order).
-    bool trace_octant = false;
     DevBuf<int32_t> sorted, sort_counts;
     DevBuf<uint8_t> keys;
     // Launch shape of the traversal passes (index into kShapes) and wave size
@@ -2169,71 +2166,11 @@ __global__ void GuideBucketScatterKernel(WaveDev w, GuideDev g)
     }
 }
 
-// Closest-hit order (bbg_render_params.trace_order, TRACE_OCTANT): before a
-// level's closest-hit pass its queue is counting-sorted by the octant of each
-// ray's direction, through the shading sort's buffers (free at that point),
-// so that a warp's rays open each 8-wide node's children in the same order.
-__global__ void __launch_bounds__(kBlock) RayOctantKeysKernel(WaveDev w, int parity)
-{
-    __shared__ int32_t bc[8];
-    const int32_t* q = w.queue[parity];
-    const int32_t n = w.counts[parity];
-    for (int32_t base = blockIdx.x * kBlock; base < n; base += gridDim.x * kBlock)
-    {
-        if (threadIdx.x < 8)
-        {
-            bc[threadIdx.x] = 0;
-        }
-        __syncthreads();
-        const int32_t j = base + int32_t(threadIdx.x);
-        if (j < n)
-        {
-            const float4 d = w.d_eta[q[j]];
-            const int32_t k = int32_t(d.x < 0) | (int32_t(d.y < 0) << 1) | (int32_t(d.z < 0) << 2);
-            w.keys[j] = uint8_t(k);
-            atomicAdd(&bc[k], 1);
-        }
-        __syncthreads();
-        if (threadIdx.x < 8 && bc[threadIdx.x] > 0)
-        {
-            atomicAdd(&w.sort_counts[threadIdx.x], bc[threadIdx.x]);
-        }
-        __syncthreads();
-    }
-}
-
-// The sorted slots back into the level's queue; the sort counters cleared
-// for the shading sort that follows.
-__global__ void RaySortBackKernel(WaveDev w, int parity)
-{
-    const int32_t n = w.counts[parity];
-    int32_t* q = w.queue[parity];
-    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
-    {
-        q[j] = w.sorted[j];
-    }
-}
-
-__global__ void SortCountsClearKernel(WaveDev w)
-{
-    if (threadIdx.x < 2 * kShadeKinds)
-    {
-        w.sort_counts[threadIdx.x] = 0;
-    }
-}
-
 bbg_status EnqueueLevel(const Grids& gr, const SceneDev& s, const WaveDev& w, const GuideCtx& gc, int parity,
-                        int shape, cudaStream_t st, bool octant_sort = false)
+                        int shape, cudaStream_t st)
 {
     const OneScene one{ s, FilmDev{} };
     ResetKernel<<<1, 1, 0, st>>>(w, parity);
-    if (octant_sort && w.sorted)
-    {
-        RayOctantKeysKernel<<<gr.kinds, kBlock, 0, st>>>(w, parity);
-        ShadeScatterKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
-        RaySortBackKernel<<<gr.scatter, kBlock, 0, st>>>(w, parity);
-        SortCountsClearKernel<<<1, 2 * kShadeKinds, 0, st>>>(w);
-    }
     LaunchTrace(shape, gr, one, w, parity, false, st);
     if (gc.guide)
     {
@@ -2271,8 +2208,7 @@ bbg_status Enqueue(bbg_integrator* I, const Grids& gr, const SceneDev& s, const 
     }
     for (int k = 0; k < iterations; ++k)
     {
-        // Camera rays (level 0) are coherent already.
-        BBG_TRY(EnqueueLevel(gr, s, w, gc, k & 1, shape, st, I->trace_octant && k > 0 && !gc.guide));
+        BBG_TRY(EnqueueLevel(gr, s, w, gc, k & 1, shape, st));
     }
     FilmKernel<<<gr.film, kBlock, 0, st>>>(one, w);
     BBG_CUDA(cudaGetLastError());
@@ -2331,11 +2267,6 @@ bbg_status PrepareSamplerAndFilter(bbg_integrator* I, const bbg_camera* cam, con
         return Fail(BBG_ERR_INVALID_ARG, "shade_order %d", p->shade_order);
     }
     I->shade_sort = p->shade_order == BBG_SHADE_SORTED;
-    if (p->trace_order != BBG_TRACE_QUEUE && p->trace_order != BBG_TRACE_OCTANT)
-    {
-        return Fail(BBG_ERR_INVALID_ARG, "trace_order %d", p->trace_order);
-    }
-    I->trace_octant = p->trace_order == BBG_TRACE_OCTANT;
     if (p->sampler != BBG_SAMPLER_INDEPENDENT &&
         (p->sampler != BBG_SAMPLER_STRATIFIED || p->x_samples <= 0 || p->spp % p->x_samples != 0))
     {
@@ -2507,7 +2438,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
                       !SameScene(I->graph_scene, s) || !SameFilm(I->graph_film, f) ||
                       I->graph_guide_handle != gc.guide || !SameGuide(I->graph_guide, gc.dev) ||
                       I->graph_guide_lr != gc.lr || I->graph_shape != trace_shape ||
-                      I->graph_shade_sort != I->shade_sort || I->graph_trace_octant != I->trace_octant))
+                      I->graph_shade_sort != I->shade_sort))
     {
         if (I->graph)
         {
@@ -2534,7 +2465,6 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
         I->graph_guide_lr = gc.lr;
         I->graph_shape = trace_shape;
         I->graph_shade_sort = I->shade_sort;
-        I->graph_trace_octant = I->trace_octant;
     }
 
     // Device time of the render itself: buffer set-up and graph capture

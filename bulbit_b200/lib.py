@@ -265,7 +265,7 @@ class GpuPathIntegrator:
     def render(self, spp=None, seed=None, camera_spec=None, wave_paths=0, use_graph=True, light_alias=False,
                path_L=False, guide=None, train=False, batch=0, lr=0.0, select=0.0, steps=0,
                sampler=abi.BBG_SAMPLER_INDEPENDENT, x_samples=1, jitter=True, shade_order=abi.BBG_SHADE_SORTED,
-               pass_through_levels=0, trace_order=abi.BBG_TRACE_QUEUE):
+               pass_through_levels=0):
         s = self.scene
         spec = camera_spec or s.camera
         cam = camera(spec)
@@ -287,7 +287,6 @@ class GpuPathIntegrator:
         p.jitter = 1 if jitter else 0
         p.shade_order = shade_order
         p.pass_through_levels = pass_through_levels
-        p.trace_order = trace_order
         film = Film(cam.width, cam.height, spp, path_L=path_L)
         fs = film.struct()
         check(get_lib().bbg_render(self.h, C.byref(cam), C.byref(p), C.byref(fs), abi.BBG_MEM_HOST,

@@ -436,12 +436,6 @@ typedef struct bbg_render_params
                              on, level by level, for at most this many extra
                              levels (0: 4096) before the render gives up with
                              BBG_ERR_TIMEOUT */
-    int32_t trace_order;  /* BBG_TRACE_QUEUE (0): closest-hit passes take each
-                             level's rays in queue order; BBG_TRACE_OCTANT:
-                             bounce levels' queues are first counting-sorted by
-                             the octant of the ray direction (plain renders of
-                             one scene with the shading sort on). Results are
-                             identical. */
 } bbg_render_params;
 
 enum
@@ -454,12 +448,6 @@ enum
 {
     BBG_SHADE_SORTED = 0,
     BBG_SHADE_QUEUE = 1
-};
-
-enum
-{
-    BBG_TRACE_QUEUE = 0,
-    BBG_TRACE_OCTANT = 1
 };
 
 /* Per-pixel film state, W*H entries each, pixel index y*W + x. The fields
