@@ -15,6 +15,8 @@
  *   bbg_accel_create       the GPU accel beside BVH: takes the reference-built
  *                          flattened tree (include/bulbit/bvh.h:46 layout) or
  *                          builds the same tree itself
+ *   bbg_accel_create_device_sah  BVH::BVH (src/accel/bvh.cpp:8-297): the same
+ *                          tree, node for node, built on the device
  *   bbg_intersect          BVH::Intersect (src/accel/bvh.cpp:299), batched
  *   bbg_intersect_any      BVH::IntersectAny (src/accel/bvh.cpp:334), batched
  *   bbg_accel_bounds       Intersectable::GetAABB (include/bulbit/intersectable.h:41)
