@@ -925,22 +925,25 @@ def main():
     if args.workload == "all":
         pt, pt_scene = run_pt(args, barrier, world)
         line["path_tracing"] = pt
-        if rank == 0:
-            line["guided_path_tracing"] = run_guided(args)
-            if not args.no_batch:
-                line["batched_scenes"] = run_batch(args)
-        barrier()
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    # Every collective of the run is behind us: the other ranks leave, and
+    # rank 0 alone runs the single-GPU extras (guided rendering, the batch of
+    # scenes, the CPU baselines) without anyone waiting on a barrier.
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    if args.workload == "all":
+        line["guided_path_tracing"] = run_guided(args)
+        if not args.no_batch:
+            line["batched_scenes"] = run_batch(args)
+    if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(scene, closest, anyq)
         if args.workload == "all":
             line["path_tracing"]["cpu_baseline"] = pt_cpu_baseline(pt_scene)
             cpu = line["path_tracing"]["cpu_baseline"]
             if cpu:
                 line["path_tracing"]["vs_cpu_baseline"] = line["path_tracing"]["value"] / cpu["value"]
-    if rank == 0:
-        print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
+    print(json.dumps(line))
 
 
 if __name__ == "__main__":

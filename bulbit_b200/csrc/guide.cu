@@ -668,8 +668,8 @@ __global__ void __launch_bounds__(kTcThreads) GuideWeightGradTcKernel(const __nv
     {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(bar)), "r"(1) : "memory");
     }
-    // The tile stores (generic proxy) become visible to the tensor cores
-    // (async proxy); the allocated address becomes visible to every thread.
+    // The staged tiles become visible to the tensor cores (the async
+    // proxy); the allocated address becomes visible to every thread.
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();

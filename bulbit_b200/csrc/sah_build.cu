@@ -261,7 +261,7 @@ __global__ void __launch_bounds__(kSahBlock) SahBlockKernel(SahDev S, const int3
 {
     __shared__ int32_t s_cnt[kBuckets];
     __shared__ uint32_t s_key[kBuckets][kKeys];
-    __shared__ int32_t s_dec[3];           // split bucket (-1: leaf), mid, child id
+    __shared__ int32_t s_dec[2];           // split bucket (-1: leaf), left count
     __shared__ uint32_t s_child[2][kKeys]; // children's bounds
     __shared__ int32_t s_scan[2][kSahBlock / 32];
     __shared__ int32_t s_total[2];
