@@ -423,20 +423,23 @@ def run_pt(args, barrier, world):
     integ.close()
     acc.close()
     # The same frame over a tree built on split references (a different tree
-    # from the reference's SAH tree: hits agree except exact ties), default
-    # launch configuration; its host build time beside the plain SAH build's.
+    # from the reference's SAH tree: hits agree except exact ties); its host
+    # build time beside the plain SAH build's.
     if args.pt_split is None and args.pt_split_report > 0:
         t0 = time.perf_counter()
         acc = lib.GpuAccel(scene, split=args.pt_split_report)
         split_build_s = time.perf_counter() - t0
         integ = lib.GpuPathIntegrator(acc, scene)
-        params.wave_paths = args.pt_wave
+        # The launch configuration tuned for the reference tree (a different
+        # tree, the same frame).
+        integ.set_tuning(tuning.block, tuning.short_stack, tuning.wave_paths)
+        params.wave_paths = 0
         split_ms, split_rays = timed()
         split_ms = max_over_ranks([split_ms], device="cuda")[0]
         out["split_reference_tree"] = {
             "budget": args.pt_split_report, "value": whole_job_rate(paths * steps, world, split_ms), "unit": "paths/s",
             "mrays_per_s": world * split_rays / (split_ms / 1e3) / 1e6, "ms_per_frame": split_ms / steps,
-            "bvh_build_s": round(split_build_s, 3)}
+            "bvh_build_s": round(split_build_s, 3), "launch_configuration": "the reference tree's tuned one"}
         integ.close()
         acc.close()
     return out, scene

@@ -109,6 +109,9 @@ constexpr int32_t kSceneMask = 0x7ff << kSceneShift;
 constexpr int32_t kMaxBatchScenes = 0x800;
 // Largest batch rendered with guides (one guide per scene).
 constexpr int32_t kMaxGuidedScenes = 64;
+// Device memory per path slot of a wave (bbg_integrator::Reserve): eight
+// float4 records, the sampler state, five int32 arrays and a sort key.
+constexpr double kWaveBytesPerPath = 8 * 16 + 8 + 5 * 4 + 1;
 // Extra levels after max_bounces + 1 for paths crossing material-less
 // surfaces, unless bbg_render_params.pass_through_levels sets another cap.
 constexpr int kMaxPassThroughLevels = 4096;
@@ -1938,6 +1941,7 @@ struct bbg_integrator
         return w;
     }
 
+    // Path state per wave slot (the arrays below): kWaveBytesPerPath.
     bbg_status Reserve(int64_t n)
     {
         if (n <= capacity) return BBG_OK;
@@ -3128,10 +3132,15 @@ bbg_status Tune(const std::vector<int64_t>& key, int64_t pixels, int32_t spp, co
             best_shape = k;
         }
     }
-    for (int e = 20; e <= 24; ++e)
+    // Larger waves leave fewer bounce levels with few rays, but hold more
+    // device memory (kWaveBytesPerPath of path state each): a wave size is
+    // tried only if its state fits in a quarter of the free device memory.
+    size_t free_bytes = 0, total_bytes = 0;
+    BBG_CUDA(cudaMemGetInfo(&free_bytes, &total_bytes));
+    for (int e = 20; e <= 26; ++e)
     {
         int64_t wave = int64_t(1) << e;
-        if (wave == w0 || wave > total)
+        if (wave == w0 || wave > total || double(wave) * kWaveBytesPerPath > 0.25 * double(free_bytes))
         {
             continue;
         }

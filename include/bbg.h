@@ -542,8 +542,9 @@ typedef struct bbg_tuning
 
 /* Chooses the configuration for renders of this scene, camera size, spp and
  * bounce limit by timing short probe renders (first each launch shape at the
- * default wave size, then each wave size from 2^20 to 2^24 paths that the
- * render can fill), keeps it for the integrator's later renders that leave
+ * default wave size, then each wave size from 2^20 to 2^26 paths that the
+ * render can fill and whose path state, about 157 bytes per path, fits in a
+ * quarter of the free device memory), keeps it for the integrator's later renders that leave
  * wave_paths at 0, and caches it per scene signature (primitive and node
  * counts, tree depth, image size, spp, bounces) for the process, so a later
  * identical scene is not timed again. params: spp and seed of the renders to
