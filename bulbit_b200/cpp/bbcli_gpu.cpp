@@ -1,29 +1,34 @@
 // bbcli_gpu: the reference CLI's render route (cli/main.cpp:191-297: scene ->
 // BVH -> filter, camera, sampler -> Integrator::Create -> Render -> image)
 // with the GPU tree and the GPU integrator in place of BVH and
-// PathIntegrator. Scenes come from the reference CLI's built-in sample
-// registry (Sample::Get, cli/samples.h:37-48), whose scene files this program
-// is linked with; the options that apply to the path tracer are the CLI's
-// (cli/main.cpp:8-33): -t -o -s -b -i -r. XML scene files need the CLI's
-// scene loader (cli/scene_loader.cpp: pugixml, tinyobjloader, tinygltf),
-// which this program does not link; they are reported and skipped, as the
-// CLI does for a scene it cannot load. Images are written as Radiance .hdr
-// (flat RGBE scanlines) or .pfm; other extensions are saved as .hdr.
+// PathIntegrator. As in the CLI (cli/main.cpp:199-203), each input is first
+// looked up in the built-in sample registry (Sample::Get, cli/samples.h:37-48)
+// and otherwise read as an XML scene file by the CLI's own scene loader
+// (LoadScene, cli/scene_loader.cpp:2147), with OBJ and glTF models through its
+// model loader (cli/model_loader.cpp); those two are compiled against this
+// project's XML, OBJ and glTF readers (bulbit_b200/cpp/scene_io), which stand
+// in for pugixml, tinyobjloader and tinygltf. A scene that fails to load is
+// reported and skipped, as the CLI does. The options that apply to the path
+// tracer are the CLI's (cli/main.cpp:8-33): -t -o -s -b -i -r. Images are
+// written as Radiance .hdr (flat RGBE scanlines) or .pfm; other extensions
+// are saved as .hdr.
 //
 // Build: compile with the reference's include directory and flags, link the
-// reference library objects, the CLI's builders and sample scenes,
-// bulbit_gpu.cpp and libbulbit_b200.so.
+// reference library objects, the CLI's builders, loaders and sample scenes,
+// the scene_io readers, bulbit_gpu.cpp and libbulbit_b200.so.
 
 #include "bulbit_gpu.hpp"
 
 #include "bulbit/parallel.h"
 #include "samples.h"
+#include "scene_loader.h"
 
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <filesystem>
 #include <memory>
 #include <string>
 #include <thread>
@@ -105,7 +110,7 @@ void PrintHelp()
 {
     std::printf(
         "\nUsage:\n"
-        "  bbcli_gpu [options] <sample_name> [<sample_name>...]\n\n"
+        "  bbcli_gpu [options] <scene.xml | sample_name> [<scene.xml | sample_name>...]\n\n"
         "Options:\n"
         "  -t <num_threads>          Host threads (scene set-up, film)  (default: hardware concurrency)\n"
         "  -o <output_file>          Output file name, .hdr or .pfm  (default: from scene or generated)\n"
@@ -194,18 +199,18 @@ int main(int argc, const char* argv[])
         std::printf("\n--- %s ---\n", input.c_str());
         auto t0 = std::chrono::steady_clock::now();
         RendererInfo ri;
-        if (!Sample::Get(&ri, input))
+        bool loaded = Sample::Get(&ri, input);
+        if (!loaded)
         {
-            if (EndsWith(input, ".xml"))
-            {
-                std::fprintf(stderr, "Cannot load %s: XML scenes need the CLI's scene loader (pugixml, "
-                                     "tinyobjloader, tinygltf), which this program does not link\n",
-                             input.c_str());
-            }
-            else
-            {
-                std::fprintf(stderr, "Failed to load scene or sample: %s\n", input.c_str());
-            }
+            // LoadScene changes into the file's directory while it reads, so
+            // it gets an absolute path (a bare file name has no parent).
+            std::error_code ec;
+            std::filesystem::path path = std::filesystem::absolute(input, ec);
+            loaded = !ec && LoadScene(&ri, path);
+        }
+        if (!loaded)
+        {
+            std::fprintf(stderr, "Failed to load scene or sample: %s\n", input.c_str());
             ++failures;
             continue;
         }

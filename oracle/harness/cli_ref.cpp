@@ -1,18 +1,21 @@
 // Test infrastructure (the oracle): renders a built-in sample scene of the
-// reference CLI (Sample::Get, cli/samples.h:37-48) through the reference's own
-// route (cli/main.cpp:191-297: BVH, Filter/Camera/Sampler::Create,
-// Integrator::Create, Render) on the host threads, and writes the image as a
-// .pfm. The GPU CLI's output is compared against it.
+// reference CLI (Sample::Get, cli/samples.h:37-48) or an XML scene file read
+// by the CLI's scene loader (LoadScene, cli/scene_loader.cpp:2147) through the
+// reference's own route (cli/main.cpp:191-297: BVH, Filter/Camera/
+// Sampler::Create, Integrator::Create, Render) on the host threads, and writes
+// the image as a .pfm. The GPU CLI's output is compared against it.
 //
-//   cli_ref [-t threads] [-s spp] [-b max_bounces] [-r scale] -o out.pfm <sample_name>
+//   cli_ref [-t threads] [-s spp] [-b max_bounces] [-r scale] -o out.pfm <scene.xml | sample_name>
 
 #include "bulbit/bulbit.h"
 #include "bulbit/parallel.h"
 #include "samples.h"
+#include "scene_loader.h"
 
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
+#include <filesystem>
 #include <memory>
 #include <string>
 #include <thread>
@@ -37,21 +40,22 @@ int main(int argc, const char* argv[])
     }
     if (input.empty() || out.empty())
     {
-        std::fprintf(stderr, "usage: cli_ref [-t n] [-s spp] [-b bounces] [-r scale] -o out.pfm <sample>\n");
+        std::fprintf(stderr, "usage: cli_ref [-t n] [-s spp] [-b bounces] [-r scale] -o out.pfm <scene.xml | sample>\n");
         return 2;
     }
     ThreadPool::global_thread_pool = std::make_unique<ThreadPool>(std::max(1, threads));
 
     RendererInfo ri;
-    if (!Sample::Get(&ri, input))
+    if (!Sample::Get(&ri, input) && !LoadScene(&ri, std::filesystem::absolute(input)))
     {
-        std::fprintf(stderr, "unknown sample %s\n", input.c_str());
+        std::fprintf(stderr, "cannot load scene or sample %s\n", input.c_str());
         return 1;
     }
     if (spp > 0) ri.camera_info.sampler_info.spp = spp;
     if (bounces >= 0) ri.integrator_info.max_bounces = bounces;
     ri.camera_info.film_info.resolution *= scale;
 
+    std::printf("primitives %zu lights %zu\n", ri.scene.GetPrimitives().size(), ri.scene.GetLights().size());
     BVH accel(ri.scene.GetPrimitives());
     Allocator alloc;
     Filter* filter = Filter::Create(alloc, ri.camera_info.film_info.filter_info);

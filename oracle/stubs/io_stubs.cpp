@@ -6,7 +6,9 @@
 //   * image reads report "no file" (an empty image) and writes do nothing, so
 //     the reflectance tables of src/bxdf/microfacet.cpp:239 are always
 //     recomputed in memory (deterministic, never loaded from a lossy file);
-//   * NanoVDBMedium members abort if ever reached (no config uses volumes).
+//   * NanoVDBMedium members abort if ever reached (no config uses volumes;
+//     the CLI's scene loader reaches the constructor only after reading a
+//     NanoVDB file, which the nanovdb shim refuses).
 #include "bulbit/image.h"
 #include "bulbit/image3d.h"
 #include "bulbit/media.h"
@@ -49,6 +51,14 @@ void WriteImage3D(const Image3D3&, const std::filesystem::path&) {}
     std::abort();
 }
 
+NanoVDBMedium::NanoVDBMedium(const Transform&, Spectrum, Spectrum, Float, Float g,
+                             nanovdb::GridHandle<nanovdb::HostBuffer>, nanovdb::GridHandle<nanovdb::HostBuffer>, Float,
+                             Float, Float)
+    : Medium(TypeIndexOf<NanoVDBMedium>())
+    , phase{ g }
+{
+    NoVolumes();
+}
 void NanoVDBMedium::Destroy() {}
 bool NanoVDBMedium::IsEmissive() const { NoVolumes(); }
 MediumSample NanoVDBMedium::SamplePoint(Point3) const { NoVolumes(); }

@@ -9,7 +9,8 @@ import re
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 SOURCES = [os.path.join(ROOT, "bulbit_b200", "csrc", f) for f in os.listdir(os.path.join(ROOT, "bulbit_b200", "csrc"))
            if f.endswith((".cu", ".cuh", ".cpp", ".h"))] + \
-          [os.path.join(ROOT, "bulbit_b200", "cpp", f) for f in os.listdir(os.path.join(ROOT, "bulbit_b200", "cpp"))]
+          [os.path.join(ROOT, "bulbit_b200", "cpp", f) for f in os.listdir(os.path.join(ROOT, "bulbit_b200", "cpp"))
+           if f.endswith((".cpp", ".h", ".hpp"))]
 
 
 def code_of(path):
