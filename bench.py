@@ -509,8 +509,8 @@ def run_guided(args):
     mlp = profile_values("guide_mlp_cornell128.md")
     out = {
         "metric": "relMSE at equal time, guided / plain", "value": (e_guided * t_guided) / (e_plain * t_plain),
-        "mlp": {"kernels": "GuideForwardKernel (mma.sync BF16), GuideWeightGradTcKernel (tcgen05, BF16 in, FP32 "
-                           "accumulators in tensor memory); bulbit_b200/csrc/guide.cu",
+        "mlp": {"kernels": "GuideForwardKernel and GuideWeightGradTcKernel (tcgen05, BF16 in, FP32 accumulators "
+                           "in tensor memory); bulbit_b200/csrc/guide.cu",
                 "forward_tensor_pipe_active": mlp.get("forward_tensor_pipe_active"),
                 "wgrad_tensor_pipe_active": mlp.get("wgrad_tensor_pipe_active"),
                 "wgrad_us_per_adam_step": mlp.get("wgrad_us"),

@@ -4,8 +4,10 @@
 // its fallback and the yardstick of its error.
 //
 // Network: 80 inputs -> 64 -> 64 -> 64 (ReLU) -> 40 outputs, BF16 weights and
-// activations, FP32 accumulation (mma.sync m16n8k16), FP32 biases and master
-// weights.
+// activations, FP32 accumulation, FP32 biases and master weights. Inference
+// runs on tcgen05.mma (128-query tiles, accumulators in tensor memory); the
+// training pass's per-sample forward and backward on mma.sync m16n8k16 tiles
+// of 16 samples, its weight gradients on tcgen05.mma.
 //   inputs  [0, 72): sin / cos(2^k * pi * p_a) for axis a, k = 0..11, where p
 //                    is the position scaled to [0, 1] by the scene bounds
 //           [72, 75) shading normal, [75, 78) outgoing direction wo,
@@ -65,6 +67,20 @@ constexpr int kBfT1 = kBfFwd;                            // W1^T [64][64]
 constexpr int kBfT2 = kBfT1 + kGuideHidden * kGuideHidden;
 constexpr int kBfT3 = kBfT2 + kGuideHidden * kGuideHidden; // W3^T [64][48]
 constexpr int kBfAll = kBfT3 + kGuideHidden * kGuideOutPad;
+// The forward image for the fifth-generation tensor cores (the inference
+// kernels), after the images above: each layer's W [n][k] as the B operand of
+// tcgen05.mma in the canonical K-major layout without swizzle, 8 x 8 core
+// matrices (8 rows of 16 bytes), 8-row groups 128 bytes apart and 8-column
+// groups (N / 8) * 128 bytes apart: element (n, k) at
+// (k / 8) * (N / 8) * 64 + (n / 8) * 64 + (n % 8) * 8 + k % 8. W3 is padded to
+// N = 48 rows with zeros (the MMA's N is a multiple of 16).
+constexpr int kTcW0 = 0;
+constexpr int kTcW1 = kTcW0 + kGuideHidden * kGuideIn;
+constexpr int kTcW2 = kTcW1 + kGuideHidden * kGuideHidden;
+constexpr int kTcW3 = kTcW2 + kGuideHidden * kGuideHidden;
+constexpr int kTcImage = kTcW3 + kGuideOutPad * kGuideHidden; // 16384 values, 32 KB
+constexpr int kBfTc = kBfAll;                                  // offset of that image in the buffer
+constexpr int kBfBuf = kBfTc + kTcImage;                       // all BF16 images of a guide
 
 constexpr float kKappaLogMin = -2.0f;
 constexpr float kKappaLogMax = 7.0f;

@@ -18,77 +18,460 @@ namespace bbg
 namespace
 {
 
-constexpr int kFwdWarps = 8;
 constexpr int kTrainWarps = 6;
+
+// ------------------------------------------------------- tensor-core helpers
+
+constexpr uint32_t kTcMaxPolls = 1u << 22; // bound on each wait for a commit of MMAs
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* p)
+{
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor: start address, leading (K direction) and
+// stride (M/N direction) byte offsets, descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t TcDesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return uint64_t((addr >> 4) & 0x3fffu) | (uint64_t((lbo >> 4) & 0x3fffu) << 16) |
+           (uint64_t((sbo >> 4) & 0x3fffu) << 32) | (uint64_t(1) << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
+// K-major, N >> 3 and M >> 4.
+__device__ __forceinline__ uint32_t TcInstr(int m, int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
+}
+
+// One tcgen05.mma.cta_group::1.kind::f16 into tensor memory at d; accumulate
+// selects D += A B over D = A B.
+__device__ __forceinline__ void TcMma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate)
+{
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(d),
+                 "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// Arrives on the mbarrier once every MMA this thread issued has completed.
+__device__ __forceinline__ void TcCommit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// Waits, at most kTcMaxPolls polls, for the mbarrier phase of the given
+// parity to complete; true if it did.
+__device__ __forceinline__ bool TcWait(uint32_t bar, uint32_t parity)
+{
+    uint32_t done = 0;
+    for (uint32_t poll = 0; poll < kTcMaxPolls && !done; ++poll)
+    {
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, p;\n\t}\n"
+                     : "=r"(done)
+                     : "r"(bar), "r"(parity)
+                     : "memory");
+        if (!done && poll >= 16)
+        {
+            __nanosleep(32);
+        }
+    }
+    return done != 0;
+}
+
+// 16 consecutive FP32 accumulator columns of the calling thread's tensor-
+// memory lane (32x32b shape: warp w reads lanes 32w..32w+31); the values are
+// valid after TcWaitLoads.
+__device__ __forceinline__ void TcLoad16(uint32_t taddr, uint32_t (&v)[16])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                 "%12, %13, %14, %15}, [%16];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                   "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                   "=r"(v[15])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void TcLoad8(uint32_t taddr, uint32_t (&v)[8])
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7])
+                 : "r"(taddr));
+}
+
+__device__ __forceinline__ void TcWaitLoads()
+{
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// A barrier across the CTA that also orders tensor-core operations (issued
+// MMAs, tensor-memory loads) and generic shared-memory writes, which the
+// MMAs read through the async proxy, with the threads' program order.
+__device__ __forceinline__ void TcSyncThreads()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
 
 // ---------------------------------------------------------------- forward
 
-// Per-warp tile of 16 queries: features -> X (smem, [16][80] bf16) ->
-// 3 hidden layers in registers -> 40 outputs.
-template <class Src>
-__device__ __forceinline__ void ForwardTile(const Src& src, int64_t tile, int64_t n, const GuideBounds& bounds,
-                                            const __nv_bfloat16* w, const float* bias, __nv_bfloat16* x, int lane)
+// Inference on the fifth-generation tensor cores: a tile is 128 queries and
+// a CTA has two threads per query. Threads t and t + 128 (warps w and w + 4,
+// which share tensor-memory lanes 32 (w % 4) .. + 31) take query t % 128 and
+// one half of its columns each. They write the query's 80 features (BF16)
+// into the A tile in shared memory (canonical K-major layout: 8-row x 16-byte
+// core matrices, 8-row groups 128 bytes apart, 8-column groups kFtLboA bytes
+// apart, so a warp's 16-byte stores of one column group are contiguous);
+// thread 0 issues the layer's MMAs (128 x N x 16, BF16 in, FP32 accumulator in
+// tensor memory, weights staged once per CTA in the same layout) and commits
+// them to an mbarrier; each thread then reads its half of the accumulator row
+// with tcgen05.ld, adds the bias, applies the ReLU and writes it back as BF16
+// into the A tile as the next layer's input (the MMAs that read it have
+// completed). The output layer's 40 values go to the query's output record.
+// The next tile's raw inputs are loaded while the current tile's layers run.
+constexpr int kFtRows = 128;                                  // queries per tile (MMA M)
+constexpr int kFtThreads = 2 * kFtRows;                       // two threads per query
+constexpr uint32_t kFtSbo = 128;                              // bytes between 8-row groups
+constexpr uint32_t kFtLboA = (kFtRows / 8) * 128;             // bytes between 8-column groups of A
+constexpr size_t kFtSmemW = size_t(kTcImage) * 2;             // 32 KB
+constexpr size_t kFtSmemBias = 1024;                          // 232 floats, padded
+constexpr size_t kFtSmemA = size_t(kGuideIn / 8) * kFtLboA;   // 20 KB (80 columns; the hidden layers use 64)
+constexpr size_t kFtOffBias = kFtSmemW;
+constexpr size_t kFtOffA = kFtOffBias + kFtSmemBias;
+constexpr size_t kFtOffBar = kFtOffA + kFtSmemA;
+constexpr size_t kFtSmem = kFtOffBar + 16;                    // + mbarrier and tensor-memory address
+constexpr uint32_t kFtCols = 64;                              // tensor-memory columns (widest layer: N = 64)
+static_assert(kBfTc % 8 == 0, "the tensor-core image starts on a 16-byte boundary");
+static_assert(kFtSmemBias >= size_t(kCBias) * 4, "bias staging");
+static_assert(kGuideGroupChunk == kFtRows, "a grouped-forward chunk is one tile");
+
+// Loads a guide's tensor-core weight image and packed biases into shared
+// memory.
+__device__ __forceinline__ void StageTcWeights(const __nv_bfloat16* wg, const float* pg, uint8_t* smem)
 {
-    // Features: two lanes per row, 40 features each.
+    const uint4* src = reinterpret_cast<const uint4*>(wg + kBfTc);
+    uint4* dst = reinterpret_cast<uint4*>(smem);
+    for (int i = threadIdx.x; i < kTcImage / 8; i += blockDim.x)
     {
-        int row = lane >> 1, half = lane & 1;
-        int64_t item = tile * 16 + row;
-        __nv_bfloat16* xr = x + row * kXLd + half * 40;
-        if (item < n && src.Valid(item))
+        dst[i] = src[i];
+    }
+    float* bs = reinterpret_cast<float*>(smem + kFtOffBias);
+    for (int i = threadIdx.x; i < kCBias; i += blockDim.x)
+    {
+        int src_at = i < kCB1 ? kB0 + i : i < kCB2 ? kB1 + (i - kCB1) : i < kCB3 ? kB2 + (i - kCB2) : kB3 + (i - kCB3);
+        bs[i] = pg[src_at];
+    }
+}
+
+// Issues one layer's MMAs (K / 16 of them) and commits them to the barrier.
+__device__ __forceinline__ void IssueTcLayer(uint32_t tmem, uint32_t a, uint32_t w, int n, int k, uint32_t bar)
+{
+    const uint32_t idesc = TcInstr(kFtRows, n);
+    const uint32_t lbo_w = uint32_t(n / 8) * 128;
+    for (int ks = 0; ks < k / 16; ++ks)
+    {
+        TcMma(tmem, TcDesc(a + 2 * ks * kFtLboA, kFtLboA, kFtSbo), TcDesc(w + 2 * ks * lbo_w, lbo_w, kFtSbo), idesc,
+              ks > 0 ? 1u : 0u);
+    }
+    TcCommit(bar);
+}
+
+// One half (32 columns) of the calling thread's hidden-layer row: accumulators
+// + bias, ReLU, BF16, stored into the A row as the next layer's input.
+__device__ __forceinline__ void HiddenHalfToA(uint32_t tmem_row, const float* bias, int half, uint8_t* a_row)
+{
+    uint32_t v[2][16];
+    TcLoad16(tmem_row + uint32_t(32 * half), v[0]);
+    TcLoad16(tmem_row + uint32_t(32 * half + 16), v[1]);
+    TcWaitLoads();
+#pragma unroll
+    for (int g = 0; g < 4; ++g)
+    {
+        uint32_t w[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
         {
-            float raw[kGuideRaw];
-            src.Raw(item, raw);
-            GuideFeatures40(raw, bounds, half, [&](int j, float v0, float v1) {
-                *reinterpret_cast<uint32_t*>(xr + j) = PackBf16(v0, v1);
-            });
+            const int c = 8 * g + 2 * q, col = 32 * half + c;
+            w[q] = PackBf16(fmaxf(__uint_as_float(v[c / 16][c % 16]) + bias[col], 0.0f),
+                            fmaxf(__uint_as_float(v[c / 16][c % 16 + 1]) + bias[col + 1], 0.0f));
+        }
+        *reinterpret_cast<uint4*>(a_row + (4 * half + g) * kFtLboA) = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
+
+// The raw inputs of one query and where its output goes (id < 0: no query).
+struct QueryIn
+{
+    float raw[kGuideRaw];
+    int64_t id;
+};
+
+// One 128-query tile through the network with the weights staged in smem;
+// prefetch() runs once the features are written. Returns false if an MMA
+// commit did not arrive in time (the tile's outputs are then not written);
+// *phase counts the barrier's completed phases.
+template <class Prefetch>
+__device__ __forceinline__ bool ForwardTcTile(const QueryIn& q, const GuideBounds& bounds, float* out, uint8_t* smem,
+                                              uint32_t tmem, uint32_t* phase, Prefetch&& prefetch)
+{
+    const int r = threadIdx.x & (kFtRows - 1), half = threadIdx.x / kFtRows;
+    uint8_t* a_row = smem + kFtOffA + size_t(r) * 16;
+    const float* bias = reinterpret_cast<const float*>(smem + kFtOffBias);
+    const uint32_t a = SmemAddr(smem + kFtOffA), w = SmemAddr(smem), bar = SmemAddr(smem + kFtOffBar);
+    const uint32_t tmem_row = tmem + (uint32_t(r & ~31) << 16);
+
+    // Features 40 half .. 40 half + 39: 20 BF16 pairs, stored as 5 16-byte
+    // rows of the A tile.
+    {
+        uint32_t x[kGuideIn / 4];
+        if (q.id >= 0)
+        {
+            GuideFeatures40(q.raw, bounds, half, [&](int j, float v0, float v1) { x[j >> 1] = PackBf16(v0, v1); });
         }
         else
         {
 #pragma unroll
-            for (int j = 0; j < 40; j += 2)
+            for (int k = 0; k < kGuideIn / 4; ++k)
             {
-                *reinterpret_cast<uint32_t*>(xr + j) = 0u;
+                x[k] = 0u;
             }
         }
-    }
-    __syncwarp();
-    uint32_t a0[5][4];
 #pragma unroll
-    for (int kt = 0; kt < 5; ++kt)
-    {
-        LoadA(x, kXLd, 0, kt * 16, lane, a0[kt]);
-    }
-    float acc[8][4];
-    uint32_t a[4][4];
-    HiddenLayer<5>(a0, w + kBf0, bias + kCB0, lane, acc);
-    AccToA(acc, a);
-    HiddenLayer<4>(a, w + kBf1, bias + kCB1, lane, acc);
-    AccToA(acc, a);
-    HiddenLayer<4>(a, w + kBf2, bias + kCB2, lane, acc);
-    AccToA(acc, a);
-    float out[5][4];
-    OutputLayer(a, w + kBf3, bias + kCB3, lane, out);
-    int g = lane >> 2, t = lane & 3;
-#pragma unroll
-    for (int half = 0; half < 2; ++half)
-    {
-        int64_t item = tile * 16 + g + 8 * half;
-        if (item < n && src.Valid(item))
+        for (int g = 0; g < kGuideIn / 16; ++g)
         {
-            float* o = src.Out(item);
+            *reinterpret_cast<uint4*>(a_row + (5 * half + g) * kFtLboA) =
+                make_uint4(x[4 * g], x[4 * g + 1], x[4 * g + 2], x[4 * g + 3]);
+        }
+    }
+    prefetch();
+
+    const struct
+    {
+        int w_off, n, k, bias_off;
+    } kLayers[4] = { { kTcW0, kGuideHidden, kGuideIn, kCB0 },
+                     { kTcW1, kGuideHidden, kGuideHidden, kCB1 },
+                     { kTcW2, kGuideHidden, kGuideHidden, kCB2 },
+                     { kTcW3, kGuideOutPad, kGuideHidden, kCB3 } };
 #pragma unroll
-            for (int nt = 0; nt < 5; ++nt)
+    for (int l = 0; l < 4; ++l)
+    {
+        TcSyncThreads(); // the A tile is written; the last layer's loads are done
+        if (threadIdx.x == 0)
+        {
+            IssueTcLayer(tmem, a, w + 2 * uint32_t(kLayers[l].w_off), kLayers[l].n, kLayers[l].k, bar);
+        }
+        const bool done = TcWait(bar, *phase & 1u);
+        *phase += 1;
+        if (!__syncthreads_and(done))
+        {
+            return false;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (l < 3)
+        {
+            HiddenHalfToA(tmem_row, bias + kLayers[l].bias_off, half, a_row);
+        }
+    }
+
+    // Output layer: half 0 takes columns 0..23, half 1 columns 24..39 (of the
+    // 48; the rest are the zero padding).
+    const float* b3 = bias + kCB3;
+    if (half == 0)
+    {
+        uint32_t v0[16], v1[8];
+        TcLoad16(tmem_row, v0);
+        TcLoad8(tmem_row + 16u, v1);
+        TcWaitLoads();
+        if (q.id >= 0)
+        {
+            float* o = out + kGuideOut * q.id;
+#pragma unroll
+            for (int c = 0; c < 16; c += 4)
             {
-                o[nt * 8 + 2 * t] = out[nt][2 * half];
-                o[nt * 8 + 2 * t + 1] = out[nt][2 * half + 1];
+                *reinterpret_cast<float4*>(o + c) =
+                    make_float4(__uint_as_float(v0[c]) + b3[c], __uint_as_float(v0[c + 1]) + b3[c + 1],
+                                __uint_as_float(v0[c + 2]) + b3[c + 2], __uint_as_float(v0[c + 3]) + b3[c + 3]);
+            }
+#pragma unroll
+            for (int c = 0; c < 8; c += 4)
+            {
+                *reinterpret_cast<float4*>(o + 16 + c) = make_float4(
+                    __uint_as_float(v1[c]) + b3[16 + c], __uint_as_float(v1[c + 1]) + b3[17 + c],
+                    __uint_as_float(v1[c + 2]) + b3[18 + c], __uint_as_float(v1[c + 3]) + b3[19 + c]);
             }
         }
     }
-    __syncwarp();
+    else
+    {
+        uint32_t v0[16];
+        TcLoad16(tmem_row + 24u, v0);
+        TcWaitLoads();
+        if (q.id >= 0)
+        {
+            float* o = out + kGuideOut * q.id + 24;
+#pragma unroll
+            for (int c = 0; c < 16; c += 4)
+            {
+                *reinterpret_cast<float4*>(o + c) = make_float4(
+                    __uint_as_float(v0[c]) + b3[24 + c], __uint_as_float(v0[c + 1]) + b3[25 + c],
+                    __uint_as_float(v0[c + 2]) + b3[26 + c], __uint_as_float(v0[c + 3]) + b3[27 + c]);
+            }
+        }
+    }
+    return true;
 }
 
-// Loads BF16 weights (the first n_bf16 values) and the packed biases into
-// shared memory.
+// Tensor memory and the mbarrier of a forward CTA: allocated by warp 0, the
+// address published to every thread.
+__device__ __forceinline__ uint32_t ForwardTcSetUp(uint8_t* smem)
+{
+    uint32_t* slot = reinterpret_cast<uint32_t*>(smem + kFtOffBar + 8);
+    if (threadIdx.x < 32)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(SmemAddr(slot)),
+                     "r"(kFtCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (threadIdx.x == 0)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(SmemAddr(smem + kFtOffBar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    TcSyncThreads();
+    return *slot;
+}
+
+__device__ __forceinline__ void ForwardTcTearDown(uint32_t tmem)
+{
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (threadIdx.x < 32)
+    {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kFtCols));
+    }
+}
+
+// The query behind entry item of the forward's input (index, when set, maps
+// entries to record ids; -1 entries are padding).
+__device__ __forceinline__ QueryIn FetchQuery(const float* raw, const int32_t* index, int64_t item, int64_t n)
+{
+    QueryIn q;
+    q.id = item < n ? (index ? int64_t(index[item]) : item) : -1;
+#pragma unroll
+    for (int k = 0; k < kGuideRaw; ++k)
+    {
+        q.raw[k] = 0.0f;
+    }
+    if (q.id >= 0)
+    {
+        const float2* p = reinterpret_cast<const float2*>(raw + kGuideRaw * q.id);
+#pragma unroll
+        for (int k = 0; k < kGuideRaw / 2; ++k)
+        {
+            const float2 v = p[k];
+            q.raw[2 * k] = v.x;
+            q.raw[2 * k + 1] = v.y;
+        }
+    }
+    return q;
+}
+
+// Persistent forward: CTA b takes tiles b, b + grid, ...
+__global__ void __launch_bounds__(kFtThreads, 4) GuideForwardKernel(const float* raw, const int32_t* index,
+                                                                    const int32_t* n_dev, int64_t n_host,
+                                                                    GuideBounds bounds, const __nv_bfloat16* wg,
+                                                                    const float* pg, float* out, int32_t* status)
+{
+    extern __shared__ __align__(128) uint8_t ft_smem[];
+    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
+    const int64_t tiles = (n + kFtRows - 1) / kFtRows;
+    if (int64_t(blockIdx.x) >= tiles)
+    {
+        return; // the whole CTA, before any tensor-memory use
+    }
+    const int r = threadIdx.x & (kFtRows - 1);
+    QueryIn q = FetchQuery(raw, index, int64_t(blockIdx.x) * kFtRows + r, n);
+    StageTcWeights(wg, pg, ft_smem);
+    const uint32_t tmem = ForwardTcSetUp(ft_smem);
+    uint32_t phase = 0;
+    bool ok = true;
+    for (int64_t tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x)
+    {
+        QueryIn next;
+        ok = ForwardTcTile(q, bounds, out, ft_smem, tmem, &phase,
+                           [&] { next = FetchQuery(raw, index, (tile + gridDim.x) * kFtRows + r, n); });
+        q = next;
+    }
+    if (!ok && threadIdx.x == 0)
+    {
+        atomicExch(status, 1); // a commit of MMAs did not arrive within the bound
+    }
+    ForwardTcTearDown(tmem);
+}
+
+// Grouped forward: each CTA takes a contiguous run of chunks (one tile each)
+// and stages a group's weights whenever the run enters a new group (a chunk
+// never spans two groups).
+__global__ void __launch_bounds__(kFtThreads, 4) GuideGroupedForwardKernel(const float* raw, const int32_t* index,
+                                                                           const int32_t* chunk_start,
+                                                                           int32_t n_groups, const GuideGroup* groups,
+                                                                           float* out)
+{
+    extern __shared__ __align__(128) uint8_t ft_smem[];
+    const int64_t chunks = chunk_start[n_groups];
+    const int64_t c0 = chunks * blockIdx.x / gridDim.x, c1 = chunks * (blockIdx.x + 1) / gridDim.x;
+    if (c0 >= c1)
+    {
+        return;
+    }
+    const int r = threadIdx.x & (kFtRows - 1);
+    const int64_t n = chunks * kGuideGroupChunk;
+    QueryIn q = FetchQuery(raw, index, c0 * kFtRows + r, n);
+    const uint32_t tmem = ForwardTcSetUp(ft_smem);
+    uint32_t phase = 0;
+    bool ok = true;
+    int32_t staged = -1;
+    for (int64_t c = c0; c < c1 && ok; ++c)
+    {
+        // The group whose chunk range holds c (CTA-uniform).
+        int32_t lo = 0, hi = n_groups - 1;
+        while (lo < hi)
+        {
+            int32_t mid = (lo + hi + 1) >> 1;
+            if (chunk_start[mid] <= c)
+            {
+                lo = mid;
+            }
+            else
+            {
+                hi = mid - 1;
+            }
+        }
+        if (lo != staged)
+        {
+            __syncthreads(); // the previous tile's MMAs and loads are done (its commit was awaited)
+            StageTcWeights(groups[lo].wg, groups[lo].pg, ft_smem);
+            staged = lo;
+        }
+        QueryIn next;
+        ok = ForwardTcTile(q, groups[lo].bounds, out, ft_smem, tmem, &phase,
+                           [&] { next = FetchQuery(raw, index, (c + 1 < c1 ? c + 1 : c1) * kFtRows + r, c1 * kFtRows); });
+        q = next;
+        if (!ok && threadIdx.x == 0)
+        {
+            atomicExch(groups[lo].status, 1); // a commit of MMAs did not arrive within the bound
+        }
+    }
+    ForwardTcTearDown(tmem);
+}
+
+// ---------------------------------------------------------------- training
+
+// Loads BF16 weights (the first n_bf16 values: the training images) and the
+// packed biases into shared memory.
 __device__ __forceinline__ void StageWeights(const __nv_bfloat16* wg, const float* pg, __nv_bfloat16* ws, float* bs,
                                              int n_bf16)
 {
@@ -105,97 +488,6 @@ __device__ __forceinline__ void StageWeights(const __nv_bfloat16* wg, const floa
     }
     __syncthreads();
 }
-
-struct ArraySrc
-{
-    const float* raw;
-    float* out;
-    const int32_t* index; // optional indirection (query i -> record index[i])
-
-    __device__ __forceinline__ int64_t Id(int64_t i) const { return index ? int64_t(index[i]) : i; }
-    __device__ __forceinline__ bool Valid(int64_t i) const { return !index || index[i] >= 0; }
-    __device__ __forceinline__ void Raw(int64_t i, float* r) const
-    {
-        const float* p = raw + kGuideRaw * Id(i);
-        for (int k = 0; k < kGuideRaw; ++k)
-        {
-            r[k] = p[k];
-        }
-    }
-    __device__ __forceinline__ float* Out(int64_t i) const { return out + kGuideOut * Id(i); }
-};
-
-__global__ void __launch_bounds__(32 * kFwdWarps, 4) GuideForwardKernel(const float* raw, const int32_t* index,
-                                                                      const int32_t* n_dev, int64_t n_host,
-                                                                      GuideBounds bounds, const __nv_bfloat16* wg,
-                                                                      const float* pg, float* out)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smem);
-    float* bs = reinterpret_cast<float*>(smem + kBfFwd * 2);
-    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem + kBfFwd * 2 + kCBias * 4);
-    StageWeights(wg, pg, ws, bs, kBfFwd);
-    const int64_t n = n_dev ? int64_t(*n_dev) : n_host;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* x = xs + warp * 16 * kXLd;
-    ArraySrc src{ raw, out, index };
-    const int64_t tiles = (n + 15) / 16;
-    for (int64_t tile = int64_t(blockIdx.x) * kFwdWarps + warp; tile < tiles; tile += int64_t(gridDim.x) * kFwdWarps)
-    {
-        ForwardTile(src, tile, n, bounds, ws, bs, x, lane);
-    }
-}
-
-constexpr size_t kFwdSmem = size_t(kBfFwd) * 2 + size_t(kCBias) * 4 + size_t(kFwdWarps) * 16 * kXLd * 2;
-
-static_assert(kGuideGroupChunk == 16 * kFwdWarps, "a chunk is one block's set of warp tiles");
-
-// Grouped forward: each block takes a contiguous run of chunks and stages a
-// group's weights whenever the run enters a new group (a chunk never spans
-// two groups), then each warp runs its tile of the chunk with them.
-__global__ void __launch_bounds__(32 * kFwdWarps, 4) GuideGroupedForwardKernel(const float* raw, const int32_t* index,
-                                                                             const int32_t* chunk_start,
-                                                                             int32_t n_groups, const GuideGroup* groups,
-                                                                             float* out)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    __nv_bfloat16* ws = reinterpret_cast<__nv_bfloat16*>(smem);
-    float* bs = reinterpret_cast<float*>(smem + kBfFwd * 2);
-    __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(smem + kBfFwd * 2 + kCBias * 4);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    __nv_bfloat16* x = xs + warp * 16 * kXLd;
-    const int64_t chunks = chunk_start[n_groups];
-    const int64_t c0 = chunks * blockIdx.x / gridDim.x, c1 = chunks * (blockIdx.x + 1) / gridDim.x;
-    const int64_t n = chunks * kGuideGroupChunk;
-    ArraySrc src{ raw, out, index };
-    int32_t staged = -1;
-    for (int64_t c = c0; c < c1; ++c)
-    {
-        // The group whose chunk range holds c (block-uniform).
-        int32_t lo = 0, hi = n_groups - 1;
-        while (lo < hi)
-        {
-            int32_t mid = (lo + hi + 1) >> 1;
-            if (chunk_start[mid] <= c)
-            {
-                lo = mid;
-            }
-            else
-            {
-                hi = mid - 1;
-            }
-        }
-        if (lo != staged)
-        {
-            __syncthreads(); // every warp is done with the previous group's weights
-            StageWeights(groups[lo].wg, groups[lo].pg, ws, bs, kBfFwd);
-            staged = lo;
-        }
-        ForwardTile(src, c * kFwdWarps + warp, n, groups[lo].bounds, ws, bs, x, lane);
-    }
-}
-
-// ---------------------------------------------------------------- training
 
 // Gradient of -w log q(dir) w.r.t. the 40 raw outputs of one sample, and the
 // loss term (q: the vMF mixture of MakeMixture).
@@ -588,27 +880,6 @@ constexpr size_t kTcSmemB = size_t(kTcGroups) * kTcLboB;      // 40 KB
 constexpr size_t kTcSmem = kTcSmemA + kTcSmemB + 16;          // + mbarrier and tensor-memory address
 constexpr uint32_t kTcCols = 128;                             // tensor-memory columns (N <= 80)
 constexpr int kTcThreads = 256;                               // 8 warps stage; warps 0-3 read 32 rows each
-constexpr uint32_t kTcMaxPolls = 1u << 22;                    // bound on the wait for the MMAs
-
-__device__ __forceinline__ uint32_t SmemAddr(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Shared-memory matrix descriptor: start address, leading (K direction) and
-// stride (M/N direction) byte offsets, descriptor version 1, no swizzle.
-__device__ __forceinline__ uint64_t TcDesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
-{
-    return uint64_t((addr >> 4) & 0x3fffu) | (uint64_t((lbo >> 4) & 0x3fffu) << 16) |
-           (uint64_t((sbo >> 4) & 0x3fffu) << 32) | (uint64_t(1) << 46);
-}
-
-// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, N >> 3 and M >> 4.
-__device__ __forceinline__ uint32_t TcInstr(int m, int n)
-{
-    return (1u << 4) | (1u << 7) | (1u << 10) | (uint32_t(n >> 3) << 17) | (uint32_t(m >> 4) << 24);
-}
 
 __global__ void __launch_bounds__(kTcThreads) GuideWeightGradTcKernel(const __nv_bfloat16* scratch, int64_t ld,
                                                                         const int32_t* n_dev, int64_t n_host,
@@ -786,10 +1057,22 @@ __global__ void GuideAdamKernel(float* params, float* m, float* v, float* grad, 
 
 __global__ void GuideConvertKernel(const float* params, __nv_bfloat16* w)
 {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kBfAll; i += gridDim.x * blockDim.x)
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kBfBuf; i += gridDim.x * blockDim.x)
     {
         float v = 0;
-        if (i < kBfFwd)
+        if (i >= kBfTc)
+        {
+            // Canonical K-major layout (see kTcW0): locate layer, then (n, k).
+            const int j = i - kBfTc;
+            const int base = j < kTcW1 ? kTcW0 : j < kTcW2 ? kTcW1 : j < kTcW3 ? kTcW2 : kTcW3;
+            const int src = j < kTcW1 ? kW0 : j < kTcW2 ? kW1 : j < kTcW3 ? kW2 : kW3;
+            const int n_in = j < kTcW1 ? kGuideIn : kGuideHidden;
+            const int n_out = j < kTcW3 ? kGuideHidden : kGuideOutPad;
+            const int e = j - base, kg = e / (n_out * 8), rem = e % (n_out * 8);
+            const int n = (rem / 64) * 8 + (rem % 64) / 8, k = kg * 8 + rem % 8;
+            v = (src != kW3 || n < kGuideOut) ? params[src + n * n_in + k] : 0.0f;
+        }
+        else if (i < kBfFwd)
         {
             // Fragment order (see kBf0): locate layer, tile, lane, element.
             int base = i < kBf1 ? kBf0 : i < kBf2 ? kBf1 : i < kBf3 ? kBf2 : kBf3;
@@ -824,13 +1107,27 @@ __global__ void GuideConvertKernel(const float* params, __nv_bfloat16* w)
 
 // ---------------------------------------------------------------- launches
 
+// Grid of the persistent forward kernels: as many CTAs per SM as their shared
+// memory allows (at most the 4 of their launch bounds; 4 x 64 tensor-memory
+// columns fit in an SM's 512). The occupancy calculator is not used: for
+// these kernels it reports one CTA per SM.
+static int ForwardGrid()
+{
+    int dev = 0, smem_sm = 0, reserved = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    const int per = int(size_t(smem_sm) / (kFtSmem + size_t(reserved)));
+    return CurrentSmCount() * std::min(4, std::max(1, per));
+}
+
 bbg_status GuideForward(bbg_guide* G, const float* raw_dev, const int32_t* index_dev, const int32_t* n_dev,
                         int64_t n_host, float* out_dev, cudaStream_t st)
 {
     int grid = 0;
     BBG_TRY(GuidePrepare(G, &grid));
-    GuideForwardKernel<<<grid, 32 * kFwdWarps, kFwdSmem, st>>>(raw_dev, index_dev, n_dev, n_host, G->bounds,
-                                                                 G->bf16.p, G->params.p, out_dev);
+    GuideForwardKernel<<<grid, kFtThreads, kFtSmem, st>>>(raw_dev, index_dev, n_dev, n_host, G->bounds, G->bf16.p,
+                                                          G->params.p, out_dev, G->tc_status.p);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
 }
@@ -854,10 +1151,8 @@ bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, c
         if (!grid_of[dev])
         {
             BBG_CUDA(cudaFuncSetAttribute(GuideGroupedForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int(kFwdSmem)));
-            int per = 1;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideGroupedForwardKernel, 32 * kFwdWarps, kFwdSmem);
-            grid_of[dev] = CurrentSmCount() * std::max(per, 1);
+                                          int(kFtSmem)));
+            grid_of[dev] = ForwardGrid();
         }
         grid = grid_of[dev];
     }
@@ -865,7 +1160,7 @@ bbg_status GuideForwardGrouped(const float* raw_dev, const int32_t* index_dev, c
     {
         return BBG_OK;
     }
-    GuideGroupedForwardKernel<<<grid, 32 * kFwdWarps, kFwdSmem, st>>>(raw_dev, index_dev, chunk_start_dev, n_groups,
+    GuideGroupedForwardKernel<<<grid, kFtThreads, kFtSmem, st>>>(raw_dev, index_dev, chunk_start_dev, n_groups,
                                                                         groups_dev, out_dev);
     BBG_CUDA(cudaGetLastError());
     return BBG_OK;
@@ -914,7 +1209,7 @@ bbg_status GuideCheckStatus(bbg_guide* G)
     BBG_CUDA(cudaMemcpy(&st, G->tc_status.p, sizeof(st), cudaMemcpyDeviceToHost));
     if (st != 0)
     {
-        return Fail(BBG_ERR_TIMEOUT, "guide training: the tensor-core weight-gradient pass did not complete in time");
+        return Fail(BBG_ERR_TIMEOUT, "guide: a tensor-core pass (forward or weight gradients) did not complete in time");
     }
     return BBG_OK;
 }
@@ -923,15 +1218,13 @@ bbg_status GuidePrepare(bbg_guide* G, int* grid)
 {
     if (!G->smem_set)
     {
-        BBG_CUDA(cudaFuncSetAttribute(GuideForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFwdSmem)));
+        BBG_CUDA(cudaFuncSetAttribute(GuideForwardKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kFtSmem)));
         BBG_CUDA(cudaFuncSetAttribute(GuideTrainKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTrainSmem)));
         BBG_CUDA(cudaFuncSetAttribute(GuideWeightGradTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       int(kTcSmem)));
         G->smem_set = true;
     }
-    int per = 1;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, GuideForwardKernel, 32 * kFwdWarps, kFwdSmem);
-    *grid = CurrentSmCount() * std::max(per, 1);
+    *grid = ForwardGrid();
     return BBG_OK;
 }
 
@@ -994,7 +1287,7 @@ bbg_status Create(const float* aabb, uint64_t seed, bbg_guide* G)
     BBG_TRY(G->adam_v.upload(zeros.data(), zeros.size(), G->stream));
     BBG_TRY(G->grad.upload(zeros.data(), zeros.size(), G->stream));
     BBG_TRY(G->loss.alloc(1));
-    BBG_TRY(G->bf16.alloc(kBfAll));
+    BBG_TRY(G->bf16.alloc(kBfBuf));
     BBG_TRY(G->step_dev.alloc(1));
     BBG_CUDA(cudaMemsetAsync(G->step_dev.p, 0, sizeof(int32_t), G->stream));
     BBG_TRY(G->tc_status.alloc(1));

@@ -11,11 +11,11 @@ struct bbg_guide
     bbg::GuideBounds bounds{};
     bbg::DevBuf<float> params;  // FP32 master parameters (kGuideParams)
     bbg::DevBuf<float> adam_m, adam_v, grad, loss;
-    bbg::DevBuf<__nv_bfloat16> bf16; // kBfAll: forward + transposed weight images
+    bbg::DevBuf<__nv_bfloat16> bf16; // kBfBuf: training forward + transposed + tensor-core forward images
     bbg::DevBuf<int32_t> step_dev; // Adam step counter
     bbg::DevBuf<__nv_bfloat16> scratch; // training: transposed activations and gradients
     bbg::DevBuf<float> partial;         // training: per-chunk weight-gradient partial sums
-    bbg::DevBuf<int32_t> tc_status;     // nonzero: a tensor-core weight-gradient pass timed out
+    bbg::DevBuf<int32_t> tc_status;     // nonzero: a tensor-core pass (forward or weight gradients) timed out
     float beta1 = 0.9f, beta2 = 0.99f;
     bool smem_set = false;
     // Staging for host-buffer calls.
@@ -33,17 +33,19 @@ struct bbg_guide
 
 namespace bbg
 {
-// Queries per chunk of the grouped forward (its warps' 16-query tiles): each
-// group's queries start on a chunk boundary, so a chunk reads one group's
-// weights.
+// Queries per chunk of the grouped forward (one 128-query tensor-core tile):
+// each group's queries start on a chunk boundary, so a chunk reads one
+// group's weights.
 constexpr int kGuideGroupChunk = 128;
 
 // One group's guide as the grouped forward reads it (the device addresses
-// of its BF16 weight image and FP32 parameters, and its scene bounds).
+// of its BF16 weight images, FP32 parameters and time-out status, and its
+// scene bounds).
 struct GuideGroup
 {
     const __nv_bfloat16* wg;
     const float* pg;
+    int32_t* status;
     GuideBounds bounds;
 };
 
@@ -66,8 +68,8 @@ bbg_status GuideReserveTraining(bbg_guide* G, int64_t capacity);
 // capacity bounds n (n from n_dev if set) and sizes the training scratch.
 bbg_status GuideAccumulate(bbg_guide* G, const float* raw_dev, const float* dirs_dev, const float* weights_dev,
                            const int32_t* n_dev, int64_t n_host, int64_t capacity, cudaStream_t st);
-// BBG_ERR_TIMEOUT if a weight-gradient pass of this guide has given up
-// waiting for its tensor-core MMAs (synchronises with the device).
+// BBG_ERR_TIMEOUT if a forward or weight-gradient pass of this guide has
+// given up waiting for its tensor-core MMAs (synchronises with the device).
 bbg_status GuideCheckStatus(bbg_guide* G);
 // One Adam step with gradient = accumulator / n (n from n_dev if set); an
 // empty batch is skipped.

@@ -2526,7 +2526,7 @@ bbg_status Render(bbg_integrator* I, const bbg_camera* cam, const bbg_render_par
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (gc.guide && gc.dev.train)
+    if (gc.guide)
     {
         BBG_TRY(GuideCheckStatus(gc.guide));
     }
@@ -2924,7 +2924,7 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
                 BBG_TRY(GuideReserveTraining(G, batch));
             }
             B->guides[i] = G;
-            B->host_groups[i] = GuideGroup{ G->bf16.p, G->params.p, G->bounds };
+            B->host_groups[i] = GuideGroup{ G->bf16.p, G->params.p, G->tc_status.p, G->bounds };
         }
         BBG_TRY(B->groups.upload(B->host_groups.data(), B->host_groups.size(), st));
     }
@@ -3028,6 +3028,10 @@ bbg_status RenderBatch(bbg_batch* B, int32_t n, bbg_integrator* const* integrato
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    for (int32_t i = 0; p0->guide && i < n; ++i)
+    {
+        BBG_TRY(GuideCheckStatus(params[i].guide));
+    }
     if (mem == BBG_MEM_HOST)
     {
         for (int32_t i = 0; i < n; ++i)
