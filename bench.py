@@ -442,6 +442,27 @@ def run_pt(args, barrier, world):
             "bvh_build_s": round(split_build_s, 3), "launch_configuration": "the reference tree's tuned one"}
         integ.close()
         acc.close()
+        # The same budget with the references split and the tree built on the
+        # device (bbg_accel_create_device_split): build time (geometry upload
+        # included; a first build in the process loads the kernels) and frame.
+        torch.cuda.synchronize()
+        lib.GpuAccel(scene, device_sah=True, split=args.pt_split_report).close()
+        t0 = time.perf_counter()
+        acc = lib.GpuAccel(scene, device_sah=True, split=args.pt_split_report)
+        dsplit_build_s = time.perf_counter() - t0
+        _, dslots = acc.export()
+        integ = lib.GpuPathIntegrator(acc, scene)
+        integ.set_tuning(tuning.block, tuning.short_stack, tuning.wave_paths)
+        params.wave_paths = 0
+        ds_ms, ds_rays = timed()
+        ds_ms = max_over_ranks([ds_ms], device="cuda")[0]
+        out["device_split_tree"] = {
+            "budget": args.pt_split_report, "value": whole_job_rate(paths * steps, world, ds_ms), "unit": "paths/s",
+            "mrays_per_s": world * ds_rays / (ds_ms / 1e3) / 1e6, "ms_per_frame": ds_ms / steps,
+            "bvh_build_s": round(dsplit_build_s, 4), "references": int(len(dslots)),
+            "launch_configuration": "the reference tree's tuned one"}
+        integ.close()
+        acc.close()
     return out, scene
 
 

@@ -162,6 +162,7 @@ EXPORTS = [
     ("bbg_ggx_energy_tables", I32, [P, P]),
     ("bbg_dielectric_energy_tables", I32, [P, P, P, P]),
     ("bbg_accel_create_split", I32, [P, C.c_float, P]),
+    ("bbg_accel_create_device_split", I32, [P, C.c_float, P]),
     ("bbg_split_references", I32, [P, C.c_float, I32, P, P, P]),
     ("bbg_batch_create", I32, [P]),
     ("bbg_batch_destroy", I32, [P]),

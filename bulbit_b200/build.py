@@ -27,7 +27,7 @@ NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "--fmad=false", "-prec-div=true", "-pre
 CXX_FLAGS = ["-O2", "-std=c++20", "-fPIC", "-pthread", "-I" + INCLUDE, "-I" + CSRC,
              "-I" + os.path.join(CUDA_HOME, "include")]
 
-CU_SOURCES = ["accel.cu", "render.cu", "noalloc.cu", "guide.cu", "lbvh.cu", "sah_build.cu"]
+CU_SOURCES = ["accel.cu", "render.cu", "noalloc.cu", "guide.cu", "lbvh.cu", "sah_build.cu", "split_build.cu"]
 CXX_SOURCES = ["host_build.cpp"]
 
 

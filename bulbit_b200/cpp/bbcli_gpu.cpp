@@ -118,8 +118,9 @@ void PrintHelp()
         "  -b <max_bounces>          Maximum path bounces  (default: from scene)\n"
         "  -i <integrator>           Integrator by index; 0 (path tracing) is the one on the GPU\n"
         "  -r <image_scale>          Scale the output image resolution  (default: 1)\n"
-        "  --tree <reference|device|split>  GPU tree: the reference's SAH tree (default), a linear BVH\n"
-        "                            built on the GPU, or the SAH tree over split references\n"
+        "  --tree <reference|device|split|device-split>  GPU tree: the reference's SAH tree (default),\n"
+        "                            a linear BVH built on the GPU, or the SAH tree over split\n"
+        "                            references built on the host or on the GPU\n"
         "  --list-samples            List the built-in sample scenes\n"
         "  --help                    Show this help message\n\n");
 }
@@ -164,6 +165,7 @@ int main(int argc, const char* argv[])
             if (t == "reference") tree = bulbit_gpu::GpuTree::Reference;
             else if (t == "device") tree = bulbit_gpu::GpuTree::DeviceLinear;
             else if (t == "split") tree = bulbit_gpu::GpuTree::SplitReferences;
+            else if (t == "device-split") tree = bulbit_gpu::GpuTree::DeviceSplitReferences;
             else
             {
                 std::fprintf(stderr, "Error: unknown tree '%s'\n", t.c_str());

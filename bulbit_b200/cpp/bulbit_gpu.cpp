@@ -462,6 +462,10 @@ void GpuBVH::Upload(const bbg_bvh* tree, GpuTree kind, float split_budget)
     {
         Check(bbg_accel_create_device_sah(&g, &accel_), "bbg_accel_create_device_sah");
     }
+    else if (kind == GpuTree::DeviceSplitReferences)
+    {
+        Check(bbg_accel_create_device_split(&g, split_budget, &accel_), "bbg_accel_create_device_split");
+    }
     else
     {
         Check(bbg_accel_create_split(&g, split_budget, &accel_), "bbg_accel_create_split");

@@ -328,12 +328,14 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
 
 enum class DeviceTree
 {
-    None,   // the tree is given or built on the host
-    Linear, // linear BVH built on the device (lbvh.cu)
-    Sah     // the reference's SAH tree built on the device (sah_build.cu)
+    None,    // the tree is given or built on the host
+    Linear,  // linear BVH built on the device (lbvh.cu)
+    Sah,     // the reference's SAH tree built on the device (sah_build.cu)
+    SahSplit // the same build over references split on the device (split_build.cu)
 };
 
-bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, DeviceTree device_tree = DeviceTree::None)
+bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, DeviceTree device_tree = DeviceTree::None,
+                       float split_budget = 0)
 {
     const bool device_build = device_tree != DeviceTree::None;
     // Host-side checks and the tree come first: a malformed scene or tree is
@@ -365,7 +367,7 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     if (device_build)
     {
         a->device_built = device_tree == DeviceTree::Linear;
-        a->device_sah = device_tree == DeviceTree::Sah;
+        a->device_sah = device_tree == DeviceTree::Sah || device_tree == DeviceTree::SahSplit;
         a->ordered = true;
     }
     else if (bvh)
@@ -426,7 +428,22 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     if (device_build)
     {
         BBG_TRY(UploadShading(a, g));
-        BBG_TRY(device_tree == DeviceTree::Sah ? BuildSahOnDevice(a, g) : BuildLbvh(a, g));
+        if (device_tree == DeviceTree::SahSplit)
+        {
+            DevBuf<float4> ref_box;
+            DevBuf<int32_t> ref_prim;
+            int32_t n_refs = 0;
+            BBG_TRY(SplitReferencesOnDevice(a, split_budget, &ref_box, &ref_prim, &n_refs));
+            BBG_TRY(BuildSahOnDevice(a, n_refs, ref_box.p, ref_prim.p));
+        }
+        else if (device_tree == DeviceTree::Sah)
+        {
+            BBG_TRY(BuildSahOnDevice(a, g->n_prims, nullptr, nullptr));
+        }
+        else
+        {
+            BBG_TRY(BuildLbvh(a, g));
+        }
         BBG_TRY(a->counters.alloc(2));
         BBG_TRY(a->work.alloc(1));
         BBG_CUDA(cudaStreamSynchronize(a->stream));
@@ -649,6 +666,24 @@ bbg_status bbg_accel_create_device_sah(const bbg_geometry* geometry, bbg_accel**
     *out = nullptr;
     auto* a = new bbg_accel;
     bbg_status s = CreateAccel(geometry, nullptr, a, DeviceTree::Sah);
+    if (s != BBG_OK)
+    {
+        bbg_accel_destroy(a);
+        return s;
+    }
+    *out = a;
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_create_device_split(const bbg_geometry* geometry, float budget, bbg_accel** out)
+{
+    if (!out || !(budget >= 0.0f) || budget > 64.0f)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_create_device_split: bad argument (budget in [0, 64])");
+    }
+    *out = nullptr;
+    auto* a = new bbg_accel;
+    bbg_status s = CreateAccel(geometry, nullptr, a, DeviceTree::SahSplit, budget);
     if (s != BBG_OK)
     {
         bbg_accel_destroy(a);

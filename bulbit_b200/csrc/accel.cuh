@@ -83,11 +83,18 @@ bbg_status LaunchIntersectAny(bbg_accel* a, const float4* rays, int64_t n, uint8
 // Builds a linear BVH on the device (lbvh.cu) over the uploaded geometry:
 // fills slots, the child-box layout, leaves, root, bounds and depth.
 bbg_status BuildLbvh(bbg_accel* a, const bbg_geometry* g);
-// Builds the reference's binned SAH tree on the device (sah_build.cu) over the
-// uploaded geometry, node for node as BuildBvh does on the host: fills the
-// reference nodes, slots, the child-box layout, leaves, root, the 8-wide
-// layout, bounds, depth and the slot order.
-bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g);
+// Builds the reference's binned SAH tree on the device (sah_build.cu), node
+// for node as BuildBvh does on the host, over n items of the uploaded
+// geometry: its primitives (ref_box null) or references (boxes, two float4
+// corners each, and the primitive each one belongs to). Fills the reference
+// nodes, slots, the child-box layout, leaves, root, the 8-wide layout,
+// bounds, depth and the slot primitives.
+bbg_status BuildSahOnDevice(bbg_accel* a, int32_t n, const float4* ref_box, const int32_t* ref_prim);
+// References for a tree over split primitives (early split clipping), made
+// on the device: at most n_prims * (1 + budget) of them, their boxes and
+// primitives; *n_refs receives the count.
+bbg_status SplitReferencesOnDevice(bbg_accel* a, float budget, DevBuf<float4>* ref_box, DevBuf<int32_t>* ref_prim,
+                                   int32_t* n_refs);
 // Looks up (once per device, the current one) the device address of the
 // allocation-free query's fixed array, which also makes the array exist on
 // that device from this point until the process exits (noalloc.cu).

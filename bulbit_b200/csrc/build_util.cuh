@@ -40,6 +40,14 @@ __device__ __forceinline__ void PrimBox(const int2* prim_shape, const int32_t* t
     }
 }
 
+// Blocks for a grid-stride loop over items: enough for every item, at most 8
+// per SM.
+inline int GridFor(int64_t items, int block, int sms)
+{
+    const int64_t blocks = (items + block - 1) / block;
+    return int(blocks < 1 ? 1 : blocks < int64_t(sms) * 8 ? blocks : int64_t(sms) * 8);
+}
+
 // Order-preserving float <-> uint mapping for atomic min / max.
 __device__ __forceinline__ uint32_t FloatKey(float f)
 {

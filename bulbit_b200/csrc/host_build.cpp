@@ -7,6 +7,7 @@
 // without FMA contraction (x86-64 baseline ISA, no -ffast-math).
 
 #include "bbg_internal.h"
+#include "split_util.h"
 
 #include <algorithm>
 #include <cmath>
@@ -215,108 +216,6 @@ struct SplitRef
     int32_t prim;
 };
 
-// Sutherland-Hodgman against one axis-aligned half-space.
-int ClipAxis(const double (*in)[3], int n, int axis, double m, bool keep_below, double (*out)[3])
-{
-    int k = 0;
-    for (int i = 0; i < n; ++i)
-    {
-        const double* a = in[i];
-        const double* b = in[(i + 1) % n];
-        bool ia = keep_below ? a[axis] <= m : a[axis] >= m;
-        bool ib = keep_below ? b[axis] <= m : b[axis] >= m;
-        if (ia)
-        {
-            std::memcpy(out[k++], a, sizeof(double) * 3);
-        }
-        if (ia != ib)
-        {
-            double t = (m - a[axis]) / (b[axis] - a[axis]);
-            for (int c = 0; c < 3; ++c)
-            {
-                out[k][c] = a[c] + t * (b[c] - a[c]);
-            }
-            out[k][axis] = m;
-            ++k;
-        }
-    }
-    return k;
-}
-
-double PolygonArea(const double (*p)[3], int n)
-{
-    double c[3] = { 0, 0, 0 };
-    for (int i = 1; i + 1 < n; ++i)
-    {
-        double u[3], v[3];
-        for (int k = 0; k < 3; ++k)
-        {
-            u[k] = p[i][k] - p[0][k];
-            v[k] = p[i + 1][k] - p[0][k];
-        }
-        c[0] += u[1] * v[2] - u[2] * v[1];
-        c[1] += u[2] * v[0] - u[0] * v[2];
-        c[2] += u[0] * v[1] - u[1] * v[0];
-    }
-    return 0.5 * std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]);
-}
-
-// Box (and area) of the triangle clipped to [lo, hi]; false if nothing is left.
-bool ClippedBox(const double tri[3][3], const double lo[3], const double hi[3], double out_lo[3], double out_hi[3],
-                double* area)
-{
-    double a[12][3], b[12][3];
-    int n = 3;
-    std::memcpy(a, tri, sizeof(double) * 9);
-    for (int axis = 0; axis < 3 && n > 0; ++axis)
-    {
-        n = ClipAxis(a, n, axis, lo[axis], false, b);
-        n = ClipAxis(b, n, axis, hi[axis], true, a);
-    }
-    if (n == 0)
-    {
-        return false;
-    }
-    *area = PolygonArea(a, n);
-    for (int c = 0; c < 3; ++c)
-    {
-        out_lo[c] = out_hi[c] = a[0][c];
-    }
-    for (int i = 1; i < n; ++i)
-    {
-        for (int c = 0; c < 3; ++c)
-        {
-            out_lo[c] = std::min(out_lo[c], a[i][c]);
-            out_hi[c] = std::max(out_hi[c], a[i][c]);
-        }
-    }
-    // The clipped polygon lies inside the box it was clipped to.
-    for (int c = 0; c < 3; ++c)
-    {
-        out_lo[c] = std::max(out_lo[c], lo[c]);
-        out_hi[c] = std::min(out_hi[c], hi[c]);
-    }
-    return true;
-}
-
-double BoxArea(const double lo[3], const double hi[3])
-{
-    double d0 = hi[0] - lo[0], d1 = hi[1] - lo[1], d2 = hi[2] - lo[2];
-    return 2 * (d0 * d1 + d1 * d2 + d2 * d0);
-}
-
-float RoundDown(double v)
-{
-    float f = float(v);
-    return double(f) > v ? std::nextafter(f, -std::numeric_limits<float>::infinity()) : f;
-}
-
-float RoundUp(double v)
-{
-    float f = float(v);
-    return double(f) < v ? std::nextafter(f, std::numeric_limits<float>::infinity()) : f;
-}
-
 } // namespace
 
 bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<float>* ref_aabbs,
@@ -352,7 +251,7 @@ bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<floa
                 r.lo[c] = std::min(std::min(tri[0][c], tri[1][c]), tri[2][c]);
                 r.hi[c] = std::max(std::max(tri[0][c], tri[1][c]), tri[2][c]);
             }
-            heap.emplace_back(BoxArea(r.lo, r.hi) - 2 * PolygonArea(tri, 3), int32_t(refs.size()));
+            heap.emplace_back(split::BoxArea(r.lo, r.hi) - 2 * split::PolygonArea(tri, 3), int32_t(refs.size()));
         }
         refs.push_back(r);
     }
@@ -363,14 +262,7 @@ bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<floa
         int32_t ri = heap.back().second;
         heap.pop_back();
         SplitRef r = refs[size_t(ri)];
-        int axis = 0;
-        for (int c = 1; c < 3; ++c)
-        {
-            if (r.hi[c] - r.lo[c] > r.hi[axis] - r.lo[axis])
-            {
-                axis = c;
-            }
-        }
+        const int axis = split::LongestAxis(r.lo, r.hi);
         const double m = 0.5 * (r.lo[axis] + r.hi[axis]);
         if (!(m > r.lo[axis] && m < r.hi[axis]))
         {
@@ -395,16 +287,16 @@ bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<floa
         SplitRef left{}, right{};
         left.prim = right.prim = r.prim;
         double al = 0, ar = 0;
-        bool hl = ClippedBox(tri, llo, lhi, left.lo, left.hi, &al);
-        bool hr = ClippedBox(tri, rlo, rhi, right.lo, right.hi, &ar);
+        bool hl = split::ClippedBox(tri, llo, lhi, left.lo, left.hi, &al);
+        bool hr = split::ClippedBox(tri, rlo, rhi, right.lo, right.hi, &ar);
         if (!hl || !hr)
         {
             continue; // the box was not tight on this axis: keep the reference whole
         }
         refs[size_t(ri)] = left;
-        heap.emplace_back(BoxArea(left.lo, left.hi) - 2 * al, ri);
+        heap.emplace_back(split::BoxArea(left.lo, left.hi) - 2 * al, ri);
         std::push_heap(heap.begin(), heap.end());
-        heap.emplace_back(BoxArea(right.lo, right.hi) - 2 * ar, int32_t(refs.size()));
+        heap.emplace_back(split::BoxArea(right.lo, right.hi) - 2 * ar, int32_t(refs.size()));
         std::push_heap(heap.begin(), heap.end());
         refs.push_back(right);
     }
@@ -424,8 +316,8 @@ bbg_status SplitReferences(const bbg_geometry& g, float budget, std::vector<floa
         }
         for (int c = 0; c < 3; ++c)
         {
-            box[c] = RoundDown(r.lo[c]) - pad;
-            box[3 + c] = RoundUp(r.hi[c]) + pad;
+            box[c] = split::RoundDown(r.lo[c]) - pad;
+            box[3 + c] = split::RoundUp(r.hi[c]) + pad;
         }
     }
     return BBG_OK;

@@ -734,12 +734,65 @@ __global__ void SahFlattenKernel(SahDev S, const uint32_t* leaves_before, int32_
 }
 
 // Slot records in leaf order (slot j holds primitive idx[j]).
-__global__ void SahSlotsKernel(const int32_t* idx, const int2* prim_shape, const int32_t* tri, const float* pos,
+// As SahPrimsKernel, over given boxes (references: box[2 r], box[2 r + 1]
+// are reference r's min and max corners).
+__global__ void SahRefsKernel(const float4* ref_box, int32_t n, float4* box, float4* cen, int32_t* idx,
+                              uint32_t* root_keys)
+{
+    uint32_t k[kKeys];
+    for (int q = 0; q < kKeys; ++q)
+    {
+        k[q] = (q % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
+    }
+    for (int32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    {
+        const float4 lo = ref_box[2 * size_t(i)], hi = ref_box[2 * size_t(i) + 1];
+        box[2 * size_t(i)] = make_float4(lo.x, lo.y, lo.z, 0);
+        box[2 * size_t(i) + 1] = make_float4(hi.x, hi.y, hi.z, 0);
+        const float4 c = make_float4((lo.x + hi.x) * 0.5f, (lo.y + hi.y) * 0.5f, (lo.z + hi.z) * 0.5f, 0);
+        cen[i] = c;
+        idx[i] = i;
+        const uint32_t v[kKeys] = { FloatKey(lo.x), FloatKey(lo.y), FloatKey(lo.z), FloatKey(hi.x),
+                                    FloatKey(hi.y), FloatKey(hi.z), FloatKey(c.x),  FloatKey(c.y),
+                                    FloatKey(c.z),  FloatKey(c.x),  FloatKey(c.y),  FloatKey(c.z) };
+        for (int q = 0; q < kKeys; ++q)
+        {
+            k[q] = (q % 6) >= 3 ? max(k[q], v[q]) : min(k[q], v[q]);
+        }
+    }
+    for (int q = 0; q < kKeys; ++q)
+    {
+        const uint32_t r = (q % 6) >= 3 ? __reduce_max_sync(0xffffffffu, k[q]) : __reduce_min_sync(0xffffffffu, k[q]);
+        if ((threadIdx.x & 31) == 0)
+        {
+            if ((q % 6) >= 3)
+            {
+                atomicMax(&root_keys[q], r);
+            }
+            else
+            {
+                atomicMin(&root_keys[q], r);
+            }
+        }
+    }
+}
+
+// Primitive of each slot: the build's item order, through the reference map
+// when the build ran over references.
+__global__ void SahSlotPrimsKernel(const int32_t* idx, const int32_t* ref_prim, int32_t n, int32_t* slot_prims)
+{
+    for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    {
+        slot_prims[j] = ref_prim ? ref_prim[idx[j]] : idx[j];
+    }
+}
+
+__global__ void SahSlotsKernel(const int32_t* slot_prims, const int2* prim_shape, const int32_t* tri, const float* pos,
                                const bbg_sphere* spheres, int32_t n, float4* slots)
 {
     for (int32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
     {
-        const int32_t prim = idx[j];
+        const int32_t prim = slot_prims[j];
         const int2 ps = prim_shape[prim];
         float4* r = slots + 3 * size_t(j);
         if (ps.x == BBG_PRIM_TRIANGLE)
@@ -892,11 +945,6 @@ __global__ void SahWide8WriteKernel(const bbg_bvh_node* nd, int32_t* w2b, int32_
     }
 }
 
-int GridFor(int64_t items, int block, int sms)
-{
-    return int(std::max<int64_t>(1, std::min<int64_t>((items + block - 1) / block, int64_t(sms) * 8)));
-}
-
 // The 8-wide collapse of the depth-first node array on the device, level by
 // level (the host reads each level's size back). Leaves the layout unbuilt if
 // a leaf cannot be encoded or the tree exceeds the layout's limits, as the
@@ -958,9 +1006,8 @@ bbg_status SahWide8(bbg_accel* a, const bbg_bvh_node* nd, int32_t n_nodes, int s
 
 } // namespace
 
-bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
+bbg_status BuildSahOnDevice(bbg_accel* a, int32_t n, const float4* ref_box, const int32_t* ref_prim)
 {
-    const int32_t n = g->n_prims;
     cudaStream_t st = a->stream;
     const int sms = CurrentSmCount();
     const int64_t max_nodes = 2 * int64_t(n) - 1;
@@ -1024,8 +1071,15 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
         init_keys[q] = (q % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
     }
     BBG_CUDA(cudaMemcpyAsync(root_keys, init_keys, sizeof(init_keys), cudaMemcpyHostToDevice, st));
-    SahPrimsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(a->prim_shape.p, a->tri_indices.p, a->positions.p,
-                                                         a->spheres.p, n, box, cen, idx, root_keys);
+    if (ref_box)
+    {
+        SahRefsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(ref_box, n, box, cen, idx, root_keys);
+    }
+    else
+    {
+        SahPrimsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(a->prim_shape.p, a->tri_indices.p, a->positions.p,
+                                                             a->spheres.p, n, box, cen, idx, root_keys);
+    }
     SahDev S{ box, cen, idx, scr_l, scr_r, leaf_at, bounds, info, path, counters };
     SahRootKernel<<<1, 1, 0, st>>>(S, root_keys, n);
     const int32_t init_counters[4] = { 1, 0, 0, 0 };
@@ -1094,9 +1148,12 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
     {
         return Fail(BBG_ERR_BAD_BVH, "device SAH build: inconsistent tree (%d nodes, %u leaves)", n_nodes, n_leaves);
     }
+    // The primitive of every slot stays on the device (slot records, export).
+    BBG_TRY(a->slot_prims.alloc(size_t(n)));
+    SahSlotPrimsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(idx, ref_prim, n, a->slot_prims.p);
     BBG_TRY(a->slots.alloc(3 * size_t(n)));
-    SahSlotsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(idx, a->prim_shape.p, a->tri_indices.p, a->positions.p,
-                                                         a->spheres.p, n, a->slots.p);
+    SahSlotsKernel<<<GridFor(n, 256, sms), 256, 0, st>>>(a->slot_prims.p, a->prim_shape.p, a->tri_indices.p,
+                                                         a->positions.p, a->spheres.p, n, a->slots.p);
     const int32_t n_interior = n_nodes - int32_t(n_leaves);
     BBG_TRY(a->wide.alloc(4 * size_t(std::max(n_interior, 1))));
     SahChildBoxKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(nd, ref, n_nodes, a->wide.p);
@@ -1105,9 +1162,6 @@ bbg_status BuildSahOnDevice(bbg_accel* a, const bbg_geometry* g)
     BBG_CUDA(cudaMemcpyAsync(&root_ref, ref, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     bbg_bvh_node root_node;
     BBG_CUDA(cudaMemcpyAsync(&root_node, nd, sizeof(root_node), cudaMemcpyDeviceToHost, st));
-    // The slot order stays on the device for export.
-    BBG_TRY(a->slot_prims.alloc(size_t(n)));
-    BBG_CUDA(cudaMemcpyAsync(a->slot_prims.p, idx, sizeof(int32_t) * size_t(n), cudaMemcpyDeviceToDevice, st));
     BBG_CUDA(cudaStreamSynchronize(st));
     a->root = root_ref;
     a->n_nodes = n_nodes;

@@ -98,10 +98,15 @@ class GpuAccel:
         """bvh: the reference's tree (nodes, slots); device_build: the linear BVH
         built on the device; device_sah: the reference's SAH tree built on the
         device (bbg_accel_create_device_sah); split: extra references per
-        primitive for the split-reference SAH build (bbg_accel_create_split)."""
+        primitive for the split-reference SAH build (bbg_accel_create_split,
+        or bbg_accel_create_device_split with device_sah)."""
         self.scene = scene
         self._g = scene.geometry()
         self.h = C.c_void_p()
+        if device_sah and split is not None:
+            check(get_lib().bbg_accel_create_device_split(C.byref(self._g), float(split), C.byref(self.h)),
+                  "bbg_accel_create_device_split")
+            return
         if device_sah:
             check(get_lib().bbg_accel_create_device_sah(C.byref(self._g), C.byref(self.h)),
                   "bbg_accel_create_device_sah")

@@ -211,6 +211,19 @@ bbg_status bbg_accel_create_device_build(const bbg_geometry* geometry, bbg_accel
  * bbg_accel_export work as for a host-built tree (export copies the tree
  * from the device). */
 bbg_status bbg_accel_create_device_sah(const bbg_geometry* geometry, bbg_accel** out);
+
+/* bbg_accel_create_split built on the device: the references are split on
+ * the device (early split clipping with the host splitter's clipping, area
+ * and rounding rules, in rounds that each split every reference whose wasted
+ * box area lies in the highest occupied power-of-two bin, where the host
+ * splits the single largest one at a time; right halves appended in
+ * reference order, so the result is deterministic), then the device SAH build
+ * of bbg_accel_create_device_sah runs over them. budget in [0, 64]; 0 gives
+ * bbg_accel_create_device_sah's tree. The reference set, and so the tree,
+ * differs from the host splitter's; closest hits agree with BVH::Intersect
+ * except between primitives hit at exactly the same t. No counterpart in the
+ * reference renderer. */
+bbg_status bbg_accel_create_device_split(const bbg_geometry* geometry, float budget, bbg_accel** out);
 bbg_status bbg_accel_destroy(bbg_accel* accel);
 
 /* Root AABB (6 floats), as BVH::GetAABB (src/accel/bvh.cpp:363). */

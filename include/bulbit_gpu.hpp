@@ -64,14 +64,17 @@ namespace bulbit_gpu
 // host. DeviceSah: that same tree, node for node, built on the GPU in
 // milliseconds. DeviceLinear: a linear BVH built on the GPU. SplitReferences:
 // the SAH build over split triangle references (faster traversal of long or
-// diagonal triangles, a longer build). The last two change only which of two
+// diagonal triangles, a host build of seconds). DeviceSplitReferences: split
+// references and the SAH build over them, both on the GPU (a fraction of a
+// second on millions of triangles). The last three change only which of two
 // hits at exactly the same t is returned.
 enum class GpuTree
 {
     Reference,
     DeviceLinear,
     SplitReferences,
-    DeviceSah
+    DeviceSah,
+    DeviceSplitReferences
 };
 
 class GpuBVH : public bulbit::Intersectable
@@ -82,7 +85,7 @@ public:
     // A tree built by the library from the primitives, in the order given
     // (primitive index = position): by default the same SAH tree as
     // BVH::BVH (bbg_bvh_build); split_budget = extra references per
-    // primitive for GpuTree::SplitReferences.
+    // primitive for GpuTree::SplitReferences and DeviceSplitReferences.
     explicit GpuBVH(const std::vector<bulbit::Primitive*>& primitives, GpuTree tree = GpuTree::Reference,
                     float split_budget = 3.0f);
     ~GpuBVH() override;

@@ -305,11 +305,14 @@ int main()
             bulbit_gpu::GpuBVH gpu_dev(scene.GetPrimitives(), bulbit_gpu::GpuTree::DeviceLinear);
             // The reference's SAH tree built on the GPU: identical records to BVH.
             bulbit_gpu::GpuBVH gpu_dev_sah(scene.GetPrimitives(), bulbit_gpu::GpuTree::DeviceSah);
+            // Split references and their SAH tree, both built on the GPU.
+            bulbit_gpu::GpuBVH gpu_dev_split(scene.GetPrimitives(), bulbit_gpu::GpuTree::DeviceSplitReferences, 2.0f);
             CompareQueries(bvh, gpu, Point3(0, 1.2f, 0), 2.5f, &r, "mesh");
             CompareQueries(bvh, gpu_own, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_own_tree");
             CompareQueries(bvh, gpu_split, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_split_tree");
             CompareQueries(bvh, gpu_dev, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_device_tree");
             CompareQueries(bvh, gpu_dev_sah, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_device_sah_tree");
+            CompareQueries(bvh, gpu_dev_split, Point3(0, 1.2f, 0), 2.5f, &r, "mesh_device_split_tree");
             // The camera's default filter (GaussianFilter) and a stratified sampler.
             GaussianFilter filter;
             Point3 eye(0.0f, 1.5f, 5.0f), at(0.0f, 1.2f, 0.0f);
