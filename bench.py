@@ -640,6 +640,26 @@ def run_batch(args):
     k = int(np.argmin([s.n_prims for s in sc]))
     alone = integs[k].render(spp=32, seed=0)
     exact = bool(np.array_equal(alone.rgb_sum, films[k].rgb_sum) and np.array_equal(alone.count, films[k].count))
+    # The same batch over split-reference trees built on the device (budget
+    # 3; hits equal the reference trees' except exact ties): the 16 builds'
+    # time (after one warm-up build that loads the kernels) and the batch.
+    lib.GpuAccel(sc[k], device_sah=True, split=3.0).close()
+    t0 = time.perf_counter()
+    saccs = [lib.GpuAccel(s, device_sah=True, split=3.0) for s in sc]
+    split_build_s = time.perf_counter() - t0
+    sintegs = [lib.GpuPathIntegrator(a, s) for a, s in zip(saccs, sc)]
+    sb = lib.GpuBatch()
+    sbt = sb.autotune(sintegs, spp=32, seeds=[0] * 16)
+    sb.render(sintegs, spp=32, seeds=[0] * 16)  # capture
+    _, sst = sb.render(sintegs, spp=32, seeds=[0] * 16)
+    split_batch = {"budget": 3.0, "value": sst.paths / (sst.device_ms / 1e3), "unit": "paths/s",
+                   "batch_ms": sst.device_ms, "mrays_per_s": (sst.closest_rays + sst.shadow_rays) / sst.device_ms / 1e3,
+                   "bvh_build_s": round(split_build_s, 2),
+                   "tuning": {"block": sbt.block, "short_stack": sbt.short_stack, "wave_paths": sbt.wave_paths}}
+    sb.close()
+    for it, a in zip(sintegs, saccs):
+        it.close()
+        a.close()
     # Guided vs plain in the batch, every scene at 96x96 (so that the 4096-spp
     # plain references stay cheap): the plain batch, then the batch with one
     # guide per scene (grouped forward per level, each guide trained online
@@ -677,7 +697,8 @@ def run_batch(args):
         "batch_default_config_ms": st_default.device_ms,
         "tuning": {"batch": {"block": bt.block, "short_stack": bt.short_stack, "wave_paths": bt.wave_paths},
                    "batch_autotune_s": round(tune_batch_s, 2), "per_scene_autotune_s": round(tune_alone_s, 2)},
-        "batch_film_equals_alone": exact, "per_scene": per_scene, "guided_batch": guided_batch,
+        "batch_film_equals_alone": exact, "device_split_trees": split_batch, "per_scene": per_scene,
+        "guided_batch": guided_batch,
         "config": {"workload": "16 uneven Cornell-box variants (seeds 0-15), 32 spp, 12 bounces, one batch",
                    "total_triangles": int(sum(s.n_prims for s in sc)), "paths": st.paths,
                    "scene_generation_s": round(gen_s, 2), "bvh_build_s": round(build_s, 2)},
