@@ -670,6 +670,16 @@ def run_batch(args):
     refs = [it.render(spp=4096, seed=7).image() for it in integs]
     b.render(integs, spp=32, seeds=[1] * 16)  # capture
     pfilms, pst = b.render(integs, spp=32, seeds=[2] * 16)
+    # At this size a scene alone (294,912 paths) leaves the GPU part-idle, so
+    # the batch is timed against the scenes rendered one after another too
+    # (same launch configuration).
+    alone96_ms = 0.0
+    for it in integs:
+        it.render(spp=32, seed=2)  # capture
+        alone96_ms += it.render(spp=32, seed=2).stats.device_ms
+    small_scenes = {"config": "the 16 scenes at 96x96, 32 spp, 12 bounces", "paths": pst.paths,
+                    "batch_ms": pst.device_ms, "sequential_ms": alone96_ms,
+                    "speedup_vs_sequential": alone96_ms / pst.device_ms}
     guides = [lib.GpuGuide(a.bounds(), seed=5) for a in accs]
     gfilms, gst = b.render(integs, spp=32, seeds=[3] * 16, guides=guides, train=True, wave_paths=1 << 22, steps=4)
     time_ratio = gst.device_ms / pst.device_ms
@@ -697,7 +707,8 @@ def run_batch(args):
         "batch_default_config_ms": st_default.device_ms,
         "tuning": {"batch": {"block": bt.block, "short_stack": bt.short_stack, "wave_paths": bt.wave_paths},
                    "batch_autotune_s": round(tune_batch_s, 2), "per_scene_autotune_s": round(tune_alone_s, 2)},
-        "batch_film_equals_alone": exact, "device_split_trees": split_batch, "per_scene": per_scene,
+        "batch_film_equals_alone": exact, "device_split_trees": split_batch, "small_scenes": small_scenes,
+        "per_scene": per_scene,
         "guided_batch": guided_batch,
         "config": {"workload": "16 uneven Cornell-box variants (seeds 0-15), 32 spp, 12 bounces, one batch",
                    "total_triangles": int(sum(s.n_prims for s in sc)), "paths": st.paths,
