@@ -566,22 +566,30 @@ def run_guided_sweep(args):
     acc = lib.GpuAccel(scene)
     integ = lib.GpuPathIntegrator(acc, scene)
     ref = integ.render(spp=16384, seed=7).image()
-    integ.render(spp=64, seed=1)  # graph capture
-    plain = [integ.render(spp=64, seed=2 + k) for k in range(3)]
+    # Plain renders in waves of 2^24 paths (one wave per frame at 512^2 and
+    # 64 spp: the fewest bounce-level ramp-downs).
+    big = 1 << 24
+    integ.render(spp=64, seed=1, wave_paths=big)  # graph capture
+    plain = [integ.render(spp=64, seed=2 + k, wave_paths=big) for k in range(3)]
     e_plain = float(np.mean([rel_mse(f.image(), ref) for f in plain]))
     t_plain = float(np.mean([f.stats.device_ms for f in plain]))
     rows = []
-    grid = [(sel, pre, 1e-2, 8) for sel in (0.1, 0.25, 0.5) for pre in (0, 10, 40)]
-    grid += [(0.25, 10, 3e-3, 8), (0.25, 10, 1e-2, 32)]
-    for sel, pre, lr, steps in grid:
+    grid = [(sel, pre, 1e-2, 8, wave) for sel in (0.1, 0.25, 0.5) for pre in (0, 10, 40)]
+    grid += [(0.25, 10, 3e-3, 8, wave), (0.25, 10, 1e-2, 32, wave)]
+    # A pretrained guide needs no small waves to learn within the frame: the
+    # same renders in waves of 2^24 paths (as the plain renders use), so the
+    # guided frame has as many bounce levels, and ramp-downs, as the plain one.
+    grid += [(0.1, 10, 1e-2, 8, big), (0.1, 40, 1e-2, 8, big), (0.1, 40, 1e-2, 32, big), (0.25, 40, 1e-2, 8, big)]
+    for sel, pre, lr, steps, wave_paths in grid:
         g = lib.GpuGuide(acc.bounds(), seed=11)
-        kw = dict(guide=g, train=True, wave_paths=wave, steps=steps, lr=lr, select=sel)
+        kw = dict(guide=g, train=True, wave_paths=wave_paths, steps=steps, lr=lr, select=sel)
         for k in range(pre):
             integ.render(spp=64, seed=1000 + k, **kw)
         films = [integ.render(spp=64, seed=2000 + k, **kw) for k in range(3)]
         e = float(np.mean([rel_mse(f.image(), ref) for f in films]))
         t = float(np.mean([f.stats.device_ms for f in films]))
-        rows.append({"select": sel, "pretrain_frames": pre, "lr": lr, "adam_steps_per_wave": steps, "relMSE": e,
+        rows.append({"select": sel, "pretrain_frames": pre, "lr": lr, "adam_steps_per_wave": steps,
+                     "wave_paths": wave_paths, "relMSE": e,
                      "device_ms": t, "relMSE_ratio": e / e_plain, "time_ratio": t / t_plain,
                      "equal_time_ratio": e * t / (e_plain * t_plain)})
         g.close()
@@ -589,7 +597,7 @@ def run_guided_sweep(args):
     acc.close()
     best = min(rows, key=lambda r: r["equal_time_ratio"])
     return {"metric": "relMSE at equal time, guided / plain (sweep)", "best": best, "rows": rows,
-            "plain": {"spp": 64, "relMSE": e_plain, "device_ms": t_plain},
+            "plain": {"spp": 64, "relMSE": e_plain, "device_ms": t_plain, "wave_paths": big},
             "config": {"workload": f"Cornell box + displaced gold icosphere (1,310,720 triangles) at {res}x{res}, "
                                    "16 bounces, 64 spp per render, relMSE against a 16384-spp plain render",
                        "wave_paths": wave, "guide_batch": 1 << 16}}
