@@ -255,6 +255,171 @@ __device__ __forceinline__ bool SplitAxis(const float4* bd, int32_t count, int32
     return *extent != 0;
 }
 
+// Bins positions [lo, hi) of a node's range (block-wide; every thread of the
+// block calls it): counts and the min / max keys of the boxes and centres in
+// each bucket, merged into s_cnt / s_key (initialised by the caller).
+__device__ __forceinline__ void BinRange(const SahDev& S, int32_t start, int32_t lo, int32_t hi, int32_t axis,
+                                         float cmin, float extent, int32_t* s_cnt, uint32_t (*s_key)[kKeys])
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    int32_t my_cnt = 0;
+    uint32_t my_key[kKeys];
+    for (int k = 0; k < kKeys; ++k)
+    {
+        my_key[k] = (k % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
+    }
+    for (int32_t base = lo; base < hi; base += kSahBlock)
+    {
+        const int32_t i = base + tid;
+        int32_t b = -1;
+        uint32_t key[kKeys];
+        if (i < hi)
+        {
+            const int32_t p = S.idx[start + i];
+            const float4 c = S.cen[p], blo = S.box[2 * size_t(p)], bhi = S.box[2 * size_t(p) + 1];
+            b = BucketOf(Axis(c, axis), cmin, extent);
+            key[0] = FloatKey(blo.x), key[1] = FloatKey(blo.y), key[2] = FloatKey(blo.z);
+            key[3] = FloatKey(bhi.x), key[4] = FloatKey(bhi.y), key[5] = FloatKey(bhi.z);
+            key[6] = FloatKey(c.x), key[7] = FloatKey(c.y), key[8] = FloatKey(c.z);
+            key[9] = key[6], key[10] = key[7], key[11] = key[8];
+        }
+        for (int32_t k = 0; k < kBuckets; ++k)
+        {
+            const unsigned m = __ballot_sync(0xffffffffu, b == k);
+            if (m == 0)
+            {
+                continue;
+            }
+            const bool in = b == k;
+            if (lane == k)
+            {
+                my_cnt += __popc(m);
+            }
+            for (int q = 0; q < kKeys; ++q)
+            {
+                const bool is_max = (q % 6) >= 3;
+                const uint32_t v = in ? key[q] : (is_max ? EmptyMaxKey() : EmptyMinKey());
+                const uint32_t r = is_max ? __reduce_max_sync(0xffffffffu, v) : __reduce_min_sync(0xffffffffu, v);
+                if (lane == k)
+                {
+                    my_key[q] = is_max ? max(my_key[q], r) : min(my_key[q], r);
+                }
+            }
+        }
+    }
+    if (lane < kBuckets && my_cnt > 0)
+    {
+        atomicAdd(&s_cnt[lane], my_cnt);
+        for (int q = 0; q < kKeys; ++q)
+        {
+            if ((q % 6) >= 3)
+            {
+                atomicMax(&s_key[lane][q], my_key[q]);
+            }
+            else
+            {
+                atomicMin(&s_key[lane][q], my_key[q]);
+            }
+        }
+    }
+}
+
+// Whether position i of a node's range holds a primitive on the wrong side of
+// the split: before mid and belonging right, or from mid on and belonging left.
+__device__ __forceinline__ bool Misplaced(const SahDev& S, int32_t start, int32_t i, int32_t mid, int32_t split,
+                                          int32_t axis, float cmin, float extent)
+{
+    const float4 c = S.cen[S.idx[start + i]];
+    const bool left = BucketOf(Axis(c, axis), cmin, extent) <= split;
+    return i < mid ? !left : left;
+}
+
+// Partition ranks over positions [lo, hi) of a node's range (block-wide):
+// every misplaced position before mid goes to scr_l, every one from mid on to
+// scr_r, each at its rank among the node's misplaced positions of its side
+// (*carry_l / *carry_r: those ranked before lo on entry, before hi on return).
+__device__ __forceinline__ void RankRange(const SahDev& S, int32_t start, int32_t lo, int32_t hi, int32_t mid,
+                                          int32_t split, int32_t axis, float cmin, float extent, int32_t* carry_l,
+                                          int32_t* carry_r, int32_t (*s_scan)[kSahBlock / 32], int32_t* s_total)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int kWarps = kSahBlock / 32;
+    for (int32_t tile = lo; tile < hi; tile += kSahTile)
+    {
+        const int32_t first = tile + tid * kSahPerThread;
+        uint32_t move = 0; // bit j: element first + j moves
+        int32_t nl = 0, nr = 0;
+#pragma unroll
+        for (int j = 0; j < kSahPerThread; ++j)
+        {
+            const int32_t i = first + j;
+            if (i < hi && Misplaced(S, start, i, mid, split, axis, cmin, extent))
+            {
+                move |= 1u << j;
+                if (i < mid)
+                {
+                    ++nl;
+                }
+                else
+                {
+                    ++nr;
+                }
+            }
+        }
+        // Block-wide exclusive prefix of nl and nr.
+        int32_t xl = nl, xr = nr;
+        for (int off = 1; off < 32; off <<= 1)
+        {
+            const int32_t yl = __shfl_up_sync(0xffffffffu, xl, off);
+            const int32_t yr = __shfl_up_sync(0xffffffffu, xr, off);
+            if (lane >= off)
+            {
+                xl += yl;
+                xr += yr;
+            }
+        }
+        if (lane == 31)
+        {
+            s_scan[0][warp] = xl;
+            s_scan[1][warp] = xr;
+        }
+        __syncthreads();
+        if (tid < 2)
+        {
+            int32_t run = 0;
+            for (int w = 0; w < kWarps; ++w)
+            {
+                const int32_t v = s_scan[tid][w];
+                s_scan[tid][w] = run;
+                run += v;
+            }
+            s_total[tid] = run;
+        }
+        __syncthreads();
+        int32_t rl = *carry_l + s_scan[0][warp] + xl - nl;
+        int32_t rr = *carry_r + s_scan[1][warp] + xr - nr;
+#pragma unroll
+        for (int j = 0; j < kSahPerThread; ++j)
+        {
+            if (move & (1u << j))
+            {
+                const int32_t i = first + j;
+                if (i < mid)
+                {
+                    S.scr_l[start + rl++] = i;
+                }
+                else
+                {
+                    S.scr_r[start + rr++] = i;
+                }
+            }
+        }
+        *carry_l += s_total[0];
+        *carry_r += s_total[1];
+        __syncthreads(); // s_scan / s_total are rewritten by the next tile
+    }
+}
+
 // One node per block (nodes of more than 32 primitives).
 __global__ void __launch_bounds__(kSahBlock) SahBlockKernel(SahDev S, const int32_t* tasks, int32_t n_tasks,
                                                             int32_t* next_big, int32_t* next_small)
@@ -265,8 +430,7 @@ __global__ void __launch_bounds__(kSahBlock) SahBlockKernel(SahDev S, const int3
     __shared__ uint32_t s_child[2][kKeys]; // children's bounds
     __shared__ int32_t s_scan[2][kSahBlock / 32];
     __shared__ int32_t s_total[2];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int kWarps = kSahBlock / 32;
+    const int tid = threadIdx.x;
 
     for (int32_t t = blockIdx.x; t < n_tasks; t += gridDim.x)
     {
@@ -300,66 +464,7 @@ __global__ void __launch_bounds__(kSahBlock) SahBlockKernel(SahDev S, const int3
             }
         }
         __syncthreads();
-        int32_t my_cnt = 0;
-        uint32_t my_key[kKeys];
-        for (int k = 0; k < kKeys; ++k)
-        {
-            my_key[k] = (k % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
-        }
-        for (int32_t base = 0; base < count; base += kSahBlock)
-        {
-            const int32_t i = base + tid;
-            int32_t b = -1;
-            uint32_t key[kKeys];
-            if (i < count)
-            {
-                const int32_t p = S.idx[start + i];
-                const float4 c = S.cen[p], lo = S.box[2 * size_t(p)], hi = S.box[2 * size_t(p) + 1];
-                b = BucketOf(Axis(c, axis), cmin, extent);
-                key[0] = FloatKey(lo.x), key[1] = FloatKey(lo.y), key[2] = FloatKey(lo.z);
-                key[3] = FloatKey(hi.x), key[4] = FloatKey(hi.y), key[5] = FloatKey(hi.z);
-                key[6] = FloatKey(c.x), key[7] = FloatKey(c.y), key[8] = FloatKey(c.z);
-                key[9] = key[6], key[10] = key[7], key[11] = key[8];
-            }
-            for (int32_t k = 0; k < kBuckets; ++k)
-            {
-                const unsigned m = __ballot_sync(0xffffffffu, b == k);
-                if (m == 0)
-                {
-                    continue;
-                }
-                const bool in = b == k;
-                if (lane == k)
-                {
-                    my_cnt += __popc(m);
-                }
-                for (int q = 0; q < kKeys; ++q)
-                {
-                    const bool is_max = (q % 6) >= 3;
-                    const uint32_t v = in ? key[q] : (is_max ? EmptyMaxKey() : EmptyMinKey());
-                    const uint32_t r = is_max ? __reduce_max_sync(0xffffffffu, v) : __reduce_min_sync(0xffffffffu, v);
-                    if (lane == k)
-                    {
-                        my_key[q] = is_max ? max(my_key[q], r) : min(my_key[q], r);
-                    }
-                }
-            }
-        }
-        if (lane < kBuckets && my_cnt > 0)
-        {
-            atomicAdd(&s_cnt[lane], my_cnt);
-            for (int q = 0; q < kKeys; ++q)
-            {
-                if ((q % 6) >= 3)
-                {
-                    atomicMax(&s_key[lane][q], my_key[q]);
-                }
-                else
-                {
-                    atomicMin(&s_key[lane][q], my_key[q]);
-                }
-            }
-        }
+        BinRange(S, start, 0, count, axis, cmin, extent, s_cnt, s_key);
         __syncthreads();
         if (tid == 0)
         {
@@ -384,83 +489,7 @@ __global__ void __launch_bounds__(kSahBlock) SahBlockKernel(SahDev S, const int3
         // order) pair with positions from mid on whose primitive belongs
         // left (in reverse order); each pair swaps.
         int32_t carry_l = 0, carry_r = 0;
-        for (int32_t tile = 0; tile < count; tile += kSahTile)
-        {
-            const int32_t first = tile + tid * kSahPerThread;
-            uint32_t move = 0; // bit j: element first + j moves
-            int32_t nl = 0, nr = 0;
-#pragma unroll
-            for (int j = 0; j < kSahPerThread; ++j)
-            {
-                const int32_t i = first + j;
-                if (i < count)
-                {
-                    const float4 c = S.cen[S.idx[start + i]];
-                    const bool left = BucketOf(Axis(c, axis), cmin, extent) <= split;
-                    if (i < mid && !left)
-                    {
-                        move |= 1u << j;
-                        ++nl;
-                    }
-                    else if (i >= mid && left)
-                    {
-                        move |= 1u << j;
-                        ++nr;
-                    }
-                }
-            }
-            // Block-wide exclusive prefix of nl and nr.
-            int32_t xl = nl, xr = nr;
-            for (int off = 1; off < 32; off <<= 1)
-            {
-                const int32_t yl = __shfl_up_sync(0xffffffffu, xl, off);
-                const int32_t yr = __shfl_up_sync(0xffffffffu, xr, off);
-                if (lane >= off)
-                {
-                    xl += yl;
-                    xr += yr;
-                }
-            }
-            if (lane == 31)
-            {
-                s_scan[0][warp] = xl;
-                s_scan[1][warp] = xr;
-            }
-            __syncthreads();
-            if (tid < 2)
-            {
-                int32_t run = 0;
-                for (int w = 0; w < kWarps; ++w)
-                {
-                    const int32_t v = s_scan[tid][w];
-                    s_scan[tid][w] = run;
-                    run += v;
-                }
-                s_total[tid] = run;
-            }
-            __syncthreads();
-            int32_t rl = carry_l + s_scan[0][warp] + xl - nl;
-            int32_t rr = carry_r + s_scan[1][warp] + xr - nr;
-#pragma unroll
-            for (int j = 0; j < kSahPerThread; ++j)
-            {
-                if (move & (1u << j))
-                {
-                    const int32_t i = first + j;
-                    if (i < mid)
-                    {
-                        S.scr_l[start + rl++] = i;
-                    }
-                    else
-                    {
-                        S.scr_r[start + rr++] = i;
-                    }
-                }
-            }
-            carry_l += s_total[0];
-            carry_r += s_total[1];
-            __syncthreads(); // s_scan / s_total are rewritten by the next tile
-        }
+        RankRange(S, start, 0, count, mid, split, axis, cmin, extent, &carry_l, &carry_r, s_scan, s_total);
         // carry_l == carry_r: the pairs. The k-th from the left meets the
         // k-th from the right.
         const int32_t pairs = carry_l;
@@ -479,6 +508,246 @@ __global__ void __launch_bounds__(kSahBlock) SahBlockKernel(SahDev S, const int3
             StoreBounds(S.bounds + 4 * size_t(id + 1), s_child[1]);
         }
         __syncthreads(); // shared state is reused by the next node
+    }
+}
+
+// Levels with few large nodes (the top of the tree, where one block per node
+// leaves most SMs idle): each node is spread over up to kWideMaxChunks blocks,
+// each taking a contiguous chunk of the node's range. The bins merge into the
+// node's global buckets by the same commutative atomics the block kernel's
+// warps use, the decision is ChooseSplit on them, and the partition ranks are
+// each chunk's ranks plus the misplaced counts of the chunks before it, so
+// the node comes out exactly as the block kernel makes it.
+constexpr int kWideMaxTasks = 256;
+constexpr int kWideMaxChunks = 1024;
+
+struct SahWide
+{
+    int32_t* cnt;  // [task][bucket]
+    uint32_t* key; // [task][bucket][kKeys]
+    int4* dec;     // [task]: split bucket (-1: leaf), left count, axis
+    float2* geo;   // [task]: centre min and extent along the axis
+    int32_t* nl;   // [task][chunk]: misplaced positions before mid; exclusive offsets after the scan
+    int32_t* nr;   // [task][chunk]: misplaced positions from mid on; likewise
+    int32_t* pairs; // [task]: swaps
+};
+
+// The range [lo, hi) of the node's count that chunk b of n takes.
+__device__ __forceinline__ void ChunkOf(int32_t count, int32_t b, int32_t n, int32_t* lo, int32_t* hi)
+{
+    const int32_t chunk = (count + n - 1) / n;
+    *lo = min(count, b * chunk);
+    *hi = min(count, *lo + chunk);
+}
+
+__global__ void SahWideInitKernel(SahWide W)
+{
+    const int32_t t = blockIdx.x;
+    for (int i = threadIdx.x; i < kBuckets * kKeys; i += blockDim.x)
+    {
+        W.key[size_t(t) * kBuckets * kKeys + i] = ((i % kKeys) % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
+    }
+    for (int i = threadIdx.x; i < kBuckets; i += blockDim.x)
+    {
+        W.cnt[t * kBuckets + i] = 0;
+    }
+}
+
+__global__ void __launch_bounds__(kSahBlock) SahWideBinKernel(SahDev S, SahWide W, const int32_t* tasks)
+{
+    __shared__ int32_t s_cnt[kBuckets];
+    __shared__ uint32_t s_key[kBuckets][kKeys];
+    const int32_t t = blockIdx.y, node = tasks[t];
+    const int4 inf = S.info[node];
+    const int32_t start = inf.x, count = inf.y;
+    float4 bd[4];
+    for (int k = 0; k < 4; ++k)
+    {
+        bd[k] = S.bounds[4 * size_t(node) + k];
+    }
+    int32_t axis = 0, lo = 0, hi = 0;
+    float extent = 0, area = 0;
+    ChunkOf(count, blockIdx.x, gridDim.x, &lo, &hi);
+    if (!SplitAxis(bd, count, &axis, &extent, &area) || lo >= hi)
+    {
+        return; // a leaf (the decide kernel emits it) or an empty chunk
+    }
+    const int tid = threadIdx.x;
+    if (tid < kBuckets)
+    {
+        s_cnt[tid] = 0;
+        for (int k = 0; k < kKeys; ++k)
+        {
+            s_key[tid][k] = (k % 6) >= 3 ? EmptyMaxKey() : EmptyMinKey();
+        }
+    }
+    __syncthreads();
+    BinRange(S, start, lo, hi, axis, Axis(bd[2], axis), extent, s_cnt, s_key);
+    __syncthreads();
+    if (tid < kBuckets && s_cnt[tid] > 0)
+    {
+        atomicAdd(&W.cnt[t * kBuckets + tid], s_cnt[tid]);
+        uint32_t* k = W.key + (size_t(t) * kBuckets + tid) * kKeys;
+        for (int q = 0; q < kKeys; ++q)
+        {
+            if ((q % 6) >= 3)
+            {
+                atomicMax(&k[q], s_key[tid][q]);
+            }
+            else
+            {
+                atomicMin(&k[q], s_key[tid][q]);
+            }
+        }
+    }
+}
+
+// One thread per node: the leaf tests and ChooseSplit, then the leaf or the
+// two children (their ranges and bounds are known before the partition).
+__global__ void SahWideDecideKernel(SahDev S, SahWide W, const int32_t* tasks, int32_t n_tasks, int32_t* next_big,
+                                    int32_t* next_small)
+{
+    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tasks)
+    {
+        return;
+    }
+    const int32_t node = tasks[t];
+    const int4 inf = S.info[node];
+    const int32_t start = inf.x, count = inf.y;
+    float4 bd[4];
+    for (int k = 0; k < 4; ++k)
+    {
+        bd[k] = S.bounds[4 * size_t(node) + k];
+    }
+    int32_t axis = 0, mid = 0;
+    float extent = 0, area = 0;
+    int32_t split = -1;
+    uint32_t lk[kKeys], rk[kKeys];
+    if (SplitAxis(bd, count, &axis, &extent, &area))
+    {
+        split = ChooseSplit(W.cnt + t * kBuckets,
+                            reinterpret_cast<const uint32_t(*)[kKeys]>(W.key + size_t(t) * kBuckets * kKeys), count,
+                            area, &mid, lk, rk);
+    }
+    W.dec[t] = make_int4(split, mid, axis, 0);
+    W.geo[t] = make_float2(Axis(bd[2], axis), extent);
+    if (split < 0)
+    {
+        EmitLeaf(S, node, start, count);
+        return;
+    }
+    const int32_t id = EmitChildren(S, node, start, count, mid, axis, next_big, next_small);
+    StoreBounds(S.bounds + 4 * size_t(id), lk);
+    StoreBounds(S.bounds + 4 * size_t(id + 1), rk);
+}
+
+__global__ void __launch_bounds__(kSahBlock) SahWideCountKernel(SahDev S, SahWide W, const int32_t* tasks)
+{
+    __shared__ int32_t s_n[2];
+    const int32_t t = blockIdx.y, node = tasks[t];
+    const int4 dec = W.dec[t];
+    const int32_t slot = t * kWideMaxChunks + blockIdx.x;
+    if (dec.x < 0)
+    {
+        return;
+    }
+    const int4 inf = S.info[node];
+    const int32_t start = inf.x, count = inf.y;
+    const float2 geo = W.geo[t];
+    int32_t lo = 0, hi = 0;
+    ChunkOf(count, blockIdx.x, gridDim.x, &lo, &hi);
+    if (threadIdx.x < 2)
+    {
+        s_n[threadIdx.x] = 0;
+    }
+    __syncthreads();
+    int32_t nl = 0, nr = 0;
+    for (int32_t i = lo + threadIdx.x; i < hi; i += blockDim.x)
+    {
+        if (Misplaced(S, start, i, dec.y, dec.x, dec.z, geo.x, geo.y))
+        {
+            if (i < dec.y)
+            {
+                ++nl;
+            }
+            else
+            {
+                ++nr;
+            }
+        }
+    }
+    nl = __reduce_add_sync(0xffffffffu, nl);
+    nr = __reduce_add_sync(0xffffffffu, nr);
+    if ((threadIdx.x & 31) == 0)
+    {
+        atomicAdd(&s_n[0], nl);
+        atomicAdd(&s_n[1], nr);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        W.nl[slot] = s_n[0];
+        W.nr[slot] = s_n[1];
+    }
+}
+
+// One thread per node: the chunks' counts become exclusive offsets.
+__global__ void SahWideOffsetsKernel(SahWide W, int32_t n_tasks, int32_t n_chunks)
+{
+    const int32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_tasks || W.dec[t].x < 0)
+    {
+        return;
+    }
+    int32_t* nl = W.nl + t * kWideMaxChunks;
+    int32_t* nr = W.nr + t * kWideMaxChunks;
+    int32_t rl = 0, rr = 0;
+    for (int32_t b = 0; b < n_chunks; ++b)
+    {
+        const int32_t vl = nl[b], vr = nr[b];
+        nl[b] = rl;
+        nr[b] = rr;
+        rl += vl;
+        rr += vr;
+    }
+    W.pairs[t] = rl; // == rr
+}
+
+__global__ void __launch_bounds__(kSahBlock) SahWideRankKernel(SahDev S, SahWide W, const int32_t* tasks)
+{
+    __shared__ int32_t s_scan[2][kSahBlock / 32];
+    __shared__ int32_t s_total[2];
+    const int32_t t = blockIdx.y, node = tasks[t];
+    const int4 dec = W.dec[t];
+    if (dec.x < 0)
+    {
+        return;
+    }
+    const int4 inf = S.info[node];
+    const int32_t start = inf.x, count = inf.y;
+    const float2 geo = W.geo[t];
+    int32_t lo = 0, hi = 0;
+    ChunkOf(count, blockIdx.x, gridDim.x, &lo, &hi);
+    int32_t carry_l = W.nl[t * kWideMaxChunks + blockIdx.x], carry_r = W.nr[t * kWideMaxChunks + blockIdx.x];
+    RankRange(S, start, lo, hi, dec.y, dec.x, dec.z, geo.x, geo.y, &carry_l, &carry_r, s_scan, s_total);
+}
+
+__global__ void __launch_bounds__(kSahBlock) SahWideSwapKernel(SahDev S, SahWide W, const int32_t* tasks)
+{
+    const int32_t t = blockIdx.y, node = tasks[t];
+    if (W.dec[t].x < 0)
+    {
+        return;
+    }
+    const int32_t start = S.info[node].x, pairs = W.pairs[t];
+    for (int32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < pairs; k += gridDim.x * blockDim.x)
+    {
+        const int32_t a = start + S.scr_l[start + k];
+        const int32_t b = start + S.scr_r[start + pairs - 1 - k];
+        const int32_t pa = S.idx[a], pb = S.idx[b];
+        S.idx[a] = pb;
+        S.idx[b] = pa;
     }
 }
 
@@ -1029,6 +1298,7 @@ bbg_status BuildSahOnDevice(bbg_accel* a, int32_t n, const float4* ref_box, cons
     uint32_t *leaf_at = nullptr, *leaves_before = nullptr, *root_keys = nullptr;
     int4* info = nullptr;
     int2* path = nullptr;
+    SahWide W{};
     const size_t un = size_t(n), un1 = size_t(n) + 1, nodes = size_t(max_nodes);
     const Piece pieces[] = {
         { reinterpret_cast<void**>(&box), 2 * un * sizeof(float4) },
@@ -1048,6 +1318,13 @@ bbg_status BuildSahOnDevice(bbg_accel* a, int32_t n, const float4* ref_box, cons
         { reinterpret_cast<void**>(&lists[1]), un * sizeof(int32_t) },
         { reinterpret_cast<void**>(&lists[2]), un * sizeof(int32_t) },
         { reinterpret_cast<void**>(&lists[3]), un * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&W.cnt), size_t(kWideMaxTasks) * kBuckets * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&W.key), size_t(kWideMaxTasks) * kBuckets * kKeys * sizeof(uint32_t) },
+        { reinterpret_cast<void**>(&W.dec), size_t(kWideMaxTasks) * sizeof(int4) },
+        { reinterpret_cast<void**>(&W.geo), size_t(kWideMaxTasks) * sizeof(float2) },
+        { reinterpret_cast<void**>(&W.nl), size_t(kWideMaxTasks) * kWideMaxChunks * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&W.nr), size_t(kWideMaxTasks) * kWideMaxChunks * sizeof(int32_t) },
+        { reinterpret_cast<void**>(&W.pairs), size_t(kWideMaxTasks) * sizeof(int32_t) },
     };
     size_t total = 0;
     for (const Piece& pc : pieces)
@@ -1103,7 +1380,20 @@ bbg_status BuildSahOnDevice(bbg_accel* a, int32_t n, const float4* ref_box, cons
         int32_t* small_cur = lists[2 + cur];
         int32_t* small_next = lists[3 - cur];
         BBG_CUDA(cudaMemsetAsync(counters + 1, 0, 2 * sizeof(int32_t), st));
-        if (n_big > 0)
+        if (n_big > 0 && n_big <= kWideMaxTasks)
+        {
+            // Few large nodes: about four blocks per SM over them all.
+            const int32_t chunks = std::min(kWideMaxChunks, std::max(1, (4 * sms + n_big - 1) / n_big));
+            const dim3 grid{ static_cast<unsigned>(chunks), static_cast<unsigned>(n_big), 1u };
+            SahWideInitKernel<<<n_big, 256, 0, st>>>(W);
+            SahWideBinKernel<<<grid, kSahBlock, 0, st>>>(S, W, big_cur);
+            SahWideDecideKernel<<<(n_big + 63) / 64, 64, 0, st>>>(S, W, big_cur, n_big, big_next, small_next);
+            SahWideCountKernel<<<grid, kSahBlock, 0, st>>>(S, W, big_cur);
+            SahWideOffsetsKernel<<<(n_big + 63) / 64, 64, 0, st>>>(W, n_big, chunks);
+            SahWideRankKernel<<<grid, kSahBlock, 0, st>>>(S, W, big_cur);
+            SahWideSwapKernel<<<grid, kSahBlock, 0, st>>>(S, W, big_cur);
+        }
+        else if (n_big > 0)
         {
             SahBlockKernel<<<std::min(n_big, 8 * sms), kSahBlock, 0, st>>>(S, big_cur, n_big, big_next, small_next);
         }
