@@ -552,10 +552,21 @@ int Int(const Value& o, const char* key, int def)
     return v.IsNumber() ? v.GetNumberAsInt() : def;
 }
 
+// A byte count or offset; a negative one keeps the default, one beyond 2^53
+// (or NaN) reads as SIZE_MAX, which every range check rejects.
 size_t Size(const Value& o, const char* key, size_t def)
 {
     const Value& v = o.Get(key);
-    return (v.IsNumber() && v.GetNumberAsDouble() >= 0) ? size_t(v.GetNumberAsDouble()) : def;
+    if (!v.IsNumber())
+    {
+        return def;
+    }
+    const double d = v.GetNumberAsDouble();
+    if (d < 0)
+    {
+        return def;
+    }
+    return d <= 9007199254740992.0 ? size_t(d) : std::numeric_limits<size_t>::max();
 }
 
 double Num(const Value& o, const char* key, double def)
@@ -719,9 +730,9 @@ bool TinyGLTF::Load(Model* model, std::string* err, std::string* warn, const cha
         buf.name = Str(b, "name");
         buf.uri = Str(b, "uri");
         const double declared = Num(b, "byteLength", -1);
-        if (declared < 0)
+        if (!(declared >= 0 && declared <= 9007199254740992.0))
         {
-            return fail("buffer " + std::to_string(i) + ": byteLength is missing");
+            return fail("buffer " + std::to_string(i) + ": byteLength is missing or out of range");
         }
         const size_t length = size_t(declared);
         if (buf.uri.empty())

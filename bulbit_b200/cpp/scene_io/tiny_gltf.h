@@ -131,7 +131,16 @@ public:
     bool IsObject() const { return type_ == OBJECT_TYPE; }
 
     double GetNumberAsDouble() const { return type_ == INT_TYPE ? double(int_value_) : real_value_; }
-    int GetNumberAsInt() const { return type_ == REAL_TYPE ? int(real_value_) : int_value_; }
+    // A real outside the int range (or NaN) reads as INT_MIN, which no
+    // index or count accepts.
+    int GetNumberAsInt() const
+    {
+        if (type_ != REAL_TYPE)
+        {
+            return int_value_;
+        }
+        return (real_value_ >= -2147483648.0 && real_value_ <= 2147483647.0) ? int(real_value_) : (-2147483647 - 1);
+    }
 
     // Array element / object member, or a shared null Value.
     const Value& Get(int idx) const;

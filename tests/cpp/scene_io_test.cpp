@@ -533,6 +533,8 @@ void GltfImagesAndErrors()
     CHECK(fails(TriangleJson(""), "no uri"));
     CHECK(fails(TriangleJson(",\"uri\":\"missing.bin\""), "cannot read"));
     CHECK(fails("{\"asset\":{\"version\":\"2.0\"},\"nodes\":[{\"mesh\":0}]}", "node 0"));
+    CHECK(fails("{\"asset\":{\"version\":\"2.0\"},\"nodes\":[{\"mesh\":1e10}]}", "node 0"));
+    CHECK(fails("{\"asset\":{\"version\":\"2.0\"},\"buffers\":[{\"byteLength\":1e300}]}", "byteLength"));
     CHECK(fails("{\"asset\":{}}", "asset.version"));
     CHECK(fails("{\"asset\":{\"version\":\"2.0\"},}", "JSON error"));
     CHECK(fails("{\"asset\":{\"version\":\"2.0\"}} x", "JSON error"));
