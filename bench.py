@@ -322,7 +322,10 @@ def run_pt(args, barrier, world):
     res = args.pt_res
     scene = scenes.cornell_icosphere(levels=8, width=res, height=res, spp=64, max_bounces=16)
     t0 = time.perf_counter()
-    acc = lib.GpuAccel(scene, split=args.pt_split)
+    if args.pt_device_split is not None:
+        acc = lib.GpuAccel(scene, device_sah=True, split=args.pt_device_split)
+    else:
+        acc = lib.GpuAccel(scene, split=args.pt_split)
     build_s = time.perf_counter() - t0
     if args.traversal != "default":
         acc.set_traversal(abi.BBG_TRAVERSAL_WIDE if args.traversal == "wide" else abi.BBG_TRAVERSAL_ORDERED)
@@ -387,6 +390,10 @@ def run_pt(args, barrier, world):
         "steps": steps, "closest_rays_per_frame": stats.closest_rays, "shadow_rays_per_frame": stats.shadow_rays,
         "default_config_ms_per_frame": default_ms / steps,
         "config": {"workload": PT_WORKLOAD if res == 1024 else f"{PT_WORKLOAD} (reduced to {res}x{res})",
+                   "tree": ("split references built on the device, budget %g" % args.pt_device_split
+                            if args.pt_device_split is not None else
+                            "split references, budget %g" % args.pt_split if args.pt_split is not None else
+                            "the reference's SAH tree"),
                    "bvh_build_s": round(build_s, 3), "default_wave_paths": args.pt_wave,
                    "tuned": {"block": tuning.block, "short_stack": tuning.short_stack,
                              "wave_paths": tuning.wave_paths, "autotune_s": round(tune_s, 2)},
@@ -776,6 +783,8 @@ def main():
     ap.add_argument("--pt-res", type=int, default=1024)
     ap.add_argument("--pt-split", type=float, default=None,
                     help="path tracing: build the tree over split references with this budget per primitive")
+    ap.add_argument("--pt-device-split", type=float, default=None,
+                    help="path tracing: the same, with the references split and the tree built on the device")
     ap.add_argument("--shade-order", default="sorted", choices=["sorted", "queue"],
                     help="path tracing: shade each level grouped by material kind, or in queue order")
     ap.add_argument("--pt-split-report", type=float, default=3.0,
