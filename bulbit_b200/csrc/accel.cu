@@ -534,24 +534,46 @@ bbg_status CreateAccel(const bbg_geometry* g, const bbg_bvh* bvh, bbg_accel* a, 
     return BBG_OK;
 }
 
-constexpr int64_t kChunkRays = int64_t(1) << 22;
+constexpr int64_t kChunkRays = int64_t(1) << 21;
+
+// Waits for every query queued on the accel's streams; errors of submitted
+// queries surface here.
+bbg_status Drain(bbg_accel* a)
+{
+    a->pending = false;
+    BBG_CUDA(cudaStreamSynchronize(a->copy_stream[0]));
+    BBG_CUDA(cudaStreamSynchronize(a->stream));
+    BBG_CUDA(cudaStreamSynchronize(a->copy_stream[1]));
+    return BBG_OK;
+}
 
 // Host-memory query: chunks of rays staged through two streams so the copies
-// of one chunk overlap the traversal of the other.
+// of one chunk overlap the traversal of the other. With wait false the call
+// returns once everything is queued.
 template <bool ANY>
-bbg_status TraceHost(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out)
+bbg_status TraceHost(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out, bool wait)
 {
     // Chunks cycle through the staging ring: the copy in of chunk k + 1 and
     // the copy out of chunk k - 1 overlap the trace of chunk k. Chunk sizes
-    // grow from 256K rays to 4M and shrink again towards the end (at most
+    // grow from 256K rays to 2M and shrink again towards the end (at most
     // half of what is left), so the first copy in and the last copy out,
     // which nothing overlaps, are short. All traces run in order on one
     // stream (the persistent kernel's work counter is per accel); a slot is
-    // refilled only after its trace and its copy out finished.
+    // refilled only after its trace and its copy out finished, whichever
+    // call (an earlier submitted one included) used it last.
     constexpr int R = bbg_accel::kHostStages;
     constexpr int64_t kFirstChunk = int64_t(1) << 18;
     const size_t out_bytes = ANY ? 1 : sizeof(bbg_hit);
     const int64_t chunk = std::min(n, kChunkRays);
+    bool grow = false;
+    for (int s = 0; s < R; ++s)
+    {
+        grow |= a->stage_in[s].n < 2 * size_t(chunk) || a->stage_out[s].n < (size_t(chunk) * out_bytes + 15) / 16;
+    }
+    if (grow && a->pending)
+    {
+        BBG_TRY(Drain(a)); // a larger slot frees the old one, which queued work may still use
+    }
     for (int s = 0; s < R; ++s)
     {
         BBG_TRY(a->stage_in[s].alloc(2 * size_t(chunk)));
@@ -560,22 +582,18 @@ bbg_status TraceHost(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out)
     cudaStream_t cin = a->copy_stream[0], cout = a->copy_stream[1], comp = a->stream;
     for (int64_t c = 0, k = 0, m = 0; c < n; c += m, ++k)
     {
-        const int s = int(k % R);
+        const int s = a->stage_next;
+        a->stage_next = (s + 1) % R;
         const int64_t left = n - c;
         const int64_t ramp_up = kFirstChunk << std::min<int64_t>(k, 4);
         const int64_t ramp_down = std::max(left / 2, kFirstChunk);
         m = std::min({ chunk, ramp_up, ramp_down, left });
-        if (k >= R)
-        {
-            BBG_CUDA(cudaStreamWaitEvent(cin, a->ev_traced[s], 0));
-        }
+        // Waiting on an event that was never recorded is no wait.
+        BBG_CUDA(cudaStreamWaitEvent(cin, a->ev_traced[s], 0));
         BBG_CUDA(cudaMemcpyAsync(a->stage_in[s].p, rays + c, size_t(m) * sizeof(bbg_ray), cudaMemcpyHostToDevice, cin));
         BBG_CUDA(cudaEventRecord(a->ev_in[s], cin));
         BBG_CUDA(cudaStreamWaitEvent(comp, a->ev_in[s], 0));
-        if (k >= R)
-        {
-            BBG_CUDA(cudaStreamWaitEvent(comp, a->ev_out[s], 0));
-        }
+        BBG_CUDA(cudaStreamWaitEvent(comp, a->ev_out[s], 0));
         if (ANY)
         {
             BBG_TRY(LaunchIntersectAny(a, a->stage_in[s].p, m, reinterpret_cast<uint8_t*>(a->stage_out[s].p), comp));
@@ -590,26 +608,57 @@ bbg_status TraceHost(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out)
                                  size_t(m) * out_bytes, cudaMemcpyDeviceToHost, cout));
         BBG_CUDA(cudaEventRecord(a->ev_out[s], cout));
     }
-    BBG_CUDA(cudaStreamSynchronize(cout));
-    BBG_CUDA(cudaStreamSynchronize(comp));
-    BBG_CUDA(cudaStreamSynchronize(cin));
-    return BBG_OK;
+    return wait ? Drain(a) : BBG_OK;
 }
 
+// One batched query. wait false (the submit forms) queues the work on the
+// accel's streams and returns; wait true returns with the results in place,
+// after any submitted work (the work counter and the staging ring are the
+// accel's own, so queries on it never overlap).
 template <bool ANY>
-bbg_status Query(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out, bbg_memory mem, void* stream)
+bbg_status Query(bbg_accel* a, const bbg_ray* rays, int64_t n, void* out, bbg_memory mem, void* stream,
+                 bool wait = true)
 {
     if (!a || (n > 0 && (!rays || !out)) || n < 0 || (mem != BBG_MEM_HOST && mem != BBG_MEM_DEVICE))
     {
         return Fail(BBG_ERR_INVALID_ARG, "intersect: bad argument");
     }
+    if (!wait && a->counting)
+    {
+        return Fail(BBG_ERR_UNSUPPORTED, "a counting accel answers only the synchronous queries");
+    }
+    if (wait && a->pending)
+    {
+        BBG_TRY(Drain(a));
+    }
+    if (n == 0)
+    {
+        a->last_nodes = a->last_prims = 0;
+        return BBG_OK;
+    }
     if (a->counting)
     {
         BBG_CUDA(cudaMemset(a->counters.p, 0, 2 * sizeof(unsigned long long)));
     }
+    if (!wait)
+    {
+        a->pending = true;
+    }
     if (mem == BBG_MEM_HOST)
     {
-        BBG_TRY(TraceHost<ANY>(a, rays, n, out));
+        BBG_TRY(TraceHost<ANY>(a, rays, n, out, wait));
+    }
+    else if (!wait)
+    {
+        const float4* r = reinterpret_cast<const float4*>(rays);
+        if (ANY)
+        {
+            BBG_TRY(LaunchIntersectAny(a, r, n, static_cast<uint8_t*>(out), a->stream));
+        }
+        else
+        {
+            BBG_TRY(LaunchIntersect(a, r, n, static_cast<float4*>(out), a->stream));
+        }
     }
     else
     {
@@ -835,6 +884,36 @@ bbg_status bbg_intersect_any(bbg_accel* a, const bbg_ray* rays, int64_t n, uint8
     }
     DeviceScope ds(a->device);
     return Query<true>(a, rays, n, occluded, mem, stream);
+}
+
+bbg_status bbg_intersect_submit(bbg_accel* a, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem)
+{
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "intersect: null accel");
+    }
+    DeviceScope ds(a->device);
+    return Query<false>(a, rays, n, hits, mem, nullptr, false);
+}
+
+bbg_status bbg_intersect_any_submit(bbg_accel* a, const bbg_ray* rays, int64_t n, uint8_t* occluded, bbg_memory mem)
+{
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "intersect: null accel");
+    }
+    DeviceScope ds(a->device);
+    return Query<true>(a, rays, n, occluded, mem, nullptr, false);
+}
+
+bbg_status bbg_accel_synchronize(bbg_accel* a)
+{
+    if (!a)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_synchronize: null accel");
+    }
+    DeviceScope ds(a->device);
+    return Drain(a);
 }
 
 bbg_status bbg_accel_set_traversal(bbg_accel* a, int32_t mode)

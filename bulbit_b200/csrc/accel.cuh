@@ -53,14 +53,21 @@ struct bbg_accel
 
     // Staging for host-memory calls: a ring of kHostStages slots; rays go in
     // on copy_stream[0], the kernels run on `stream`, results come back on
-    // copy_stream[1], ordered by per-slot events.
-    static constexpr int kHostStages = 3;
+    // copy_stream[1], ordered by per-slot events. The ring position carries
+    // over from call to call, so submitted queries chain through it. Twelve
+    // slots of up to 2M rays let the copy in run eleven chunks ahead of the
+    // traversal, also where the chunks are short (a batch's ramp down and the
+    // next one's ramp up): through a closest-hit batch, whose traversal is
+    // slower than its copy, into the next batch's rays.
+    static constexpr int kHostStages = 12;
     bbg::DevBuf<float4> stage_in[kHostStages];
     bbg::DevBuf<float4> stage_out[kHostStages];
     cudaStream_t copy_stream[2] = { nullptr, nullptr };
     cudaEvent_t ev_in[kHostStages] = {};     // slot's rays copied in
     cudaEvent_t ev_traced[kHostStages] = {}; // slot's rays traced (stage_in free)
     cudaEvent_t ev_out[kHostStages] = {};    // slot's results copied out (stage_out free)
+    int stage_next = 0;                      // ring slot of the next chunk
+    bool pending = false;                    // submitted queries not yet synchronised
 
     // Traversal counters (nodes, prims) of the last call when enabled.
     bool counting = false;

@@ -202,6 +202,26 @@ class GpuAccel:
         check(get_lib().bbg_intersect_any(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(occ_ptr), abi.BBG_MEM_HOST,
                                           None), "bbg_intersect_any")
 
+    def submit_host_ptr(self, rays_ptr, n, hits_ptr):
+        """bbg_intersect_submit over host buffers: returns once queued."""
+        check(get_lib().bbg_intersect_submit(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(hits_ptr),
+                                             abi.BBG_MEM_HOST), "bbg_intersect_submit")
+
+    def submit_any_host_ptr(self, rays_ptr, n, occ_ptr):
+        check(get_lib().bbg_intersect_any_submit(self.h, C.c_void_p(rays_ptr), n, C.c_void_p(occ_ptr),
+                                                 abi.BBG_MEM_HOST), "bbg_intersect_any_submit")
+
+    def submit_device(self, rays_t, hits_t):
+        check(get_lib().bbg_intersect_submit(self.h, _dev_ptr(rays_t), rays_t.shape[0], _dev_ptr(hits_t),
+                                             abi.BBG_MEM_DEVICE), "bbg_intersect_submit")
+
+    def submit_any_device(self, rays_t, occ_t):
+        check(get_lib().bbg_intersect_any_submit(self.h, _dev_ptr(rays_t), rays_t.shape[0], _dev_ptr(occ_t),
+                                                 abi.BBG_MEM_DEVICE), "bbg_intersect_any_submit")
+
+    def synchronize(self):
+        check(get_lib().bbg_accel_synchronize(self.h), "bbg_accel_synchronize")
+
 
 def sampler_draws(px, py, seed, sample, n):
     out = np.zeros(n, np.float32)

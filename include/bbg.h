@@ -235,7 +235,9 @@ bbg_status bbg_accel_export(const bbg_accel* accel, bbg_bvh_node* nodes_out, int
 
 /* Batched BVH::Intersect: one bbg_hit per ray. stream is a cudaStream_t
  * (NULL = the handle's own stream); the call returns after the results are in
- * hits. */
+ * hits. Host-memory queries are staged through twelve device slots of up to
+ * 2M rays (96 MiB each), allocated by the first host query of that size and
+ * kept with the handle, so the copies overlap the traversal. */
 bbg_status bbg_intersect(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem,
                          void* stream);
 
@@ -261,6 +263,26 @@ bbg_status bbg_intersect_static(bbg_accel* accel, const bbg_ray* rays, int64_t n
  * [t_min, t_max]. */
 bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
                              bbg_memory mem, void* stream);
+
+/* bbg_intersect and bbg_intersect_any that return once the query is queued;
+ * the results are in place after bbg_accel_synchronize (or after any
+ * synchronous query on the same accel, which first waits for the submitted
+ * ones). Submitted host-memory queries chain through the accel's staging:
+ * the copy in of the next query's rays overlaps the traversal of the one
+ * before it, so a closest-hit batch and an any-hit batch submitted back to
+ * back cost about their copies, not copies plus traversals. Host buffers
+ * must stay valid and unchanged until then; in page-locked memory
+ * (cudaHostAlloc / cudaHostRegister) the call returns before the copies
+ * run, from pageable memory the copies of results block the caller as the
+ * synchronous call does. Device buffers are traced on the handle's stream.
+ * Results equal the synchronous calls'. A counting accel
+ * (bbg_accel_set_counting) refuses them (BBG_ERR_UNSUPPORTED). Errors of the
+ * queued work are returned by bbg_accel_synchronize. No counterpart in the
+ * reference, whose queries are per ray. */
+bbg_status bbg_intersect_submit(bbg_accel* accel, const bbg_ray* rays, int64_t n, bbg_hit* hits, bbg_memory mem);
+bbg_status bbg_intersect_any_submit(bbg_accel* accel, const bbg_ray* rays, int64_t n, uint8_t* occluded,
+                                    bbg_memory mem);
+bbg_status bbg_accel_synchronize(bbg_accel* accel);
 
 /* Traversal order. WIDE (the default) traverses the tree collapsed into
  * 8-wide nodes with byte-quantised child boxes (rounded outward), children
