@@ -313,7 +313,7 @@ def run_e2e(args, acc, closest, anyq, barrier):
         acc.intersect_host_ptr(pin_c.data_ptr(), n, pin_h.data_ptr())
         acc.intersect_any_host_ptr(pin_a.data_ptr(), n, pin_o.data_ptr())
 
-    secs = []
+    secs = [measure_copy_rates()]
     for step in (submitted, synchronous):
         step()
         barrier()
@@ -324,7 +324,66 @@ def run_e2e(args, acc, closest, anyq, barrier):
         torch.cuda.synchronize()
         secs.append(time.perf_counter() - t0)
         barrier()
-    return steps, secs[0], secs[1]
+    return steps, secs[1], secs[2], secs[0]
+
+
+def e2e_line(value, sync_value, steps, secs, rates, bytes_in, bytes_out):
+    """The e2e object: the rate, the bytes a step moves, and the step time
+    against the least time those copies take at the measured rates."""
+    line = {"value": value, "unit": "Mrays/s", "h2d_bytes_per_step": bytes_in, "d2h_bytes_per_step": bytes_out,
+            "calls": "bbg_intersect_submit + bbg_intersect_any_submit + bbg_accel_synchronize per step",
+            "synchronous_calls_value": sync_value}
+    if steps and rates:
+        bound = copy_bound_ms(rates, bytes_in, bytes_out)
+        step_ms = secs * 1e3 / steps
+        line["copy_bound"] = {**{k: round(v, 1) for k, v in rates.items()}, "bound_ms": bound, "step_ms": step_ms,
+                              "frac": bound / step_ms}
+    return line
+
+
+def measure_copy_rates(nbytes=256 << 20, reps=4):
+    """Pinned host<->device copy rates (GB/s) on this box: host to device
+    alone, device to host alone, and each direction while both run (two
+    streams), timed with CUDA events (cudaMemcpyAsync through torch)."""
+    import torch
+    h_in = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    h_out = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    d_in = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    d_out = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    s_in, s_out = torch.cuda.Stream(), torch.cuda.Stream()
+
+    def timed(ops):
+        torch.cuda.synchronize()
+        start = torch.cuda.Event(enable_timing=True)
+        start.record()
+        ends = []
+        for st, fn in ops:
+            st.wait_event(start)
+            with torch.cuda.stream(st):
+                for _ in range(reps):
+                    fn()
+                e = torch.cuda.Event(enable_timing=True)
+                e.record(st)
+                ends.append(e)
+        torch.cuda.synchronize()
+        return max(start.elapsed_time(e) for e in ends) / 1e3
+
+    h2d = (s_in, lambda: d_in.copy_(h_in, non_blocking=True))
+    d2h = (s_out, lambda: h_out.copy_(d_out, non_blocking=True))
+    timed([h2d, d2h])  # warm-up
+    rates = {"h2d_gbs": nbytes * reps / timed([h2d]) / 1e9, "d2h_gbs": nbytes * reps / timed([d2h]) / 1e9,
+             "both_each_gbs": nbytes * reps / timed([h2d, d2h]) / 1e9}
+    del h_in, h_out, d_in, d_out
+    return rates
+
+
+def copy_bound_ms(rates, bytes_in, bytes_out):
+    """Least time to move a step's bytes: both directions at their shared
+    rate while the smaller transfer lasts, the rest at the one-way rate."""
+    both = min(bytes_in, bytes_out)
+    rest_in, rest_out = bytes_in - both, bytes_out - both
+    return 1e3 * (both / (rates["both_each_gbs"] * 1e9) + rest_in / (rates["h2d_gbs"] * 1e9)
+                  + rest_out / (rates["d2h_gbs"] * 1e9))
 
 
 PT_WORKLOAD = ("path tracing: closed Cornell box + displaced gold icosphere (8 subdivisions, 1,310,734 "
@@ -918,9 +977,9 @@ def main():
     any_ms = [e[1].elapsed_time(e[2]) for e in ev]
 
     # End to end through the C ABI with host (pinned) buffers: copies inside.
-    e2e_steps, e2e_s, e2e_sync_s = 0, float("nan"), float("nan")
+    e2e_steps, e2e_s, e2e_sync_s, copy_rates = 0, float("nan"), float("nan"), None
     if not args.no_e2e:
-        e2e_steps, e2e_s, e2e_sync_s = run_e2e(args, acc, closest, anyq, barrier)
+        e2e_steps, e2e_s, e2e_sync_s, copy_rates = run_e2e(args, acc, closest, anyq, barrier)
     ms, e2e_s, e2e_sync_s = max_over_ranks([ms, e2e_s, e2e_sync_s], device="cuda")
 
     rays_per_step = 2 * n_rays
@@ -960,10 +1019,7 @@ def main():
                      "per_ray": {"nodes": nodes_c / n_rays, "prims": prims_c / n_rays,
                                  "any_nodes": nodes_a / n_rays, "any_prims": prims_a / n_rays},
                      "avg_launch_ms": {"closest": avg_closest_ms, "any": statistics.mean(any_ms)}},
-        "e2e": {"value": e2e_value, "unit": "Mrays/s", "h2d_bytes_per_step": 2 * n_rays * 32,
-                "d2h_bytes_per_step": n_rays * 16 + n_rays * 1,
-                "calls": "bbg_intersect_submit + bbg_intersect_any_submit + bbg_accel_synchronize per step",
-                "synchronous_calls_value": e2e_sync},
+        "e2e": e2e_line(e2e_value, e2e_sync, e2e_steps, e2e_s, copy_rates, 2 * n_rays * 32, n_rays * 16 + n_rays * 1),
         "gpu_launches": 2 * args.steps,
         "clocks": clock_info,
     }
