@@ -535,6 +535,19 @@ void GpuBVH::OccludedBatch(const bbg_ray* rays, int64_t n, uint8_t* occluded) co
     Check(bbg_intersect_any(accel_, rays, n, occluded, BBG_MEM_HOST, nullptr), "bbg_intersect_any");
 }
 
+void GpuBVH::QueryBatches(const bbg_ray* rays, int64_t n, bbg_hit* hits, const bbg_ray* shadow_rays, int64_t m,
+                          uint8_t* occluded) const
+{
+    std::lock_guard<std::mutex> lock(mutex_);
+    bbg_status s = bbg_intersect_submit(accel_, rays, n, hits, BBG_MEM_HOST);
+    if (s == BBG_OK)
+    {
+        s = bbg_intersect_any_submit(accel_, shadow_rays, m, occluded, BBG_MEM_HOST);
+    }
+    bbg_status w = bbg_accel_synchronize(accel_); // also after a failed submission: nothing stays queued
+    Check(s != BBG_OK ? s : w, "bbg_intersect_submit");
+}
+
 // ---------------------------------------------------------------- GpuPathIntegrator
 
 GpuPathIntegrator::GpuPathIntegrator(const GpuBVH* accel, std::vector<Light*> lights, const Sampler* sampler,

@@ -274,7 +274,9 @@ bbg_status bbg_intersect_any(bbg_accel* accel, const bbg_ray* rays, int64_t n, u
  * must stay valid and unchanged until then; in page-locked memory
  * (cudaHostAlloc / cudaHostRegister) the call returns before the copies
  * run, from pageable memory the copies of results block the caller as the
- * synchronous call does. Device buffers are traced on the handle's stream.
+ * synchronous call does. A host batch larger than every earlier one on the
+ * handle (below 2M rays) regrows the staging and so first waits for the
+ * queued work. Device buffers are traced on the handle's stream.
  * Results equal the synchronous calls'. A counting accel
  * (bbg_accel_set_counting) refuses them (BBG_ERR_UNSUPPORTED). Errors of the
  * queued work are returned by bbg_accel_synchronize. No counterpart in the

@@ -107,6 +107,13 @@ public:
     // thread; one call at a time uses the accel's staging buffers).
     void IntersectBatch(const bbg_ray* rays, int64_t n, bbg_hit* hits) const;
     void OccludedBatch(const bbg_ray* rays, int64_t n, uint8_t* occluded) const;
+    // Both batches submitted at once, then waited for: the shadow rays'
+    // upload overlaps the closest-hit traversal (bbg_intersect_submit,
+    // bbg_intersect_any_submit, bbg_accel_synchronize). Results equal
+    // IntersectBatch's and OccludedBatch's; from page-locked buffers the
+    // copies run while the other batch is traced.
+    void QueryBatches(const bbg_ray* rays, int64_t n, bbg_hit* hits, const bbg_ray* shadow_rays, int64_t m,
+                      uint8_t* occluded) const;
 
     const std::vector<const bulbit::Primitive*>& Primitives() const { return prims_; }
     int32_t IndexOf(const bulbit::Primitive* p) const;

@@ -198,10 +198,28 @@ void CompareQueries(const BVH& bvh, const bulbit_gpu::GpuBVH& gpu, Point3 center
                                                           hits[i].t == a.t));
         same_batch += same;
     });
+    // Both batches submitted together give the separate calls' results.
+    std::vector<bbg_ray> shadow(br);
+    for (int i = 0; i < n_batch; ++i)
+    {
+        shadow[i].t_max = hits[i].prim >= 0 ? hits[i].t * 0.5f : 10.0f;
+    }
+    std::vector<uint8_t> occ(n_batch), occ_pair(n_batch);
+    std::vector<bbg_hit> hits_pair(n_batch);
+    gpu.OccludedBatch(shadow.data(), n_batch, occ.data());
+    gpu.QueryBatches(br.data(), n_batch, hits_pair.data(), shadow.data(), n_batch, occ_pair.data());
+    bool pair_same = occ == occ_pair;
+    for (int i = 0; i < n_batch && pair_same; ++i)
+    {
+        pair_same = hits_pair[i].prim == hits[i].prim && hits_pair[i].t == hits[i].t && hits_pair[i].u == hits[i].u &&
+                    hits_pair[i].v == hits[i].v;
+    }
     r->Add(tag + "_single_same", same_single / double(n_single));
     r->Add(tag + "_any_same", same_any / double(n_single));
     r->Add(tag + "_batch_same", same_batch / double(n_batch));
-    r->Expect(same_single >= n_single - 2 && same_any >= n_single - 2 && same_batch >= n_batch - 20, tag + "_queries_ok");
+    r->Add(tag + "_paired_batches_same", pair_same ? 1.0 : 0.0);
+    r->Expect(same_single >= n_single - 2 && same_any >= n_single - 2 && same_batch >= n_batch - 20 && pair_same,
+              tag + "_queries_ok");
 }
 
 void CompareRender(Scene& scene, const BVH& bvh, const bulbit_gpu::GpuBVH& gpu, const Camera& camera,
