@@ -151,6 +151,7 @@ EXPORTS = [
     ("bbg_intersect_submit", I32, [P, P, I64, P, I32]),
     ("bbg_intersect_any_submit", I32, [P, P, I64, P, I32]),
     ("bbg_accel_synchronize", I32, [P]),
+    ("bbg_accel_export_wide8", I32, [P, P, P]),
     ("bbg_intersect_static", I32, [P, P, I64, P]),
     ("bbg_accel_set_traversal", I32, [P, I32]),
     ("bbg_accel_set_counting", I32, [P, I32]),

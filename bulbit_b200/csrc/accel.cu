@@ -230,82 +230,10 @@ bbg_status UploadShading(bbg_accel* a, const bbg_geometry* g)
     return BBG_OK;
 }
 
-// Which binary nodes become wide nodes: the choice that minimises the summed
-// surface area of the wide nodes (the surface-area cost of opening them; a
-// leaf is tested whenever its own box is hit, whichever wide node holds it,
-// so leaves add the same cost to every choice). This is the optimal collapse
-// of Ylitie, Karras and Laine (HPG 2017, section 3.1) without merging leaves:
-// cost[b][i] is the least cost of binary subtree b as at most i children of
-// one wide node, each child a binary leaf or a binary node that becomes a
-// wide node of its own, and i > 1 children are shared between the two
-// subtrees of b.
-struct Wide8Plan
-{
-    std::vector<float> cost;    // [node * 8 + i - 1]
-    std::vector<uint8_t> split; // [node * 8 + i - 1]: 0 as with i - 1 children, else the left subtree's share
-
-    void Compute(const std::vector<bbg_bvh_node>& nodes)
-    {
-        const size_t n = nodes.size();
-        cost.assign(8 * n, 0.0f);
-        split.assign(8 * n, 0);
-        double dist[9];
-        for (size_t b = n; b-- > 0;) // children follow their parent in the depth-first layout
-        {
-            const bbg_bvh_node& x = nodes[b];
-            if (x.count > 0)
-            {
-                continue; // a leaf: one child, no wide node
-            }
-            Child8 c;
-            std::memcpy(c.lo, x.bmin, sizeof(c.lo));
-            std::memcpy(c.hi, x.bmax, sizeof(c.hi));
-            const size_t l = b + 1, r = size_t(x.offset);
-            uint8_t best_k[9] = {};
-            for (int j = 2; j <= 8; ++j)
-            {
-                dist[j] = 1e300;
-                for (int k = 1; k < j; ++k)
-                {
-                    double v = double(cost[8 * l + k - 1]) + double(cost[8 * r + j - k - 1]);
-                    if (v < dist[j])
-                    {
-                        dist[j] = v;
-                        best_k[j] = uint8_t(k);
-                    }
-                }
-            }
-            cost[8 * b] = float(Wide8Area(c) + dist[8]); // one child: b is a wide node
-            for (int i = 2; i <= 8; ++i)
-            {
-                const bool fewer = double(cost[8 * b + i - 2]) <= dist[i];
-                cost[8 * b + i - 1] = fewer ? cost[8 * b + i - 2] : float(dist[i]);
-                split[8 * b + i - 1] = fewer ? 0 : best_k[i];
-            }
-            split[8 * b + 7] = best_k[8]; // what b's own wide node holds
-        }
-    }
-
-    // Appends the children of binary subtree b given at most i of them.
-    void Gather(const std::vector<bbg_bvh_node>& nodes, int32_t b, int i, int32_t* out, int* n) const
-    {
-        while (nodes[b].count == 0 && i > 1 && split[8 * size_t(b) + i - 1] == 0)
-        {
-            --i;
-        }
-        if (nodes[b].count > 0 || i == 1)
-        {
-            out[(*n)++] = b;
-            return;
-        }
-        const int k = split[8 * size_t(b) + i - 1];
-        Gather(nodes, b + 1, k, out, n);
-        Gather(nodes, nodes[b].offset, i - k, out, n);
-    }
-};
-
 // Collapses the binary tree (reference layout) into the 8-wide layout, the
-// wide nodes chosen by Wide8Plan. Nodes are numbered breadth first, a node's
+// wide nodes chosen by the surface-area plan (Wide8PlanNode, computed bottom
+// up: children follow their parent in the depth-first layout, so a reverse
+// sweep sees them first). Nodes are numbered breadth first, a node's
 // interior children consecutively. Returns false (no wide layout) if the
 // tree is too large for the stack-entry or leaf encodings (2^23 nodes, 2^26
 // slots, 31 primitives in a leaf) or too deep for the stack.
@@ -318,8 +246,15 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
         c.bnode = b;
         return c;
     };
-    Wide8Plan plan;
-    plan.Compute(nodes);
+    std::vector<float> cost(8 * nodes.size(), 0.0f); // leaves cost 0
+    std::vector<uint8_t> split(8 * nodes.size(), 0);
+    for (size_t b = nodes.size(); b-- > 0;)
+    {
+        if (nodes[b].count == 0)
+        {
+            Wide8PlanNode(nodes[b], &cost[8 * (b + 1)], &cost[8 * size_t(nodes[b].offset)], &cost[8 * b], &split[8 * b]);
+        }
+    }
     struct Pending
     {
         int32_t bnode, wnode, depth;
@@ -332,21 +267,11 @@ bool BuildWide8(const std::vector<bbg_bvh_node>& nodes, std::vector<float4>* out
     {
         Pending pd = queue[qi];
         Child8 cs[8];
-        int n = 0;
-        if (nodes[pd.bnode].count > 0)
+        int32_t bs[8];
+        const int n = Wide8Gather(nodes.data(), split.data(), pd.bnode, bs);
+        for (int c = 0; c < n; ++c)
         {
-            cs[n++] = child_of(pd.bnode); // a single-leaf tree
-        }
-        else
-        {
-            int32_t bs[8];
-            const int k = plan.split[8 * size_t(pd.bnode) + 7];
-            plan.Gather(nodes, pd.bnode + 1, k, bs, &n);
-            plan.Gather(nodes, nodes[pd.bnode].offset, 8 - k, bs, &n);
-            for (int c = 0; c < n; ++c)
-            {
-                cs[c] = child_of(bs[c]);
-            }
+            cs[c] = child_of(bs[c]);
         }
         float plo[3], phi[3];
         Wide8Union(cs, n, plo, phi);
@@ -889,6 +814,22 @@ bbg_status bbg_accel_bounds(const bbg_accel* a, float* aabb_out)
         return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_bounds: null argument");
     }
     std::memcpy(aabb_out, a->bounds, sizeof(a->bounds));
+    return BBG_OK;
+}
+
+bbg_status bbg_accel_export_wide8(const bbg_accel* a, float* nodes_out, int32_t* n_nodes_out)
+{
+    if (!a || !n_nodes_out)
+    {
+        return Fail(BBG_ERR_INVALID_ARG, "bbg_accel_export_wide8: bad argument");
+    }
+    const int32_t n = a->wide8.p ? a->n_wide8 : 0;
+    *n_nodes_out = n;
+    if (nodes_out && n > 0)
+    {
+        DeviceScope ds(a->device);
+        BBG_CUDA(cudaMemcpy(nodes_out, a->wide8.p, size_t(n) * 6 * sizeof(float4), cudaMemcpyDeviceToHost));
+    }
     return BBG_OK;
 }
 

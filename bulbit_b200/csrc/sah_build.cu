@@ -1105,63 +1105,92 @@ __global__ void SahChildBoxKernel(const bbg_bvh_node* nd, const int32_t* ref, in
     }
 }
 
-// The 8-wide collapse of one level, as the host collapses a reference tree
-// (accel.cu, BuildWide8): wide node w stands for binary node w2b[w]; it takes
-// that node's two children and opens the interior child of largest area
-// until it holds eight or only leaves. Pass 0 counts each wide node's
-// interior children (and flags leaves the layout cannot encode); pass 1,
-// with the exclusive prefix of those counts, numbers them breadth first in
-// child order and writes the node.
-__device__ __forceinline__ int Collapse8(const bbg_bvh_node* nd, int32_t b, Child8 cs[8])
+// The surface-area plan of the 8-wide collapse (Wide8PlanNode), bottom up as
+// the host computes it: each leaf walks toward the root, and at every node the
+// second child to arrive (an atomic count) computes the node's entries from
+// both children's and walks on; the first one stops there. No thread waits.
+// The children's entries are written by other threads: the writer fences
+// before its count, the reader fences after its count and reads through L2.
+__global__ void SahPlanParentKernel(const bbg_bvh_node* nd, int32_t n, int32_t* parent)
 {
-    auto child_of = [&](int32_t c) {
-        Child8 ch;
-        for (int a = 0; a < 3; ++a)
+    for (int32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+    {
+        if (b == 0)
         {
-            ch.lo[a] = nd[c].bmin[a];
-            ch.hi[a] = nd[c].bmax[a];
+            parent[0] = -1;
         }
-        ch.bnode = c;
-        return ch;
-    };
-    int n = 0;
-    if (nd[b].count > 0)
-    {
-        cs[n++] = child_of(b); // a single-leaf tree
-        return n;
-    }
-    cs[n++] = child_of(b + 1);
-    cs[n++] = child_of(nd[b].offset);
-    while (n < 8)
-    {
-        int best = -1;
-        double best_area = -1;
-        for (int j = 0; j < n; ++j)
+        if (nd[b].count == 0)
         {
-            if (nd[cs[j].bnode].count == 0 && Wide8Area(cs[j]) > best_area)
+            parent[b + 1] = b;
+            parent[nd[b].offset] = b;
+        }
+    }
+}
+
+__global__ void SahPlanKernel(const bbg_bvh_node* nd, int32_t n, const int32_t* parent, int32_t* arrivals,
+                              float* cost, uint8_t* split)
+{
+    for (int32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x)
+    {
+        if (nd[b].count == 0)
+        {
+            continue; // walks start at the leaves (whose entries stay 0)
+        }
+        for (int32_t p = parent[b]; p >= 0; p = parent[p])
+        {
+            __threadfence();
+            if (atomicAdd(arrivals + p, 1) == 0)
             {
-                best_area = Wide8Area(cs[j]);
-                best = j;
+                break; // the other child's walk finishes p
+            }
+            __threadfence();
+            const bbg_bvh_node x = nd[p];
+            float cl[8], cr[8], cp[8];
+            uint8_t sp[8];
+            for (int i = 0; i < 8; ++i)
+            {
+                cl[i] = __ldcg(cost + 8 * size_t(p + 1) + i);
+                cr[i] = __ldcg(cost + 8 * size_t(x.offset) + i);
+            }
+            Wide8PlanNode(x, cl, cr, cp, sp);
+            for (int i = 0; i < 8; ++i)
+            {
+                __stcg(cost + 8 * size_t(p) + i, cp[i]);
+                split[8 * size_t(p) + i] = sp[i];
             }
         }
-        if (best < 0)
+    }
+}
+
+// The 8-wide collapse of one level, as the host collapses a reference tree
+// (accel.cu, BuildWide8): wide node w stands for binary node w2b[w] and holds
+// the children the plan gives it. Pass 0 counts each wide node's interior
+// children (and flags leaves the layout cannot encode); pass 1, with the
+// exclusive prefix of those counts, numbers them breadth first in child order
+// and writes the node.
+__device__ __forceinline__ int Collapse8(const bbg_bvh_node* nd, const uint8_t* split, int32_t b, Child8 cs[8])
+{
+    int32_t bs[8];
+    const int n = Wide8Gather(nd, split, b, bs);
+    for (int c = 0; c < n; ++c)
+    {
+        for (int a = 0; a < 3; ++a)
         {
-            break;
+            cs[c].lo[a] = nd[bs[c]].bmin[a];
+            cs[c].hi[a] = nd[bs[c]].bmax[a];
         }
-        const int32_t c = cs[best].bnode;
-        cs[best] = child_of(c + 1);
-        cs[n++] = child_of(nd[c].offset);
+        cs[c].bnode = bs[c];
     }
     return n;
 }
 
-__global__ void SahWide8CountKernel(const bbg_bvh_node* nd, const int32_t* w2b, int32_t begin, int32_t end,
-                                    int32_t* inner, int32_t* bad)
+__global__ void SahWide8CountKernel(const bbg_bvh_node* nd, const uint8_t* split, const int32_t* w2b, int32_t begin,
+                                    int32_t end, int32_t* inner, int32_t* bad)
 {
     for (int32_t w = begin + blockIdx.x * blockDim.x + threadIdx.x; w < end; w += gridDim.x * blockDim.x)
     {
         Child8 cs[8];
-        const int n = Collapse8(nd, w2b[w], cs);
+        const int n = Collapse8(nd, split, w2b[w], cs);
         int32_t k = 0;
         for (int c = 0; c < n; ++c)
         {
@@ -1179,13 +1208,13 @@ __global__ void SahWide8CountKernel(const bbg_bvh_node* nd, const int32_t* w2b, 
     }
 }
 
-__global__ void SahWide8WriteKernel(const bbg_bvh_node* nd, int32_t* w2b, int32_t begin, int32_t end,
-                                    const int32_t* offsets, float4* wide8)
+__global__ void SahWide8WriteKernel(const bbg_bvh_node* nd, const uint8_t* split, int32_t* w2b, int32_t begin,
+                                    int32_t end, const int32_t* offsets, float4* wide8)
 {
     for (int32_t w = begin + blockIdx.x * blockDim.x + threadIdx.x; w < end; w += gridDim.x * blockDim.x)
     {
         Child8 cs[8];
-        const int n = Collapse8(nd, w2b[w], cs);
+        const int n = Collapse8(nd, split, w2b[w], cs);
         float plo[3], phi[3];
         Wide8Union(cs, n, plo, phi);
         int32_t slot_of[8];
@@ -1227,7 +1256,19 @@ bbg_status SahWide8(bbg_accel* a, const bbg_bvh_node* nd, int32_t n_nodes, int s
     const int32_t capacity = std::max(interior, 1);
     constexpr int64_t kMaxWide = (int64_t(1) << 23) - 1;
     cudaStream_t st = a->stream;
-    DevBuf<int32_t> w2b, inner, offsets, flag;
+    DevBuf<int32_t> w2b, inner, offsets, flag, parent, arrivals;
+    DevBuf<float> cost;
+    DevBuf<uint8_t> split;
+    BBG_TRY(parent.alloc(size_t(n_nodes)));
+    BBG_TRY(arrivals.alloc(size_t(n_nodes)));
+    BBG_TRY(cost.alloc(8 * size_t(n_nodes)));
+    BBG_TRY(split.alloc(8 * size_t(n_nodes)));
+    BBG_CUDA(cudaMemsetAsync(arrivals.p, 0, sizeof(int32_t) * size_t(n_nodes), st));
+    BBG_CUDA(cudaMemsetAsync(cost.p, 0, sizeof(float) * 8 * size_t(n_nodes), st)); // leaves cost 0
+    BBG_CUDA(cudaMemsetAsync(split.p, 0, 8 * size_t(n_nodes), st));
+    SahPlanParentKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(nd, n_nodes, parent.p);
+    SahPlanKernel<<<GridFor(n_nodes, 256, sms), 256, 0, st>>>(nd, n_nodes, parent.p, arrivals.p, cost.p, split.p);
+    BBG_CUDA(cudaGetLastError());
     BBG_TRY(w2b.alloc(size_t(capacity)));
     BBG_TRY(inner.alloc(size_t(capacity) + 1));
     BBG_TRY(offsets.alloc(size_t(capacity) + 1));
@@ -1248,7 +1289,7 @@ bbg_status SahWide8(bbg_accel* a, const bbg_bvh_node* nd, int32_t n_nodes, int s
             return BBG_OK;
         }
         const int32_t m = end - begin;
-        SahWide8CountKernel<<<GridFor(m, 128, sms), 128, 0, st>>>(nd, w2b.p, begin, end, inner.p, flag.p);
+        SahWide8CountKernel<<<GridFor(m, 128, sms), 128, 0, st>>>(nd, split.p, w2b.p, begin, end, inner.p, flag.p);
         // offsets[m], the level's total, needs inner[m] = 0.
         BBG_CUDA(cudaMemsetAsync(inner.p + m, 0, sizeof(int32_t), st));
         BBG_CUDA(cub::DeviceScan::ExclusiveSum(scan_tmp.p, scan_bytes, inner.p, offsets.p, m + 1, st));
@@ -1261,7 +1302,8 @@ bbg_status SahWide8(bbg_accel* a, const bbg_bvh_node* nd, int32_t n_nodes, int s
             a->wide8.reset();
             return BBG_OK;
         }
-        SahWide8WriteKernel<<<GridFor(m, 128, sms), 128, 0, st>>>(nd, w2b.p, begin, end, offsets.p, a->wide8.p);
+        SahWide8WriteKernel<<<GridFor(m, 128, sms), 128, 0, st>>>(nd, split.p, w2b.p, begin, end, offsets.p,
+                                                                  a->wide8.p);
         BBG_CUDA(cudaGetLastError());
         begin = end;
         end += state[0];

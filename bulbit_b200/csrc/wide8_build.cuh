@@ -11,6 +11,8 @@
 #include <cstring>
 #include <cuda_runtime.h>
 
+#include "bbg.h"
+
 namespace bbg
 {
 
@@ -125,11 +127,16 @@ __host__ __device__ inline void QuantizeNode8(const Child8* cs, int n, const int
     {
         double p = plo[a];
         double ext = double(phi[a]) - p;
+        // The least e with p + 255 2^e >= phi: frexp (exact, unlike log2,
+        // whose last bit the host's and the device's libraries may round
+        // differently) places ext / 255 in [2^(x-1), 2^x), so x - 2 is a
+        // lower bound, and the exact test below raises it.
         int e = -126;
         if (ext > 0)
         {
-            e = int(ceil(log2(ext / 255.0)));
-            e = e < -126 ? -126 : e;
+            int x = 0;
+            frexp(ext / 255.0, &x);
+            e = x - 2 < -126 ? -126 : x - 2;
         }
         while (e < 127 && p + 255.0 * ldexp(1.0, e) < double(phi[a]))
         {
@@ -172,6 +179,99 @@ constexpr int kWide8LeafCountBits = 5;
 __host__ __device__ inline int32_t Wide8LeafRef(int32_t first_slot, int32_t count)
 {
     return ~((first_slot << kWide8LeafCountBits) | count);
+}
+
+// Which binary nodes become wide nodes: the choice that minimises the summed
+// surface area of the wide nodes (the surface-area cost of opening them; a
+// leaf is tested whenever its own box is hit, whichever wide node holds it,
+// so leaves add the same cost to every choice). This is the optimal collapse
+// of Ylitie, Karras and Laine (HPG 2017, section 3.1) without merging leaves:
+// cost[i - 1] is the least cost of a binary subtree as at most i children of
+// one wide node, each child a binary leaf or a binary node that becomes a
+// wide node of its own; i > 1 children are shared between the two subtrees,
+// the left one taking split[i - 1] (0: as with i - 1 children). Leaves cost
+// 0. Interior node x's entries from its children's (cost_l, cost_r); both
+// the host and the device run this, in double precision, so they agree.
+// split[7] is what x's own wide node holds: the left subtree's share of 8.
+__host__ __device__ inline void Wide8PlanNode(const bbg_bvh_node& x, const float cost_l[8], const float cost_r[8],
+                                              float cost[8], uint8_t split[8])
+{
+    Child8 c;
+    for (int a = 0; a < 3; ++a)
+    {
+        c.lo[a] = x.bmin[a];
+        c.hi[a] = x.bmax[a];
+    }
+    double dist[9];
+    uint8_t best_k[9] = {};
+    for (int j = 2; j <= 8; ++j)
+    {
+        dist[j] = 1e300;
+        for (int k = 1; k < j; ++k)
+        {
+            const double v = double(cost_l[k - 1]) + double(cost_r[j - k - 1]);
+            if (v < dist[j])
+            {
+                dist[j] = v;
+                best_k[j] = uint8_t(k);
+            }
+        }
+    }
+    cost[0] = float(Wide8Area(c) + dist[8]); // one child: x is a wide node
+    split[0] = 0;
+    for (int i = 2; i <= 8; ++i)
+    {
+        const bool fewer = double(cost[i - 2]) <= dist[i];
+        cost[i - 1] = fewer ? cost[i - 2] : float(dist[i]);
+        split[i - 1] = fewer ? 0 : best_k[i];
+    }
+    split[7] = best_k[8];
+}
+
+// The children of the wide node that stands for interior binary node b
+// (depth-first layout nd, plan split[8 per node]), left subtree's first, in
+// order; returns their count. A single-leaf tree's root is its one child.
+__host__ __device__ inline int Wide8Gather(const bbg_bvh_node* nd, const uint8_t* split, int32_t b, int32_t out[8])
+{
+    if (nd[b].count > 0)
+    {
+        out[0] = b;
+        return 1;
+    }
+    // Pending (subtree, at most so many children), each yielding at least
+    // one: the pending budgets and the children out never exceed eight. (A
+    // split point outside 1..j-1, which a computed plan never holds, makes
+    // the subtree one child, so no plan content can overrun the arrays.)
+    int32_t sb[8];
+    int si[8];
+    int sp = 0, n = 0;
+    int k0 = split[8 * size_t(b) + 7];
+    k0 = k0 < 1 ? 1 : k0 > 7 ? 7 : k0;
+    sb[sp] = nd[b].offset;
+    si[sp++] = 8 - k0;
+    sb[sp] = b + 1;
+    si[sp++] = k0;
+    while (sp > 0)
+    {
+        --sp;
+        const int32_t x = sb[sp];
+        int j = si[sp];
+        while (nd[x].count == 0 && j > 1 && split[8 * size_t(x) + j - 1] == 0)
+        {
+            --j;
+        }
+        const int k = nd[x].count == 0 && j > 1 ? split[8 * size_t(x) + j - 1] : 0;
+        if (k < 1 || k >= j)
+        {
+            out[n++] = x;
+            continue;
+        }
+        sb[sp] = nd[x].offset;
+        si[sp++] = j - k;
+        sb[sp] = x + 1;
+        si[sp++] = k;
+    }
+    return n;
 }
 
 } // namespace bbg

@@ -162,6 +162,15 @@ class GpuAccel:
         abi.BBG_TRAVERSAL_REFERENCE."""
         check(get_lib().bbg_accel_set_traversal(self.h, mode), "bbg_accel_set_traversal")
 
+    def export_wide8(self):
+        """The 8-wide node layout as (n, 24) float32 (empty where not built)."""
+        n = C.c_int32(0)
+        check(get_lib().bbg_accel_export_wide8(self.h, None, C.byref(n)), "bbg_accel_export_wide8")
+        out = np.zeros((n.value, 24), np.float32)
+        if n.value:
+            check(get_lib().bbg_accel_export_wide8(self.h, _p(out), C.byref(n)), "bbg_accel_export_wide8")
+        return out
+
     def set_counting(self, on):
         check(get_lib().bbg_accel_set_counting(self.h, 1 if on else 0), "bbg_accel_set_counting")
 

@@ -229,6 +229,12 @@ bbg_status bbg_accel_destroy(bbg_accel* accel);
 /* Root AABB (6 floats), as BVH::GetAABB (src/accel/bvh.cpp:363). */
 bbg_status bbg_accel_bounds(const bbg_accel* accel, float* aabb_out);
 
+/* Copies the 8-wide node layout back (24 floats per node, in the node
+ * format of bulbit_b200/csrc/dev_geometry.cuh); *n_nodes_out receives the
+ * node count, 0 where the layout is not built. nodes_out NULL asks for the
+ * count only. No counterpart in the reference, whose tree is binary. */
+bbg_status bbg_accel_export_wide8(const bbg_accel* accel, float* nodes_out, int32_t* n_nodes_out);
+
 /* Copies the uploaded tree back: n_nodes nodes and n_slots slot entries. */
 bbg_status bbg_accel_export(const bbg_accel* accel, bbg_bvh_node* nodes_out, int32_t* slot_prims_out,
                             int32_t* n_nodes_out, int32_t* n_slots_out);

@@ -4,7 +4,8 @@ BuildRecursive / FlattenBVH (src/accel/bvh.cpp:8-297) node for node: the two
 flattened trees are byte-identical (boxes, axes, child offsets, leaf ranges)
 and so are the slot orders, on soups and meshes from a few thousand to a
 million primitives, spheres, coincident primitives (leaves by zero centroid
-extent) and pairs split by nth_element. Queries and renders over it then
+extent) and pairs split by nth_element; so are the 8-wide layouts collapsed
+from them on the device and on the host. Queries and renders over it then
 equal those over the host-built tree bit for bit, in every traversal mode."""
 import numpy as np
 import pytest
@@ -48,6 +49,27 @@ def test_device_sah_tree_equals_host_build(name):
     assert np.array_equal(slots, host_slots)
     assert np.array_equal(acc.bounds(), np.concatenate([host_nodes[0]["bmin"], host_nodes[0]["bmax"]]))
     acc.close()
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_device_wide_layout_equals_host_collapse(name):
+    """The 8-wide layout collapsed on the device (SahPlanKernel and the
+    level-by-level collapse, sah_build.cu) equals the host collapse of the
+    same tree (BuildWide8, accel.cu) byte for byte: the same surface-area plan
+    in the same double-precision arithmetic, the same breadth-first
+    numbering, slot assignment and quantisation. Where a leaf holds more
+    primitives than the layout encodes (the 64 coincident triangles), both
+    leave it unbuilt."""
+    scene = CASES[name]()
+    host = lib.GpuAccel(scene)
+    dev = lib.GpuAccel(scene, device_sah=True)
+    wh, wd = host.export_wide8(), dev.export_wide8()
+    print(f"{name}: {len(wh)} wide nodes")
+    assert (len(wh) > 0) == (name != "coincident")
+    assert wh.shape == wd.shape
+    assert np.array_equal(wh.view(np.uint32), wd.view(np.uint32))
+    host.close()
+    dev.close()
 
 
 def test_device_sah_queries_equal_host_tree():
