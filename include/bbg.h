@@ -605,7 +605,7 @@ bbg_status bbg_batch_autotune(bbg_batch* batch, int32_t n, bbg_integrator* const
  * StartPixelSample(pixel, sample) with the given seed, computed on the device. */
 bbg_status bbg_sampler_draws(int32_t px, int32_t py, int32_t seed, int32_t sample, int32_t n, float* out);
 
-/* Material::GetBSDF (src/material/*.cpp) at a surface with shading normal +z
+/* Material::GetBSDF (the src/material sources) at a surface with shading normal +z
  * and tangent +x (local = world directions; front_face selects the
  * dielectric's relative eta), then BSDF::f, PDF and Sample_f
  * (include/bulbit/bsdf.h:73-125) for n queries (wo, wi, u: 3 floats each).
